@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Ray-cast throughput of libgzg on B200 (one JSON line on rank 0).
+
+Workload (the headline single-GPU configuration): a displaced icosphere of
+1,310,720 triangles (SAH BVH2, <= 4 prims per leaf, converted to 8-wide
+quantised nodes) and 16,777,216 rays: 8,388,608 coherent pinhole rays at
+4096 x 2048 and 8,388,608 incoherent rays (origins uniform in the bounds,
+directions uniform on the sphere, tMax uniform in [0.1, 2] * diagonal).
+A step is one closest-hit pass over all rays.  Inputs (512 MiB of rays) and
+outputs (256 MiB of hits) are larger than the 126 MB L2, so no flush is done.
+
+  value     closest-hit Mrays/s, rays resident in HBM, CUDA events around the
+            K timed launches, max over ranks
+  e2e       the same through gzg_gpu_traverse_batch (the drop-in call) from
+            pinned host Ray_C + tMax to host Intersection_C records
+  roofline  algorithmic bytes of the traversal kernel (48 B ray I/O + 80 B per
+            wide node + 48 B per triangle, counts from an instrumented replay)
+            over the average launch time, against the measured HBM copy
+            bandwidth
+  cpu_baseline  the oracle (CPU restatement of the reference traversal) on the
+            host cores
+
+--impl reference times that CPU implementation alone (the reference's own
+Swift/Mojo build cannot run here).  Multi-GPU (torchrun): every rank traces
+its own full ray set against a replica of the scene (weak scaling, no
+collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s (closest-hit/shadow) & spp/s, batched vs plain on B200 at equal relMSE"
+FULL = dict(subdiv=8, width=4096, height=2048, incoherent=8388608)
+SMALL = dict(subdiv=7, width=2048, height=1024, incoherent=2097152)  # profiler case, rays > L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="small case for profiler captures")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    return ap.parse_args()
+
+
+def workload(small, rank):
+    from gonzales_b200 import scenes
+
+    cfg = SMALL if small else FULL
+    hs = scenes.raycast_scene(subdiv=cfg["subdiv"]).build()
+    o, d, t = scenes.raycast_rays(hs, cfg["width"], cfg["height"], cfg["incoherent"], seed=0xC1 + 7 * rank)
+    name = "raycast_icosphere_%dtri_%dM_rays" % (hs.triangle_count, round(len(t) / 2 ** 20))
+    return cfg, hs, o, d, t, name
+
+
+def measured_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """SM clock and throttle reasons from NVML every 20 ms in a thread."""
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode())
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001
+            self.error = repr(e)
+
+    def _run(self):
+        nv = self._nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                r = fn(self._h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def cpu_baseline(hs, o, d, t, budget_s=20.0):
+    """The oracle traversal on all host threads; a strided sample of the
+    workload sized to roughly budget_s seconds of wall time."""
+    from gonzales_b200 import scenes
+    from oracle import pyoracle as O
+
+    cores = os.cpu_count() or 1
+    meshes = [(m.points, m.vertex_indices) for m in hs.meshes]
+    probe = np.arange(0, len(t), max(1, len(t) // 200000))
+    r6 = scenes.pack_reference_rays(o[probe], d[probe])
+    t0 = time.perf_counter()
+    O.traverse(hs.nodes, hs.prims, meshes, r6, t[probe], threads=cores)
+    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(len(t), max(len(probe), rate * budget_s)))
+    stride = max(1, len(t) // n)
+    sel = np.arange(0, len(t), stride)
+    r6 = scenes.pack_reference_rays(o[sel], d[sel])
+    t0 = time.perf_counter()
+    O.traverse(hs.nodes, hs.prims, meshes, r6, t[sel], threads=cores)
+    el = time.perf_counter() - t0
+    return {"value": len(sel) / el / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "sample": "every %d-th ray of the workload (%d rays, coherent and incoherent in proportion), "
+                      "closest hit, oracle BVH2 + Moller-Trumbore, %d threads" % (stride, len(sel), cores)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    from gonzales_b200 import scenes
+    from oracle import pyoracle as O
+
+    cfg, hs, o, d, t, name = workload(args.small, 0)
+    cores = os.cpu_count() or 1
+    meshes = [(m.points, m.vertex_indices) for m in hs.meshes]
+    # A step traces a strided sample of 1/8 of the rays (coherent and
+    # incoherent in proportion) so K + W steps stay within minutes.
+    stride = 8
+    sel = np.arange(0, len(t), stride)
+    r6 = scenes.pack_reference_rays(o[sel], d[sel])
+    ts = t[sel]
+    for _ in range(args.warmup):
+        O.traverse(hs.nodes, hs.prims, meshes, r6, ts, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.traverse(hs.nodes, hs.prims, meshes, r6, ts, threads=cores)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = len(sel) * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "rays": int(len(t)), "sample_rays_per_step": int(len(sel)),
+                   "triangles": hs.triangle_count},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                         "sample": "every 8th ray (%d rays) per step, closest hit, oracle BVH2 + Moller-Trumbore "
+                                   "(CPU restatement of the reference traversal; the Swift/Mojo reference has no "
+                                   "toolchain here)" % len(sel)},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from gonzales_b200 import GpuAccelerator, options, scenes
+    from gonzales_b200 import _ffi as F
+
+    cfg, hs, o, d, t, name = workload(args.small, rank)
+    n = len(t)
+    acc = GpuAccelerator(hs)
+    info = acc.info()
+    stream = torch.cuda.current_stream()
+    rays_d = torch.from_numpy(scenes.pack_device_rays(o, d, t)).cuda()
+    hits_d = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    anyp_d = torch.empty(n, dtype=torch.int32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # instrumented replay (untimed): node / triangle fetch counts per launch
+    cnt = torch.zeros(3, dtype=torch.int64, device="cuda")
+    acc.trace_closest(rays_d, hits_d, options(fetch_counters=cnt.data_ptr()))
+    torch.cuda.synchronize()
+    nodes_per_launch, tris_per_launch, rays_counted = [int(x) for x in cnt.cpu()]
+    assert rays_counted == n, (rays_counted, n)
+
+    for _ in range(args.warmup):
+        acc.trace_closest(rays_d, hits_d)
+    barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    with sampler:
+        barrier()
+        t_first = torch.cuda.Event(enable_timing=True)
+        t_last = torch.cuda.Event(enable_timing=True)
+        t_first.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            acc.trace_closest(rays_d, hits_d)
+            ends[k].record(stream)
+        t_last.record(stream)
+        barrier()
+    elapsed_ms = t_first.elapsed_time(t_last)
+    launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist is not None:
+        tt = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+    assert acc.error_word() == 0
+
+    # any-hit (shadow) pass, same rays
+    for _ in range(args.warmup):
+        acc.trace_any(rays_d, anyp_d)
+    barrier()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        acc.trace_any(rays_d, anyp_d)
+    a1.record(stream)
+    barrier()
+    any_ms = a0.elapsed_time(a1) / args.steps
+
+    # end to end through the drop-in C-ABI call, pinned host buffers
+    rays_h = torch.from_numpy(scenes.pack_reference_rays(o, d)).pin_memory()
+    tmax_h = torch.from_numpy(t).pin_memory()
+    out_h = torch.zeros(n * 48, dtype=torch.uint8).pin_memory()
+    out_np = out_h.numpy().view(F.INTERSECTION_DTYPE)
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        acc.intersect_batch(rays_h.numpy(), tmax_h.numpy(), out=out_np)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        acc.intersect_batch(rays_h.numpy(), tmax_h.numpy(), out=out_np)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+
+    if rank == 0:
+        ms_per_step = elapsed_ms / args.steps
+        value = world * n / (ms_per_step / 1000.0) / 1e6
+        avg_launch_s = statistics.mean(launch_ms) / 1000.0
+        alg_bytes = n * 48 + nodes_per_launch * 80 + tris_per_launch * 48
+        peak, peak_kind = measured_hbm()
+        achieved = alg_bytes / avg_launch_s / 1e9
+        traffic = None
+        prof = ROOT / "profiles" / "k_wide_closest_raycast.json"
+        if prof.exists() and not args.small:
+            traffic = json.loads(prof.read_text()).get("dram_bytes_per_full_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
+            "config": {"workload": name, "triangles": hs.triangle_count, "rays": n, "coherent_rays":
+                       cfg["width"] * cfg["height"], "incoherent_rays": cfg["incoherent"], "traversal": "wide8",
+                       "leaf_test": "moller_trumbore", "l2": "inputs 512 MiB + outputs 256 MiB > L2, no flush",
+                       "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                       "wide_nodes": info["wide_nodes"], "wide_depth": info["wide_depth"],
+                       "bvh2_nodes": info["bvh2_nodes"]},
+            "any_hit_mrays_s": world * n / any_ms * 1000.0 / 1e6,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_wide (closest hit)",
+                         "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_per_launch / n,
+                         "tris_per_ray": tris_per_launch / n},
+            "e2e": {"value": world * n / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": n * 28,
+                    "d2h_bytes_per_step": n * 48, "call": "gzg_gpu_traverse_batch (pinned host Ray_C + tMax -> "
+                                                         "Intersection_C)"},
+            "gpu_launches": args.steps,
+            "clocks": sampler.summary(),
+        }
+        if world == 1 and not args.skip_cpu:
+            line["cpu_baseline"] = cpu_baseline(hs, o, d, t)
+        print(json.dumps(line), flush=True)
+    acc.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

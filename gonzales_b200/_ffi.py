@@ -1,0 +1,126 @@
+"""ctypes binding of libgzg.so (include/gzg.h, include/gzg_host.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+libgzg.so is missing or fails to load, every call raises GzgError.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libgzg.so"
+
+GZG_OK = 0
+STATUS_NAMES = {
+    0: "GZG_OK",
+    1: "GZG_ERR_INVALID_ARGUMENT",
+    2: "GZG_ERR_NO_DEVICE",
+    3: "GZG_ERR_CUDA",
+    4: "GZG_ERR_OUT_OF_MEMORY",
+    5: "GZG_ERR_BAD_SCENE",
+    6: "GZG_ERR_KERNEL_FAULT",
+    7: "GZG_ERR_LIMIT",
+    8: "GZG_ERR_TIMEOUT",
+}
+
+TRAVERSAL_WIDE = 0
+TRAVERSAL_BVH2 = 1
+LEAF_MOLLER_TRUMBORE = 0
+LEAF_WATERTIGHT = 1
+
+
+class GzgError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+# ---------------------------------------------------------------- records
+# numpy dtypes with the byte layouts of gzg.h (== mojo_kernel.h).
+
+PRIM_ID_DTYPE = np.dtype(
+    {"names": ["id1", "id2", "material_index", "type"], "formats": ["<i8", "<i8", "<i8", "i1"],
+     "offsets": [0, 8, 16, 24], "itemsize": 32})
+INTERSECTION_DTYPE = np.dtype(
+    {"names": ["prim_id", "t_hit", "u", "v", "hit"], "formats": [PRIM_ID_DTYPE, "<f4", "<f4", "<f4", "i1"],
+     "offsets": [0, 32, 36, 40, 44], "itemsize": 48})
+BVH2_NODE_DTYPE = np.dtype(
+    {"names": ["bounds_min", "bounds_max", "offset", "count"], "formats": [("<f4", 3), ("<f4", 3), "<i4", "<i4"],
+     "offsets": [0, 12, 24, 28], "itemsize": 32})
+MATERIAL_DTYPE = np.dtype(
+    {"names": ["type", "albedo", "emission"], "formats": ["i1", ("<f4", 3), ("<f4", 3)],
+     "offsets": [0, 4, 16], "itemsize": 28})
+RAY_DTYPE = np.dtype([("org", "<f4", 3), ("dir", "<f4", 3)])  # Ray_C, 24 bytes
+
+
+class TriangleMeshC(C.Structure):
+    _fields_ = [("points", C.c_void_p), ("face_indices", C.c_void_p), ("vertex_indices", C.c_void_p)]
+
+
+class TraceOptions(C.Structure):
+    _fields_ = [("traversal", C.c_int32), ("leaf_test", C.c_int32), ("block_size", C.c_int32),
+                ("blocks_per_sm", C.c_int32), ("fetch_counters", C.c_void_p)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("bvh2_nodes", C.c_int64), ("prims", C.c_int64), ("triangles", C.c_int64),
+                ("wide_nodes", C.c_int64), ("wide_depth", C.c_int32), ("bvh2_depth", C.c_int32),
+                ("device_bytes", C.c_int64)]
+
+
+VP = C.c_void_p
+I64 = C.c_int64
+ST = C.c_int32
+
+# name -> (restype, argtypes); every symbol declared in include/gzg*.h.
+PROTOTYPES = {
+    "gzg_gpu_available": (C.c_bool, []),
+    "gzg_last_error": (C.c_char_p, []),
+    "gzg_gpu_upload_scene": (ST, [VP, I64, VP, I64, VP, I64, VP, VP, VP, VP, I64, C.POINTER(VP)]),
+    "gzg_gpu_free_scene": (ST, [VP]),
+    "gzg_gpu_traverse_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
+    "gzg_gpu_occluded_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
+    "gzg_trace_closest_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
+    "gzg_trace_any_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
+    "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),
+    "gzg_scene_info_get": (ST, [VP, C.POINTER(SceneInfo)]),
+    "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),
+    "gzg_host_triangle_bounds": (ST, [VP, VP, I64, VP]),
+    "gzg_host_build_bvh2": (ST, [VP, I64, VP, C.POINTER(I64), VP, C.c_int32]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libgzg.so once; raises GzgError if it is absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise GzgError(2, f"{LIB_PATH} is not built (run gonzales_b200/build.py)")
+        handle = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status):
+    if status != GZG_OK:
+        msg = lib().gzg_last_error()
+        raise GzgError(status, msg.decode() if msg else "")
+
+
+def ptr(a):
+    """Address of a numpy array's data (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data
+
+
+def options(traversal=TRAVERSAL_WIDE, leaf_test=LEAF_MOLLER_TRUMBORE, block_size=0, blocks_per_sm=0,
+            fetch_counters=None):
+    """fetch_counters: device address (int) of 3 uint64 (nodes, triangles, rays) or None."""
+    return TraceOptions(traversal, leaf_test, block_size, blocks_per_sm, fetch_counters)

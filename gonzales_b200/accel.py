@@ -1,0 +1,119 @@
+"""GPU accelerator: the host-facing mirror of Gonzales' Accelerator
+(Sources/libgonzales/Accelerators/Accelerator.swift) on its GPU path.
+
+  Accelerator.uploadToGPU      -> GpuAccelerator(host_scene)     (gzg_gpu_upload_scene)
+  intersectBatchGPU            -> intersect_batch(rays, tmax)    (gzg_gpu_traverse_batch)
+  Visibility.occluded          -> occluded_batch(rays, tmax)     (gzg_gpu_occluded_batch)
+  BoundingHierarchy.deinit     -> close() / context manager      (gzg_gpu_free_scene)
+
+plus device-resident calls on torch CUDA tensors (trace_closest / trace_any).
+Rays on the host are Ray_C records (RAY_DTYPE or an (n, 6) float32 array);
+device rays are (n, 8) float32 tensors: origin, tMax, direction, unused.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi as F
+from .scene import HostScene
+
+
+def gpu_available():
+    return bool(F.lib().gzg_gpu_available())
+
+
+def _host_rays(rays):
+    rays = np.ascontiguousarray(rays)
+    if rays.dtype == F.RAY_DTYPE:
+        return rays
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+    return rays
+
+
+def _stream_handle(stream):
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+class GpuAccelerator:
+    def __init__(self, host_scene: HostScene):
+        self.host = host_scene
+        meshes = host_scene.mesh_structs()
+        pts, fi, vi = host_scene.counts()
+        handle = C.c_void_p()
+        F.check(F.lib().gzg_gpu_upload_scene(
+            F.ptr(host_scene.nodes), len(host_scene.nodes), F.ptr(host_scene.prims), len(host_scene.prims),
+            C.addressof(meshes), len(host_scene.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
+            F.ptr(host_scene.materials), len(host_scene.materials), C.byref(handle)))
+        self.handle = handle
+
+    # ------------------------------------------------------------ lifetime
+    def close(self):
+        if self.handle:
+            F.check(F.lib().gzg_gpu_free_scene(self.handle))
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ queries
+    def info(self):
+        info = F.SceneInfo()
+        F.check(F.lib().gzg_scene_info_get(self.handle, C.byref(info)))
+        return {name: getattr(info, name) for name, _ in F.SceneInfo._fields_}
+
+    def error_word(self, clear=True):
+        w = C.c_uint32(0)
+        F.check(F.lib().gzg_scene_error_word(self.handle, C.byref(w), 1 if clear else 0))
+        return w.value
+
+    def intersect_batch(self, rays, tmax, options=None, out=None):
+        """Closest hit for host rays; returns INTERSECTION_DTYPE records."""
+        rays = _host_rays(rays)
+        tmax = np.ascontiguousarray(tmax, dtype=np.float32)
+        n = len(tmax)
+        if out is None:
+            out = np.zeros(n, F.INTERSECTION_DTYPE)
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_gpu_traverse_batch(self.handle, F.ptr(rays), F.ptr(tmax), n, F.ptr(out), opt))
+        return out
+
+    def occluded_batch(self, rays, tmax, options=None, out=None):
+        rays = _host_rays(rays)
+        tmax = np.ascontiguousarray(tmax, dtype=np.float32)
+        n = len(tmax)
+        if out is None:
+            out = np.zeros(n, np.uint8)
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_gpu_occluded_batch(self.handle, F.ptr(rays), F.ptr(tmax), n, F.ptr(out), opt))
+        return out
+
+    def trace_closest(self, rays_d, hits_d, options=None, stream=None):
+        """rays_d: (n, 8) float32 CUDA tensor; hits_d: (n, 4) float32 CUDA tensor
+        receiving (t, u, v, prim-as-int32-bits)."""
+        n = rays_d.shape[0]
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_trace_closest_device(self.handle, rays_d.data_ptr(), n, hits_d.data_ptr(), opt,
+                                                 _stream_handle(stream)))
+
+    def trace_any(self, rays_d, hit_prim_d, options=None, stream=None):
+        n = rays_d.shape[0]
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_trace_any_device(self.handle, rays_d.data_ptr(), n, hit_prim_d.data_ptr(), opt,
+                                             _stream_handle(stream)))
+
+    def hits_to_intersections(self, hits_d, out_d, stream=None):
+        F.check(F.lib().gzg_hits_to_intersections_device(self.handle, hits_d.data_ptr(), hits_d.shape[0],
+                                                         out_d.data_ptr(), _stream_handle(stream)))

@@ -1,0 +1,451 @@
+// api.cu - the C ABI of libgzg.so (include/gzg.h): scene upload, host batch
+// calls (drop-in for the reference's mojo_gpu_* exports, kernel.mojo:399-673)
+// and device-resident trace calls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gzg_internal.h"
+#include "kernels.h"
+
+namespace gzg {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+gzg_status set_error(gzg_status code, const std::string &msg) {
+        g_last_error = msg;
+        return code;
+}
+gzg_status clear_error() {
+        g_last_error.clear();
+        return GZG_OK;
+}
+
+namespace {
+
+gzg_status cuda_fail(cudaError_t e, const char *what) {
+        const gzg_status code = (e == cudaErrorMemoryAllocation) ? GZG_ERR_OUT_OF_MEMORY : GZG_ERR_CUDA;
+        return set_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GZG_CK(call, what)                                  \
+        do {                                                \
+                cudaError_t e_ = (call);                    \
+                if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+        } while (0)
+
+// Switches to the scene's device for the duration of a call.
+class DeviceGuard {
+      public:
+        explicit DeviceGuard(int dev) {
+                cudaGetDevice(&prev_);
+                if (prev_ != dev) cudaSetDevice(dev);
+                dev_ = dev;
+        }
+        ~DeviceGuard() {
+                if (prev_ != dev_) cudaSetDevice(prev_);
+        }
+
+      private:
+        int prev_ = 0, dev_ = 0;
+};
+
+constexpr int kSlots = 3;
+constexpr int64_t kChunk = 1 << 20;  // rays per pipelined chunk
+
+// Per-call staging: device buffers and pinned host buffers for kSlots chunks
+// in flight, each slot with its own stream.
+struct Staging {
+        cudaStream_t st[kSlots] = {};
+        void *d_in[kSlots] = {}, *d_tmax[kSlots] = {}, *d_out[kSlots] = {};
+        void *h_in[kSlots] = {}, *h_tmax[kSlots] = {}, *h_out[kSlots] = {};
+        ~Staging() {
+                for (int k = 0; k < kSlots; ++k) {
+                        if (st[k]) cudaStreamDestroy(st[k]);
+                        cudaFree(d_in[k]);
+                        cudaFree(d_tmax[k]);
+                        cudaFree(d_out[k]);
+                        cudaFreeHost(h_in[k]);
+                        cudaFreeHost(h_tmax[k]);
+                        cudaFreeHost(h_out[k]);
+                }
+        }
+};
+
+bool is_pinned(const void *p) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+}  // namespace gzg
+
+using namespace gzg;
+
+struct gzg_scene {
+        int device = 0;
+        DevScene dev{};
+        std::vector<void *> allocs;
+        gzg_scene_info info{};
+        std::mutex pool_mu;
+        std::vector<std::unique_ptr<Staging>> pool;
+
+        ~gzg_scene() {
+                DeviceGuard g(device);
+                pool.clear();
+                for (void *p : allocs) cudaFree(p);
+        }
+
+        template <class T>
+        gzg_status upload(const T *host, size_t count, const T **dst, const char *what) {
+                void *d = nullptr;
+                const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+                GZG_CK(cudaMalloc(&d, bytes), what);
+                allocs.push_back(d);
+                if (count) GZG_CK(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice), what);
+                info.device_bytes += (int64_t)bytes;
+                *dst = reinterpret_cast<const T *>(d);
+                return GZG_OK;
+        }
+
+        gzg_status acquire(std::unique_ptr<Staging> *out) {
+                {
+                        std::lock_guard<std::mutex> lk(pool_mu);
+                        if (!pool.empty()) {
+                                *out = std::move(pool.back());
+                                pool.pop_back();
+                                return GZG_OK;
+                        }
+                }
+                auto s = std::make_unique<Staging>();
+                for (int k = 0; k < kSlots; ++k) {
+                        GZG_CK(cudaStreamCreateWithFlags(&s->st[k], cudaStreamNonBlocking), "staging stream");
+                        GZG_CK(cudaMalloc(&s->d_in[k], kChunk * sizeof(gzg_ray_d)), "staging device buffer");
+                        GZG_CK(cudaMalloc(&s->d_tmax[k], kChunk * sizeof(float)), "staging device buffer");
+                        GZG_CK(cudaMalloc(&s->d_out[k], kChunk * sizeof(gzg_intersection)), "staging device buffer");
+                        GZG_CK(cudaHostAlloc(&s->h_in[k], kChunk * sizeof(gzg_ray), cudaHostAllocDefault), "pinned buffer");
+                        GZG_CK(cudaHostAlloc(&s->h_tmax[k], kChunk * sizeof(float), cudaHostAllocDefault), "pinned buffer");
+                        GZG_CK(cudaHostAlloc(&s->h_out[k], kChunk * sizeof(gzg_intersection), cudaHostAllocDefault),
+                               "pinned buffer");
+                }
+                *out = std::move(s);
+                return GZG_OK;
+        }
+        void release(std::unique_ptr<Staging> s) {
+                std::lock_guard<std::mutex> lk(pool_mu);
+                pool.push_back(std::move(s));
+        }
+};
+
+namespace {
+
+LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o) {
+        LaunchParams p;
+        p.traversal = o ? o->traversal : GZG_TRAVERSAL_WIDE;
+        p.leaf_test = o ? o->leaf_test : GZG_LEAF_MOLLER_TRUMBORE;
+        p.block_size = o ? o->block_size : 0;
+        p.blocks_per_sm = o ? o->blocks_per_sm : 0;
+        p.wide_depth = s->info.wide_depth;
+        p.counters = o ? reinterpret_cast<unsigned long long *>(o->fetch_counters) : nullptr;
+        return p;
+}
+
+gzg_status check_options(const gzg_trace_options *o) {
+        if (!o) return GZG_OK;
+        if (o->traversal != GZG_TRAVERSAL_WIDE && o->traversal != GZG_TRAVERSAL_BVH2)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "unknown traversal");
+        if (o->leaf_test != GZG_LEAF_MOLLER_TRUMBORE && o->leaf_test != GZG_LEAF_WATERTIGHT)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "unknown leaf test");
+        return GZG_OK;
+}
+
+gzg_status read_error_word(gzg_scene *s, uint32_t *word, bool clear) {
+        GZG_CK(cudaMemcpy(word, s->dev.err, 4, cudaMemcpyDeviceToHost), "error word read");
+        if (clear) GZG_CK(cudaMemset(s->dev.err, 0, 4), "error word clear");
+        return GZG_OK;
+}
+
+gzg_status kernel_fault(uint32_t w) {
+        std::string m = "kernel error word 0x" + std::to_string(w) + ":";
+        if (w & kErrStackOverflow) m += " traversal stack overflow";
+        if (w & kErrStepCap) m += " step cap exceeded (cyclic or corrupt tree)";
+        if (w & kErrBadIndex) m += " index out of range";
+        return set_error(GZG_ERR_KERNEL_FAULT, m);
+}
+
+// Host batch: chunks of Ray_C + tMax through kSlots streams; results are
+// `out_bytes` per ray in format `out_fmt`.
+gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int64_t count, void *results,
+                      size_t out_bytes, int out_fmt, const gzg_trace_options *opt) {
+        if (!s || count < 0 || (count > 0 && (!rays || !tmax || !results)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "batch call: null pointer or negative count");
+        gzg_status st = check_options(opt);
+        if (st != GZG_OK) return st;
+        if (count == 0) return clear_error();
+        DeviceGuard g(s->device);
+        std::unique_ptr<Staging> stg;
+        st = s->acquire(&stg);
+        if (st != GZG_OK) return st;
+        const LaunchParams p = params_for(s, opt);
+        const bool direct = is_pinned(rays) && is_pinned(tmax) && is_pinned(results);
+        const int64_t nchunks = (count + kChunk - 1) / kChunk;
+        char *res = reinterpret_cast<char *>(results);
+        auto drain = [&](int64_t c) -> gzg_status {
+                const int k = (int)(c % kSlots);
+                GZG_CK(cudaStreamSynchronize(stg->st[k]), "batch chunk");
+                const int64_t off = c * kChunk, n = std::min(kChunk, count - off);
+                std::memcpy(res + off * out_bytes, stg->h_out[k], (size_t)n * out_bytes);
+                return GZG_OK;
+        };
+        for (int64_t c = 0; c < nchunks; ++c) {
+                const int k = (int)(c % kSlots);
+                const int64_t off = c * kChunk, n = std::min(kChunk, count - off);
+                cudaStream_t stream = stg->st[k];
+                const void *src_rays = rays + off;
+                const void *src_tmax = tmax + off;
+                if (!direct) {
+                        if (c >= kSlots) {
+                                st = drain(c - kSlots);
+                                if (st != GZG_OK) return st;
+                        }
+                        std::memcpy(stg->h_in[k], rays + off, (size_t)n * sizeof(gzg_ray));
+                        std::memcpy(stg->h_tmax[k], tmax + off, (size_t)n * sizeof(float));
+                        src_rays = stg->h_in[k];
+                        src_tmax = stg->h_tmax[k];
+                }
+                GZG_CK(cudaMemcpyAsync(stg->d_in[k], src_rays, (size_t)n * sizeof(gzg_ray), cudaMemcpyHostToDevice, stream),
+                       "ray upload");
+                GZG_CK(cudaMemcpyAsync(stg->d_tmax[k], src_tmax, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, stream),
+                       "tMax upload");
+                GZG_CK(launch_trace(s->dev, p, kRayReference, out_fmt, stg->d_in[k],
+                                    reinterpret_cast<const float *>(stg->d_tmax[k]), n, stg->d_out[k], stream),
+                       "trace launch");
+                void *dst = direct ? (void *)(res + off * out_bytes) : stg->h_out[k];
+                GZG_CK(cudaMemcpyAsync(dst, stg->d_out[k], (size_t)n * out_bytes, cudaMemcpyDeviceToHost, stream),
+                       "result download");
+        }
+        if (!direct) {
+                for (int64_t c = std::max<int64_t>(0, nchunks - kSlots); c < nchunks; ++c) {
+                        st = drain(c);
+                        if (st != GZG_OK) return st;
+                }
+        }
+        for (int k = 0; k < kSlots; ++k) GZG_CK(cudaStreamSynchronize(stg->st[k]), "batch sync");
+        s->release(std::move(stg));
+        uint32_t w = 0;
+        st = read_error_word(s, &w, true);
+        if (st != GZG_OK) return st;
+        if (w) return kernel_fault(w);
+        return clear_error();
+}
+
+}  // namespace
+
+extern "C" {
+
+GZG_API bool gzg_gpu_available(void) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+                cudaGetLastError();
+                return false;
+        }
+        int dev = 0, major = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        return major == 10;
+}
+
+GZG_API const char *gzg_last_error(void) { return g_last_error.c_str(); }
+
+GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count,
+                                        const gzg_prim_id *prim_ids, int64_t prim_count,
+                                        const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                                        const int64_t *mesh_points_counts, const int64_t *mesh_face_indices_counts,
+                                        const int64_t *mesh_vertex_indices_counts, const gzg_material *materials,
+                                        int64_t material_count, gzg_scene **out_scene) {
+        (void)mesh_face_indices_counts;
+        if (!out_scene) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_gpu_upload_scene: out_scene is NULL");
+        *out_scene = nullptr;
+        if (bvh2_node_count <= 0 || !bvh2_nodes || prim_count < 0 || (prim_count > 0 && !prim_ids) || mesh_count < 0 ||
+            (mesh_count > 0 && (!meshes || !mesh_points_counts || !mesh_vertex_indices_counts)) || material_count < 0 ||
+            (material_count > 0 && !materials))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_gpu_upload_scene: bad arguments");
+        if (prim_count > INT32_MAX || bvh2_node_count > INT32_MAX)
+                return set_error(GZG_ERR_LIMIT, "gzg_gpu_upload_scene: more than 2^31 prims or nodes");
+        // Host-side validation and conversion first: a malformed scene is
+        // reported as GZG_ERR_BAD_SCENE whether or not a device is present.
+        WideBvh wide;
+        int32_t bvh2_depth = 0;
+        gzg_status st = build_wide_bvh(bvh2_nodes, bvh2_node_count, prim_ids, prim_count, meshes, mesh_count,
+                                       mesh_points_counts, mesh_vertex_indices_counts, &wide, &bvh2_depth);
+        if (st != GZG_OK) return st;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+                cudaGetLastError();
+                return set_error(GZG_ERR_NO_DEVICE, "gzg_gpu_upload_scene: no CUDA device");
+        }
+        if (wide.nodes.size() >= (size_t)UINT32_MAX || wide.v0.size() >= (size_t)INT32_MAX)
+                return set_error(GZG_ERR_LIMIT, "gzg_gpu_upload_scene: wide tree exceeds 32-bit indexing");
+
+        // Triangles in prim-array order for the reference-order BVH2 kernel.
+        std::vector<float4_> pv0((size_t)prim_count), pv1((size_t)prim_count), pv2((size_t)prim_count);
+        for (int64_t k = 0; k < prim_count; ++k) {
+                int64_t mesh, base;
+                float4_ z{0, 0, 0, 0};
+                pv0[k] = pv1[k] = pv2[k] = z;
+                if (!prim_triangle(prim_ids[k], &mesh, &base)) continue;
+                if (mesh < 0 || mesh >= mesh_count || base < 0 || base + 2 >= mesh_vertex_indices_counts[mesh]) {
+                        // Prims outside any leaf are not validated by the tree walk; keep them inert.
+                        continue;
+                }
+                const gzg_triangle_mesh &m = meshes[mesh];
+                float4_ *dst[3] = {&pv0[k], &pv1[k], &pv2[k]};
+                bool ok = true;
+                for (int c = 0; c < 3; ++c) {
+                        const int64_t v = m.vertex_indices[base + c];
+                        if (v < 0 || v * 4 + 3 > mesh_points_counts[mesh]) {
+                                ok = false;
+                                break;
+                        }
+                        *dst[c] = float4_{m.points[v * 4], m.points[v * 4 + 1], m.points[v * 4 + 2], 0.0f};
+                }
+                if (!ok) {
+                        pv0[k] = pv1[k] = pv2[k] = z;
+                        continue;
+                }
+                int one = 1;
+                std::memcpy(&pv0[k].w, &one, 4);
+        }
+
+        auto scene = std::make_unique<gzg_scene>();
+        cudaGetDevice(&scene->device);
+        DevScene &d = scene->dev;
+        const uint4 *wn;
+        st = scene->upload(reinterpret_cast<const uint4 *>(wide.nodes.data()), wide.nodes.size() * 5, &wn, "wide nodes");
+        if (st != GZG_OK) return st;
+        d.wide = wn;
+        const float4 *f;
+        st = scene->upload(reinterpret_cast<const float4 *>(wide.v0.data()), wide.v0.size(), &f, "triangles");
+        if (st != GZG_OK) return st;
+        d.tv0 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(wide.v1.data()), wide.v1.size(), &f, "triangles");
+        if (st != GZG_OK) return st;
+        d.tv1 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(wide.v2.data()), wide.v2.size(), &f, "triangles");
+        if (st != GZG_OK) return st;
+        d.tv2 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(bvh2_nodes), (size_t)bvh2_node_count * 2, &f, "bvh2 nodes");
+        if (st != GZG_OK) return st;
+        d.bvh2 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(pv0.data()), pv0.size(), &f, "prim triangles");
+        if (st != GZG_OK) return st;
+        d.pv0 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(pv1.data()), pv1.size(), &f, "prim triangles");
+        if (st != GZG_OK) return st;
+        d.pv1 = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(pv2.data()), pv2.size(), &f, "prim triangles");
+        if (st != GZG_OK) return st;
+        d.pv2 = f;
+        const gzg_prim_id *pp;
+        st = scene->upload(prim_ids, (size_t)prim_count, &pp, "prim ids");
+        if (st != GZG_OK) return st;
+        d.prims = pp;
+        const uint32_t zero = 0;
+        const uint32_t *ew;
+        st = scene->upload(&zero, 1, &ew, "error word");
+        if (st != GZG_OK) return st;
+        d.err = const_cast<uint32_t *>(ew);
+        d.bvh2_count = bvh2_node_count;
+        d.prim_count = prim_count;
+        d.wide_count = (uint32_t)wide.nodes.size();
+
+        gzg_scene_info &info = scene->info;
+        info.bvh2_nodes = bvh2_node_count;
+        info.prims = prim_count;
+        info.triangles = (int64_t)wide.v0.size();
+        info.wide_nodes = (int64_t)wide.nodes.size();
+        info.wide_depth = wide.depth;
+        info.bvh2_depth = bvh2_depth;
+        (void)materials;
+        (void)material_count;
+        *out_scene = scene.release();
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_gpu_free_scene(gzg_scene *scene) {
+        delete scene;
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays, const float *t_max_values,
+                                          int64_t count, gzg_intersection *results, const gzg_trace_options *options) {
+        return host_batch(scene, rays, t_max_values, count, results, sizeof(gzg_intersection), kOutIntersection, options);
+}
+
+GZG_API gzg_status gzg_gpu_occluded_batch(gzg_scene *scene, const gzg_ray *rays, const float *t_max_values,
+                                          int64_t count, uint8_t *occluded, const gzg_trace_options *options) {
+        return host_batch(scene, rays, t_max_values, count, occluded, 1, kOutOccluded, options);
+}
+
+GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count, gzg_hit_d *hits,
+                                            const gzg_trace_options *options, void *stream) {
+        if (!scene || count < 0 || (count > 0 && (!rays || !hits)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_trace_closest_device: bad arguments");
+        gzg_status st = check_options(options);
+        if (st != GZG_OK) return st;
+        DeviceGuard g(scene->device);
+        GZG_CK(launch_trace(scene->dev, params_for(scene, options), kRayDevice, kOutHit, rays, nullptr, count, hits,
+                            reinterpret_cast<cudaStream_t>(stream)),
+               "gzg_trace_closest_device launch");
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count, int32_t *hit_prim,
+                                        const gzg_trace_options *options, void *stream) {
+        if (!scene || count < 0 || (count > 0 && (!rays || !hit_prim)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_trace_any_device: bad arguments");
+        gzg_status st = check_options(options);
+        if (st != GZG_OK) return st;
+        DeviceGuard g(scene->device);
+        GZG_CK(launch_trace(scene->dev, params_for(scene, options), kRayDevice, kOutAnyPrim, rays, nullptr, count,
+                            hit_prim, reinterpret_cast<cudaStream_t>(stream)),
+               "gzg_trace_any_device launch");
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_hits_to_intersections_device(gzg_scene *scene, const gzg_hit_d *hits, int64_t count,
+                                                    gzg_intersection *out, void *stream) {
+        if (!scene || count < 0 || (count > 0 && (!hits || !out)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_hits_to_intersections_device: bad arguments");
+        DeviceGuard g(scene->device);
+        GZG_CK(launch_hits_to_isect(scene->dev, hits, count, out, reinterpret_cast<cudaStream_t>(stream)),
+               "gzg_hits_to_intersections_device launch");
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_scene_info_get(const gzg_scene *scene, gzg_scene_info *info) {
+        if (!scene || !info) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_info_get: null pointer");
+        *info = scene->info;
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_scene_error_word(gzg_scene *scene, uint32_t *word, int clear) {
+        if (!scene || !word) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_error_word: null pointer");
+        DeviceGuard g(scene->device);
+        gzg_status st = read_error_word(scene, word, clear != 0);
+        if (st != GZG_OK) return st;
+        return clear_error();
+}
+
+}  // extern "C"

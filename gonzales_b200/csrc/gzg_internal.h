@@ -1,0 +1,81 @@
+// gzg_internal.h - shared declarations of libgzg's translation units.
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gzg.h"
+#include "../../include/gzg_host.h"
+
+namespace gzg {
+
+// Thread-local last error (gzg_last_error).
+gzg_status set_error(gzg_status code, const std::string &msg);
+gzg_status clear_error();
+
+// ------------------------------------------------------------------ layouts
+
+// Wide node: 8 children, 80 bytes, fetched as five 16-byte loads.
+//   bytes  0-11  origin p (float x3) of the quantisation grid
+//   bytes 12-14  per-axis exponent e (biased like IEEE binary32: step = 2^(e-127))
+//   byte  15     imask: bit s set when child slot s is an interior node
+//   bytes 16-19  child_base: node index of the first interior child; interior
+//                children are stored contiguously in slot order
+//   bytes 20-23  tri_base: first triangle record of this node's leaf children
+//   bytes 24-31  meta[s]: 0 = empty or interior; leaf = 0x80 | (count-1) << 5 | offset,
+//                triangles tri_base+offset .. +count-1 (count <= 4, offset < 32)
+//   bytes 32-79  qlo_x[8] qlo_y[8] qlo_z[8] qhi_x[8] qhi_y[8] qhi_z[8]:
+//                child box = p + q * 2^(e-127), rounded outward at build time
+// Slot s holds the child lying farthest toward the octant whose sign bits are
+// s (bit set = positive side), so a ray visits slots in the order key = s ^ oct
+// (oct = sign bits of the direction) to go roughly front to back.
+struct alignas(16) WideNode {
+        float px, py, pz;
+        uint8_t ex, ey, ez, imask;
+        uint32_t child_base;
+        uint32_t tri_base;
+        uint8_t meta[8];
+        uint8_t qlo[3][8];
+        uint8_t qhi[3][8];
+};
+static_assert(sizeof(WideNode) == 80, "wide node must be 80 bytes");
+
+// Triangle records in leaf order: three float4 streams (v0, v1, v2); v0.w holds
+// the prim index (into the uploaded prim-id array) as int32 bits.
+struct float4_ {
+        float x, y, z, w;
+};
+
+struct WideBvh {
+        std::vector<WideNode> nodes;
+        std::vector<float4_> v0, v1, v2;
+        int32_t depth = 0;
+};
+
+// Converts a validated reference BVH2 + prims + meshes into the wide layout.
+// Returns GZG_OK or an error (with set_error called).
+gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const gzg_prim_id *prims,
+                          int64_t prim_count, const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                          const int64_t *points_counts, const int64_t *vertex_index_counts, WideBvh *out,
+                          int32_t *bvh2_depth);
+
+// Decodes PrimId_C to (mesh, first vertex-index slot) as kernel.mojo:270-279;
+// returns false for prims the reference never intersects.
+inline bool prim_triangle(const gzg_prim_id &p, int64_t *mesh, int64_t *base) {
+        if (p.type == 0) {
+                *mesh = p.id1;
+                *base = p.id2;
+                return true;
+        }
+        if (p.type == 1 || p.type == 2 || p.type == 3) {
+                if (p.id2 == -1) return false;
+                *mesh = p.id2 >> 32;
+                *base = (p.id2 & 0xFFFFFFFFll) * 3;
+                return true;
+        }
+        return false;
+}
+
+}  // namespace gzg

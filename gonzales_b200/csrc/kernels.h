@@ -1,0 +1,26 @@
+// kernels.h - host-callable launchers of the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device.cuh"
+
+namespace gzg {
+
+struct LaunchParams {
+        int traversal;   // gzg_traversal
+        int leaf_test;   // gzg_leaf_test
+        int wide_depth;  // levels of the wide tree (selects the stack size)
+        int block_size;
+        int blocks_per_sm;
+        unsigned long long *counters;  // optional fetch counters (device)
+};
+
+// ray_fmt: RayFormat; out_fmt: OutFormat.  Asynchronous on `st`.
+cudaError_t launch_trace(const DevScene &s, const LaunchParams &p, int ray_fmt, int out_fmt, const void *rays,
+                         const float *tmax, int64_t n, void *out, cudaStream_t st);
+
+cudaError_t launch_hits_to_isect(const DevScene &s, const void *hits, int64_t n, void *out, cudaStream_t st);
+
+}  // namespace gzg

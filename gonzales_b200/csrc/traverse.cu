@@ -1,0 +1,378 @@
+// traverse.cu - closest-hit and any-hit traversal kernels for sm_100a.
+//
+// k_wide: 8-wide quantised nodes (layout in gzg_internal.h).  One ray per
+//   thread.  The current "node group" (child base, 8-bit hit mask in
+//   front-to-back key order, interior mask) lives in registers; groups still to
+//   visit go to a short per-thread stack in shared memory laid out
+//   [depth][blockDim] so consecutive threads hit consecutive banks.  Node
+//   records are fetched as five 128-bit read-only loads; child planes are
+//   8-bit offsets turned into floats with a byte permute and one add.  Leaf
+//   triangles are tested as soon as their node is opened, in leaf order.
+// k_bvh2: the host's BVH2 traversed exactly as the reference's
+//   traverse_bvh2_core (kernel.mojo:223-364), one thread per ray, with the
+//   reference's slab arithmetic (kernel.mojo:171-206) in _rn intrinsics.
+//
+// Both kernels are bounded: a step cap equal to the node count (each node is
+// visited at most once per ray in a tree) and a stack-depth check set a bit in
+// the scene's error word and end the ray instead of trapping.
+#include "device.cuh"
+#include "kernels.h"
+
+namespace gzg {
+
+// 8-bit quantised plane -> float: 0x4B0000qq is 2^23 + q exactly.
+__device__ __forceinline__ float qbyte(uint32_t word, uint32_t sel) {
+        return __uint_as_float(__byte_perm(word, 0x4B000000u, sel)) - 8388608.0f;
+}
+
+struct WideRay {
+        float ox, oy, oz, dx, dy, dz;
+        float rdx, rdy, rdz;
+        uint32_t oct;  // sign bits of the inverse direction
+};
+
+// Tests the 8 child boxes of a wide node against [0, thit].  Produces the
+// interior hit mask in key order (bit (slot ^ oct)), the node's interior mask,
+// child base, and the triangle hit mask relative to tri_base.
+__device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const WideRay &r, float thit,
+                                          uint32_t &node_hits, uint32_t &imask, uint32_t &child_base,
+                                          uint32_t &tri_hits, uint32_t &tri_base) {
+        const uint4 n0 = __ldg(node + 0);
+        const uint4 n1 = __ldg(node + 1);
+        const uint4 n2 = __ldg(node + 2);
+        const uint4 n3 = __ldg(node + 3);
+        const uint4 n4 = __ldg(node + 4);
+        const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+        const uint32_t ew = n0.w;
+        imask = ew >> 24;
+        child_base = n1.x;
+        tri_base = n1.y;
+        // step * rdir (exact power-of-two scaling) and the grid origin in t.
+        const float sx = __uint_as_float((ew & 0xFFu) << 23) * r.rdx;
+        const float sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23) * r.rdy;
+        const float sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23) * r.rdz;
+        const float ax = (px - r.ox) * r.rdx;
+        const float ay = (py - r.oy) * r.rdy;
+        const float az = (pz - r.oz) * r.rdz;
+        // near/far plane words by ray sign (lo planes are near for rdir >= 0)
+        const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+        const uint32_t lx0 = n2.x, lx1 = n2.y, ly0 = n2.z, ly1 = n2.w, lz0 = n3.x, lz1 = n3.y;
+        const uint32_t hx0 = n3.z, hx1 = n3.w, hy0 = n4.x, hy1 = n4.y, hz0 = n4.z, hz1 = n4.w;
+        const uint32_t nearx[2] = {nx ? hx0 : lx0, nx ? hx1 : lx1};
+        const uint32_t farx[2] = {nx ? lx0 : hx0, nx ? lx1 : hx1};
+        const uint32_t neary[2] = {ny ? hy0 : ly0, ny ? hy1 : ly1};
+        const uint32_t fary[2] = {ny ? ly0 : hy0, ny ? ly1 : hy1};
+        const uint32_t nearz[2] = {nz ? hz0 : lz0, nz ? hz1 : lz1};
+        const uint32_t farz[2] = {nz ? lz0 : hz0, nz ? lz1 : hz1};
+        const uint32_t meta[2] = {n1.z, n1.w};
+        uint32_t nh = 0, th = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+                const int w = k >> 2;
+                const uint32_t sel = (uint32_t)(k & 3) | 0x7440u;
+                const float tnx = fmaf(qbyte(nearx[w], sel), sx, ax);
+                const float tny = fmaf(qbyte(neary[w], sel), sy, ay);
+                const float tnz = fmaf(qbyte(nearz[w], sel), sz, az);
+                const float tfx = fmaf(qbyte(farx[w], sel), sx, ax);
+                const float tfy = fmaf(qbyte(fary[w], sel), sy, ay);
+                const float tfz = fmaf(qbyte(farz[w], sel), sz, az);
+                const float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+                const float tfar = fminf(fminf(tfx, tfy), fminf(tfz, thit)) * 1.0000003f;
+                if (tnear <= tfar) {
+                        const uint32_t m = (meta[w] >> (8 * (k & 3))) & 0xFFu;
+                        if ((imask >> k) & 1u) {
+                                nh |= 1u << (k ^ r.oct);
+                        } else if (m & 0x80u) {
+                                const uint32_t cnt = ((m >> 5) & 3u) + 1u;
+                                th |= ((1u << cnt) - 1u) << (m & 31u);
+                        }
+                }
+        }
+        node_hits = nh;
+        tri_hits = th;
+}
+
+template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
+__global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict__ rays, const float *__restrict__ tmaxs,
+                                              int64_t n, void *__restrict__ out) {
+        extern __shared__ uint2 smem_stack[];
+        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        const RayIn in = load_ray<RAYFMT>(rays, tmaxs, i);
+        WideRay r;
+        r.ox = in.ox;
+        r.oy = in.oy;
+        r.oz = in.oz;
+        r.dx = in.dx;
+        r.dy = in.dy;
+        r.dz = in.dz;
+        r.rdx = __fdiv_rn(1.0f, in.dx);
+        r.rdy = __fdiv_rn(1.0f, in.dy);
+        r.rdz = __fdiv_rn(1.0f, in.dz);
+        r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
+                ((__float_as_uint(r.rdz) >> 31) << 2);
+
+        uint2 *stack = smem_stack + threadIdx.x;
+        const int stride = blockDim.x;
+        int sp = 0;
+        float thit = in.tmax, bu = 0.0f, bv = 0.0f;
+        int prim = -1;
+        uint32_t steps = 0, n_nodes = 0, n_tris = 0;
+        // The root is key 0 of a virtual parent whose only interior slot is oct.
+        uint2 group = make_uint2(0u, (1u << 24) | (1u << r.oct));
+        for (;;) {
+                uint32_t tri_hits = 0, tri_base = 0;
+                uint32_t hits = group.y >> 24;
+                if (hits) {
+                        const uint32_t key = __ffs(hits) - 1;
+                        hits &= hits - 1;
+                        const uint32_t im = group.y & 0xFFu;
+                        const uint32_t slot = key ^ r.oct;
+                        const uint32_t node = group.x + __popc(im & ((1u << slot) - 1u));
+                        if (hits) {
+                                if (sp >= STACK) {
+                                        atomicOr(s.err, kErrStackOverflow);
+                                        break;
+                                }
+                                stack[sp * stride] = make_uint2(group.x, (hits << 24) | im);
+                                ++sp;
+                        }
+                        if (++steps > s.wide_count) {
+                                atomicOr(s.err, kErrStepCap);
+                                break;
+                        }
+                        uint32_t nh, nim, cb;
+                        open_node(s.wide + 5 * (size_t)node, r, thit, nh, nim, cb, tri_hits, tri_base);
+                        ++n_nodes;
+                        group = make_uint2(cb, (nh << 24) | nim);
+                }
+                bool done = false;
+                while (tri_hits) {
+                        const uint32_t b = __ffs(tri_hits) - 1;
+                        tri_hits &= tri_hits - 1;
+                        const uint32_t ti = tri_base + b;
+                        ++n_tris;
+                        const float4 a = __ldg(s.tv0 + ti);
+                        const float4 bb = __ldg(s.tv1 + ti);
+                        const float4 c = __ldg(s.tv2 + ti);
+                        float t, u, v;
+                        if (leaf_test<LEAF>(r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, a, bb, c, thit, t, u, v)) {
+                                thit = t;
+                                bu = u;
+                                bv = v;
+                                prim = __float_as_int(a.w);
+                                if (ANY) {
+                                        done = true;
+                                        break;
+                                }
+                        }
+                }
+                if (done) break;
+                if ((group.y >> 24) == 0) {
+                        if (sp == 0) break;
+                        --sp;
+                        group = stack[sp * stride];
+                }
+        }
+        if (prim < 0) {
+                thit = in.tmax;
+                bu = 0.0f;
+                bv = 0.0f;
+        }
+        store_hit<OUTFMT>(s, out, i, prim, thit, bu, bv);
+        add_counters(s, n_nodes, n_tris);
+}
+
+// The reference's slab test (kernel.mojo:171-206), separately rounded.
+__device__ __forceinline__ bool ref_aabb(const float4 &lo, const float4 &hi, const float rd[3], const float ord[3],
+                                         const bool nm[3], float tmax, float &tnear_out) {
+        const float mn[3] = {lo.x, lo.y, lo.z};
+        const float mx[3] = {lo.w, hi.x, hi.y};
+        float tn[3], tf[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+                const float nr = nm[k] ? mn[k] : mx[k];
+                const float fr = nm[k] ? mx[k] : mn[k];
+                tn[k] = __fsub_rn(__fmul_rn(nr, rd[k]), ord[k]);
+                tf[k] = __fsub_rn(__fmul_rn(fr, rd[k]), ord[k]);
+        }
+        float tnear = tn[0] > tn[1] ? tn[0] : tn[1];
+        tnear = tn[2] > tnear ? tn[2] : tnear;
+        tnear = 0.0f > tnear ? 0.0f : tnear;
+        float tfar = tf[0] < tf[1] ? tf[0] : tf[1];
+        tfar = tf[2] < tfar ? tf[2] : tfar;
+        tfar = tmax < tfar ? tmax : tfar;
+        tfar = __fmul_rn(tfar, 1.0000003f);
+        tnear_out = tnear;
+        return tnear <= tfar;
+}
+
+template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
+__global__ void __launch_bounds__(128) k_bvh2(DevScene s, const void *__restrict__ rays, const float *__restrict__ tmaxs,
+                                              int64_t n, void *__restrict__ out) {
+        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        const RayIn in = load_ray<RAYFMT>(rays, tmaxs, i);
+        const float rd[3] = {__fdiv_rn(1.0f, in.dx), __fdiv_rn(1.0f, in.dy), __fdiv_rn(1.0f, in.dz)};
+        const float ord[3] = {__fmul_rn(in.ox, rd[0]), __fmul_rn(in.oy, rd[1]), __fmul_rn(in.oz, rd[2])};
+        const bool nm[3] = {rd[0] >= 0.0f, rd[1] >= 0.0f, rd[2] >= 0.0f};
+        int stack[64];
+        int to_visit = 0;
+        int64_t current = 0;
+        int hit_index = -1;
+        float thit = in.tmax, bu = 0.0f, bv = 0.0f;
+        int64_t steps = 0;
+        uint32_t n_nodes = 0, n_tris = 0;
+        for (;;) {
+                if (++steps > s.bvh2_count) {
+                        atomicOr(s.err, kErrStepCap);
+                        break;
+                }
+                const float4 *nd = s.bvh2 + 2 * current;
+                const float4 hi = __ldg(nd + 1);
+                const int count = __float_as_int(hi.w);
+                ++n_nodes;
+                if (count > 0) {
+                        const int off = __float_as_int(hi.z);
+                        for (int j = 0; j < count; ++j) {
+                                const int k = off + j;
+                                const float4 a = __ldg(s.pv0 + k);
+                                if (__float_as_int(a.w) == 0) continue;  // id2 == -1 / not a triangle
+                                const float4 b = __ldg(s.pv1 + k);
+                                const float4 c = __ldg(s.pv2 + k);
+                                ++n_tris;
+                                float t, u, v;
+                                if (leaf_test<LEAF>(in.ox, in.oy, in.oz, in.dx, in.dy, in.dz, a, b, c, thit, t, u, v)) {
+                                        thit = t;
+                                        bu = u;
+                                        bv = v;
+                                        hit_index = k;
+                                }
+                        }
+                        if (ANY && hit_index >= 0) break;
+                        if (to_visit == 0) break;
+                        current = stack[--to_visit];
+                } else {
+                        const int64_t li = current + 1, ri = __float_as_int(hi.z);
+                        const float4 l0 = __ldg(s.bvh2 + 2 * li), l1 = __ldg(s.bvh2 + 2 * li + 1);
+                        const float4 r0 = __ldg(s.bvh2 + 2 * ri), r1 = __ldg(s.bvh2 + 2 * ri + 1);
+                        n_nodes += 2;
+                        float lt, rt;
+                        const bool lh = ref_aabb(l0, l1, rd, ord, nm, thit, lt);
+                        const bool rh = ref_aabb(r0, r1, rd, ord, nm, thit, rt);
+                        if (lh && rh) {
+                                if (to_visit >= 64) {
+                                        atomicOr(s.err, kErrStackOverflow);
+                                        break;
+                                }
+                                if (lt <= rt) {
+                                        current = li;
+                                        stack[to_visit] = (int)ri;
+                                } else {
+                                        current = ri;
+                                        stack[to_visit] = (int)li;
+                                }
+                                ++to_visit;
+                        } else if (lh) {
+                                current = li;
+                        } else if (rh) {
+                                current = ri;
+                        } else {
+                                if (to_visit == 0) break;
+                                current = stack[--to_visit];
+                        }
+                }
+        }
+        if (hit_index < 0) {
+                thit = in.tmax;
+                bu = 0.0f;
+                bv = 0.0f;
+        }
+        store_hit<OUTFMT>(s, out, i, hit_index, thit, bu, bv);
+        add_counters(s, n_nodes, n_tris);
+}
+
+__global__ void k_hits_to_isect(DevScene s, const float4 *__restrict__ hits, int64_t n, void *__restrict__ out) {
+        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        const float4 h = __ldcs(hits + i);
+        const int prim = __float_as_int(h.w);
+        if (prim >= (int)s.prim_count) {
+                atomicOr(s.err, kErrBadIndex);
+                store_hit<kOutIntersection>(s, out, i, -1, h.x, 0.0f, 0.0f);
+                return;
+        }
+        store_hit<kOutIntersection>(s, out, i, prim, h.x, h.y, h.z);
+}
+
+// ------------------------------------------------------------ launchers
+
+namespace {
+
+template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
+cudaError_t launch_wide_depth(const DevScene &s, int depth, const void *rays, const float *tmax, int64_t n, void *out,
+                              int block, cudaStream_t st) {
+        const int64_t grid = (n + block - 1) / block;
+        if (depth <= 16) {
+                size_t sm = (size_t)16 * block * sizeof(uint2);
+                k_wide<RAYFMT, OUTFMT, ANY, 16, LEAF><<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
+        } else if (depth <= 32) {
+                size_t sm = (size_t)32 * block * sizeof(uint2);
+                k_wide<RAYFMT, OUTFMT, ANY, 32, LEAF><<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
+        } else {
+                auto k = k_wide<RAYFMT, OUTFMT, ANY, 64, LEAF>;
+                size_t sm = (size_t)64 * block * sizeof(uint2);
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                k<<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
+        }
+        return cudaGetLastError();
+}
+
+template <int RAYFMT, int OUTFMT, bool ANY>
+cudaError_t launch_fmt(const DevScene &s, const LaunchParams &p, const void *rays, const float *tmax, int64_t n,
+                       void *out, cudaStream_t st) {
+        const int block = 128;
+        if (p.traversal == GZG_TRAVERSAL_BVH2) {
+                const int64_t grid = (n + block - 1) / block;
+                if (p.leaf_test == GZG_LEAF_WATERTIGHT)
+                        k_bvh2<RAYFMT, OUTFMT, ANY, GZG_LEAF_WATERTIGHT><<<(unsigned)grid, block, 0, st>>>(s, rays, tmax, n, out);
+                else
+                        k_bvh2<RAYFMT, OUTFMT, ANY, GZG_LEAF_MOLLER_TRUMBORE><<<(unsigned)grid, block, 0, st>>>(s, rays, tmax, n, out);
+                return cudaGetLastError();
+        }
+        if (p.leaf_test == GZG_LEAF_WATERTIGHT)
+                return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_WATERTIGHT>(s, p.wide_depth, rays, tmax, n, out, block, st);
+        return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_MOLLER_TRUMBORE>(s, p.wide_depth, rays, tmax, n, out, block, st);
+}
+
+}  // namespace
+
+cudaError_t launch_trace(const DevScene &scene, const LaunchParams &p, int ray_fmt, int out_fmt, const void *rays,
+                         const float *tmax, int64_t n, void *out, cudaStream_t st) {
+        if (n <= 0) return cudaSuccess;
+        DevScene s = scene;
+        s.counters = p.counters;
+        if (ray_fmt == kRayDevice) {
+                switch (out_fmt) {
+                case kOutHit: return launch_fmt<kRayDevice, kOutHit, false>(s, p, rays, tmax, n, out, st);
+                case kOutIntersection: return launch_fmt<kRayDevice, kOutIntersection, false>(s, p, rays, tmax, n, out, st);
+                case kOutAnyPrim: return launch_fmt<kRayDevice, kOutAnyPrim, true>(s, p, rays, tmax, n, out, st);
+                default: return launch_fmt<kRayDevice, kOutOccluded, true>(s, p, rays, tmax, n, out, st);
+                }
+        }
+        switch (out_fmt) {
+        case kOutHit: return launch_fmt<kRayReference, kOutHit, false>(s, p, rays, tmax, n, out, st);
+        case kOutIntersection: return launch_fmt<kRayReference, kOutIntersection, false>(s, p, rays, tmax, n, out, st);
+        case kOutAnyPrim: return launch_fmt<kRayReference, kOutAnyPrim, true>(s, p, rays, tmax, n, out, st);
+        default: return launch_fmt<kRayReference, kOutOccluded, true>(s, p, rays, tmax, n, out, st);
+        }
+}
+
+cudaError_t launch_hits_to_isect(const DevScene &s, const void *hits, int64_t n, void *out, cudaStream_t st) {
+        if (n <= 0) return cudaSuccess;
+        const int block = 256;
+        k_hits_to_isect<<<(unsigned)((n + block - 1) / block), block, 0, st>>>(s, reinterpret_cast<const float4 *>(hits), n, out);
+        return cudaGetLastError();
+}
+
+}  // namespace gzg

@@ -1,0 +1,165 @@
+"""Host-side scene assembly: the part of Gonzales' Swift host that turns meshes
+into the arrays its native plugin consumes.
+
+Mirrors, in the reference:
+  - TriangleMesh / cStruct        Sources/libgonzales/Shape/Triangle.swift:4-87
+    (world-space float4 points, int64 vertex indices, int64 face indices)
+  - shape batching into prims     Sources/libgonzales/Api/SceneDescription.swift:700-760
+    (each triangle a GeometricPrimitive with a running idx; area lights as AreaLight prims)
+  - prim-id packing               Sources/libgonzales/Accelerators/BoundingHierarchy.swift:21-56
+    (type 1 geometric / 3 area light, id2 = mesh << 32 | tri)
+  - materials for the plugin      Sources/libgonzales/Accelerators/BoundingHierarchy.swift:91-150
+  - SAH BVH2 build                Sources/libgonzales/Accelerators/BoundingHierarchyBuilder.swift:66-339
+    (run by libgzg's host builder, gzg_host_build_bvh2)
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _ffi as F
+
+PRIM_TRIANGLE = 0
+PRIM_GEOMETRIC = 1
+PRIM_TRANSFORMED = 2
+PRIM_AREA_LIGHT = 3
+
+MATERIAL_NONE = 0
+MATERIAL_DIFFUSE = 1
+MATERIAL_AREA_LIGHT = 2
+
+
+@dataclass
+class Mesh:
+    """A triangle mesh in world space (TriangleMesh, Shape/Triangle.swift:4-87)."""
+
+    points: np.ndarray          # (n, 4) float32, w unused
+    vertex_indices: np.ndarray  # (3 * ntri,) int64
+    face_indices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+
+    @property
+    def triangle_count(self):
+        return len(self.vertex_indices) // 3
+
+
+def make_mesh(points, triangles):
+    pts = np.asarray(points, dtype=np.float32).reshape(-1, 3)
+    p4 = np.ones((len(pts), 4), np.float32)
+    p4[:, :3] = pts
+    vi = np.ascontiguousarray(np.asarray(triangles, dtype=np.int64).reshape(-1))
+    return Mesh(points=np.ascontiguousarray(p4), vertex_indices=vi)
+
+
+def triangle_bounds(mesh):
+    """Per-triangle bounds (Triangle.worldBound) via libgzg's host helper."""
+    n = mesh.triangle_count
+    out = np.empty((n, 6), np.float32)
+    F.check(F.lib().gzg_host_triangle_bounds(F.ptr(mesh.points), F.ptr(mesh.vertex_indices), n, F.ptr(out)))
+    return out
+
+
+def build_bvh2(bounds6, threads=0):
+    """SAH BVH2 over prim bounds; returns (nodes, order)."""
+    bounds6 = np.ascontiguousarray(bounds6, dtype=np.float32)
+    n = len(bounds6)
+    nodes = np.zeros(max(2 * n, 1), F.BVH2_NODE_DTYPE)
+    order = np.zeros(max(n, 1), np.int64)
+    count = F.I64(0)
+    F.check(F.lib().gzg_host_build_bvh2(F.ptr(bounds6), n, F.ptr(nodes), F.C.byref(count), F.ptr(order), threads))
+    return nodes[: count.value].copy(), order[:n].copy()
+
+
+@dataclass
+class HostScene:
+    """The arrays a Gonzales BoundingHierarchy hands to the native plugin."""
+
+    meshes: list
+    prims: np.ndarray      # PRIM_ID_DTYPE, in BVH leaf order
+    nodes: np.ndarray      # BVH2_NODE_DTYPE
+    materials: np.ndarray  # MATERIAL_DTYPE
+    prim_order: np.ndarray  # k-th leaf prim = input prim prim_order[k]
+
+    def mesh_structs(self):
+        arr = (F.TriangleMeshC * max(len(self.meshes), 1))()
+        for i, m in enumerate(self.meshes):
+            arr[i] = F.TriangleMeshC(m.points.ctypes.data,
+                                     m.face_indices.ctypes.data if len(m.face_indices) else None,
+                                     m.vertex_indices.ctypes.data)
+        return arr
+
+    def counts(self):
+        pts = np.array([m.points.size for m in self.meshes], np.int64)
+        fi = np.array([len(m.face_indices) for m in self.meshes], np.int64)
+        vi = np.array([len(m.vertex_indices) for m in self.meshes], np.int64)
+        return pts, fi, vi
+
+    @property
+    def triangle_count(self):
+        return int(sum(m.triangle_count for m in self.meshes))
+
+
+class SceneBuilder:
+    """Collects meshes the way SceneDescription.worldEnd batches shapes.
+
+    add_mesh(..., material) creates one GeometricPrimitive per triangle
+    (type 1, id1 = running geometric-prim index, id2 = mesh << 32 | tri);
+    add_area_light creates AreaLight prims (type 3, id1 = light index) whose
+    material index is resolved like BoundingHierarchy.prepareMaterials
+    (area-light materials follow the surface materials).
+    """
+
+    def __init__(self):
+        self.meshes = []
+        self._prims = []       # list of (mesh, first_tri, ntri, type, material or light)
+        self._materials = []   # (type, albedo, emission)
+        self._lights = []      # emission per area light
+        self._geometric = 0
+
+    def add_material(self, albedo=(0.5, 0.5, 0.5)):
+        self._materials.append((MATERIAL_DIFFUSE, tuple(albedo), (0.0, 0.0, 0.0)))
+        return len(self._materials) - 1
+
+    def add_mesh(self, points, triangles, material=0):
+        mesh = make_mesh(points, triangles)
+        self.meshes.append(mesh)
+        idx = len(self.meshes) - 1
+        self._prims.append((idx, mesh.triangle_count, PRIM_GEOMETRIC, material, self._geometric))
+        self._geometric += mesh.triangle_count
+        return idx
+
+    def add_area_light(self, points, triangles, emission):
+        mesh = make_mesh(points, triangles)
+        self.meshes.append(mesh)
+        idx = len(self.meshes) - 1
+        first_light = len(self._lights)
+        for _ in range(mesh.triangle_count):
+            self._lights.append(tuple(emission))
+        self._prims.append((idx, mesh.triangle_count, PRIM_AREA_LIGHT, None, first_light))
+        return idx
+
+    def build(self, threads=0):
+        n_surface = len(self._materials)
+        mats = np.zeros(n_surface + len(self._lights), F.MATERIAL_DTYPE)
+        for i, (t, a, e) in enumerate(self._materials):
+            mats[i] = (t, a, e)
+        for j, e in enumerate(self._lights):
+            mats[n_surface + j] = (MATERIAL_AREA_LIGHT, (0, 0, 0), e)
+
+        total = sum(p[1] for p in self._prims)
+        prims = np.zeros(total, F.PRIM_ID_DTYPE)
+        bounds = np.zeros((total, 6), np.float32)
+        k = 0
+        for mesh_idx, ntri, ptype, material, first in self._prims:
+            tri = np.arange(ntri, dtype=np.int64)
+            sl = slice(k, k + ntri)
+            prims["id1"][sl] = first + tri
+            prims["id2"][sl] = (np.int64(mesh_idx) << 32) | tri
+            prims["type"][sl] = ptype
+            if ptype == PRIM_AREA_LIGHT:
+                prims["material_index"][sl] = n_surface + first + tri
+            else:
+                prims["material_index"][sl] = material
+            bounds[sl] = triangle_bounds(self.meshes[mesh_idx])
+            k += ntri
+        nodes, order = build_bvh2(bounds, threads)
+        return HostScene(meshes=self.meshes, prims=prims[order].copy(), nodes=nodes, materials=mats,
+                         prim_order=order)

@@ -1,0 +1,212 @@
+"""Seeded synthetic workloads (no scene files are available offline).
+
+  ray-cast workload:  an icosphere subdivided `subdiv` times (20 * 4**subdiv
+      triangles; 1,310,720 at subdiv 8) displaced radially by 1 + 0.05 * n(p),
+      n = 3-octave seeded value noise in [-1, 1]; coherent pinhole rays at
+      width x height pixel centres with seeded jitter, plus incoherent rays with
+      origins uniform in the mesh bounds, directions uniform on the sphere and
+      tMax uniform in [0.1, 2] * |bounds diagonal|.
+  box scene: five inward walls of the unit cube, two rotated boxes with seeded
+      sizes in [0.2, 0.35], a ceiling area-light quad with radiance (15, 11, 4),
+      diffuse albedo uniform in [0.1, 0.8]^3 per object.
+"""
+import math
+
+import numpy as np
+
+from .scene import SceneBuilder
+
+# ---------------------------------------------------------------- icosphere
+
+
+def icosphere(subdiv):
+    """Unit icosphere: (points (V, 3) float64, triangles (F, 3) int64)."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(subdiv):
+        nv = len(v)
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        lo = np.minimum(e[:, 0], e[:, 1])
+        hi = np.maximum(e[:, 0], e[:, 1])
+        key = lo * nv + hi
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b = uniq // nv, uniq % nv
+        mid = v[a] + v[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        v = np.concatenate([v, mid])
+        nf = len(f)
+        m01 = inv[:nf] + nv
+        m12 = inv[nf:2 * nf] + nv
+        m20 = inv[2 * nf:] + nv
+        f = np.concatenate([
+            np.stack([f[:, 0], m01, m20], 1),
+            np.stack([f[:, 1], m12, m01], 1),
+            np.stack([f[:, 2], m20, m12], 1),
+            np.stack([m01, m12, m20], 1),
+        ])
+    return v, f
+
+
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ (iy.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F))
+    h ^= iz.astype(np.uint64) * np.uint64(0x165667B19E3779F9)
+    h ^= np.uint64(seed) * np.uint64(0x27D4EB2F165667C5)
+    h ^= h >> np.uint64(31)
+    h *= np.uint64(0xBF58476D1CE4E5B9)
+    h ^= h >> np.uint64(29)
+    return (h >> np.uint64(11)).astype(np.float64) * (2.0 / 9007199254740992.0) - 1.0  # [-1, 1)
+
+
+def value_noise(p, seed, octaves=3, base_freq=4.0):
+    """Seeded value noise: trilinear interpolation of lattice values with a
+    smoothstep fade, summed over octaves (frequency x2, amplitude /2) and
+    normalised to [-1, 1]."""
+    total = np.zeros(len(p))
+    norm = 0.0
+    for o in range(octaves):
+        freq = base_freq * (2 ** o)
+        amp = 0.5 ** o
+        q = p * freq
+        i0 = np.floor(q).astype(np.int64)
+        fr = q - i0
+        w = fr * fr * (3 - 2 * fr)
+        acc = np.zeros(len(p))
+        with np.errstate(over="ignore"):
+            for dx in (0, 1):
+                for dy in (0, 1):
+                    for dz in (0, 1):
+                        val = _hash3(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed * 131 + o)
+                        wx = w[:, 0] if dx else 1 - w[:, 0]
+                        wy = w[:, 1] if dy else 1 - w[:, 1]
+                        wz = w[:, 2] if dz else 1 - w[:, 2]
+                        acc += val * wx * wy * wz
+        total += amp * acc
+        norm += amp
+    return total / norm
+
+
+def displaced_icosphere(subdiv=8, amplitude=0.05, seed=0xC1):
+    v, f = icosphere(subdiv)
+    r = 1.0 + amplitude * value_noise(v, seed)
+    return (v * r[:, None]).astype(np.float32), f
+
+
+def raycast_scene(subdiv=8, seed=0xC1):
+    """One displaced icosphere as a single mesh of geometric prims."""
+    pts, tris = displaced_icosphere(subdiv, seed=seed)
+    sb = SceneBuilder()
+    mat = sb.add_material((0.5, 0.5, 0.5))
+    sb.add_mesh(pts, tris, mat)
+    return sb
+
+
+# ---------------------------------------------------------------- rays
+
+
+def _normalize(d):
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def coherent_rays(width, height, seed, eye=(0.0, 0.0, 3.2), fov_deg=45.0):
+    """Pinhole rays through pixel centres + seeded jitter, looking at the origin."""
+    rng = np.random.default_rng(seed)
+    n = width * height
+    px = np.arange(n, dtype=np.int64) % width
+    py = np.arange(n, dtype=np.int64) // width
+    jx = rng.uniform(-0.5, 0.5, n)
+    jy = rng.uniform(-0.5, 0.5, n)
+    tan_half = math.tan(math.radians(fov_deg) / 2.0)
+    aspect = width / height
+    sx = ((px + 0.5 + jx) / width * 2.0 - 1.0) * tan_half * aspect
+    sy = (1.0 - (py + 0.5 + jy) / height * 2.0) * tan_half
+    d = _normalize(np.stack([sx, sy, -np.ones(n)], 1))
+    o = np.broadcast_to(np.asarray(eye, np.float64), (n, 3))
+    t = np.full(n, np.inf)
+    return o, d, t
+
+
+def incoherent_rays(n, lo, hi, seed):
+    rng = np.random.default_rng(seed)
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    o = lo + (hi - lo) * rng.random((n, 3))
+    d = _normalize(rng.normal(size=(n, 3)))
+    diag = float(np.linalg.norm(hi - lo))
+    t = rng.uniform(0.1, 2.0, n) * diag
+    return o, d, t
+
+
+def pack_device_rays(o, d, t):
+    """(n, 8) float32: origin, tMax, direction, 0 (gzg_ray_d)."""
+    n = len(t)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 3] = t
+    r[:, 4:7] = d
+    return r
+
+
+def pack_reference_rays(o, d):
+    """(n, 6) float32 Ray_C records."""
+    r = np.empty((len(o), 6), np.float32)
+    r[:, 0:3] = o
+    r[:, 3:6] = d
+    return r
+
+
+def raycast_rays(host_scene, n_coherent_w, n_coherent_h, n_incoherent, seed=0xC1):
+    """Coherent rays then incoherent rays, as float32 arrays (o, d, tmax)."""
+    o1, d1, t1 = coherent_rays(n_coherent_w, n_coherent_h, seed + 1)
+    pts = np.concatenate([m.points[:, :3] for m in host_scene.meshes])
+    o2, d2, t2 = incoherent_rays(n_incoherent, pts.min(0), pts.max(0), seed + 2)
+    o = np.concatenate([o1, o2]).astype(np.float32)
+    d = np.concatenate([d1, d2]).astype(np.float32)
+    t = np.concatenate([t1, t2]).astype(np.float32)
+    return o, d, t
+
+
+# ---------------------------------------------------------------- box scene
+
+
+def _quad(p0, p1, p2, p3):
+    return np.array([p0, p1, p2, p3], np.float64), np.array([[0, 1, 2], [0, 2, 3]], np.int64)
+
+
+def _box(size, angle, center):
+    s = size / 2.0
+    c, si = math.cos(angle), math.sin(angle)
+    corners = np.array([[x, y, z] for x in (-s, s) for y in (-s, s) for z in (-s, s)], np.float64)
+    rot = np.array([[c, 0, si], [0, 1, 0], [-si, 0, c]])
+    pts = corners @ rot.T + np.asarray(center)
+    tris = np.array([[0, 1, 3], [0, 3, 2], [4, 6, 7], [4, 7, 5], [0, 4, 5], [0, 5, 1], [2, 3, 7], [2, 7, 6],
+                     [0, 2, 6], [0, 6, 4], [1, 5, 7], [1, 7, 3]], np.int64)
+    return pts, tris
+
+
+def box_scene(seed=0xB0):
+    """Unit cube [0,1]^3 open toward +z (camera side), two boxes, ceiling light."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    walls = [
+        _quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)),   # floor y=0
+        _quad((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0)),   # ceiling y=1
+        _quad((0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0)),   # back z=0
+        _quad((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0)),   # left x=0
+        _quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1)),   # right x=1
+    ]
+    pts = np.concatenate([w[0] for w in walls])
+    tris = np.concatenate([w[1] + 4 * i for i, w in enumerate(walls)])
+    sb.add_mesh(pts, tris, sb.add_material(rng.uniform(0.1, 0.8, 3)))
+    for cx, cz in ((0.3, 0.35), (0.68, 0.62)):
+        size = rng.uniform(0.2, 0.35)
+        ang = rng.uniform(0, math.pi / 2)
+        bp, bt = _box(size, ang, (cx, size / 2.0 + 1e-4, cz))
+        sb.add_mesh(bp, bt, sb.add_material(rng.uniform(0.1, 0.8, 3)))
+    lp, lt = _quad((0.35, 0.999, 0.35), (0.35, 0.999, 0.65), (0.65, 0.999, 0.65), (0.65, 0.999, 0.35))
+    sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
+    return sb

@@ -1,0 +1,263 @@
+/*
+ * gzg.h - C ABI of libgzg.so, the B200 (sm_100a) ray-traversal library for the
+ * Gonzales path tracer.
+ *
+ * The library replaces the GPU half of Gonzales' native plugin
+ * (Sources/mojoKernel/include/mojo_kernel.h, exported by libmojo.so).  The host
+ * (Swift in Gonzales, Python in this repository's harness) keeps parsing scenes,
+ * building the SAH BVH2 and owning the primitive arrays; it hands those arrays to
+ * gzg_gpu_upload_scene, which copies them to the device, re-lays them out for
+ * B200 (wide quantised nodes, leaf-ordered triangle records) and returns an
+ * opaque scene handle.
+ *
+ * Conventions
+ *   - Every entry point returns gzg_status (0 = success).  gzg_last_error()
+ *     returns a message for the calling thread's most recent failure.
+ *   - Pointers named host_* / passed to the *_batch calls are HOST memory and
+ *     are only borrowed for the call.  Pointers passed to the *_device calls
+ *     are DEVICE memory owned by the caller.
+ *   - `stream` arguments are cudaStream_t values passed as void* (NULL = the
+ *     legacy default stream).  *_device calls are asynchronous on that stream;
+ *     *_batch calls are synchronous.
+ *   - One scene handle may be used from several host threads at once (the
+ *     Gonzales tile renderer calls from cores-1 tasks, TileRenderer.swift:77);
+ *     each *_batch call takes its own staging buffers from a locked pool.
+ *   - No entry point falls back to a CPU implementation: without a usable
+ *     CUDA device they return GZG_ERR_NO_DEVICE.
+ */
+#ifndef GZG_H
+#define GZG_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GZG_API __attribute__((visibility("default")))
+
+typedef int32_t gzg_status;
+enum {
+        GZG_OK = 0,
+        GZG_ERR_INVALID_ARGUMENT = 1, /* null pointer, negative count, bad enum          */
+        GZG_ERR_NO_DEVICE = 2,        /* no CUDA device / driver                          */
+        GZG_ERR_CUDA = 3,             /* a CUDA runtime call failed                       */
+        GZG_ERR_OUT_OF_MEMORY = 4,    /* device or pinned-host allocation failed          */
+        GZG_ERR_BAD_SCENE = 5,        /* malformed BVH / index out of range / cycle       */
+        GZG_ERR_KERNEL_FAULT = 6,     /* a kernel reported an error through its flag word */
+        GZG_ERR_LIMIT = 7,            /* scene exceeds a documented size limit            */
+        GZG_ERR_TIMEOUT = 8           /* a bounded host wait ran out                      */
+};
+
+/* ------------------------------------------------------------------------- */
+/* Reference-compatible records.  Byte-for-byte the layouts of                */
+/* mojo_kernel.h:4-58 (and the padded Mojo structs of kernel.mojo:7-80), so a */
+/* Swift caller passes its existing arrays by pointer cast.                   */
+/* ------------------------------------------------------------------------- */
+
+/* PrimId_C (mojo_kernel.h:4-9).  type 0: triangle, id1 = mesh, id2 = 3*tri.
+ * type 1/3: geometric primitive / area light, id2 = mesh << 32 | tri.
+ * type 2 (or id2 == -1): not a triangle; never intersected (kernel.mojo:273-275). */
+typedef struct gzg_prim_id {
+        int64_t id1;
+        int64_t id2;
+        int64_t material_index;
+        int8_t type;
+        int8_t pad_[7];
+} gzg_prim_id;
+
+/* Material_C (mojo_kernel.h:11-15): type 0 none, 1 diffuse, 2 area light. */
+typedef struct gzg_material {
+        int8_t type;
+        int8_t pad_[3];
+        float albedo[3];
+        float emission[3];
+} gzg_material;
+
+/* TriangleMesh_C (mojo_kernel.h:17-21): points are float4 (x,y,z,pad) in world
+ * space; vertex_indices hold 3 int64 per triangle. */
+typedef struct gzg_triangle_mesh {
+        const float *points;
+        const int64_t *face_indices;
+        const int64_t *vertex_indices;
+} gzg_triangle_mesh;
+
+/* Ray_C (mojo_kernel.h:23-26). */
+typedef struct gzg_ray {
+        float org_x, org_y, org_z;
+        float dir_x, dir_y, dir_z;
+} gzg_ray;
+
+/* Intersection_C (mojo_kernel.h:28-34).  On a miss: prim_id = {-1,-1,0,0},
+ * t_hit = tMax, u = v = 0, hit = 0 (kernel.mojo:360-364). */
+typedef struct gzg_intersection {
+        gzg_prim_id prim_id;
+        float t_hit;
+        float u;
+        float v;
+        int8_t hit;
+        int8_t pad_[3];
+} gzg_intersection;
+
+/* PathState_C (mojo_kernel.h:36-44). */
+typedef struct gzg_path_state {
+        gzg_ray ray;
+        float throughput[3];
+        float estimate[3];
+        float albedo[3];
+        int32_t pad0_;
+        uint64_t pcg_state;
+        uint64_t pcg_inc;
+        int8_t active;
+        int8_t pad1_[7];
+} gzg_path_state;
+
+/* BVH2Node (mojo_kernel.h:46-51; BVH2Node.swift:7-16): depth-first layout,
+ * left child = index + 1, interior: offset = right child, count = 0;
+ * leaf: offset = first prim in the prim-id array, count > 0. */
+typedef struct gzg_bvh2_node {
+        float bounds_min[3];
+        float bounds_max[3];
+        int32_t offset;
+        int32_t count;
+} gzg_bvh2_node;
+
+/* ------------------------------------------------------------------------- */
+/* Device-resident records (the fast path; caller-owned device memory).       */
+/* ------------------------------------------------------------------------- */
+
+/* 32-byte ray: origin + tMax, direction + unused lane (two 16-byte loads). */
+typedef struct gzg_ray_d {
+        float org_x, org_y, org_z, t_max;
+        float dir_x, dir_y, dir_z, pad_;
+} gzg_ray_d;
+
+/* 16-byte hit: prim = index into the uploaded prim-id array, -1 on a miss
+ * (then t = tMax, u = v = 0, as the reference's miss record). */
+typedef struct gzg_hit_d {
+        float t, u, v;
+        int32_t prim;
+} gzg_hit_d;
+
+/* ------------------------------------------------------------------------- */
+/* Traversal options                                                          */
+/* ------------------------------------------------------------------------- */
+
+typedef enum gzg_traversal {
+        /* Wide (8-ary) nodes with 8-bit child boxes quantised outward, leaf
+         * triangles in leaf order, shared-memory short stack.  Default. */
+        GZG_TRAVERSAL_WIDE = 0,
+        /* The uploaded BVH2 traversed in the reference's exact order and slab
+         * arithmetic (kernel.mojo:171-206, 223-364), one thread per ray.
+         * Bit-exact with the reference including ties. */
+        GZG_TRAVERSAL_BVH2 = 1
+} gzg_traversal;
+
+typedef enum gzg_leaf_test {
+        /* Moller-Trumbore in the reference's operation order without FMA
+         * contraction (kernel.mojo:122-156). Default. */
+        GZG_LEAF_MOLLER_TRUMBORE = 0,
+        /* Watertight shear/edge-function test (Shape/Triangle.swift:269-352). */
+        GZG_LEAF_WATERTIGHT = 1
+} gzg_leaf_test;
+
+typedef struct gzg_trace_options {
+        int32_t traversal; /* gzg_traversal */
+        int32_t leaf_test; /* gzg_leaf_test */
+        int32_t block_size; /* 0 = library default */
+        int32_t blocks_per_sm; /* 0 = library default */
+        /* Optional DEVICE pointer to 3 uint64 counters that the kernel adds to:
+         * [0] nodes fetched (wide nodes, or BVH2 node records), [1] triangles
+         * tested, [2] rays traced.  NULL = no counting. */
+        uint64_t *fetch_counters;
+} gzg_trace_options;
+
+/* Scene summary filled by gzg_scene_info. */
+typedef struct gzg_scene_info {
+        int64_t bvh2_nodes;
+        int64_t prims;
+        int64_t triangles;     /* intersectable triangles after dropping id2 == -1 prims */
+        int64_t wide_nodes;
+        int32_t wide_depth;    /* levels of the wide tree (root = 1) */
+        int32_t bvh2_depth;
+        int64_t device_bytes;  /* bytes of device memory held by the scene */
+} gzg_scene_info;
+
+typedef struct gzg_scene gzg_scene;
+
+/* ------------------------------------------------------------------------- */
+/* Entry points                                                               */
+/* ------------------------------------------------------------------------- */
+
+/* Replaces mojo_gpu_available (kernel.mojo:399-401): true when a CUDA device
+ * of compute capability 10.x is visible. */
+GZG_API bool gzg_gpu_available(void);
+
+/* Message for the calling thread's last failed call ("" if none). */
+GZG_API const char *gzg_last_error(void);
+
+/* Replaces mojo_gpu_upload_scene (kernel.mojo:430-587, mojo_kernel.h:67-71).
+ * Same arguments; the counts are numbers of float / int64 elements per mesh
+ * exactly as BoundingHierarchy.uploadToGPU passes them
+ * (BoundingHierarchy.swift:160-173).  Unlike the reference it validates every
+ * node link and index (GZG_ERR_BAD_SCENE) and returns a status instead of
+ * printing and returning NULL. */
+GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count,
+                                        const gzg_prim_id *prim_ids, int64_t prim_count,
+                                        const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                                        const int64_t *mesh_points_counts,
+                                        const int64_t *mesh_face_indices_counts,
+                                        const int64_t *mesh_vertex_indices_counts,
+                                        const gzg_material *materials, int64_t material_count,
+                                        gzg_scene **out_scene);
+
+/* Replaces mojo_gpu_free_scene (kernel.mojo:848-854).  NULL is a no-op. */
+GZG_API gzg_status gzg_gpu_free_scene(gzg_scene *scene);
+
+/* Replaces mojo_gpu_traverse_batch (kernel.mojo:608-673): closest hit for
+ * `count` host rays with per-ray tMax, results into host Intersection_C
+ * records.  Synchronous; copies are pipelined in chunks over pinned staging
+ * buffers.  options may be NULL (defaults). */
+GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays,
+                                          const float *t_max_values, int64_t count,
+                                          gzg_intersection *results,
+                                          const gzg_trace_options *options);
+
+/* Shadow / any-hit batch (new; Visibility.occluded, Core/Visibility.swift:5-24,
+ * answers it with a closest-hit query, BoundingHierarchy.swift:348-384).
+ * occluded[i] = 1 iff some triangle is hit with 0 < t <= tMax[i]. */
+GZG_API gzg_status gzg_gpu_occluded_batch(gzg_scene *scene, const gzg_ray *rays,
+                                          const float *t_max_values, int64_t count,
+                                          uint8_t *occluded, const gzg_trace_options *options);
+
+/* Device-resident closest hit: rays and hits are device pointers. */
+GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
+                                            gzg_hit_d *hits, const gzg_trace_options *options,
+                                            void *stream);
+
+/* Device-resident any hit: hit_prim[i] = index of a prim hit with
+ * 0 < t <= tMax (the first one found), or -1. */
+GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
+                                        int32_t *hit_prim, const gzg_trace_options *options,
+                                        void *stream);
+
+/* Expands device hits into reference Intersection_C records on the device
+ * (prim-id lookup; the miss record of kernel.mojo:362-364). */
+GZG_API gzg_status gzg_hits_to_intersections_device(gzg_scene *scene, const gzg_hit_d *hits,
+                                                    int64_t count, gzg_intersection *out,
+                                                    void *stream);
+
+/* Scene statistics. */
+GZG_API gzg_status gzg_scene_info_get(const gzg_scene *scene, gzg_scene_info *info);
+
+/* Reads (and with clear != 0 resets) the scene's device error word, which
+ * kernels set instead of trapping (stack overflow, step cap, bad index). */
+GZG_API gzg_status gzg_scene_error_word(gzg_scene *scene, uint32_t *word, int clear);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GZG_H */

@@ -1,0 +1,128 @@
+/*
+ * oracle.h - CPU restatement of the Gonzales hot path, used ONLY as the
+ * correctness checker (tests, smoke check) and as the timed CPU baseline.
+ * Nothing in the product library links or calls this code.
+ *
+ * Restated from the reference (paths relative to the Gonzales source tree):
+ *   SAH BVH2 build + flatten   Sources/libgonzales/Accelerators/BoundingHierarchyBuilder.swift:66-339
+ *   bounds helpers             Sources/libgonzales/Geometry/Bounds3.swift, Geometry/Geometry.swift:46-61
+ *   triangle bound             Sources/libgonzales/Shape/Triangle.swift:248-256
+ *   traversal + MT leaf test   Sources/mojoKernel/kernel.mojo:84-95, 122-156, 171-206, 223-364
+ *   watertight leaf test       Sources/libgonzales/Shape/Triangle.swift:269-352
+ *   Swift slab test (KATs)     Sources/libgonzales/Geometry/Bounds3.swift:143-164
+ *   Z-Sobol sampler            Sources/libgonzales/Sampler/ZSobolSampler.swift:6-280
+ *
+ * Parity pins: the Sobol utilities against the reference's own KATs
+ * (Tests/libgonzalesTests/SobolSamplerTests.swift), the bounds helpers and the
+ * Swift slab test against Tests/libgonzalesTests/BoundsTests.swift, the Sobol
+ * matrices against the published first dimensions of the Sobol sequence.  The
+ * reference has no traversal or BVH tests and cannot run here (no Swift or Mojo
+ * toolchain), so traversal parity is pinned by this restatement only.
+ *
+ * Built with -ffp-contract=off: every float operation rounds separately, in the
+ * reference's source order.
+ */
+#ifndef GZG_ORACLE_H
+#define GZG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Layouts identical to mojo_kernel.h:4-58 (and include/gzg.h). */
+typedef struct orc_prim_id {
+        int64_t id1, id2, material_index;
+        int8_t type;
+        int8_t pad_[7];
+} orc_prim_id;
+typedef struct orc_mesh {
+        const float *points;
+        const int64_t *face_indices;
+        const int64_t *vertex_indices;
+} orc_mesh;
+typedef struct orc_ray {
+        float ox, oy, oz, dx, dy, dz;
+} orc_ray;
+typedef struct orc_isect {
+        orc_prim_id prim_id;
+        float t, u, v;
+        int8_t hit;
+        int8_t pad_[3];
+} orc_isect;
+typedef struct orc_node {
+        float mn[3], mx[3];
+        int32_t offset, count;
+} orc_node;
+
+/* --- BVH build ---------------------------------------------------------- */
+
+/* Bound of every triangle: union(Bounds3f(p0, p1), p2) with Swift min/max. */
+void orc_triangle_bounds(const float *points4, const int64_t *vertex_indices, int64_t ntri,
+                         float *bounds6);
+
+/* SAH build over n prim bounds (minx,miny,minz,maxx,maxy,maxz per prim).
+ * Writes the flattened nodes (capacity 2n) and the sorted prim order
+ * (order[k] = input index of the k-th prim in the leaf order).
+ * Returns the node count (0 for n == 0). */
+int64_t orc_build_bvh2(const float *bounds6, int64_t n, orc_node *nodes, int64_t *order);
+
+/* --- traversal ---------------------------------------------------------- */
+
+/* counters (optional, may be NULL): per ray {interior steps, leaf visits,
+ * triangle tests, node fetches}. */
+void orc_traverse_batch(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                        const orc_ray *rays, const float *tmax, int64_t n, int watertight,
+                        orc_isect *out, int32_t *hit_index, uint32_t *counters, int threads);
+
+/* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
+int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1,
+                              const float *p2, float tmax, float *t, float *u, float *v);
+/* The watertight leaf test alone (Triangle.swift:269-352), tHit in/out. */
+int orc_intersect_triangle_watertight(const float *o, const float *d, const float *p0,
+                                      const float *p1, const float *p2, float *thit, float *b0,
+                                      float *b1, float *b2);
+/* The reference's slab test (kernel.mojo:171-206) for one ray and box. */
+int orc_intersect_aabb(const float *mn, const float *mx, const float *o, const float *d, float tmax,
+                       float *tnear);
+/* The Swift slab test Bounds3.intersects (Bounds3.swift:143-164). */
+int orc_bounds_intersects_swift(const float *mn, const float *mx, const float *o, const float *d,
+                                float thit);
+float orc_bounds_surface_area(const float *mn, const float *mx);
+int orc_bounds_maximum_extent(const float *mn, const float *mx);
+
+/* --- Z-Sobol ------------------------------------------------------------ */
+
+/* Matrices: 1024 dims x 52 uint32 (SobolGenerator/main.swift:11-76 output). */
+void orc_sobol_set_matrices(const uint32_t *m);
+uint32_t orc_reverse_bits32(uint32_t v);
+uint64_t orc_encode_morton2(uint32_t x, uint32_t y);
+uint32_t orc_mix_bits(uint64_t v);
+uint32_t orc_owen_scramble(uint32_t v, uint32_t seed);
+int64_t orc_next_power_of_two(int64_t v);
+float orc_sobol_sample(int64_t index, int dimension, uint32_t seed);
+
+typedef struct orc_zsobol {
+        int64_t seed;
+        int32_t log2spp;
+        int32_t n_base4_digits;
+        uint64_t morton_index;
+        int32_t dimension;
+} orc_zsobol;
+void orc_zsobol_init(orc_zsobol *s, int64_t spp, int32_t res_x, int32_t res_y, int64_t seed);
+void orc_zsobol_start_pixel_sample(orc_zsobol *s, int32_t px, int32_t py, int64_t index, int32_t dim);
+uint64_t orc_zsobol_sample_index(const orc_zsobol *s);
+float orc_zsobol_get1d(orc_zsobol *s);
+void orc_zsobol_get2d(orc_zsobol *s, float *out2);
+void orc_zsobol_get3d(orc_zsobol *s, float *out3);
+/* Batch: for each pixel-sample (px, py, index) the first `ndims` values drawn
+ * by the sequence of get calls in `kinds` (1/2/3 per call), dim starting at 0. */
+void orc_zsobol_batch(int64_t spp, int32_t res_x, int32_t res_y, int64_t seed, const int32_t *px,
+                      const int32_t *py, const int64_t *index, int64_t n, const int32_t *kinds,
+                      int32_t nkinds, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

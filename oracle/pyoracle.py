@@ -1,0 +1,180 @@
+"""ctypes wrapper of liboracle.so, the CPU restatement of the Gonzales hot path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg, as the checker.  The product library never uses it.
+"""
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+SOBOL = HERE.parent / "gonzales_b200" / "data" / "sobol_1024x52.bin"
+
+NODE_DTYPE = np.dtype({"names": ["bounds_min", "bounds_max", "offset", "count"],
+                       "formats": [("<f4", 3), ("<f4", 3), "<i4", "<i4"], "offsets": [0, 12, 24, 28], "itemsize": 32})
+PRIM_DTYPE = np.dtype({"names": ["id1", "id2", "material_index", "type"], "formats": ["<i8", "<i8", "<i8", "i1"],
+                       "offsets": [0, 8, 16, 24], "itemsize": 32})
+ISECT_DTYPE = np.dtype({"names": ["prim_id", "t_hit", "u", "v", "hit"],
+                        "formats": [PRIM_DTYPE, "<f4", "<f4", "<f4", "i1"], "offsets": [0, 32, 36, 40, 44],
+                        "itemsize": 48})
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("points", C.c_void_p), ("face_indices", C.c_void_p), ("vertex_indices", C.c_void_p)]
+
+
+class ZSobolState(C.Structure):
+    _fields_ = [("seed", C.c_int64), ("log2spp", C.c_int32), ("n_base4_digits", C.c_int32),
+                ("morton_index", C.c_uint64), ("dimension", C.c_int32)]
+
+
+_lib = None
+
+
+def build():
+    src = [HERE / "oracle.cpp", HERE / "oracle.h"]
+    if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp, i64, f32, i32, u32, u64 = C.c_void_p, C.c_int64, C.c_float, C.c_int32, C.c_uint32, C.c_uint64
+        sig = {
+            "orc_triangle_bounds": (None, [vp, vp, i64, vp]),
+            "orc_build_bvh2": (i64, [vp, i64, vp, vp]),
+            "orc_traverse_batch": (None, [vp, vp, vp, vp, vp, i64, C.c_int, vp, vp, vp, C.c_int]),
+            "orc_intersect_triangle_mt": (C.c_int, [vp, vp, vp, vp, vp, f32, vp, vp, vp]),
+            "orc_intersect_triangle_watertight": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+            "orc_intersect_aabb": (C.c_int, [vp, vp, vp, vp, f32, vp]),
+            "orc_bounds_intersects_swift": (C.c_int, [vp, vp, vp, vp, f32]),
+            "orc_bounds_surface_area": (f32, [vp, vp]),
+            "orc_bounds_maximum_extent": (C.c_int, [vp, vp]),
+            "orc_sobol_set_matrices": (None, [vp]),
+            "orc_reverse_bits32": (u32, [u32]),
+            "orc_encode_morton2": (u64, [u32, u32]),
+            "orc_mix_bits": (u32, [u64]),
+            "orc_owen_scramble": (u32, [u32, u32]),
+            "orc_next_power_of_two": (i64, [i64]),
+            "orc_sobol_sample": (f32, [i64, C.c_int, u32]),
+            "orc_zsobol_init": (None, [vp, i64, i32, i32, i64]),
+            "orc_zsobol_start_pixel_sample": (None, [vp, i32, i32, i64, i32]),
+            "orc_zsobol_sample_index": (u64, [vp]),
+            "orc_zsobol_get1d": (f32, [vp]),
+            "orc_zsobol_get2d": (None, [vp, vp]),
+            "orc_zsobol_get3d": (None, [vp, vp]),
+            "orc_zsobol_batch": (None, [i64, i32, i32, i64, vp, vp, vp, i64, vp, i32, vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        m = np.fromfile(SOBOL, dtype="<u4")
+        L.orc_sobol_set_matrices(m.ctypes.data)
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def triangle_bounds(points4, vertex_indices):
+    points4 = np.ascontiguousarray(points4, np.float32)
+    vi = np.ascontiguousarray(vertex_indices, np.int64)
+    n = len(vi) // 3
+    out = np.empty((n, 6), np.float32)
+    lib().orc_triangle_bounds(_p(points4), _p(vi), n, _p(out))
+    return out
+
+
+def build_bvh2(bounds6):
+    bounds6 = np.ascontiguousarray(bounds6, np.float32)
+    n = len(bounds6)
+    nodes = np.zeros(max(2 * n, 1), NODE_DTYPE)
+    order = np.zeros(max(n, 1), np.int64)
+    cnt = lib().orc_build_bvh2(_p(bounds6), n, _p(nodes), _p(order))
+    return nodes[:cnt].copy(), order[:n].copy()
+
+
+def traverse(nodes, prims, meshes, rays6, tmax, watertight=False, counters=False, threads=0):
+    """Closest hit per ray.  meshes: list of (points4 float32, vertex_indices int64).
+    Returns (isect records, hit index into prims, counters or None)."""
+    nodes = np.ascontiguousarray(nodes)
+    prims = np.ascontiguousarray(prims)
+    rays6 = np.ascontiguousarray(rays6, np.float32).reshape(-1, 6)
+    tmax = np.ascontiguousarray(tmax, np.float32)
+    n = len(tmax)
+    keep = []
+    arr = (_Mesh * max(len(meshes), 1))()
+    for i, (p4, vi) in enumerate(meshes):
+        p4 = np.ascontiguousarray(p4, np.float32)
+        vi = np.ascontiguousarray(vi, np.int64)
+        keep += [p4, vi]
+        arr[i] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+    out = np.zeros(n, ISECT_DTYPE)
+    hit_index = np.zeros(n, np.int32)
+    cnt = np.zeros((n, 4), np.uint32) if counters else None
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    lib().orc_traverse_batch(_p(nodes), _p(prims), C.addressof(arr), _p(rays6), _p(tmax), n, 1 if watertight else 0,
+                             _p(out), _p(hit_index), _p(cnt), threads)
+    return out, hit_index, cnt
+
+
+def mt(o, d, p0, p1, p2, tmax):
+    a = [np.ascontiguousarray(x, np.float32) for x in (o, d, p0, p1, p2)]
+    t, u, v = C.c_float(), C.c_float(), C.c_float()
+    hit = lib().orc_intersect_triangle_mt(*[_p(x) for x in a], tmax, C.byref(t), C.byref(u), C.byref(v))
+    return bool(hit), t.value, u.value, v.value
+
+
+def watertight(o, d, p0, p1, p2, thit):
+    a = [np.ascontiguousarray(x, np.float32) for x in (o, d, p0, p1, p2)]
+    th, b0, b1, b2 = C.c_float(thit), C.c_float(), C.c_float(), C.c_float()
+    hit = lib().orc_intersect_triangle_watertight(*[_p(x) for x in a], C.byref(th), C.byref(b0), C.byref(b1),
+                                                  C.byref(b2))
+    return bool(hit), th.value, b0.value, b1.value, b2.value
+
+
+def aabb(mn, mx, o, d, tmax):
+    a = [np.ascontiguousarray(x, np.float32) for x in (mn, mx, o, d)]
+    tn = C.c_float()
+    hit = lib().orc_intersect_aabb(*[_p(x) for x in a], tmax, C.byref(tn))
+    return bool(hit), tn.value
+
+
+def bounds_intersects_swift(mn, mx, o, d, thit):
+    a = [np.ascontiguousarray(x, np.float32) for x in (mn, mx, o, d)]
+    return bool(lib().orc_bounds_intersects_swift(*[_p(x) for x in a], thit))
+
+
+def surface_area(mn, mx):
+    a = [np.ascontiguousarray(x, np.float32) for x in (mn, mx)]
+    return lib().orc_bounds_surface_area(*[_p(x) for x in a])
+
+
+def maximum_extent(mn, mx):
+    a = [np.ascontiguousarray(x, np.float32) for x in (mn, mx)]
+    return lib().orc_bounds_maximum_extent(*[_p(x) for x in a])
+
+
+def zsobol_batch(spp, res_x, res_y, px, py, index, kinds, seed=1234):
+    px = np.ascontiguousarray(px, np.int32)
+    py = np.ascontiguousarray(py, np.int32)
+    index = np.ascontiguousarray(index, np.int64)
+    kinds = np.ascontiguousarray(kinds, np.int32)
+    per = int(kinds.sum())
+    out = np.zeros((len(px), per), np.float32)
+    lib().orc_zsobol_batch(spp, res_x, res_y, seed, _p(px), _p(py), _p(index), len(px), _p(kinds), len(kinds),
+                           _p(out))
+    return out

@@ -1,0 +1,250 @@
+"""GPU parity of the libgzg traversal kernels against the oracle (the CPU
+restatement of kernel.mojo's traverse_bvh2_core) on identical rays.
+
+  BVH2 mode (reference node order and slab arithmetic): bit-exact, no ties.
+  wide mode: every ray exact, a counted equal-t tie, or a counted
+      "reference-culled" hit (the reference's slab test culled a node the
+      conservative wide boxes keep); never a missed or farther hit.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gonzales_b200 import GpuAccelerator, options, scenes
+from gonzales_b200 import _ffi as F
+from oracle import pyoracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def torch_mod():
+    import torch
+
+    return torch
+
+
+def device_closest(acc, o, d, t, opt=None):
+    torch = torch_mod()
+    rays = torch.from_numpy(scenes.pack_device_rays(o, d, t)).cuda()
+    hits = torch.empty((len(t), 4), dtype=torch.float32, device="cuda")
+    acc.trace_closest(rays, hits, opt)
+    torch.cuda.synchronize()
+    h = hits.cpu().numpy()
+    return h[:, 3].view(np.int32).copy(), h[:, 0].copy(), h[:, 1].copy(), h[:, 2].copy()
+
+
+def device_any(acc, o, d, t, opt=None):
+    torch = torch_mod()
+    rays = torch.from_numpy(scenes.pack_device_rays(o, d, t)).cuda()
+    out = torch.empty(len(t), dtype=torch.int32, device="cuda")
+    acc.trace_any(rays, out, opt)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def small():
+    hs, o, d, t = H.small_raycast(subdiv=4, n_side=64, n_incoherent=8192)
+    acc = GpuAccelerator(hs)
+    isect, idx, _ = H.oracle_closest(hs, o, d, t)
+    yield hs, acc, o, d, t, isect, idx
+    acc.close()
+
+
+def _check(hs, o, d, t, gpu, isect, idx, watertight=False):
+    prim, tt, u, v = gpu
+    return H.classify(hs, o, d, t, prim, tt, u, v, idx, isect["t_hit"], isect["u"], isect["v"], watertight)
+
+
+def test_bvh2_mode_is_bit_exact(small):
+    hs, acc, o, d, t, isect, idx = small
+    gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+    counts, fails = _check(hs, o, d, t, gpu, isect, idx)
+    assert counts["exact"] == counts["rays"], counts
+
+
+def test_wide_mode_parity(small):
+    hs, acc, o, d, t, isect, idx = small
+    gpu = device_closest(acc, o, d, t)
+    counts, fails = _check(hs, o, d, t, gpu, isect, idx)
+    assert counts["fail"] == 0, (counts, fails[:10])
+    assert counts["exact"] >= 0.999 * counts["rays"], counts
+    assert acc.error_word() == 0
+
+
+@pytest.mark.parametrize("traversal", [F.TRAVERSAL_WIDE, F.TRAVERSAL_BVH2])
+def test_any_hit(small, traversal):
+    hs, acc, o, d, t, isect, idx = small
+    anyp = device_any(acc, o, d, t, options(traversal=traversal))
+    hit_o = idx >= 0
+    hit_g = anyp >= 0
+    # every ray the reference hits is occluded on the GPU
+    assert np.all(hit_g[hit_o])
+    # every GPU any-hit prim is a genuine hit within (0, tMax]
+    for i in np.nonzero(hit_g)[0][:: max(1, hit_g.sum() // 500)]:
+        p0, p1, p2 = H.prim_triangle(hs, int(anyp[i]))
+        assert O.mt(o[i], d[i], p0, p1, p2, float(t[i]))[0]
+    extra = np.nonzero(hit_g & ~hit_o)[0]
+    for i in extra:
+        p0, p1, p2 = H.prim_triangle(hs, int(anyp[i]))
+        assert O.mt(o[i], d[i], p0, p1, p2, float(t[i]))[0]
+    if traversal == F.TRAVERSAL_BVH2:
+        assert len(extra) == 0
+
+
+def test_intersection_records_drop_in(small):
+    """gzg_gpu_traverse_batch returns the reference's Intersection_C records."""
+    hs, acc, o, d, t, isect, idx = small
+    rays = scenes.pack_reference_rays(o, d)
+    res = acc.intersect_batch(rays, t, options(traversal=F.TRAVERSAL_BVH2))
+    assert res.tobytes() == isect.tobytes()
+    res_w = acc.intersect_batch(rays, t)
+    same = res_w.tobytes() == isect.tobytes()
+    if not same:
+        diff = np.nonzero(res_w["prim_id"]["id1"] != isect["prim_id"]["id1"])[0]
+        assert len(diff) <= 0.001 * len(t)
+
+
+def test_host_batch_pinned_and_pageable_agree(small):
+    torch = torch_mod()
+    hs, acc, o, d, t, isect, idx = small
+    reps = 1300000 // len(t) + 1  # more than one pipelined chunk
+    o2, d2, t2 = np.tile(o, (reps, 1)), np.tile(d, (reps, 1)), np.tile(t, reps)
+    rays = scenes.pack_reference_rays(o2, d2)
+    page = acc.intersect_batch(rays, t2)
+    pr = torch.from_numpy(rays).pin_memory()
+    pt = torch.from_numpy(t2).pin_memory()
+    po = torch.zeros(len(t2) * 48, dtype=torch.uint8).pin_memory()
+    out = po.numpy().view(F.INTERSECTION_DTYPE)
+    acc.intersect_batch(pr.numpy(), pt.numpy(), out=out)
+    assert out.tobytes() == page.tobytes()
+    n = len(t)
+    assert page[:n].tobytes() == page[n:2 * n].tobytes()
+    occ = acc.occluded_batch(rays, t2)
+    assert np.array_equal(occ[:n] != 0, device_any(acc, o, d, t) >= 0)
+
+
+def test_watertight_leaf_test(small):
+    hs, acc, o, d, t, _, _ = small
+    isect, idx, _ = H.oracle_closest(hs, o, d, t, watertight=True)
+    gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2, leaf_test=F.LEAF_WATERTIGHT))
+    counts, _ = _check(hs, o, d, t, gpu, isect, idx, watertight=True)
+    assert counts["exact"] == counts["rays"], counts
+    gpu = device_closest(acc, o, d, t, options(leaf_test=F.LEAF_WATERTIGHT))
+    counts, fails = _check(hs, o, d, t, gpu, isect, idx, watertight=True)
+    assert counts["fail"] == 0, counts
+
+
+def test_empty_batch_and_tiny_tmax(small):
+    torch = torch_mod()
+    hs, acc, o, d, t, _, _ = small
+    rays = torch.zeros((0, 8), dtype=torch.float32, device="cuda")
+    hits = torch.zeros((0, 4), dtype=torch.float32, device="cuda")
+    acc.trace_closest(rays, hits)
+    assert len(acc.intersect_batch(np.zeros((0, 6), np.float32), np.zeros(0, np.float32))) == 0
+    tt = np.full(len(t), 1e-12, np.float32)
+    prim, th, u, v = device_closest(acc, o, d, tt)
+    assert (prim == -1).all() and (th == tt).all() and (u == 0).all() and (v == 0).all()
+
+
+def test_axis_aligned_rays_reference_nan_quirk():
+    """Rays with a zero direction component and zero origin component: the
+    reference's slab test turns 0 * inf into NaN and culls every box.  BVH2
+    mode reproduces that; wide mode finds the hits (reference-culled)."""
+    hs = scenes.raycast_scene(subdiv=3).build()
+    n = 64
+    o = np.zeros((n, 3), np.float32)
+    o[:, 2] = np.linspace(-3, 3, n)
+    d = np.zeros((n, 3), np.float32)
+    d[:, 0] = 1.0
+    t = np.full(n, np.inf, np.float32)
+    with GpuAccelerator(hs) as acc:
+        isect, idx, _ = H.oracle_closest(hs, o, d, t)
+        assert (idx == -1).all()
+        gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+        assert _check(hs, o, d, t, gpu, isect, idx)[0]["exact"] == n
+        gpu = device_closest(acc, o, d, t)
+        counts, _ = _check(hs, o, d, t, gpu, isect, idx)
+        assert counts["fail"] == 0 and counts["reference_culled"] > 0
+
+
+def test_coincident_triangles_tie_rule():
+    """Two identical triangles: the reference keeps the later one at equal t."""
+    sb = scenes.SceneBuilder()
+    m = sb.add_material()
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    sb.add_mesh(tri, [[0, 1, 2]], m)
+    sb.add_mesh(tri, [[0, 1, 2]], m)
+    hs = sb.build()
+    o = np.array([[0.2, 0.2, 1.0]], np.float32)
+    d = np.array([[0, 0, -1]], np.float32)
+    t = np.array([np.inf], np.float32)
+    with GpuAccelerator(hs) as acc:
+        isect, idx, _ = H.oracle_closest(hs, o, d, t)
+        gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+        assert gpu[0][0] == idx[0]
+        gpu = device_closest(acc, o, d, t)
+        counts, _ = _check(hs, o, d, t, gpu, isect, idx)
+        assert counts["fail"] == 0 and counts["exact"] + counts["tie"] == 1
+
+
+def test_box_scene_parity():
+    hs = scenes.box_scene().build()
+    rng = np.random.default_rng(7)
+    n = 20000
+    o = rng.uniform(0.05, 0.95, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    t = np.full(n, np.inf, np.float32)
+    with GpuAccelerator(hs) as acc:
+        isect, idx, _ = H.oracle_closest(hs, o, d, t)
+        assert (idx >= 0).mean() > 0.99  # closed box from inside
+        gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+        assert _check(hs, o, d, t, gpu, isect, idx)[0]["exact"] == n
+        gpu = device_closest(acc, o, d, t)
+        counts, fails = _check(hs, o, d, t, gpu, isect, idx)
+        assert counts["fail"] == 0, counts
+
+
+def test_golden_vectors():
+    """Committed oracle outputs (tests/golden/raycast_small.npz, made by
+    tests/golden/make_golden.py) against the live GPU kernels."""
+    g = np.load(GOLDEN / "raycast_small.npz")
+    hs = scenes.raycast_scene(subdiv=int(g["subdiv"])).build()
+    assert hs.nodes.tobytes() == g["nodes"].tobytes()
+    o, d, t = g["o"], g["d"], g["t"]
+    with GpuAccelerator(hs) as acc:
+        prim, th, u, v = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+        assert np.array_equal(prim, g["prim"])
+        assert np.array_equal(H.bits(th), H.bits(g["t_hit"]))
+        assert np.array_equal(H.bits(u), H.bits(g["u"])) and np.array_equal(H.bits(v), H.bits(g["v"]))
+        prim, th, u, v = device_closest(acc, o, d, t)
+        counts, _ = H.classify(hs, o, d, t, prim, th, u, v, g["prim"], g["t_hit"], g["u"], g["v"])
+        assert counts["fail"] == 0
+
+
+def test_full_size_raycast_parity():
+    """The full ray-cast workload (1,310,720 triangles, 8M coherent + 8M
+    incoherent rays) against the oracle on every ray."""
+    hs = scenes.raycast_scene(subdiv=8).build()
+    o, d, t = scenes.raycast_rays(hs, 4096, 2048, 8388608)
+    isect, idx, _ = H.oracle_closest(hs, o, d, t)
+    with GpuAccelerator(hs) as acc:
+        info = acc.info()
+        assert info["triangles"] == 1310720
+        gpu = device_closest(acc, o, d, t)
+        counts, fails = _check(hs, o, d, t, gpu, isect, idx)
+        out = Path(__file__).resolve().parent.parent / "gpurun_out"
+        if out.is_dir():
+            (out / "parity_full_raycast.json").write_text(json.dumps({"wide": counts, "info": info}))
+        assert counts["fail"] == 0, (counts, fails[:10])
+        gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+        assert np.array_equal(gpu[0], idx)
+        assert np.array_equal(H.bits(gpu[1]), H.bits(isect["t_hit"]))
+        anyp = device_any(acc, o, d, t)
+        assert np.all(anyp[idx >= 0] >= 0)
+        assert acc.error_word() == 0

@@ -1,0 +1,170 @@
+"""CPU-only tests of the host side of libgzg: the library loads and exports
+every declared entry point, the host SAH builder reproduces the reference
+builder (via the oracle restatement) exactly, and argument errors are reported
+as status codes."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gonzales_b200 import _ffi as F
+from gonzales_b200 import scene as S
+from gonzales_b200 import scenes
+from oracle import pyoracle as O
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        names |= set(re.findall(r"GZG_API\s+[\w\s\*]+?\b(gzg_\w+)\s*\(", h.read_text()))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(F.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    declared = declared_symbols()
+    assert declared, "no declarations parsed"
+    missing = declared - exported
+    assert not missing, missing
+    # only declared gzg_ symbols are exported
+    extra = {s for s in exported if s.startswith("gzg_")} - declared
+    assert not extra, extra
+
+
+def test_ffi_prototypes_cover_declarations():
+    assert set(F.PROTOTYPES) == declared_symbols()
+    F.lib()  # loads and binds every prototype
+
+
+def test_record_layouts_match_reference_header():
+    assert F.PRIM_ID_DTYPE.itemsize == 32
+    assert F.INTERSECTION_DTYPE.itemsize == 48
+    assert F.BVH2_NODE_DTYPE.itemsize == 32
+    assert F.MATERIAL_DTYPE.itemsize == 28
+    assert F.RAY_DTYPE.itemsize == 24
+
+
+@pytest.mark.parametrize("subdiv", [0, 1, 3, 5])
+def test_host_builder_matches_reference_builder(subdiv):
+    hs = scenes.raycast_scene(subdiv=subdiv).build()
+    b = S.triangle_bounds(hs.meshes[0])
+    bo = O.triangle_bounds(hs.meshes[0].points, hs.meshes[0].vertex_indices)
+    assert np.array_equal(b.view(np.uint32), bo.view(np.uint32))
+    nodes, order = O.build_bvh2(b)
+    assert nodes.tobytes() == hs.nodes.tobytes()
+    assert np.array_equal(order, hs.prim_order)
+
+
+def test_host_builder_box_scene_matches():
+    hs = scenes.box_scene().build()
+    bounds = np.concatenate([S.triangle_bounds(m) for m in hs.meshes])
+    nodes, order = O.build_bvh2(bounds)
+    assert nodes.tobytes() == hs.nodes.tobytes()
+    assert np.array_equal(order, hs.prim_order)
+
+
+def _rand_bounds(rng, n, degenerate=False):
+    lo = rng.uniform(-1, 1, (n, 3)).astype(np.float32)
+    if degenerate:
+        lo[:] = lo[0]
+    ext = rng.uniform(0, 0.2, (n, 3)).astype(np.float32)
+    b = np.concatenate([lo, lo + ext], 1).astype(np.float32)
+    if degenerate:
+        b[:] = b[0]
+    return b
+
+
+@pytest.mark.parametrize("n,degenerate,threads", [(1, False, 1), (2, False, 1), (3, False, 2), (7, True, 4),
+                                                  (1000, False, 8), (250000, False, 8), (250000, False, 1)])
+def test_host_builder_edge_cases(n, degenerate, threads):
+    rng = np.random.default_rng(n)
+    b = _rand_bounds(rng, n, degenerate)
+    if n == 3:
+        b[1] = b[0]  # duplicate prims
+    nodes, order = S.build_bvh2(b, threads=threads)
+    onodes, oorder = O.build_bvh2(b)
+    assert nodes.tobytes() == onodes.tobytes()
+    assert np.array_equal(order, oorder)
+    assert sorted(order.tolist()) == list(range(n))
+    if degenerate:
+        assert len(nodes) == 1 and nodes[0]["count"] == n  # identical centroids -> one leaf
+
+
+def test_host_builder_zero_area_prims():
+    # flat prims in a plane: bounds.surfaceArea() == 0 at the root -> one leaf
+    b = np.zeros((5, 6), np.float32)
+    b[:, 0] = np.arange(5)
+    b[:, 3] = np.arange(5)
+    nodes, order = S.build_bvh2(b)
+    onodes, oorder = O.build_bvh2(b)
+    assert nodes.tobytes() == onodes.tobytes() and np.array_equal(order, oorder)
+
+
+def test_host_builder_argument_errors():
+    L = F.lib()
+    cnt = F.I64(0)
+    assert L.gzg_host_build_bvh2(None, -1, None, C.byref(cnt), None, 0) == 1
+    assert b"bad arguments" in L.gzg_last_error()
+    assert L.gzg_host_build_bvh2(None, 0, None, C.byref(cnt), None, 0) == 0 and cnt.value == 0
+    assert L.gzg_host_triangle_bounds(None, None, -5, None) == 1
+
+
+def test_free_null_scene_is_noop():
+    assert F.lib().gzg_gpu_free_scene(None) == 0
+
+
+def test_upload_rejects_bad_arguments_before_touching_a_device():
+    L = F.lib()
+    h = C.c_void_p()
+    assert L.gzg_gpu_upload_scene(None, 0, None, 0, None, 0, None, None, None, None, 0, C.byref(h)) == 1
+    assert L.gzg_gpu_upload_scene(None, 1, None, 0, None, 0, None, None, None, None, 0, None) == 1
+
+
+def _upload_status(hs):
+    meshes = hs.mesh_structs()
+    pts, fi, vi = hs.counts()
+    h = C.c_void_p()
+    st = F.lib().gzg_gpu_upload_scene(F.ptr(hs.nodes), len(hs.nodes), F.ptr(hs.prims), len(hs.prims),
+                                      C.addressof(meshes), len(hs.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
+                                      F.ptr(hs.materials), len(hs.materials), C.byref(h))
+    if st == 0:
+        F.lib().gzg_gpu_free_scene(h)
+    return st, F.lib().gzg_last_error().decode()
+
+
+def test_upload_rejects_cyclic_bvh():
+    hs = scenes.raycast_scene(subdiv=1).build()
+    hs.nodes[0]["offset"] = 0  # right child points back at the root
+    st, msg = _upload_status(hs)
+    assert st == 5 and "child link" in msg
+
+
+def test_upload_rejects_out_of_range_vertex():
+    hs = scenes.raycast_scene(subdiv=1).build()
+    hs.meshes[0].vertex_indices[4] = 10 ** 9
+    st, msg = _upload_status(hs)
+    assert st == 5 and "out of range" in msg
+
+
+def test_upload_rejects_bad_leaf_range():
+    hs = scenes.raycast_scene(subdiv=1).build()
+    leaf = np.nonzero(hs.nodes["count"] > 0)[0][0]
+    hs.nodes[leaf]["offset"] = len(hs.prims)
+    st, msg = _upload_status(hs)
+    assert st == 5 and "leaf range" in msg
+
+
+def test_upload_valid_scene_without_device_reports_no_device():
+    from tests.conftest import HAS_GPU
+
+    if HAS_GPU:
+        pytest.skip("device present")
+    st, _ = _upload_status(scenes.raycast_scene(subdiv=1).build())
+    assert st == 2
