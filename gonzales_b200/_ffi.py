@@ -25,6 +25,7 @@ STATUS_NAMES = {
 
 TRAVERSAL_WIDE = 0
 TRAVERSAL_BVH2 = 1
+TRAVERSAL_WIDE_ONE_RAY_PER_THREAD = 2
 LEAF_MOLLER_TRUMBORE = 0
 LEAF_WATERTIGHT = 1
 

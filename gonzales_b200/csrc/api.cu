@@ -163,7 +163,8 @@ LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o) {
 
 gzg_status check_options(const gzg_trace_options *o) {
         if (!o) return GZG_OK;
-        if (o->traversal != GZG_TRAVERSAL_WIDE && o->traversal != GZG_TRAVERSAL_BVH2)
+        if (o->traversal != GZG_TRAVERSAL_WIDE && o->traversal != GZG_TRAVERSAL_BVH2 &&
+            o->traversal != GZG_TRAVERSAL_WIDE_ONE_RAY_PER_THREAD)
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "unknown traversal");
         if (o->leaf_test != GZG_LEAF_MOLLER_TRUMBORE && o->leaf_test != GZG_LEAF_WATERTIGHT)
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "unknown leaf test");

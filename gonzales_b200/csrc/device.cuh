@@ -183,11 +183,10 @@ __device__ __forceinline__ void store_hit(const DevScene &s, void *out, int64_t 
                 uint4 w0, w1;
                 if (prim >= 0) {
                         const uint4 *src = reinterpret_cast<const uint4 *>(s.prims + prim);
+                        // the whole 32-byte PrimId_C, padding included, as the
+                        // reference copies the struct (kernel.mojo:360-361)
                         w0 = __ldg(src);
                         w1 = __ldg(src + 1);
-                        // type byte + zeroed padding
-                        w1.z &= 0xFFu;
-                        w1.w = 0u;
                 } else {
                         w0 = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
                         w1 = make_uint4(0u, 0u, 0u, 0u);

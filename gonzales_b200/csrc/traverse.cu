@@ -183,6 +183,151 @@ __global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict
         add_counters(s, n_nodes, n_tris);
 }
 
+// Persistent variant of k_wide.  The grid is sized to the resident capacity
+// (SM count x blocks per SM); warp w owns the 32-ray chunks w, w + W, w + 2W,
+// ... (W = warps in the grid) and hands out the rays of its current chunk in
+// order.  A lane whose ray finishes takes the next ray at the top of the next
+// iteration, so lanes are not left idle while the slowest ray of a fixed
+// 32-ray batch finishes.  Each iteration opens one node and tests its
+// triangles.  No atomics or per-launch state: the assignment is static.
+template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
+__global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void *__restrict__ rays,
+                                                         const float *__restrict__ tmaxs, int64_t n,
+                                                         void *__restrict__ out) {
+        extern __shared__ uint2 smem_stack[];
+        const unsigned FULL = 0xFFFFFFFFu;
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned lt_mask = (1u << lane) - 1u;
+        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+        int64_t chunk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        int64_t cursor = chunk * 32;
+        int64_t chunk_end = cursor + 32 < n ? cursor + 32 : n;
+
+        uint2 *stack = smem_stack + threadIdx.x;
+        const int stride = blockDim.x;
+        int64_t ray_i = -1;
+        WideRay r;
+        float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
+        int prim = -1, sp = 0;
+        uint2 group = make_uint2(0u, 0u);
+        uint32_t steps = 0, n_nodes = 0, n_tris = 0;
+
+        for (;;) {
+                // ---- refill idle lanes from this warp's chunk sequence (warp-uniform cursor)
+                unsigned need = __ballot_sync(FULL, ray_i < 0);
+                while (need != 0u && cursor < n) {
+                        if (cursor >= chunk_end) {
+                                chunk += nwarps;
+                                cursor = chunk * 32;
+                                chunk_end = cursor + 32 < n ? cursor + 32 : n;
+                                if (cursor >= n) break;
+                        }
+                        const int avail = (int)(chunk_end - cursor);
+                        const int rank = __popc(need & lt_mask);
+                        if (ray_i < 0 && rank < avail) {
+                                ray_i = cursor + rank;
+                                const RayIn in = load_ray<RAYFMT>(rays, tmaxs, ray_i);
+                                r.ox = in.ox;
+                                r.oy = in.oy;
+                                r.oz = in.oz;
+                                r.dx = in.dx;
+                                r.dy = in.dy;
+                                r.dz = in.dz;
+                                r.rdx = __fdiv_rn(1.0f, in.dx);
+                                r.rdy = __fdiv_rn(1.0f, in.dy);
+                                r.rdz = __fdiv_rn(1.0f, in.dz);
+                                r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
+                                        ((__float_as_uint(r.rdz) >> 31) << 2);
+                                tmax = in.tmax;
+                                thit = in.tmax;
+                                bu = bv = 0.0f;
+                                prim = -1;
+                                sp = 0;
+                                steps = 0;
+                                group = make_uint2(0u, (1u << 24) | (1u << r.oct));
+                        }
+                        const int npop = __popc(need);
+                        cursor += npop < avail ? npop : avail;
+                        need = __ballot_sync(FULL, ray_i < 0);
+                }
+                if (__all_sync(FULL, ray_i < 0)) break;
+                if (ray_i < 0) continue;
+
+                // ---- one traversal step: open one node, test its triangles
+                bool finished = false;
+                uint32_t tri_hits = 0, tri_base = 0;
+                uint32_t hits = group.y >> 24;
+                if (hits) {
+                        const uint32_t key = __ffs(hits) - 1;
+                        hits &= hits - 1;
+                        const uint32_t im = group.y & 0xFFu;
+                        const uint32_t slot = key ^ r.oct;
+                        const uint32_t node = group.x + __popc(im & ((1u << slot) - 1u));
+                        bool fault = false;
+                        if (hits) {
+                                if (sp >= STACK) {
+                                        atomicOr(s.err, kErrStackOverflow);
+                                        fault = true;
+                                } else {
+                                        stack[sp * stride] = make_uint2(group.x, (hits << 24) | im);
+                                        ++sp;
+                                }
+                        }
+                        if (++steps > s.wide_count) {
+                                atomicOr(s.err, kErrStepCap);
+                                fault = true;
+                        }
+                        if (fault) {
+                                group.y = 0u;
+                                sp = 0;
+                        } else {
+                                uint32_t nh, nim, cb;
+                                open_node(s.wide + 5 * (size_t)node, r, thit, nh, nim, cb, tri_hits, tri_base);
+                                ++n_nodes;
+                                group = make_uint2(cb, (nh << 24) | nim);
+                        }
+                }
+                while (tri_hits) {
+                        const uint32_t b = __ffs(tri_hits) - 1;
+                        tri_hits &= tri_hits - 1;
+                        const uint32_t ti = tri_base + b;
+                        ++n_tris;
+                        const float4 a = __ldg(s.tv0 + ti);
+                        const float4 bb = __ldg(s.tv1 + ti);
+                        const float4 c = __ldg(s.tv2 + ti);
+                        float t, u, v;
+                        if (leaf_test<LEAF>(r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, a, bb, c, thit, t, u, v)) {
+                                thit = t;
+                                bu = u;
+                                bv = v;
+                                prim = __float_as_int(a.w);
+                                if (ANY) {
+                                        finished = true;
+                                        break;
+                                }
+                        }
+                }
+                if (!finished && (group.y >> 24) == 0) {
+                        if (sp == 0)
+                                finished = true;
+                        else {
+                                --sp;
+                                group = stack[sp * stride];
+                        }
+                }
+                if (finished) {
+                        if (prim < 0) {
+                                thit = tmax;
+                                bu = 0.0f;
+                                bv = 0.0f;
+                        }
+                        store_hit<OUTFMT>(s, out, ray_i, prim, thit, bu, bv);
+                        ray_i = -1;
+                }
+        }
+        add_counters(s, n_nodes, n_tris);
+}
+
 // The reference's slab test (kernel.mojo:171-206), separately rounded.
 __device__ __forceinline__ bool ref_aabb(const float4 &lo, const float4 &hi, const float rd[3], const float ord[3],
                                          const bool nm[3], float tmax, float &tnear_out) {
@@ -309,23 +454,53 @@ __global__ void k_hits_to_isect(DevScene s, const float4 *__restrict__ hits, int
 
 namespace {
 
-template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
-cudaError_t launch_wide_depth(const DevScene &s, int depth, const void *rays, const float *tmax, int64_t n, void *out,
-                              int block, cudaStream_t st) {
-        const int64_t grid = (n + block - 1) / block;
-        if (depth <= 16) {
-                size_t sm = (size_t)16 * block * sizeof(uint2);
-                k_wide<RAYFMT, OUTFMT, ANY, 16, LEAF><<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
-        } else if (depth <= 32) {
-                size_t sm = (size_t)32 * block * sizeof(uint2);
-                k_wide<RAYFMT, OUTFMT, ANY, 32, LEAF><<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
-        } else {
-                auto k = k_wide<RAYFMT, OUTFMT, ANY, 64, LEAF>;
-                size_t sm = (size_t)64 * block * sizeof(uint2);
-                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-                k<<<(unsigned)grid, block, sm, st>>>(s, rays, tmax, n, out);
+using TraceKernel = void (*)(DevScene, const void *, const float *, int64_t, void *);
+
+// Launches a wide-node kernel with a STACK-deep shared-memory stack.  The
+// persistent kernel gets one wave of resident blocks (SM count x blocks per
+// SM, from the occupancy calculator unless blocks_per_sm is given), capped at
+// the blocks the ray count needs; the one-ray-per-thread kernel one thread per
+// ray.
+cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, int blocks_per_sm, const DevScene &s,
+                               const void *rays, const float *tmax, int64_t n, void *out, cudaStream_t st) {
+        const int block = 128;
+        const size_t smem = (size_t)stack * block * sizeof(uint2);
+        if (smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
         }
+        int64_t grid = (n + block - 1) / block;
+        if (persistent) {
+                int dev = 0, sms = 0, per_sm = blocks_per_sm;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                if (per_sm <= 0) {
+                        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem);
+                        if (e != cudaSuccess) return e;
+                        if (per_sm <= 0) per_sm = 1;
+                }
+                const int64_t wave = (int64_t)sms * per_sm;
+                if (wave < grid) grid = wave;
+        }
+        k<<<(unsigned)grid, block, smem, st>>>(s, rays, tmax, n, out);
         return cudaGetLastError();
+}
+
+template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
+cudaError_t launch_wide_depth(const DevScene &s, const LaunchParams &p, const void *rays, const float *tmax, int64_t n,
+                              void *out, cudaStream_t st) {
+        const bool persistent = p.traversal == GZG_TRAVERSAL_WIDE;
+        const int bps = p.blocks_per_sm;
+        if (p.wide_depth <= 16) {
+                TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 16, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 16, LEAF>;
+                return launch_wide_kernel(k, 16, persistent, bps, s, rays, tmax, n, out, st);
+        }
+        if (p.wide_depth <= 32) {
+                TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 32, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 32, LEAF>;
+                return launch_wide_kernel(k, 32, persistent, bps, s, rays, tmax, n, out, st);
+        }
+        TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 64, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 64, LEAF>;
+        return launch_wide_kernel(k, 64, persistent, bps, s, rays, tmax, n, out, st);
 }
 
 template <int RAYFMT, int OUTFMT, bool ANY>
@@ -341,8 +516,8 @@ cudaError_t launch_fmt(const DevScene &s, const LaunchParams &p, const void *ray
                 return cudaGetLastError();
         }
         if (p.leaf_test == GZG_LEAF_WATERTIGHT)
-                return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_WATERTIGHT>(s, p.wide_depth, rays, tmax, n, out, block, st);
-        return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_MOLLER_TRUMBORE>(s, p.wide_depth, rays, tmax, n, out, block, st);
+                return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_WATERTIGHT>(s, p, rays, tmax, n, out, st);
+        return launch_wide_depth<RAYFMT, OUTFMT, ANY, GZG_LEAF_MOLLER_TRUMBORE>(s, p, rays, tmax, n, out, st);
 }
 
 }  // namespace

@@ -161,5 +161,9 @@ class SceneBuilder:
             bounds[sl] = triangle_bounds(self.meshes[mesh_idx])
             k += ntri
         nodes, order = build_bvh2(bounds, threads)
-        return HostScene(meshes=self.meshes, prims=prims[order].copy(), nodes=nodes, materials=mats,
+        # Reorder whole 32-byte records (a field-wise structured copy would
+        # leave the padding bytes undefined).
+        raw = prims.view(np.uint8).reshape(-1, F.PRIM_ID_DTYPE.itemsize)[order]
+        sorted_prims = np.ascontiguousarray(raw).view(F.PRIM_ID_DTYPE).reshape(-1)
+        return HostScene(meshes=self.meshes, prims=sorted_prims, nodes=nodes, materials=mats,
                          prim_order=order)

@@ -147,12 +147,16 @@ typedef struct gzg_hit_d {
 
 typedef enum gzg_traversal {
         /* Wide (8-ary) nodes with 8-bit child boxes quantised outward, leaf
-         * triangles in leaf order, shared-memory short stack.  Default. */
+         * triangles in leaf order, shared-memory short stack; persistent
+         * warps that refill finished lanes from a static ray sequence.
+         * Default. */
         GZG_TRAVERSAL_WIDE = 0,
         /* The uploaded BVH2 traversed in the reference's exact order and slab
          * arithmetic (kernel.mojo:171-206, 223-364), one thread per ray.
          * Bit-exact with the reference including ties. */
-        GZG_TRAVERSAL_BVH2 = 1
+        GZG_TRAVERSAL_BVH2 = 1,
+        /* The wide traversal with one thread per ray and no refill. */
+        GZG_TRAVERSAL_WIDE_ONE_RAY_PER_THREAD = 2
 } gzg_traversal;
 
 typedef enum gzg_leaf_test {

@@ -67,9 +67,10 @@ def test_bvh2_mode_is_bit_exact(small):
     assert counts["exact"] == counts["rays"], counts
 
 
-def test_wide_mode_parity(small):
+@pytest.mark.parametrize("traversal", [F.TRAVERSAL_WIDE, F.TRAVERSAL_WIDE_ONE_RAY_PER_THREAD])
+def test_wide_mode_parity(small, traversal):
     hs, acc, o, d, t, isect, idx = small
-    gpu = device_closest(acc, o, d, t)
+    gpu = device_closest(acc, o, d, t, options(traversal=traversal))
     counts, fails = _check(hs, o, d, t, gpu, isect, idx)
     assert counts["fail"] == 0, (counts, fails[:10])
     assert counts["exact"] >= 0.999 * counts["rays"], counts
