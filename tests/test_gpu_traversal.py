@@ -203,7 +203,7 @@ def test_box_scene_parity():
     t = np.full(n, np.inf, np.float32)
     with GpuAccelerator(hs) as acc:
         isect, idx, _ = H.oracle_closest(hs, o, d, t)
-        assert (idx >= 0).mean() > 0.99  # closed box from inside
+        assert (idx >= 0).mean() > 0.7  # five walls: rays toward the open +z side escape
         gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
         assert _check(hs, o, d, t, gpu, isect, idx)[0]["exact"] == n
         gpu = device_closest(acc, o, d, t)
