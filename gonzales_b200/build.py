@@ -44,7 +44,7 @@ def build(force=False, verbose=False):
         if src.suffix == ".cu":
             cmd += CUDA_FLAGS
         else:
-            cmd += ["-x", "c++"]
+            cmd += ["-x", "c++", "-Wno-deprecated-gpu-targets"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
