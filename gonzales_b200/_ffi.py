@@ -81,6 +81,7 @@ PROTOTYPES = {
     "gzg_gpu_free_scene": (ST, [VP]),
     "gzg_gpu_traverse_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
     "gzg_gpu_occluded_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
+    "gzg_gpu_traverse_batch_static": (ST, [VP, VP, VP, I64, VP]),
     "gzg_trace_closest_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_trace_any_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),

@@ -450,3 +450,13 @@ GZG_API gzg_status gzg_scene_error_word(gzg_scene *scene, uint32_t *word, int cl
 }
 
 }  // extern "C"
+
+namespace gzg {
+
+void scene_view(const gzg_scene *scene, DevScene *view, int *device, int *wide_depth) {
+        *view = scene->dev;
+        *device = scene->device;
+        *wide_depth = scene->info.wide_depth;
+}
+
+}  // namespace gzg

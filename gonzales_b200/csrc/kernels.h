@@ -23,4 +23,7 @@ cudaError_t launch_trace(const DevScene &s, const LaunchParams &p, int ray_fmt, 
 
 cudaError_t launch_hits_to_isect(const DevScene &s, const void *hits, int64_t n, void *out, cudaStream_t st);
 
+// Device view, device ordinal and wide-tree depth of an uploaded scene.
+void scene_view(const gzg_scene *scene, DevScene *view, int *device, int *wide_depth);
+
 }  // namespace gzg

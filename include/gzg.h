@@ -229,6 +229,20 @@ GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays,
                                           gzg_intersection *results,
                                           const gzg_trace_options *options);
 
+/* Closest hit for host rays like gzg_gpu_traverse_batch (default options),
+ * for callers that must not allocate: it makes no cudaMalloc, cudaFree or
+ * pinned-host allocation, and stages rays, tMax values and results through a
+ * fixed array in the library's device image (a file-scope __device__ array of
+ * 4,980,736 bytes, held on every GPU that loads the library until exit).
+ * At most 65,536 rays per call (more: GZG_ERR_LIMIT).  The first call on a
+ * device looks up that array's device address, so make it before any stream
+ * capture.  Calls share the array and are serialised by a process-wide lock.
+ * No counterpart in the reference: Gonzales' GPU batch call allocates device
+ * buffers on every call. */
+GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, const gzg_ray *rays,
+                                                 const float *t_max_values, int64_t count,
+                                                 gzg_intersection *results);
+
 /* Shadow / any-hit batch (new; Visibility.occluded, Core/Visibility.swift:5-24,
  * answers it with a closest-hit query, BoundingHierarchy.swift:348-384).
  * occluded[i] = 1 iff some triangle is hit with 0 < t <= tMax[i]. */
