@@ -31,12 +31,12 @@ struct DevScene {
 
 // Adds per-thread fetch counts into s.counters (one atomic per converged
 // group of lanes; __reduce_add_sync is exact for any active mask).
-__device__ __forceinline__ void add_counters(const DevScene &s, uint32_t nodes, uint32_t tris) {
+__device__ __forceinline__ void add_counters(const DevScene &s, uint32_t nodes, uint32_t tris, uint32_t rays) {
         if (s.counters == nullptr) return;
         const unsigned mask = __activemask();
         const unsigned n = __reduce_add_sync(mask, nodes);
         const unsigned t = __reduce_add_sync(mask, tris);
-        const unsigned r = __popc(mask);
+        const unsigned r = __reduce_add_sync(mask, rays);
         if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) {
                 atomicAdd(s.counters, (unsigned long long)n);
                 atomicAdd(s.counters + 1, (unsigned long long)t);

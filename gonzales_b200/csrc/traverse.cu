@@ -54,6 +54,13 @@ __device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const 
         const float ax = (px - r.ox) * r.rdx;
         const float ay = (py - r.oy) * r.rdy;
         const float az = (pz - r.oz) * r.rdz;
+        // Far planes carry the relative slack 1.0000003 of the reference's
+        // tFar (kernel.mojo:204) in their per-node constants instead of one
+        // multiply per child; thit is scaled the same way once.
+        const float kSlack = 1.0000003f;
+        const float fsx = sx * kSlack, fsy = sy * kSlack, fsz = sz * kSlack;
+        const float fax = ax * kSlack, fay = ay * kSlack, faz = az * kSlack;
+        const float thit_far = thit * kSlack;
         // near/far plane words by ray sign (lo planes are near for rdir >= 0)
         const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
         const uint32_t lx0 = n2.x, lx1 = n2.y, ly0 = n2.z, ly1 = n2.w, lz0 = n3.x, lz1 = n3.y;
@@ -73,11 +80,11 @@ __device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const 
                 const float tnx = fmaf(qbyte(nearx[w], sel), sx, ax);
                 const float tny = fmaf(qbyte(neary[w], sel), sy, ay);
                 const float tnz = fmaf(qbyte(nearz[w], sel), sz, az);
-                const float tfx = fmaf(qbyte(farx[w], sel), sx, ax);
-                const float tfy = fmaf(qbyte(fary[w], sel), sy, ay);
-                const float tfz = fmaf(qbyte(farz[w], sel), sz, az);
+                const float tfx = fmaf(qbyte(farx[w], sel), fsx, fax);
+                const float tfy = fmaf(qbyte(fary[w], sel), fsy, fay);
+                const float tfz = fmaf(qbyte(farz[w], sel), fsz, faz);
                 const float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-                const float tfar = fminf(fminf(tfx, tfy), fminf(tfz, thit)) * 1.0000003f;
+                const float tfar = fminf(fminf(tfx, tfy), fminf(tfz, thit_far));
                 if (tnear <= tfar) {
                         const uint32_t m = (meta[w] >> (8 * (k & 3))) & 0xFFu;
                         if ((imask >> k) & 1u) {
@@ -180,7 +187,7 @@ __global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict
                 bv = 0.0f;
         }
         store_hit<OUTFMT>(s, out, i, prim, thit, bu, bv);
-        add_counters(s, n_nodes, n_tris);
+        add_counters(s, n_nodes, n_tris, 1u);
 }
 
 // Persistent variant of k_wide.  The grid is sized to the resident capacity
@@ -210,7 +217,7 @@ __global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void 
         float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
         int prim = -1, sp = 0;
         uint2 group = make_uint2(0u, 0u);
-        uint32_t steps = 0, n_nodes = 0, n_tris = 0;
+        uint32_t steps = 0, n_nodes = 0, n_tris = 0, n_rays = 0;
 
         for (;;) {
                 // ---- refill idle lanes from this warp's chunk sequence (warp-uniform cursor)
@@ -323,9 +330,10 @@ __global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void 
                         }
                         store_hit<OUTFMT>(s, out, ray_i, prim, thit, bu, bv);
                         ray_i = -1;
+                        ++n_rays;
                 }
         }
-        add_counters(s, n_nodes, n_tris);
+        add_counters(s, n_nodes, n_tris, n_rays);
 }
 
 // The reference's slab test (kernel.mojo:171-206), separately rounded.
@@ -434,7 +442,7 @@ __global__ void __launch_bounds__(128) k_bvh2(DevScene s, const void *__restrict
                 bv = 0.0f;
         }
         store_hit<OUTFMT>(s, out, i, hit_index, thit, bu, bv);
-        add_counters(s, n_nodes, n_tris);
+        add_counters(s, n_nodes, n_tris, 1u);
 }
 
 __global__ void k_hits_to_isect(DevScene s, const float4 *__restrict__ hits, int64_t n, void *__restrict__ out) {
@@ -491,6 +499,10 @@ cudaError_t launch_wide_depth(const DevScene &s, const LaunchParams &p, const vo
                               void *out, cudaStream_t st) {
         const bool persistent = p.traversal == GZG_TRAVERSAL_WIDE;
         const int bps = p.blocks_per_sm;
+        if (p.wide_depth <= 8) {
+                TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 8, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 8, LEAF>;
+                return launch_wide_kernel(k, 8, persistent, bps, s, rays, tmax, n, out, st);
+        }
         if (p.wide_depth <= 16) {
                 TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 16, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 16, LEAF>;
                 return launch_wide_kernel(k, 16, persistent, bps, s, rays, tmax, n, out, st);
