@@ -161,6 +161,61 @@ def cpu_baseline(hs, o, d, t, budget_s=20.0):
                       "closest hit, oracle BVH2 + Moller-Trumbore, %d threads" % (stride, len(sel), cores)}
 
 
+RENDER = dict(width=256, height=256, spp=16, max_depth=5, rr_min_bounce=3)
+
+
+def render_leg(acc_box, args, stream, barrier):
+    """The box-scene path tracer (256 x 256, 16 spp, depth 5, roulette from
+    bounce 3): one frame per step through a graph-captured wavefront."""
+    import torch
+
+    from gonzales_b200 import GpuAccelerator, Renderer, scenes
+    from gonzales_b200 import _ffi as F
+
+    hs = scenes.box_scene().build()
+    acc = GpuAccelerator(hs)
+    p = F.render_params(**RENDER, use_graph=1)
+    W, H = RENDER["width"], RENDER["height"]
+    rgb = torch.zeros((H, W, 3), device="cuda")
+    w = torch.zeros((H, W), device="cuda")
+    steps = max(3, min(args.steps, 20))
+    with Renderer(acc, p) as r:
+        for _ in range(max(3, args.warmup)):
+            r.render(rgb, w)
+        barrier()
+        s0 = r.stats()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            r.render(rgb, w)
+        e1.record(stream)
+        barrier()
+        s1 = r.stats()
+    acc.close()
+    ms = e0.elapsed_time(e1) / steps
+    rays = sum(s1[k] - s0[k] for k in ("camera_rays", "extension_rays", "shadow_rays", "probe_rays")) / steps
+    spp = W * H * RENDER["spp"]
+    return {"config": "box scene 36 tris, %dx%d, %d spp, max depth %d, roulette from bounce %d, MIS as written"
+                      % (W, H, RENDER["spp"], RENDER["max_depth"], RENDER["rr_min_bounce"]),
+            "spp_per_s": spp / ms * 1000.0, "ms_per_frame": ms, "mrays_per_s": rays / ms / 1000.0,
+            "rays_per_frame": rays, "steps": steps, "graph": True}
+
+
+def cpu_render_baseline():
+    """The oracle integrator on all host threads, the same full frame."""
+    from gonzales_b200 import scenes
+    from oracle import pyoracle as O
+
+    hs = scenes.box_scene().build()
+    p = O.render_params(RENDER["width"], RENDER["height"], RENDER["spp"], max_depth=RENDER["max_depth"],
+                        rr_min_bounce=RENDER["rr_min_bounce"])
+    t0 = time.perf_counter()
+    O.render(hs, p)
+    el = time.perf_counter() - t0
+    return RENDER["width"] * RENDER["height"] * RENDER["spp"] / el
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -301,6 +356,8 @@ def run_ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
 
+    render = render_leg(acc_box=None, args=args, stream=stream, barrier=barrier) if not args.small else None
+
     if rank == 0:
         ms_per_step = elapsed_ms / args.steps
         value = world * n / (ms_per_step / 1000.0) / 1e6
@@ -334,8 +391,12 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "clocks": sampler.summary(),
         }
+        if render is not None:
+            line["render"] = render
         if world == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(hs, o, d, t)
+            if render is not None:
+                line["cpu_baseline"]["render_spp_per_s"] = cpu_render_baseline()
         print(json.dumps(line), flush=True)
     acc.close()
     if dist is not None:

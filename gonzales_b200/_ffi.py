@@ -69,6 +69,29 @@ class SceneInfo(C.Structure):
                 ("device_bytes", C.c_int64)]
 
 
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("rr_min_bounce", C.c_int32), ("mis_corrected", C.c_int32), ("seed", C.c_int64),
+                ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
+                ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
+                ("sampler_spp", C.c_int32), ("wave_paths", C.c_int32), ("use_graph", C.c_int32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("camera_rays", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("probe_rays", C.c_uint64), ("waves", C.c_uint64)]
+
+
+def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
+                  eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
+                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, wave_paths=0, use_graph=0):
+    """gzg_render_params with the reference's defaults (Gaussian filter radius 2,
+    sigma 0.5; Z-Sobol seed 1234; roulette from bounce 2)."""
+    return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
+                        (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
+                        first_sample, sampler_spp, wave_paths, use_graph)
+
+
 VP = C.c_void_p
 I64 = C.c_int64
 ST = C.c_int32
@@ -86,6 +109,12 @@ PROTOTYPES = {
     "gzg_trace_any_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),
     "gzg_scene_info_get": (ST, [VP, C.POINTER(SceneInfo)]),
+    "gzg_renderer_create": (ST, [VP, C.POINTER(RenderParams), C.POINTER(VP)]),
+    "gzg_renderer_destroy": (ST, [VP]),
+    "gzg_renderer_render": (ST, [VP, VP, VP, VP, VP]),
+    "gzg_renderer_stats": (ST, [VP, C.POINTER(RenderStats)]),
+    "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),
+    "gzg_zsobol_fill_device": (ST, [I64, C.c_int32, C.c_int32, I64, VP, VP, VP, I64, VP, C.c_int32, VP, VP]),
     "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),
     "gzg_host_triangle_bounds": (ST, [VP, VP, I64, VP]),
     "gzg_host_build_bvh2": (ST, [VP, I64, VP, C.POINTER(I64), VP, C.c_int32]),

@@ -117,3 +117,54 @@ class GpuAccelerator:
     def hits_to_intersections(self, hits_d, out_d, stream=None):
         F.check(F.lib().gzg_hits_to_intersections_device(self.handle, hits_d.data_ptr(), hits_d.shape[0],
                                                          out_d.data_ptr(), _stream_handle(stream)))
+
+    def render(self, params):
+        """Renders on the device (gzg_render_image); returns host film sums
+        (rgb (H, W, 3), squares (H, W, 3), weights (H, W)) and statistics."""
+        W, H = params.width, params.height
+        rgb = np.zeros((H, W, 3), np.float32)
+        sq = np.zeros((H, W, 3), np.float32)
+        w = np.zeros((H, W), np.float32)
+        stats = F.RenderStats()
+        F.check(F.lib().gzg_render_image(self.handle, C.byref(params), F.ptr(rgb), F.ptr(sq), F.ptr(w),
+                                         C.byref(stats)))
+        return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
+
+
+class Renderer:
+    """A wavefront renderer bound to one scene (gzg_renderer_*); renders into
+    caller-owned device films (torch CUDA tensors)."""
+
+    def __init__(self, accel, params):
+        self.accel = accel
+        self.params = params
+        h = C.c_void_p()
+        F.check(F.lib().gzg_renderer_create(accel.handle, C.byref(params), C.byref(h)))
+        self.handle = h
+
+    def render(self, film_rgb, film_w, film_sq=None, stream=None):
+        F.check(F.lib().gzg_renderer_render(self.handle, film_rgb.data_ptr(),
+                                            film_sq.data_ptr() if film_sq is not None else None,
+                                            film_w.data_ptr(), _stream_handle(stream)))
+
+    def stats(self):
+        s = F.RenderStats()
+        F.check(F.lib().gzg_renderer_stats(self.handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in F.RenderStats._fields_}
+
+    def close(self):
+        if self.handle:
+            F.check(F.lib().gzg_renderer_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -44,7 +44,8 @@ def build(force=False, verbose=False):
         if src.suffix == ".cu":
             cmd += CUDA_FLAGS
         else:
-            cmd += ["-x", "c++", "-Wno-deprecated-gpu-targets"]
+            cmd += ["-x", "c++", "-Wno-deprecated-gpu-targets",
+                    "-DGZG_SOBOL_PATH=" + str(PKG / "data" / "sobol_1024x52.bin")]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

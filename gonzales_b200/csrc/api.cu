@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -158,6 +159,7 @@ LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o) {
         p.blocks_per_sm = o ? o->blocks_per_sm : 0;
         p.wide_depth = s->info.wide_depth;
         p.counters = o ? reinterpret_cast<unsigned long long *>(o->fetch_counters) : nullptr;
+        p.n_dev = nullptr;
         return p;
 }
 
@@ -378,8 +380,61 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         info.wide_nodes = (int64_t)wide.nodes.size();
         info.wide_depth = wide.depth;
         info.bvh2_depth = bvh2_depth;
-        (void)materials;
-        (void)material_count;
+
+        // Shading data for the path integrator.  Materials: albedo + type,
+        // emission (Material_C, mojo_kernel.h:11-15).  Lights: one per
+        // area-light triangle prim, in light-index order (SceneDescription
+        // creates one AreaLight per triangle), power = average radiance x area
+        // x pi (AreaLight.swift:47-49), with the running power sum the power
+        // light sampler searches (PowerLightSampler.swift:20-38).
+        std::vector<float4_> mats((size_t)std::max<int64_t>(material_count, 0) * 2);
+        for (int64_t k = 0; k < material_count; ++k) {
+                const gzg_material &m = materials[k];
+                mats[2 * k] = float4_{m.albedo[0], m.albedo[1], m.albedo[2], (float)m.type};
+                mats[2 * k + 1] = float4_{m.emission[0], m.emission[1], m.emission[2], 0.0f};
+        }
+        std::vector<std::pair<int64_t, int64_t>> light_prims;
+        for (int64_t k = 0; k < prim_count; ++k) {
+                int64_t mesh, base;
+                if (prim_ids[k].type == 3 && prim_triangle(prim_ids[k], &mesh, &base)) light_prims.push_back({prim_ids[k].id1, k});
+        }
+        std::sort(light_prims.begin(), light_prims.end());
+        std::vector<float4_> lights;
+        std::vector<float> cdf;
+        float total = 0.0f, run = 0.0f;
+        for (size_t i = 0; i < light_prims.size(); ++i) {
+                const int64_t k = light_prims[i].second;
+                const float4_ a = pv0[k], b = pv1[k], c = pv2[k];
+                const float e1[3] = {b.x - a.x, b.y - a.y, b.z - a.z}, e2[3] = {c.x - a.x, c.y - a.y, c.z - a.z};
+                const float cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                            cz = e1[0] * e2[1] - e1[1] * e2[0];
+                const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
+                float le[3] = {0, 0, 0};
+                const int64_t mi = prim_ids[k].material_index;
+                if (mi >= 0 && mi < material_count)
+                        for (int j = 0; j < 3; ++j) le[j] = materials[mi].emission[j];
+                const float power = (le[0] + le[1] + le[2]) / 3.0f * area * 3.14159265358979323846f;
+                lights.push_back(float4_{a.x, a.y, a.z, area});
+                lights.push_back(float4_{b.x, b.y, b.z, power});
+                lights.push_back(float4_{c.x, c.y, c.z, 0.0f});
+                lights.push_back(float4_{le[0], le[1], le[2], 0.0f});
+                run = i == 0 ? power : run + power;
+                cdf.push_back(run);
+                total = total + power;
+        }
+        st = scene->upload(reinterpret_cast<const float4 *>(mats.data()), mats.size(), &f, "materials");
+        if (st != GZG_OK) return st;
+        d.materials = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(lights.data()), lights.size(), &f, "lights");
+        if (st != GZG_OK) return st;
+        d.lights = f;
+        const float *cdf_d;
+        st = scene->upload(cdf.data(), cdf.size(), &cdf_d, "light cdf");
+        if (st != GZG_OK) return st;
+        d.light_cdf = cdf_d;
+        d.material_count = (int32_t)material_count;
+        d.light_count = (int32_t)light_prims.size();
+        d.light_total_power = total;
         *out_scene = scene.release();
         return clear_error();
 }

@@ -27,7 +27,20 @@ struct DevScene {
         uint32_t wide_count;
         uint32_t *err;
         unsigned long long *counters;  // optional fetch counters (nodes, triangles, rays)
+        const uint32_t *n_dev;         // optional device-side ray count (overrides the launch's n)
+        // shading data (path integrator)
+        const float4 *materials;       // 2 x float4 per material: albedo + type, emission
+        const float4 *lights;          // 4 x float4 per area light: p0 + area, p1 + power, p2, emission
+        const float *light_cdf;        // running sum of light powers
+        int32_t material_count;
+        int32_t light_count;
+        float light_total_power;
 };
+
+// The launch's ray count: the device-side count when one is given.
+__device__ __forceinline__ int64_t ray_count(const DevScene &s, int64_t n) {
+        return s.n_dev ? (int64_t)*s.n_dev : n;
+}
 
 // Adds per-thread fetch counts into s.counters (one atomic per converged
 // group of lanes; __reduce_add_sync is exact for any active mask).

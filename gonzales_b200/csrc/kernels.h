@@ -15,6 +15,7 @@ struct LaunchParams {
         int block_size;
         int blocks_per_sm;
         unsigned long long *counters;  // optional fetch counters (device)
+        const uint32_t *n_dev;         // optional device-side ray count; n is then the capacity
 };
 
 // ray_fmt: RayFormat; out_fmt: OutFormat.  Asynchronous on `st`.

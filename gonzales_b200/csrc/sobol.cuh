@@ -1,0 +1,158 @@
+// sobol.cuh - Z-Sobol sampler on the device (Sources/libgonzales/Sampler/
+// ZSobolSampler.swift:6-280).  The integer path (Morton index, base-4 digit
+// permutation, matrix product, Owen scramble) is bit-exact with the
+// reference; the final value is (float)bits * 2^-32 clamped to 1 - 1e-6.
+#pragma once
+
+#include <stdint.h>
+
+namespace gzg {
+
+constexpr int kSobolDims = 1024;
+constexpr int kSobolColumns = 52;
+
+struct ZSobol {
+        uint64_t morton;  // (Morton(px, py) << log2spp) | sample index
+        int32_t dim;      // next dimension
+};
+
+struct ZSobolConfig {
+        const uint32_t *matrices;  // kSobolDims x kSobolColumns
+        uint64_t seed;             // sampler seed (1234, Sampler/Random.swift:66)
+        int32_t log2spp;
+        int32_t n_base4_digits;
+};
+
+__device__ __forceinline__ uint32_t zs_reverse_bits(uint32_t v) { return __brev(v); }
+
+// mixBits (ZSobolSampler.swift:90-101).
+__device__ __forceinline__ uint32_t zs_mix_bits(uint64_t v) {
+        uint32_t x = (uint32_t)(v & 0xFFFFFFFFull);
+        x ^= (uint32_t)(v >> 32);
+        x ^= x >> 16;
+        x *= 0x85ebca77u;
+        x ^= x >> 13;
+        x *= 0xc2b2ae35u;
+        x ^= x >> 16;
+        return x;
+}
+
+// FastOwenScrambler (ZSobolSampler.swift:43-67).
+__device__ __forceinline__ uint32_t zs_owen(uint32_t v, uint32_t seed) {
+        v = __brev(v);
+        v ^= v * 0x3d20adeau;
+        v += seed;
+        v *= (seed >> 16) | 1u;
+        v ^= v * 0x05526c56u;
+        v ^= v * 0x53a22864u;
+        return __brev(v);
+}
+
+// encodeMorton2 (ZSobolSampler.swift:70-88).
+__device__ __forceinline__ uint64_t zs_morton2(uint32_t x, uint32_t y) {
+        uint64_t a = x, b = y;
+        a = (a | (a << 16)) & 0x0000FFFF0000FFFFull;
+        a = (a | (a << 8)) & 0x00FF00FF00FF00FFull;
+        a = (a | (a << 4)) & 0x0F0F0F0F0F0F0F0Full;
+        a = (a | (a << 2)) & 0x3333333333333333ull;
+        a = (a | (a << 1)) & 0x5555555555555555ull;
+        b = (b | (b << 16)) & 0x0000FFFF0000FFFFull;
+        b = (b | (b << 8)) & 0x00FF00FF00FF00FFull;
+        b = (b | (b << 4)) & 0x0F0F0F0F0F0F0F0Full;
+        b = (b | (b << 2)) & 0x3333333333333333ull;
+        b = (b | (b << 1)) & 0x5555555555555555ull;
+        return a | (b << 1);
+}
+
+__device__ __forceinline__ uint64_t zs_shr(uint64_t v, int s) { return s >= 64 ? 0ull : (v >> s); }
+
+// getSampleIndex (ZSobolSampler.swift:138-166); the 24 permutations of
+// ZSobolSampler.swift:105-112 packed two bits per entry.
+__device__ __forceinline__ uint64_t zs_sample_index(const ZSobolConfig &c, const ZSobol &s) {
+        // perm[p][d] = (kPermPacked[p] >> (2 * d)) & 3
+        const uint8_t kPermPacked[24] = {0xE4, 0xB4, 0xD8, 0x78, 0x6C, 0x9C, 0xE1, 0xB1, 0xC9, 0x39, 0x2D, 0x8D,
+                                         0xC6, 0x36, 0xD2, 0x72, 0x4E, 0x1E, 0x27, 0x87, 0x1B, 0x4B, 0x63, 0x93};
+        uint64_t idx = 0;
+        const bool pow2 = (c.log2spp & 1) == 1;
+        const int last = pow2 ? 1 : 0;
+        const uint64_t dmul = 0x55555555ull * (uint64_t)(int64_t)s.dim;
+        for (int di = c.n_base4_digits - 1; di >= last; --di) {
+                const int shift = 2 * di - (pow2 ? 1 : 0);
+                const int digit = (int)(zs_shr(s.morton, shift) & 3u);
+                const uint64_t higher = zs_shr(s.morton, shift + 2);
+                const uint32_t h = zs_mix_bits(higher ^ dmul);
+                const int p = (int)((h >> 24) % 24u);
+                const int pd = (kPermPacked[p] >> (2 * digit)) & 3;
+                idx |= (uint64_t)pd << shift;
+        }
+        if (pow2) {
+                int digit = (int)(s.morton & 1u);
+                const uint32_t h = zs_mix_bits((s.morton >> 1) ^ dmul);
+                digit ^= (int)(h & 1u);
+                idx |= (uint64_t)digit;
+        }
+        return idx;
+}
+
+// sobolSample (ZSobolSampler.swift:6-31): XOR of the matrix columns of the set
+// index bits, scrambled, times 2^-32, clamped below 1.
+__device__ __forceinline__ float zs_sobol_sample(const ZSobolConfig &c, uint64_t index, int dim, uint32_t scramble) {
+        const uint32_t *m = c.matrices + (size_t)dim * kSobolColumns;
+        uint32_t acc = 0;
+        uint64_t cur = index;
+        while (cur != 0) {
+                const int bit = __ffsll((long long)cur) - 1;
+                if (bit >= kSobolColumns) break;
+                acc ^= __ldg(m + bit);
+                cur &= cur - 1;
+        }
+        const uint32_t r = zs_owen(acc, scramble);
+        const float f = __fmul_rn(__uint2float_rn(r), 2.32830643653869628906e-10f);
+        const float one_minus_eps = 1.0f - 1e-6f;
+        return one_minus_eps < f ? one_minus_eps : f;
+}
+
+// getSampleHash (ZSobolSampler.swift:188-199); the second hash is 0 because
+// mixBits returns 32 bits.
+__device__ __forceinline__ uint32_t zs_hash(const ZSobolConfig &c, int dim) {
+        return zs_mix_bits((uint64_t)(int64_t)dim ^ c.seed);
+}
+
+// startPixelSample (ZSobolSampler.swift:130-136).
+__device__ __forceinline__ void zs_start(const ZSobolConfig &c, ZSobol &s, uint32_t px, uint32_t py, uint32_t index) {
+        s.dim = 0;
+        s.morton = (zs_morton2(px, py) << c.log2spp) | (uint64_t)index;
+}
+
+// get1D (ZSobolSampler.swift:203-219).
+__device__ __forceinline__ float zs_get1d(const ZSobolConfig &c, ZSobol &s) {
+        const uint64_t idx = zs_sample_index(c, s);
+        const uint32_t h = zs_hash(c, s.dim);
+        if (s.dim >= kSobolDims) s.dim = 2;
+        s.dim += 1;
+        return zs_sobol_sample(c, idx, s.dim - 1, h);
+}
+
+// get2D (ZSobolSampler.swift:221-244).
+__device__ __forceinline__ void zs_get2d(const ZSobolConfig &c, ZSobol &s, float &a, float &b) {
+        const uint64_t idx = zs_sample_index(c, s);
+        const uint32_t h0 = zs_hash(c, s.dim);
+        if (s.dim + 1 >= kSobolDims) s.dim = 2;
+        s.dim += 2;
+        a = zs_sobol_sample(c, idx, s.dim - 2, h0);
+        b = zs_sobol_sample(c, idx, s.dim - 1, 0u);
+}
+
+// get3D (ZSobolSampler.swift:249-280).
+__device__ __forceinline__ void zs_get3d(const ZSobolConfig &c, ZSobol &s, float &a, float &b, float &d) {
+        const uint64_t idx = zs_sample_index(c, s);
+        const uint32_t h0 = zs_hash(c, s.dim);
+        const uint32_t h2 = zs_hash(c, s.dim + 2);
+        if (s.dim + 2 >= kSobolDims) s.dim = 2;
+        s.dim += 3;
+        a = zs_sobol_sample(c, idx, s.dim - 3, h0);
+        b = zs_sobol_sample(c, idx, s.dim - 2, 0u);
+        d = zs_sobol_sample(c, idx, s.dim - 1, h2);
+}
+
+}  // namespace gzg

@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict
                                               int64_t n, void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
         const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        n = ray_count(s, n);
         if (i >= n) return;
         const RayIn in = load_ray<RAYFMT>(rays, tmaxs, i);
         WideRay r;
@@ -203,6 +204,7 @@ __global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void 
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
         const unsigned FULL = 0xFFFFFFFFu;
+        n = ray_count(s, n);
         const unsigned lane = threadIdx.x & 31u;
         const unsigned lt_mask = (1u << lane) - 1u;
         const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -364,6 +366,7 @@ template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
 __global__ void __launch_bounds__(128) k_bvh2(DevScene s, const void *__restrict__ rays, const float *__restrict__ tmaxs,
                                               int64_t n, void *__restrict__ out) {
         const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        n = ray_count(s, n);
         if (i >= n) return;
         const RayIn in = load_ray<RAYFMT>(rays, tmaxs, i);
         const float rd[3] = {__fdiv_rn(1.0f, in.dx), __fdiv_rn(1.0f, in.dy), __fdiv_rn(1.0f, in.dz)};
@@ -539,6 +542,7 @@ cudaError_t launch_trace(const DevScene &scene, const LaunchParams &p, int ray_f
         if (n <= 0) return cudaSuccess;
         DevScene s = scene;
         s.counters = p.counters;
+        s.n_dev = p.n_dev;
         if (ray_fmt == kRayDevice) {
                 switch (out_fmt) {
                 case kOutHit: return launch_fmt<kRayDevice, kOutHit, false>(s, p, rays, tmax, n, out, st);

@@ -207,6 +207,8 @@ def box_scene(seed=0xB0):
         ang = rng.uniform(0, math.pi / 2)
         bp, bt = _box(size, ang, (cx, size / 2.0 + 1e-4, cz))
         sb.add_mesh(bp, bt, sb.add_material(rng.uniform(0.1, 0.8, 3)))
-    lp, lt = _quad((0.35, 0.999, 0.35), (0.35, 0.999, 0.65), (0.65, 0.999, 0.65), (0.65, 0.999, 0.35))
+    # wound so cross(p1 - p0, p2 - p0) points down (-y): area lights emit on
+    # the side their geometric normal faces
+    lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
     sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
     return sb

@@ -267,6 +267,67 @@ GZG_API gzg_status gzg_hits_to_intersections_device(gzg_scene *scene, const gzg_
                                                     int64_t count, gzg_intersection *out,
                                                     void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Path integrator (wavefront)                                                */
+/* ------------------------------------------------------------------------- */
+
+/* Parameters of a render.  The integrator is Gonzales' MIS path integrator
+ * (Integrator/VolumePathIntegrator.swift:67-463) with every random dimension
+ * drawn from the Z-Sobol sampler, restructured as a wavefront: generate ->
+ * extend -> shade -> shadow (any hit) [-> BSDF probe] -> accumulate. */
+typedef struct gzg_render_params {
+        int32_t width, height, spp, max_depth;
+        int32_t rr_min_bounce;   /* Russian roulette from this bounce (reference: 2, "bounce > 1") */
+        int32_t mis_corrected;   /* 0: MIS as written (the BSDF strategy gets weight 0 because its
+                                    light density is queried with tHit = 0, Core/Sampleable.swift:55);
+                                    1: corrected MIS */
+        int64_t seed;            /* Z-Sobol seed (reference: 1234, Sampler/Random.swift:66) */
+        float eye[3], target[3], up[3];
+        float fov_deg;           /* full field of view of the shorter image side */
+        float filter_radius, filter_sigma; /* Gaussian pixel filter (reference default 2, 0.5) */
+        int32_t first_sample;    /* render sample indices [first_sample, first_sample + spp) */
+        int32_t sampler_spp;     /* ...of a Z-Sobol sampler with this many samples per pixel (0: spp) */
+        int32_t wave_paths;      /* paths in flight per wave (0: library default) */
+        int32_t use_graph;       /* capture one wave as a CUDA graph and replay it */
+} gzg_render_params;
+
+typedef struct gzg_renderer gzg_renderer;
+
+/* Render statistics (cumulative over the renderer's lifetime). */
+typedef struct gzg_render_stats {
+        uint64_t camera_rays, extension_rays, shadow_rays, probe_rays;
+        uint64_t waves;
+} gzg_render_stats;
+
+/* Creates a renderer (device buffers for one wave) for a scene uploaded with
+ * materials.  Replaces the Tile.render bounce loop (Core/Tile.swift:19-223). */
+GZG_API gzg_status gzg_renderer_create(gzg_scene *scene, const gzg_render_params *params,
+                                       gzg_renderer **out);
+GZG_API gzg_status gzg_renderer_destroy(gzg_renderer *renderer);
+
+/* Adds one render pass to DEVICE film buffers (caller-owned, row-major):
+ * film_rgb[3*W*H] += sample radiance, film_sq[3*W*H] += its square (may be
+ * NULL), film_w[W*H] += sample weight.  The image is film_rgb / film_w (the
+ * reference's Pixel.normalized, Core/Pixel.swift:12-16).  Asynchronous on
+ * `stream`. */
+GZG_API gzg_status gzg_renderer_render(gzg_renderer *renderer, float *film_rgb, float *film_sq, float *film_w,
+                                       void *stream);
+
+GZG_API gzg_status gzg_renderer_stats(const gzg_renderer *renderer, gzg_render_stats *stats);
+
+/* Device Z-Sobol values (Sampler/ZSobolSampler.swift:6-280): for each of n
+ * pixel samples (device arrays px, py, index) the values of the get1D / get2D /
+ * get3D calls listed in the HOST array kinds (1, 2 or 3 each, at most 64),
+ * starting at dimension 0, written row by row to the DEVICE array out.
+ * The sampler is ZSobolSampler(samplesPerPixel:fullResolution:seed:). */
+GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res_x, int32_t res_y, int64_t seed,
+                                          const int32_t *px, const int32_t *py, const int64_t *index, int64_t n,
+                                          const int32_t *kinds, int32_t nkinds, float *out, void *stream);
+
+/* Convenience: renders into HOST films (overwritten); synchronous. */
+GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *params, float *film_rgb,
+                                    float *film_sq, float *film_w, gzg_render_stats *stats);
+
 /* Scene statistics. */
 GZG_API gzg_status gzg_scene_info_get(const gzg_scene *scene, gzg_scene_info *info);
 

@@ -1,0 +1,533 @@
+// integrator.cpp - CPU restatement of Gonzales' MIS path integrator (test
+// infrastructure: checker and CPU baseline).  Compiled with -ffp-contract=off.
+//
+// Restated from (paths relative to Sources/libgonzales):
+//   bounce loop / shade       Integrator/VolumePathIntegrator.swift:325-463
+//   MIS, light + BSDF sample  Integrator/VolumePathIntegrator.swift:67-266
+//   Russian roulette          Integrator/VolumePathIntegrator.swift:269-283
+//   power heuristic           Sampler/Sampling.swift:27-30
+//   concentric disk / cosine  Sampler/Sampling.swift:3-25
+//   light choice              Light/PowerLightSampler.swift:1-48
+//   area light                Light/AreaLight.swift:13-49
+//   triangle sample / area    Shape/Triangle.swift:517-544; Core/Sampleable.swift:33-68
+//   hit interaction / frame   Shape/Triangle.swift:363-474; Geometry/Geometry.swift:64-77;
+//                             Reflection/BsdfFrame.swift:13-21; Core/ShadingFrame.swift
+//   diffuse BSDF              Bsdf/DiffuseBsdf.swift; Reflection/Bsdf.swift:20-52;
+//                             Reflection/FramedBsdf.swift:16-83; Reflection/BsdfSample.swift:13-15
+//   spawn / offsets           Core/Interaction.swift:15-54; Utility/Utility.swift:4
+//   camera sample, weight     Core/Tile.swift:27-59; Sampler/Sampler.swift:69-82
+//   Gaussian filter           Filter/GaussianFilter.swift:8-130
+//   film sums                 Core/Film.swift:107-119; Core/Pixel.swift
+//
+// Decisions where the reference has no executing code (its MIS loop has no
+// callers): every random dimension comes from the path's Z-Sobol sampler, in
+// the order the Swift code draws them (camera 2D + lens 2D, then per bounce:
+// light choice 1D, light point 2D, MIS BSDF sample 3D, continuation 3D,
+// roulette 1D when it applies).  mis_corrected = 0 keeps the reference's
+// arithmetic as written: the BSDF strategy's light density is queried with
+// tHit = 0 (Core/Sampleable.swift:55-58), which rejects every hit, so that
+// strategy's weight is 0; mis_corrected = 1 queries with tHit = infinity and
+// evaluates the probe's emission toward the surface.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+#include "oracle.h"
+
+namespace {
+
+const float kPi = 3.14159265358979323846f;
+const float kInfF = std::numeric_limits<float>::infinity();
+
+struct V3 {
+        float x, y, z;
+};
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 mul(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline V3 mulv(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V3 neg(V3 a) { return v3(-a.x, -a.y, -a.z); }
+inline float dot(V3 a, V3 b) {
+        float s = a.x * b.x;
+        s = s + a.y * b.y;
+        return s + a.z * b.z;
+}
+inline V3 cross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline float length_sq(V3 a) { return dot(a, a); }
+inline V3 normalize(V3 a) {
+        float l = std::sqrt(dot(a, a));
+        return v3(a.x / l, a.y / l, a.z / l);
+}
+inline float max_value(V3 a) { return std::max(a.x, std::max(a.y, a.z)); }
+inline bool is_black(V3 a) { return a.x == 0.0f && a.y == 0.0f && a.z == 0.0f; }
+
+// powerHeuristic (Sampler/Sampling.swift:27-30).
+inline float power_heuristic(float f, float g) {
+        if (f == 0.0f || g == 0.0f) return 0.0f;
+        return (f * f) / (f * f + g * g);
+}
+
+// concentricSampleDisk / cosineSampleHemisphere (Sampler/Sampling.swift:3-25).
+V3 cosine_hemisphere(float u0, float u1) {
+        float ox = 2.0f * u0 - 1.0f, oy = 2.0f * u1 - 1.0f;
+        float dx = 0.0f, dy = 0.0f;
+        if (!(ox == 0.0f && oy == 0.0f)) {
+                float theta, r;
+                if (std::fabs(ox) > std::fabs(oy)) {
+                        r = ox;
+                        theta = (kPi / 4.0f) * (oy / ox);
+                } else {
+                        r = oy;
+                        theta = (kPi / 2.0f) - (kPi / 4.0f) * (ox / oy);
+                }
+                dx = r * std::cos(theta);
+                dy = r * std::sin(theta);
+        }
+        float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
+        return v3(dx, dy, z);
+}
+
+// makeCoordinateSystem (Geometry/Geometry.swift:64-77).
+void coordinate_system(V3 v1, V3 *v2, V3 *v3o) {
+        if (std::fabs(v1.x) > std::fabs(v1.y)) {
+                float l = std::sqrt(v1.x * v1.x + v1.z * v1.z);
+                *v2 = v3(-v1.z / l, 0.0f, v1.x / l);
+        } else {
+                float l = std::sqrt(v1.y * v1.y + v1.z * v1.z);
+                *v2 = v3(0.0f, v1.z / l, -v1.y / l);
+        }
+        *v3o = cross(v1, *v2);
+}
+
+// Shading frame of a hit without UVs or vertex normals (Triangle.swift:395-452
+// with degenerate UVs; BsdfFrame.swift:13-21; ShadingFrame(y:z:)).
+struct Frame {
+        V3 x, y, z;
+        V3 to_local(V3 v) const { return v3(dot(v, x), dot(v, y), dot(v, z)); }
+        V3 to_world(V3 v) const { return add(add(mul(x, v.x), mul(y, v.y)), mul(z, v.z)); }
+};
+
+bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame *f) {
+        V3 gn = cross(sub(p2, p0), sub(p1, p0));
+        if (length_sq(gn) == 0.0f) return false;
+        V3 dpdu, dpdv;
+        coordinate_system(normalize(gn), &dpdu, &dpdv);
+        V3 s = normalize(dpdu);
+        V3 t = cross(s, ns);
+        if (length_sq(t) > 0.0f) {
+                t = normalize(t);
+                s = cross(t, ns);
+        } else {
+                coordinate_system(ns, &s, &t);
+        }
+        f->y = normalize(s);
+        f->z = ns;
+        f->x = cross(f->y, f->z);
+        return true;
+}
+
+// erfinv of GaussianFilter.swift:27-91.
+float erfinv(float y) {
+        const float center = 0.7f;
+        const float a[4] = {0.886226899f, -1.645349621f, 0.914624893f, -0.140543331f};
+        const float b[4] = {-2.118377725f, 1.442710462f, -0.329097515f, 0.012229801f};
+        const float c[4] = {-1.970840454f, -1.624906493f, 3.429567803f, 1.641345311f};
+        const float d[2] = {3.543889200f, 1.637067800f};
+        const float ay = std::fabs(y);
+        const float two_over_sqrt_pi = 2.0f / std::sqrt(kPi);
+        float x;
+        if (ay <= center) {
+                float z = y * y;
+                float num = a[3] * z + a[2];
+                num = num * z + a[1];
+                num = num * z + a[0];
+                float den = b[3] * z + b[2];
+                den = den * z + b[1];
+                den = den * z + b[0];
+                den = den * z + 1.0f;
+                x = y * num / den;
+        } else if (ay < 1.0f) {
+                float z = std::sqrt(-std::log((1.0f - ay) / 2.0f));
+                float num = c[3] * z + c[2];
+                num = num * z + c[1];
+                num = num * z + c[0];
+                float den = d[1] * z + d[0];
+                den = den * z + 1.0f;
+                float sign = std::signbit(y) ? -1.0f : 1.0f;
+                x = sign * num / den;
+        } else if (ay == 1.0f) {
+                return std::signbit(y) ? -kInfF : kInfF;
+        } else {
+                return std::numeric_limits<float>::quiet_NaN();
+        }
+        x -= (std::erf(x) - y) / (two_over_sqrt_pi * std::exp(-(x * x)));
+        x -= (std::erf(x) - y) / (two_over_sqrt_pi * std::exp(-(x * x)));
+        return x;
+}
+
+// GaussianFilter.sample's sample1D (GaussianFilter.swift:95-111).
+void gaussian_sample_1d(float u, float radius, float sigma, float *x_out, float *density) {
+        float norm = 0.5f * (1.0f + std::erf(radius / (sigma * std::sqrt(2.0f))));
+        float us = (1.0f - norm) + u * (2.0f * norm - 1.0f);
+        float x = sigma * std::sqrt(2.0f) * erfinv(2.0f * us - 1.0f);
+        float pdf = std::exp(-x * x / (2.0f * sigma * sigma)) / (sigma * std::sqrt(2.0f * kPi));
+        *density = pdf / (2.0f * norm - 1.0f);
+        *x_out = std::max(-radius, std::min(radius, x));
+}
+
+// GaussianFilter.gaussian / evaluate (GaussianFilter.swift:15-25).
+float gaussian(float x, float sigma) {
+        return 1.0f / std::sqrt(2.0f * kPi * sigma * sigma) * std::exp(-(x * x) / (2.0f * sigma * sigma));
+}
+
+struct Light {
+        V3 p0, p1, p2;
+        V3 le;
+        float area;
+        float power;
+};
+
+struct Scene {
+        const orc_node *nodes;
+        const orc_prim_id *prims;
+        const orc_mesh *meshes;
+        const orc_material *materials;
+        int64_t n_materials;
+        std::vector<Light> lights;
+        std::vector<float> cumulative;
+        float total_power = 0.0f;
+        const orc_render_params *p;
+};
+
+bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
+        const orc_prim_id &pr = sc.prims[k];
+        int64_t mesh, base;
+        if (pr.type == 0) {
+                mesh = pr.id1;
+                base = pr.id2;
+        } else if (pr.type >= 1 && pr.type <= 3 && pr.id2 != -1) {
+                mesh = pr.id2 >> 32;
+                base = (pr.id2 & 0xFFFFFFFFll) * 3;
+        } else {
+                return false;
+        }
+        const orc_mesh &m = sc.meshes[mesh];
+        const float *a = m.points + 4 * m.vertex_indices[base];
+        const float *b = m.points + 4 * m.vertex_indices[base + 1];
+        const float *c = m.points + 4 * m.vertex_indices[base + 2];
+        *p0 = v3(a[0], a[1], a[2]);
+        *p1 = v3(b[0], b[1], b[2]);
+        *p2 = v3(c[0], c[1], c[2]);
+        return true;
+}
+
+struct Hit {
+        bool hit;
+        int32_t prim;
+        float t, u, v;
+};
+
+Hit trace(const Scene &sc, V3 o, V3 d, float tmax) {
+        orc_ray r{o.x, o.y, o.z, d.x, d.y, d.z};
+        orc_isect is;
+        int32_t idx;
+        orc_trace_one(sc.nodes, sc.prims, sc.meshes, &r, tmax, &is, &idx);
+        return Hit{is.hit != 0, idx, is.t, is.u, is.v};
+}
+
+// offsetRayOrigin(point:normal:direction:) (Core/Interaction.swift:26-35).
+V3 offset_origin(V3 p, V3 n, V3 dir) {
+        V3 off = mul(n, 0.0001f);
+        return dot(dir, n) > 0.0f ? add(p, off) : add(p, neg(off));
+}
+
+// PowerLightSampler.chooseLight with the lowerBound search of
+// PowerLightSampler.swift:4-18.
+int choose_light(const Scene &sc, float u, float *pdf) {
+        const float key = u * sc.total_power;
+        int lo = 0, hi = (int)sc.cumulative.size();
+        while (lo < hi) {
+                int mid = lo + (hi - lo) / 2;
+                if (sc.cumulative[mid] == key) {
+                        lo = mid;
+                        break;
+                } else if (sc.cumulative[mid] < key) {
+                        lo = mid + 1;
+                } else {
+                        hi = mid;
+                }
+        }
+        if (lo >= (int)sc.lights.size()) lo = (int)sc.lights.size() - 1;
+        *pdf = sc.lights[lo].power / sc.total_power;
+        return lo;
+}
+
+// Watertight triangle intersection used by Triangle.intersect for the
+// corrected MIS light density.
+bool hit_light(const Light &l, V3 o, V3 d, float *t) {
+        float th = kInfF, b0, b1, b2;
+        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        const float a[3] = {l.p0.x, l.p0.y, l.p0.z}, b[3] = {l.p1.x, l.p1.y, l.p1.z}, c[3] = {l.p2.x, l.p2.y, l.p2.z};
+        if (!orc_intersect_triangle_watertight(oo, dd, a, b, c, &th, &b0, &b1, &b2)) return false;
+        *t = th;
+        return true;
+}
+
+struct PathResult {
+        V3 L;
+        uint64_t ext = 0, shadow = 0, probe = 0;
+};
+
+// One path: VolumePathIntegrator.bounces (:448-463) with shadeBounce (:373-430)
+// and surfaceEstimate (:325-371).
+PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
+        const orc_render_params &P = *sc.p;
+        PathResult res;
+        V3 L = v3(0, 0, 0), thr = v3(1, 1, 1);
+        for (int bounce = 0; bounce <= P.max_depth; ++bounce) {
+                Hit h = trace(sc, o, d, kInfF);
+                ++res.ext;
+                if (!h.hit) break;  // no environment light in these scenes
+                if (is_black(thr)) break;
+                if (bounce >= P.max_depth) break;
+                V3 p0, p1, p2;
+                prim_tri(sc, h.prim, &p0, &p1, &p2);
+                const float b0 = (1.0f - h.u) - h.v;
+                const V3 pos = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
+                const V3 ng = normalize(cross(sub(p0, p2), sub(p1, p2)));
+                const V3 wo = normalize(neg(d));
+                const orc_prim_id &pr = sc.prims[h.prim];
+                const bool is_light = pr.type == 3;
+                if (bounce == 0 && is_light) {
+                        const orc_material &lm = sc.materials[pr.material_index];
+                        if (dot(ng, wo) > 0.0f) L = add(L, mulv(thr, v3(lm.emission[0], lm.emission[1], lm.emission[2])));
+                }
+                // Area lights have materialIndex 0 in their interaction
+                // (Core/SurfaceInteraction.swift:20).
+                const orc_material &mat = sc.materials[is_light ? 0 : pr.material_index];
+                const V3 refl = v3(mat.albedo[0], mat.albedo[1], mat.albedo[2]);
+                const V3 f_val = mul(refl, 1.0f / kPi);
+                Frame fr;
+                if (!make_frame(p0, p1, p2, ng, &fr)) break;
+                const V3 wo_l = fr.to_local(wo);
+
+                // ---- sampleOneLight -> estimateDirect -> sampleMultipleImportance
+                float choose_pdf;
+                const int li = choose_light(sc, orc_zsobol_get1d(smp), &choose_pdf);
+                const Light &lt = sc.lights[li];
+                float u2[2];
+                orc_zsobol_get2d(smp, u2);
+                V3 light_est = v3(0, 0, 0);
+                V3 light_dir = v3(0, 0, 0);
+                float light_pdf = 0.0f;
+                {
+                        const float su0 = std::sqrt(u2[0]);
+                        const float lb0 = 1.0f - su0, lb1 = u2[1] * su0;
+                        const V3 lp = add(add(mul(lt.p0, lb0), mul(lt.p1, lb1)), mul(lt.p2, (1.0f - lb0) - lb1));
+                        const V3 ln = normalize(cross(sub(lt.p1, lt.p0), sub(lt.p2, lt.p0)));
+                        float pdf = 1.0f / lt.area;
+                        const V3 inc = normalize(sub(lp, pos));
+                        const V3 dl = sub(pos, lp);
+                        const float d2 = dot(dl, dl);
+                        const float angle = std::fabs(dot(ln, neg(inc)));
+                        pdf = pdf * (d2 / angle);
+                        const V3 dir = inc;
+                        const bool lit = dot(ln, neg(dir)) > 0.0f;
+                        if (lit && !std::isinf(pdf)) {
+                                // Visibility.occluded: spawnRay(from:target:) (Interaction.swift:15-24)
+                                const V3 so = add(pos, mul(sub(lp, pos), 0.0001f));
+                                const V3 sd = sub(lp, so);
+                                Hit sh = trace(sc, so, sd, 1.0f - 0.00001f);
+                                ++res.shadow;
+                                if (!sh.hit) {
+                                        const bool reflect = dot(dir, ng) * dot(wo, ng) > 0.0f;
+                                        const V3 f = reflect ? f_val : v3(0, 0, 0);
+                                        const V3 scatter = mul(f, std::fabs(dot(dir, ng)));
+                                        light_est = mulv(scatter, lt.le);
+                                        light_dir = dir;
+                                        light_pdf = pdf;
+                                }
+                        }
+                }
+                // brdfDensity: probabilityDensityWorldSpace (FramedBsdf.swift:36-43)
+                float brdf_density = 0.0f;
+                {
+                        const V3 wi_l = fr.to_local(light_dir);
+                        if (wo_l.z != 0.0f && wo_l.z * wi_l.z > 0.0f) brdf_density = std::fabs(wi_l.z) / kPi;
+                }
+                const float light_w = power_heuristic(light_pdf, brdf_density);
+                V3 contrib = light_pdf == 0.0f ? v3(0, 0, 0) : mul(mul(light_est, light_w), 1.0f / light_pdf);
+
+                // sampleDistributionFunction (VolumePathIntegrator.swift:91-133)
+                float u3[3];
+                orc_zsobol_get3d(smp, u3);
+                {
+                        V3 wi_l = cosine_hemisphere(u3[0], u3[1]);
+                        if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
+                        const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? std::fabs(wi_l.z) / kPi : 0.0f;
+                        const V3 wi = fr.to_world(wi_l);
+                        V3 est = mul(f_val, std::fabs(dot(wi, ng)));
+                        if (P.mis_corrected && !is_black(est) && pdf_b > 0.0f) {
+                                const V3 po = offset_origin(pos, ng, wi);
+                                Hit ph = trace(sc, po, wi, kInfF);
+                                ++res.probe;
+                                V3 radiance = v3(0, 0, 0);
+                                if (ph.hit && sc.prims[ph.prim].type == 3) {
+                                        V3 q0, q1, q2;
+                                        prim_tri(sc, ph.prim, &q0, &q1, &q2);
+                                        const V3 qn = normalize(cross(sub(q0, q2), sub(q1, q2)));
+                                        const orc_material &lm = sc.materials[sc.prims[ph.prim].material_index];
+                                        if (dot(qn, neg(wi)) > 0.0f)
+                                                radiance = v3(lm.emission[0], lm.emission[1], lm.emission[2]);
+                                }
+                                est = mulv(est, radiance);
+                                float light_density = 0.0f;
+                                float tl;
+                                if (hit_light(lt, po, wi, &tl)) {
+                                        const V3 hp = add(po, mul(wi, tl));
+                                        const V3 dq = sub(pos, hp);
+                                        const float dd2 = dot(dq, dq);
+                                        const V3 lnn = normalize(cross(sub(lt.p0, lt.p2), sub(lt.p1, lt.p2)));
+                                        const float ang = std::fabs(dot(lnn, neg(wi)));
+                                        const float dens = dd2 / (ang * lt.area);
+                                        light_density = std::isinf(dens) ? 0.0f : dens;
+                                }
+                                const float bw = power_heuristic(pdf_b, light_density);
+                                contrib = add(contrib, mul(mul(est, bw), 1.0f / pdf_b));
+                        }
+                }
+                L = add(L, mulv(thr, mul(contrib, 1.0f / choose_pdf)));
+
+                // continuation: bsdf.sampleWorldSpace(outgoing:uSample: get3D)
+                orc_zsobol_get3d(smp, u3);
+                V3 wi_l = cosine_hemisphere(u3[0], u3[1]);
+                if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
+                const float pdf_c = (wo_l.z * wi_l.z > 0.0f) ? std::fabs(wi_l.z) / kPi : 0.0f;
+                if (pdf_c == 0.0f || std::isnan(pdf_c)) break;
+                const V3 wi = fr.to_world(wi_l);
+                thr = mulv(thr, mul(f_val, std::fabs(dot(wi, ng)) / pdf_c));
+                o = offset_origin(pos, ng, wi);
+                d = wi;
+                // stopWithRussianRoulette (:269-283), roulette value from Z-Sobol
+                const float mv = max_value(thr);
+                if (mv < 1.0f && bounce >= P.rr_min_bounce) {
+                        const float q = std::max(0.0f, 1.0f - mv);
+                        if (orc_zsobol_get1d(smp) < q) break;
+                        thr = mul(thr, 1.0f / (1.0f - q));
+                }
+        }
+        res.L = L;
+        return res;
+}
+
+}  // namespace
+
+extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                           const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                           const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
+                           uint64_t *counters, int threads) {
+        Scene sc;
+        sc.nodes = nodes;
+        sc.prims = prims;
+        sc.meshes = meshes;
+        sc.materials = materials;
+        sc.n_materials = n_materials;
+        sc.p = params;
+        // Lights: area-light prims in light-index order (SceneDescription.worldEnd
+        // appends one AreaLight per triangle; PowerLightSampler.init).
+        std::vector<std::pair<int64_t, int64_t>> order;
+        for (int64_t k = 0; k < n_prims; ++k)
+                if (prims[k].type == 3) order.push_back({prims[k].id1, k});
+        std::sort(order.begin(), order.end());
+        for (auto &e : order) {
+                Light l;
+                prim_tri(sc, e.second, &l.p0, &l.p1, &l.p2);
+                const orc_material &m = materials[prims[e.second].material_index];
+                l.le = v3(m.emission[0], m.emission[1], m.emission[2]);
+                l.area = 0.5f * std::sqrt(length_sq(cross(sub(l.p1, l.p0), sub(l.p2, l.p0))));
+                const float avg = (l.le.x + l.le.y + l.le.z) / 3.0f;
+                l.power = avg * l.area * kPi;
+                sc.lights.push_back(l);
+        }
+        float run = 0.0f;
+        for (size_t i = 0; i < sc.lights.size(); ++i) {
+                run = i == 0 ? sc.lights[0].power : run + sc.lights[i].power;
+                sc.cumulative.push_back(run);
+        }
+        sc.total_power = 0.0f;
+        for (const Light &l : sc.lights) sc.total_power = sc.total_power + l.power;
+
+        const orc_render_params &P = *params;
+        const int W = P.width, H = P.height;
+        const int sampler_spp = P.sampler_spp > 0 ? P.sampler_spp : P.spp;
+        // camera basis (right-handed: +x right, +y up in the image)
+        const V3 eye = v3(P.eye[0], P.eye[1], P.eye[2]);
+        const V3 fwd = normalize(sub(v3(P.target[0], P.target[1], P.target[2]), eye));
+        const V3 right = normalize(cross(fwd, v3(P.up[0], P.up[1], P.up[2])));
+        const V3 upv = cross(right, fwd);
+        const float tan_half = std::tan(P.fov_deg * kPi / 180.0f / 2.0f);
+        const float aspect = (float)W / (float)H;
+        const float sx0 = aspect > 1.0f ? -aspect : -1.0f, sx1 = -sx0;
+        const float sy0 = aspect > 1.0f ? -1.0f : -1.0f / aspect, sy1 = -sy0;
+        if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+        std::atomic<int> next_row{0};
+        std::vector<uint64_t> cnt(4 * threads, 0);
+        std::vector<std::thread> pool;
+        for (int ti = 0; ti < threads; ++ti)
+                pool.emplace_back([&, ti]() {
+                        for (;;) {
+                                const int py = next_row.fetch_add(1);
+                                if (py >= H) break;
+                                for (int px = 0; px < W; ++px) {
+                                        float acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0}, accw = 0.0f;
+                                        for (int si = 0; si < P.spp; ++si) {
+                                                orc_zsobol smp;
+                                                orc_zsobol_init(&smp, sampler_spp, W, H, P.seed);
+                                                orc_zsobol_start_pixel_sample(&smp, px, py, P.first_sample + si, 0);
+                                                float u2[2];
+                                                orc_zsobol_get2d(&smp, u2);
+                                                float dx, dy, denx, deny;
+                                                gaussian_sample_1d(u2[0], P.filter_radius, P.filter_sigma, &dx, &denx);
+                                                gaussian_sample_1d(u2[1], P.filter_radius, P.filter_sigma, &dy, &deny);
+                                                const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
+                                                float lens[2];
+                                                orc_zsobol_get2d(&smp, lens);
+                                                const float scx = sx0 + fx / (float)W * (sx1 - sx0);
+                                                const float scy = sy1 - fy / (float)H * (sy1 - sy0);
+                                                const V3 dcam = normalize(v3(scx * tan_half, scy * tan_half, 1.0f));
+                                                const V3 dir = add(add(mul(right, dcam.x), mul(upv, dcam.y)), mul(fwd, dcam.z));
+                                                const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
+                                                const float fv = std::max(0.0f, gaussian(ddx, P.filter_sigma)) *
+                                                                 std::max(0.0f, gaussian(ddy, P.filter_sigma));
+                                                const float w = fv / (denx * deny);
+                                                PathResult pr = trace_path(sc, &smp, eye, dir);
+                                                cnt[4 * ti + 0] += 1;
+                                                cnt[4 * ti + 1] += pr.ext;
+                                                cnt[4 * ti + 2] += pr.shadow;
+                                                cnt[4 * ti + 3] += pr.probe;
+                                                const float lv[3] = {pr.L.x, pr.L.y, pr.L.z};
+                                                for (int c = 0; c < 3; ++c) {
+                                                        acc[c] += lv[c];
+                                                        acc2[c] += lv[c] * lv[c];
+                                                }
+                                                accw += w;
+                                        }
+                                        const size_t pix = (size_t)py * W + px;
+                                        for (int c = 0; c < 3; ++c) {
+                                                sum_rgb[3 * pix + c] += acc[c];
+                                                if (sum_sq) sum_sq[3 * pix + c] += acc2[c];
+                                        }
+                                        sum_w[pix] += accw;
+                                }
+                        }
+                });
+        for (auto &t : pool) t.join();
+        if (counters)
+                for (int ti = 0; ti < threads; ++ti)
+                        for (int k = 0; k < 4; ++k) counters[k] += cnt[4 * ti + k];
+}

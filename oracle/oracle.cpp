@@ -553,6 +553,11 @@ void orc_traverse_batch(const orc_node *nodes, const orc_prim_id *prims, const o
         });
 }
 
+void orc_trace_one(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes, const orc_ray *ray,
+                   float tmax, orc_isect *out, int32_t *hit_index) {
+        traverse_one(nodes, prims, meshes, *ray, tmax, 0, out, hit_index, nullptr);
+}
+
 int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1, const float *p2,
                               float tmax, float *t, float *u, float *v) {
         return mt_test(o, d, p0, p1, p2, tmax, t, u, v);

@@ -76,6 +76,40 @@ void orc_traverse_batch(const orc_node *nodes, const orc_prim_id *prims, const o
                         const orc_ray *rays, const float *tmax, int64_t n, int watertight,
                         orc_isect *out, int32_t *hit_index, uint32_t *counters, int threads);
 
+/* One closest-hit query (MT leaf test). */
+void orc_trace_one(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes, const orc_ray *ray,
+                   float tmax, orc_isect *out, int32_t *hit_index);
+
+/* --- path integrator ---------------------------------------------------- */
+
+typedef struct orc_material {
+        int8_t type;
+        int8_t pad_[3];
+        float albedo[3];
+        float emission[3];
+} orc_material;
+
+typedef struct orc_render_params {
+        int32_t width, height, spp, max_depth;
+        int32_t rr_min_bounce;  /* Russian roulette when bounce >= this (reference: 2) */
+        int32_t mis_corrected;  /* 0: as written (BSDF strategy weight 0), 1: corrected */
+        int64_t seed;           /* Z-Sobol seed (reference: 1234) */
+        float eye[3], target[3], up[3];
+        float fov_deg;
+        float filter_radius, filter_sigma;
+        int32_t first_sample;   /* sample indices [first_sample, first_sample + spp) of a sampler */
+        int32_t sampler_spp;    /* of sampler_spp samples per pixel (0: spp) */
+} orc_render_params;
+
+/* Renders the scene; per pixel (row-major) accumulates the film sums of the
+ * reference's Pixel (light sum, weight sum; Core/Pixel.swift, Core/Film.swift:
+ * 107-119) plus the per-channel sum of squares of the sample values.
+ * counters (optional): {camera rays, extension rays, shadow rays, probe rays}. */
+void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
+                uint64_t *counters, int threads);
+
 /* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
 int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1,
                               const float *p2, float tmax, float *t, float *u, float *v);

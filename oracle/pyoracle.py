@@ -36,7 +36,7 @@ _lib = None
 
 
 def build():
-    src = [HERE / "oracle.cpp", HERE / "oracle.h"]
+    src = [HERE / "oracle.cpp", HERE / "integrator.cpp", HERE / "oracle.h"]
     if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -178,3 +178,48 @@ def zsobol_batch(spp, res_x, res_y, px, py, index, kinds, seed=1234):
     lib().orc_zsobol_batch(spp, res_x, res_y, seed, _p(px), _p(py), _p(index), len(px), _p(kinds), len(kinds),
                            _p(out))
     return out
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("rr_min_bounce", C.c_int32), ("mis_corrected", C.c_int32), ("seed", C.c_int64),
+                ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
+                ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
+                ("sampler_spp", C.c_int32)]
+
+
+def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
+                  eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
+                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0):
+    return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
+                        (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
+                        first_sample, sampler_spp)
+
+
+def render(hs, params, threads=0):
+    """Film sums of the oracle integrator: (sum_rgb (H,W,3), sum_sq (H,W,3),
+    sum_w (H,W), counters {camera, extension, shadow, probe})."""
+    L = lib()
+    if not getattr(L, "_render_bound", False):
+        L.orc_render.restype = None
+        L.orc_render.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.POINTER(RenderParams)] + \
+            [C.c_void_p] * 4 + [C.c_int]
+        L._render_bound = True
+    keep = []
+    arr = (_Mesh * max(len(hs.meshes), 1))()
+    for i, m in enumerate(hs.meshes):
+        p4 = np.ascontiguousarray(m.points, np.float32)
+        vi = np.ascontiguousarray(m.vertex_indices, np.int64)
+        keep += [p4, vi]
+        arr[i] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+    mats = np.ascontiguousarray(hs.materials)
+    W, H = params.width, params.height
+    s = np.zeros((H, W, 3), np.float32)
+    s2 = np.zeros((H, W, 3), np.float32)
+    sw = np.zeros((H, W), np.float32)
+    cnt = np.zeros(4, np.uint64)
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    L.orc_render(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr), _p(mats),
+                 len(mats), len(hs.prims), C.byref(params), _p(s), _p(s2), _p(sw), _p(cnt), threads)
+    return s, s2, sw, {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
