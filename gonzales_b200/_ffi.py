@@ -52,6 +52,10 @@ MATERIAL_DTYPE = np.dtype(
     {"names": ["type", "albedo", "emission"], "formats": ["i1", ("<f4", 3), ("<f4", 3)],
      "offsets": [0, 4, 16], "itemsize": 28})
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("dir", "<f4", 3)])  # Ray_C, 24 bytes
+PATH_STATE_DTYPE = np.dtype(
+    {"names": ["ray", "throughput", "estimate", "albedo", "pcg_state", "pcg_inc", "active"],
+     "formats": [RAY_DTYPE, ("<f4", 3), ("<f4", 3), ("<f4", 3), "<u8", "<u8", "i1"],
+     "offsets": [0, 24, 36, 48, 64, 72, 80], "itemsize": 88})
 
 
 class TriangleMeshC(C.Structure):
@@ -105,6 +109,7 @@ PROTOTYPES = {
     "gzg_gpu_traverse_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
     "gzg_gpu_occluded_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
     "gzg_gpu_traverse_batch_static": (ST, [VP, VP, VP, I64, VP]),
+    "gzg_gpu_shade_batch": (ST, [VP, VP, I64, VP]),
     "gzg_trace_closest_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_trace_any_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),

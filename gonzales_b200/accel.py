@@ -118,6 +118,12 @@ class GpuAccelerator:
         F.check(F.lib().gzg_hits_to_intersections_device(self.handle, hits_d.data_ptr(), hits_d.shape[0],
                                                          out_d.data_ptr(), _stream_handle(stream)))
 
+    def shade_batch(self, paths, intersections):
+        """gzg_gpu_shade_batch on PATH_STATE_DTYPE records (updated in place)."""
+        assert paths.dtype == F.PATH_STATE_DTYPE and intersections.dtype == F.INTERSECTION_DTYPE
+        F.check(F.lib().gzg_gpu_shade_batch(self.handle, F.ptr(paths), len(paths), F.ptr(intersections)))
+        return paths
+
     def render(self, params):
         """Renders on the device (gzg_render_image); returns host film sums
         (rgb (H, W, 3), squares (H, W, 3), weights (H, W)) and statistics."""

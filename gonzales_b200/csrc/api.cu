@@ -435,6 +435,34 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         d.material_count = (int32_t)material_count;
         d.light_count = (int32_t)light_prims.size();
         d.light_total_power = total;
+
+        // Device copies of the meshes, for calls that take reference
+        // Intersection_C records and decode (mesh, triangle) from the prim id
+        // the way shade_core does (kernel.mojo:705-721).
+        std::vector<gzg_triangle_mesh> dev_meshes((size_t)mesh_count);
+        std::vector<int64_t> sizes((size_t)mesh_count * 2);
+        for (int64_t k = 0; k < mesh_count; ++k) {
+                const float *pts = nullptr;
+                const int64_t *vi = nullptr;
+                st = scene->upload(meshes[k].points, (size_t)std::max<int64_t>(mesh_points_counts[k], 0), &pts,
+                                   "mesh points");
+                if (st != GZG_OK) return st;
+                st = scene->upload(meshes[k].vertex_indices, (size_t)std::max<int64_t>(mesh_vertex_indices_counts[k], 0),
+                                   &vi, "mesh vertex indices");
+                if (st != GZG_OK) return st;
+                dev_meshes[k] = gzg_triangle_mesh{pts, nullptr, vi};
+                sizes[2 * k] = mesh_points_counts[k];
+                sizes[2 * k + 1] = mesh_vertex_indices_counts[k];
+        }
+        const gzg_triangle_mesh *dm;
+        st = scene->upload(dev_meshes.data(), dev_meshes.size(), &dm, "mesh table");
+        if (st != GZG_OK) return st;
+        d.meshes = dm;
+        const int64_t *ms;
+        st = scene->upload(sizes.data(), sizes.size(), &ms, "mesh sizes");
+        if (st != GZG_OK) return st;
+        d.mesh_sizes = ms;
+        d.mesh_count = mesh_count;
         *out_scene = scene.release();
         return clear_error();
 }

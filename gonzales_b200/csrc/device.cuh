@@ -35,6 +35,10 @@ struct DevScene {
         int32_t material_count;
         int32_t light_count;
         float light_total_power;
+        // the host's meshes on the device (TriangleMesh_C with device pointers)
+        const gzg_triangle_mesh *meshes;
+        const int64_t *mesh_sizes;     // per mesh: point floats, vertex indices
+        int64_t mesh_count;
 };
 
 // The launch's ray count: the device-side count when one is given.

@@ -61,9 +61,15 @@ gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const 
                           const int64_t *points_counts, const int64_t *vertex_index_counts, WideBvh *out,
                           int32_t *bvh2_depth);
 
+#ifdef __CUDACC__
+#define GZG_HOST_DEVICE __host__ __device__
+#else
+#define GZG_HOST_DEVICE
+#endif
+
 // Decodes PrimId_C to (mesh, first vertex-index slot) as kernel.mojo:270-279;
 // returns false for prims the reference never intersects.
-inline bool prim_triangle(const gzg_prim_id &p, int64_t *mesh, int64_t *base) {
+GZG_HOST_DEVICE inline bool prim_triangle(const gzg_prim_id &p, int64_t *mesh, int64_t *base) {
         if (p.type == 0) {
                 *mesh = p.id1;
                 *base = p.id2;

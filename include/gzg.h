@@ -243,6 +243,15 @@ GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, const gzg_ray
                                                  const float *t_max_values, int64_t count,
                                                  gzg_intersection *results);
 
+/* Replaces mojo_gpu_shade_batch (kernel.mojo:788-846, mojo_kernel.h:76-77):
+ * the live shading step of the tile loop (Core/Tile.swift:137-155) on host
+ * PathState_C and Intersection_C arrays (shade_core, kernel.mojo:676-773):
+ * area-light hits add emission and end the path, diffuse hits bounce with a
+ * PCG32-driven cosine sample, misses end the path.  Synchronous.  Needs the
+ * scene's materials and meshes from gzg_gpu_upload_scene. */
+GZG_API gzg_status gzg_gpu_shade_batch(gzg_scene *scene, gzg_path_state *paths, int64_t count,
+                                       const gzg_intersection *intersections);
+
 /* Shadow / any-hit batch (new; Visibility.occluded, Core/Visibility.swift:5-24,
  * answers it with a closest-hit query, BoundingHierarchy.swift:348-384).
  * occluded[i] = 1 iff some triangle is hit with 0 < t <= tMax[i]. */

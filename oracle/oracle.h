@@ -110,6 +110,23 @@ void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh 
                 const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                 uint64_t *counters, int threads);
 
+/* PathState_C (mojo_kernel.h:36-44). */
+typedef struct orc_path_state {
+        orc_ray ray;
+        float throughput[3];
+        float estimate[3];
+        float albedo[3];
+        int32_t pad0_;
+        uint64_t pcg_state;
+        uint64_t pcg_inc;
+        int8_t active;
+        int8_t pad1_[7];
+} orc_path_state;
+
+/* shade_core over a batch (kernel.mojo:676-773, mojo_cpu_shade_batch :378-390). */
+void orc_shade_batch(orc_path_state *paths, int64_t n, const orc_isect *isects, const orc_mesh *meshes,
+                     const orc_material *materials);
+
 /* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
 int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1,
                               const float *p2, float tmax, float *t, float *u, float *v);

@@ -36,7 +36,7 @@ _lib = None
 
 
 def build():
-    src = [HERE / "oracle.cpp", HERE / "integrator.cpp", HERE / "oracle.h"]
+    src = [HERE / "oracle.cpp", HERE / "integrator.cpp", HERE / "shade.cpp", HERE / "oracle.h"]
     if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -223,3 +223,28 @@ def render(hs, params, threads=0):
     L.orc_render(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr), _p(mats),
                  len(mats), len(hs.prims), C.byref(params), _p(s), _p(s2), _p(sw), _p(cnt), threads)
     return s, s2, sw, {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
+
+
+PATH_DTYPE = np.dtype({"names": ["ray", "throughput", "estimate", "albedo", "pcg_state", "pcg_inc", "active"],
+                       "formats": [("<f4", 6), ("<f4", 3), ("<f4", 3), ("<f4", 3), "<u8", "<u8", "i1"],
+                       "offsets": [0, 24, 36, 48, 64, 72, 80], "itemsize": 88})
+
+
+def shade_batch(hs, paths, isects):
+    """shade_core over a batch (in place on a copy); returns the new paths."""
+    L = lib()
+    if not getattr(L, "_shade_bound", False):
+        L.orc_shade_batch.restype = None
+        L.orc_shade_batch.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L._shade_bound = True
+    out = np.ascontiguousarray(paths).copy()
+    keep = []
+    arr = (_Mesh * max(len(hs.meshes), 1))()
+    for i, m in enumerate(hs.meshes):
+        p4 = np.ascontiguousarray(m.points, np.float32)
+        vi = np.ascontiguousarray(m.vertex_indices, np.int64)
+        keep += [p4, vi]
+        arr[i] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+    L.orc_shade_batch(_p(out), len(out), _p(np.ascontiguousarray(isects)), C.addressof(arr),
+                      _p(np.ascontiguousarray(hs.materials)))
+    return out
