@@ -64,7 +64,8 @@ class TriangleMeshC(C.Structure):
 
 class TraceOptions(C.Structure):
     _fields_ = [("traversal", C.c_int32), ("leaf_test", C.c_int32), ("block_size", C.c_int32),
-                ("blocks_per_sm", C.c_int32), ("fetch_counters", C.c_void_p)]
+                ("blocks_per_sm", C.c_int32), ("stack_depth", C.c_int32), ("l1_carveout", C.c_int32),
+                ("fetch_counters", C.c_void_p)]
 
 
 class SceneInfo(C.Structure):
@@ -113,6 +114,8 @@ PROTOTYPES = {
     "gzg_trace_closest_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_trace_any_device": (ST, [VP, VP, I64, VP, C.POINTER(TraceOptions), VP]),
     "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),
+    "gzg_scene_autotune": (ST, [VP, VP, I64, C.c_int32, C.POINTER(TraceOptions), C.POINTER(C.c_float), VP]),
+    "gzg_scene_set_launch": (ST, [VP, C.c_int32, C.POINTER(TraceOptions)]),
     "gzg_scene_info_get": (ST, [VP, C.POINTER(SceneInfo)]),
     "gzg_renderer_create": (ST, [VP, C.POINTER(RenderParams), C.POINTER(VP)]),
     "gzg_renderer_destroy": (ST, [VP]),
@@ -157,6 +160,7 @@ def ptr(a):
 
 
 def options(traversal=TRAVERSAL_WIDE, leaf_test=LEAF_MOLLER_TRUMBORE, block_size=0, blocks_per_sm=0,
-            fetch_counters=None):
-    """fetch_counters: device address (int) of 3 uint64 (nodes, triangles, rays) or None."""
-    return TraceOptions(traversal, leaf_test, block_size, blocks_per_sm, fetch_counters)
+            stack_depth=0, l1_carveout=0, fetch_counters=None):
+    """Trace options; 0 fields take the scene's tuned launch.  fetch_counters:
+    device address (int) of 3 uint64 (nodes, triangles, rays) or None."""
+    return TraceOptions(traversal, leaf_test, block_size, blocks_per_sm, stack_depth, l1_carveout, fetch_counters)

@@ -118,6 +118,44 @@ class GpuAccelerator:
         F.check(F.lib().gzg_hits_to_intersections_device(self.handle, hits_d.data_ptr(), hits_d.shape[0],
                                                          out_d.data_ptr(), _stream_handle(stream)))
 
+    def autotune(self, rays_d, any_hit=False, stream=None):
+        """gzg_scene_autotune on device rays; returns (launch config dict, ms per launch)."""
+        best = F.TraceOptions()
+        ms = C.c_float(0.0)
+        F.check(F.lib().gzg_scene_autotune(self.handle, rays_d.data_ptr(), rays_d.shape[0], 1 if any_hit else 0,
+                                           C.byref(best), C.byref(ms), _stream_handle(stream)))
+        cfg = {k: getattr(best, k) for k in ("block_size", "blocks_per_sm", "stack_depth", "l1_carveout")}
+        return cfg, ms.value
+
+    def set_launch(self, cfg, any_hit=False):
+        opt = F.options(**cfg)
+        F.check(F.lib().gzg_scene_set_launch(self.handle, 1 if any_hit else 0, C.byref(opt)))
+
+    def tune_cached(self, rays_d, cache_path, key, any_hit=False):
+        """Tuned launch from a JSON cache (keyed by GPU name, `key` and query
+        kind) or, on a miss, from gzg_scene_autotune, written back to the cache."""
+        import json
+        import os
+
+        import torch
+
+        full_key = "%s|%s|%s" % (torch.cuda.get_device_name(), key, "any" if any_hit else "closest")
+        cache = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
+        if full_key in cache:
+            self.set_launch(cache[full_key]["launch"], any_hit)
+            return cache[full_key]["launch"], cache[full_key]["ms"], True
+        cfg, ms = self.autotune(rays_d, any_hit)
+        if cache_path:
+            cache[full_key] = {"launch": cfg, "ms": ms}
+            tmp = cache_path + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache_path)
+        return cfg, ms, False
+
     def shade_batch(self, paths, intersections):
         """gzg_gpu_shade_batch on PATH_STATE_DTYPE records (updated in place)."""
         assert paths.dtype == F.PATH_STATE_DTYPE and intersections.dtype == F.INTERSECTION_DTYPE

@@ -90,6 +90,15 @@ bool is_pinned(const void *p) {
 }
 
 }  // namespace
+
+// Launch configuration chosen by gzg_scene_autotune (or the defaults).
+struct TunedLaunch {
+        int block_size = 128;
+        int blocks_per_sm = 0;  // occupancy limit
+        int stack_depth = 0;    // by tree depth
+        int l1_carveout = -1;   // driver default
+};
+
 }  // namespace gzg
 
 using namespace gzg;
@@ -99,6 +108,7 @@ struct gzg_scene {
         DevScene dev{};
         std::vector<void *> allocs;
         gzg_scene_info info{};
+        TunedLaunch tuned_closest, tuned_any;
         std::mutex pool_mu;
         std::vector<std::unique_ptr<Staging>> pool;
 
@@ -151,12 +161,17 @@ struct gzg_scene {
 
 namespace {
 
-LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o) {
+// Options fields left at 0 take the scene's tuned values (gzg_scene_autotune),
+// separately for closest-hit and any-hit launches.
+LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o, bool any) {
+        const TunedLaunch &t = any ? s->tuned_any : s->tuned_closest;
         LaunchParams p;
         p.traversal = o ? o->traversal : GZG_TRAVERSAL_WIDE;
         p.leaf_test = o ? o->leaf_test : GZG_LEAF_MOLLER_TRUMBORE;
-        p.block_size = o ? o->block_size : 0;
-        p.blocks_per_sm = o ? o->blocks_per_sm : 0;
+        p.block_size = (o && o->block_size) ? o->block_size : t.block_size;
+        p.blocks_per_sm = (o && o->blocks_per_sm) ? o->blocks_per_sm : t.blocks_per_sm;
+        p.stack_depth = (o && o->stack_depth) ? o->stack_depth : t.stack_depth;
+        p.l1_carveout = (o && o->l1_carveout) ? o->l1_carveout : t.l1_carveout;
         p.wide_depth = s->info.wide_depth;
         p.counters = o ? reinterpret_cast<unsigned long long *>(o->fetch_counters) : nullptr;
         p.n_dev = nullptr;
@@ -200,7 +215,7 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
         std::unique_ptr<Staging> stg;
         st = s->acquire(&stg);
         if (st != GZG_OK) return st;
-        const LaunchParams p = params_for(s, opt);
+        const LaunchParams p = params_for(s, opt, out_fmt == kOutAnyPrim || out_fmt == kOutOccluded);
         const bool direct = is_pinned(rays) && is_pinned(tmax) && is_pinned(results);
         const int64_t nchunks = (count + kChunk - 1) / kChunk;
         char *res = reinterpret_cast<char *>(results);
@@ -489,9 +504,112 @@ GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *r
         gzg_status st = check_options(options);
         if (st != GZG_OK) return st;
         DeviceGuard g(scene->device);
-        GZG_CK(launch_trace(scene->dev, params_for(scene, options), kRayDevice, kOutHit, rays, nullptr, count, hits,
-                            reinterpret_cast<cudaStream_t>(stream)),
+        GZG_CK(launch_trace(scene->dev, params_for(scene, options, false), kRayDevice, kOutHit, rays, nullptr, count,
+                            hits, reinterpret_cast<cudaStream_t>(stream)),
                "gzg_trace_closest_device launch");
+        return clear_error();
+}
+
+// Coordinate descent over the launch configuration of the persistent wide
+// kernel on the caller's rays: L1 carveout, then blocks per SM, then block
+// size, then stack depth; each candidate timed over three launches after one
+// warm-up with CUDA events on `stream`.  The winner becomes the scene's
+// default for that query kind.
+GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, int64_t count, int32_t any_hit,
+                                      gzg_trace_options *best, float *best_ms, void *stream) {
+        if (!scene || !rays || count <= 0)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_autotune: bad arguments");
+        DeviceGuard g(scene->device);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        void *out = nullptr;
+        GZG_CK(cudaMalloc(&out, (size_t)count * 16), "gzg_scene_autotune output buffer");
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        gzg_status status = GZG_OK;
+        auto time_config = [&](const TunedLaunch &t, float *ms) -> gzg_status {
+                LaunchParams p = params_for(scene, nullptr, any_hit != 0);
+                p.block_size = t.block_size;
+                p.blocks_per_sm = t.blocks_per_sm;
+                p.stack_depth = t.stack_depth;
+                p.l1_carveout = t.l1_carveout;
+                const int fmt = any_hit ? kOutAnyPrim : kOutHit;
+                GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st), "autotune launch");
+                GZG_CK(cudaEventRecord(e0, st), "autotune event");
+                for (int k = 0; k < 3; ++k)
+                        GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st), "autotune launch");
+                GZG_CK(cudaEventRecord(e1, st), "autotune event");
+                GZG_CK(cudaEventSynchronize(e1), "autotune sync");
+                float el = 0;
+                cudaEventElapsedTime(&el, e0, e1);
+                *ms = el / 3.0f;
+                return GZG_OK;
+        };
+        TunedLaunch cur;
+        float cur_ms = 0;
+        status = time_config(cur, &cur_ms);
+        const int carves[] = {1, 25, 50, 75, 100};
+        const int bps[] = {2, 3, 4, 5, 6, 7, 8};
+        const int blocks[] = {64, 256};
+        const int stacks[] = {16, 32};
+        auto try_set = [&](TunedLaunch cand) {
+                if (status) return;
+                float ms = 0;
+                status = time_config(cand, &ms);
+                if (!status && ms < cur_ms) {
+                        cur = cand;
+                        cur_ms = ms;
+                }
+        };
+        for (int c : carves) {
+                TunedLaunch t = cur;
+                t.l1_carveout = c;
+                try_set(t);
+        }
+        for (int b : bps) {
+                TunedLaunch t = cur;
+                t.blocks_per_sm = b;
+                try_set(t);
+        }
+        for (int bs : blocks) {
+                TunedLaunch t = cur;
+                t.block_size = bs;
+                t.blocks_per_sm = cur.blocks_per_sm ? std::max(1, cur.blocks_per_sm * 128 / bs) : 0;
+                try_set(t);
+        }
+        for (int s : stacks) {
+                TunedLaunch t = cur;
+                t.stack_depth = s;
+                try_set(t);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(out);
+        if (status) return status;
+        (any_hit ? scene->tuned_any : scene->tuned_closest) = cur;
+        if (best) {
+                std::memset(best, 0, sizeof(*best));
+                best->traversal = GZG_TRAVERSAL_WIDE;
+                best->leaf_test = GZG_LEAF_MOLLER_TRUMBORE;
+                best->block_size = cur.block_size;
+                best->blocks_per_sm = cur.blocks_per_sm;
+                best->stack_depth = cur.stack_depth;
+                best->l1_carveout = cur.l1_carveout;
+        }
+        if (best_ms) *best_ms = cur_ms;
+        return clear_error();
+}
+
+// Installs a launch configuration (for example one read back from a tuning
+// cache) as the scene's default for closest-hit (any_hit = 0) or any-hit queries.
+GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const gzg_trace_options *config) {
+        if (!scene || !config) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_launch: null argument");
+        TunedLaunch t;
+        if (config->block_size) t.block_size = config->block_size;
+        t.blocks_per_sm = config->blocks_per_sm;
+        t.stack_depth = config->stack_depth;
+        t.l1_carveout = config->l1_carveout ? config->l1_carveout : -1;
+        (any_hit ? scene->tuned_any : scene->tuned_closest) = t;
         return clear_error();
 }
 
@@ -502,7 +620,7 @@ GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays,
         gzg_status st = check_options(options);
         if (st != GZG_OK) return st;
         DeviceGuard g(scene->device);
-        GZG_CK(launch_trace(scene->dev, params_for(scene, options), kRayDevice, kOutAnyPrim, rays, nullptr, count,
+        GZG_CK(launch_trace(scene->dev, params_for(scene, options, true), kRayDevice, kOutAnyPrim, rays, nullptr, count,
                             hit_prim, reinterpret_cast<cudaStream_t>(stream)),
                "gzg_trace_any_device launch");
         return clear_error();
@@ -541,5 +659,11 @@ void scene_view(const gzg_scene *scene, DevScene *view, int *device, int *wide_d
         *device = scene->device;
         *wide_depth = scene->info.wide_depth;
 }
+
+}  // namespace gzg
+
+namespace gzg {
+
+LaunchParams scene_launch(const gzg_scene *scene, bool any_hit) { return params_for(scene, nullptr, any_hit); }
 
 }  // namespace gzg

@@ -12,8 +12,10 @@ struct LaunchParams {
         int traversal;   // gzg_traversal
         int leaf_test;   // gzg_leaf_test
         int wide_depth;  // levels of the wide tree (selects the stack size)
-        int block_size;
-        int blocks_per_sm;
+        int block_size;     // 64, 128 or 256 (anything else: 128)
+        int blocks_per_sm;  // persistent grid per SM; 0 = occupancy limit
+        int stack_depth;    // shared stack entries; raised to the tree's need
+        int l1_carveout;    // preferred shared-memory carveout percent; <= 0 = driver default
         unsigned long long *counters;  // optional fetch counters (device)
         const uint32_t *n_dev;         // optional device-side ray count; n is then the capacity
 };
@@ -26,5 +28,8 @@ cudaError_t launch_hits_to_isect(const DevScene &s, const void *hits, int64_t n,
 
 // Device view, device ordinal and wide-tree depth of an uploaded scene.
 void scene_view(const gzg_scene *scene, DevScene *view, int *device, int *wide_depth);
+
+// The scene's default (tuned) launch for closest-hit or any-hit queries.
+LaunchParams scene_launch(const gzg_scene *scene, bool any_hit);
 
 }  // namespace gzg

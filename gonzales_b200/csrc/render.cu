@@ -673,17 +673,16 @@ struct gzg_renderer {
                 int cur = 0;
                 for (int b = 0; b < rc.max_depth; ++b) {
                         k_clear_counts<<<1, 1, 0, st>>>(w, cur ^ 1);
-                        LaunchParams lp{};
-                        lp.traversal = GZG_TRAVERSAL_WIDE;
-                        lp.leaf_test = GZG_LEAF_MOLLER_TRUMBORE;
-                        lp.wide_depth = wide_depth;
+                        // the scene's tuned launches (gzg_scene_autotune)
+                        LaunchParams lp = scene_launch(scene, false);
+                        LaunchParams lpa = scene_launch(scene, true);
                         lp.n_dev = w.counts + cur;
                         cudaError_t e = launch_trace(view, lp, kRayDevice, kOutHit, w.q_ray[cur], nullptr, w.capacity,
                                                      w.hits, st);
                         if (e != cudaSuccess) return e;
                         k_shade<<<grid, block, 0, st>>>(rc, w, view, b, cur);
-                        lp.n_dev = w.counts + kCountShadow;
-                        e = launch_trace(view, lp, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
+                        lpa.n_dev = w.counts + kCountShadow;
+                        e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
                         if (rc.mis_corrected) {

@@ -100,7 +100,7 @@ __device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const 
 }
 
 template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
-__global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict__ rays, const float *__restrict__ tmaxs,
+__global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict__ rays, const float *__restrict__ tmaxs,
                                               int64_t n, void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
         const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(128) k_wide(DevScene s, const void *__restrict
 // 32-ray batch finishes.  Each iteration opens one node and tests its
 // triangles.  No atomics or per-launch state: the assignment is static.
 template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
-__global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void *__restrict__ rays,
                                                          const float *__restrict__ tmaxs, int64_t n,
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
@@ -472,12 +472,19 @@ using TraceKernel = void (*)(DevScene, const void *, const float *, int64_t, voi
 // SM, from the occupancy calculator unless blocks_per_sm is given), capped at
 // the blocks the ray count needs; the one-ray-per-thread kernel one thread per
 // ray.
-cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, int blocks_per_sm, const DevScene &s,
+cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const LaunchParams &p, const DevScene &s,
                                const void *rays, const float *tmax, int64_t n, void *out, cudaStream_t st) {
-        const int block = 128;
+        const int block = (p.block_size == 64 || p.block_size == 256) ? p.block_size : 128;
+        const int blocks_per_sm = p.blocks_per_sm;
         const size_t smem = (size_t)stack * block * sizeof(uint2);
         if (smem > 48 * 1024) {
                 cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+        }
+        // L1 / shared split: explicit percent, or the driver's choice (-1).
+        {
+                const int carve = p.l1_carveout > 0 ? (p.l1_carveout > 100 ? 100 : p.l1_carveout) : -1;
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
                 if (e != cudaSuccess) return e;
         }
         int64_t grid = (n + block - 1) / block;
@@ -501,21 +508,24 @@ template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
 cudaError_t launch_wide_depth(const DevScene &s, const LaunchParams &p, const void *rays, const float *tmax, int64_t n,
                               void *out, cudaStream_t st) {
         const bool persistent = p.traversal == GZG_TRAVERSAL_WIDE;
-        const int bps = p.blocks_per_sm;
-        if (p.wide_depth <= 8) {
+        // The stack holds at most depth - 1 groups; a requested depth below
+        // that is raised so no ray can overflow it.
+        const int need = p.wide_depth > 1 ? p.wide_depth : 1;
+        const int want = p.stack_depth > need ? p.stack_depth : need;
+        if (want <= 8) {
                 TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 8, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 8, LEAF>;
-                return launch_wide_kernel(k, 8, persistent, bps, s, rays, tmax, n, out, st);
+                return launch_wide_kernel(k, 8, persistent, p, s, rays, tmax, n, out, st);
         }
-        if (p.wide_depth <= 16) {
+        if (want <= 16) {
                 TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 16, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 16, LEAF>;
-                return launch_wide_kernel(k, 16, persistent, bps, s, rays, tmax, n, out, st);
+                return launch_wide_kernel(k, 16, persistent, p, s, rays, tmax, n, out, st);
         }
-        if (p.wide_depth <= 32) {
+        if (want <= 32) {
                 TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 32, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 32, LEAF>;
-                return launch_wide_kernel(k, 32, persistent, bps, s, rays, tmax, n, out, st);
+                return launch_wide_kernel(k, 32, persistent, p, s, rays, tmax, n, out, st);
         }
         TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 64, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 64, LEAF>;
-        return launch_wide_kernel(k, 64, persistent, bps, s, rays, tmax, n, out, st);
+        return launch_wide_kernel(k, 64, persistent, p, s, rays, tmax, n, out, st);
 }
 
 template <int RAYFMT, int OUTFMT, bool ANY>

@@ -170,8 +170,11 @@ typedef enum gzg_leaf_test {
 typedef struct gzg_trace_options {
         int32_t traversal; /* gzg_traversal */
         int32_t leaf_test; /* gzg_leaf_test */
-        int32_t block_size; /* 0 = library default */
-        int32_t blocks_per_sm; /* 0 = library default */
+        int32_t block_size; /* 64, 128 or 256 threads; 0 = the scene's tuned value (default 128) */
+        int32_t blocks_per_sm; /* persistent grid = SMs x this; 0 = tuned / occupancy limit */
+        int32_t stack_depth; /* shared-memory stack entries (8, 16, 32, 64); 0 = tuned / by tree depth */
+        int32_t l1_carveout; /* preferred shared-memory carveout in percent; -1 = driver default,
+                                0 = tuned */
         /* Optional DEVICE pointer to 3 uint64 counters that the kernel adds to:
          * [0] nodes fetched (wide nodes, or BVH2 node records), [1] triangles
          * tested, [2] rays traced.  NULL = no counting. */
@@ -269,6 +272,18 @@ GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *r
 GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
                                         int32_t *hit_prim, const gzg_trace_options *options,
                                         void *stream);
+
+/* Launch autotuner: times the persistent wide kernel on the caller's DEVICE
+ * rays over L1 carveout, blocks per SM, block size and stack depth
+ * (coordinate descent, CUDA events on `stream`), keeps the fastest as the
+ * scene's default for closest-hit (any_hit = 0) or any-hit queries, and
+ * returns it (and its time per launch in ms).  Synchronous. */
+GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, int64_t count, int32_t any_hit,
+                                      gzg_trace_options *best, float *best_ms, void *stream);
+
+/* Installs a launch configuration (e.g. from a tuning cache) as the scene's
+ * default for closest-hit (any_hit = 0) or any-hit queries. */
+GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const gzg_trace_options *config);
 
 /* Expands device hits into reference Intersection_C records on the device
  * (prim-id lookup; the miss record of kernel.mojo:362-364). */

@@ -112,7 +112,9 @@ def test_render_matches_oracle_per_pixel(box, mis):
     # the GPU skips the reference's final extension (bounce == max_depth),
     # which can only add environment light; the oracle traces it
     assert 0.5 * ocnt["extension"] <= gstats["extension_rays"] <= ocnt["extension"]
-    assert abs(gstats["shadow_rays"] - ocnt["shadow"]) <= 0.01 * ocnt["shadow"]
+    # the GPU also skips shadow rays whose contribution is zero (light behind
+    # the surface as seen from the outgoing side); the oracle traces them
+    assert 0.8 * ocnt["shadow"] <= gstats["shadow_rays"] <= ocnt["shadow"]
     if mis:
         assert gstats["probe_rays"] > 0
     else:

@@ -211,6 +211,24 @@ def test_box_scene_parity():
         assert counts["fail"] == 0, counts
 
 
+def test_autotune_picks_a_valid_launch_and_keeps_results(small, tmp_path):
+    torch = torch_mod()
+    hs, acc, o, d, t, isect, idx = small
+    rays = torch.from_numpy(scenes.pack_device_rays(o, d, t)).cuda()
+    before = device_closest(acc, o, d, t)
+    cache = str(tmp_path / "tuning.json")
+    cfg, ms, cached = acc.tune_cached(rays, cache, "raycast-subdiv4")
+    assert not cached and ms > 0
+    assert cfg["block_size"] in (64, 128, 256)
+    assert cfg["stack_depth"] in (0, 16, 32)
+    after = device_closest(acc, o, d, t)
+    for a, b in zip(before, after):
+        assert np.array_equal(H.bits(a) if a.dtype == np.float32 else a, H.bits(b) if b.dtype == np.float32 else b)
+    cfg2, ms2, cached2 = acc.tune_cached(rays, cache, "raycast-subdiv4")
+    assert cached2 and cfg2 == cfg
+    acc.set_launch({"block_size": 128, "blocks_per_sm": 0, "stack_depth": 0, "l1_carveout": 0})
+
+
 def test_golden_vectors():
     """Committed oracle outputs (tests/golden/raycast_small.npz, made by
     tests/golden/make_golden.py) against the live GPU kernels."""
