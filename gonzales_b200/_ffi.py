@@ -52,6 +52,8 @@ MATERIAL_DTYPE = np.dtype(
     {"names": ["type", "albedo", "emission"], "formats": ["i1", ("<f4", 3), ("<f4", 3)],
      "offsets": [0, 4, 16], "itemsize": 28})
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("dir", "<f4", 3)])  # Ray_C, 24 bytes
+INSTANCE_DTYPE = np.dtype([("object_to_world", "<f4", 12), ("world_to_object", "<f4", 12), ("blas", "<i4"),
+                           ("pad", "<i4")])  # gzg_instance, 104 bytes
 PATH_STATE_DTYPE = np.dtype(
     {"names": ["ray", "throughput", "estimate", "albedo", "pcg_state", "pcg_inc", "active"],
      "formats": [RAY_DTYPE, ("<f4", 3), ("<f4", 3), ("<f4", 3), "<u8", "<u8", "i1"],
@@ -116,6 +118,9 @@ PROTOTYPES = {
     "gzg_hits_to_intersections_device": (ST, [VP, VP, I64, VP, VP]),
     "gzg_scene_autotune": (ST, [VP, VP, I64, C.c_int32, C.POINTER(TraceOptions), C.POINTER(C.c_float), VP]),
     "gzg_scene_set_launch": (ST, [VP, C.c_int32, C.POINTER(TraceOptions)]),
+    "gzg_host_instance_bounds": (ST, [VP, I64, VP, I64, VP]),
+    "gzg_instanced_scene_create": (ST, [VP, I64, VP, I64, VP, I64, VP, I64, C.POINTER(VP)]),
+    "gzg_trace_closest_instanced_device": (ST, [VP, VP, I64, VP, VP, C.POINTER(TraceOptions), VP]),
     "gzg_scene_info_get": (ST, [VP, C.POINTER(SceneInfo)]),
     "gzg_renderer_create": (ST, [VP, C.POINTER(RenderParams), C.POINTER(VP)]),
     "gzg_renderer_destroy": (ST, [VP]),

@@ -175,6 +175,85 @@ class GpuAccelerator:
         return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
 
 
+def instance_bounds(blas_hosts, instances):
+    """World bounds per instance (gzg_host_instance_bounds) from the bottom-level
+    BVH2 root boxes."""
+    bb = np.zeros((len(blas_hosts), 6), np.float32)
+    for i, hs in enumerate(blas_hosts):
+        bb[i, :3] = hs.nodes[0]["bounds_min"]
+        bb[i, 3:] = hs.nodes[0]["bounds_max"]
+    instances = np.ascontiguousarray(instances, F.INSTANCE_DTYPE)
+    out = np.zeros((len(instances), 6), np.float32)
+    F.check(F.lib().gzg_host_instance_bounds(F.ptr(bb), len(bb), F.ptr(instances), len(instances), F.ptr(out)))
+    return out
+
+
+class InstancedAccelerator:
+    """A two-level scene (TransformedPrimitive, Primitive/TransformedPrimitive.swift):
+    bottom-level GpuAccelerators, instances (INSTANCE_DTYPE) and a top-level
+    SAH BVH2 the host builds over the instance bounds."""
+
+    def __init__(self, blas_accels, instances):
+        from .scene import build_bvh2
+
+        self.blas = list(blas_accels)
+        self.instances = np.ascontiguousarray(instances, F.INSTANCE_DTYPE)
+        self.bounds = instance_bounds([a.host for a in self.blas], self.instances)
+        self.tlas_nodes, self.leaf_instance = build_bvh2(self.bounds)
+        handles = (C.c_void_p * len(self.blas))(*[a.handle.value for a in self.blas])
+        h = C.c_void_p()
+        F.check(F.lib().gzg_instanced_scene_create(handles, len(self.blas), F.ptr(self.instances),
+                                                   len(self.instances), F.ptr(self.tlas_nodes),
+                                                   len(self.tlas_nodes), F.ptr(self.leaf_instance),
+                                                   len(self.leaf_instance), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            F.check(F.lib().gzg_gpu_free_scene(self.handle))
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        info = F.SceneInfo()
+        F.check(F.lib().gzg_scene_info_get(self.handle, C.byref(info)))
+        return {name: getattr(info, name) for name, _ in F.SceneInfo._fields_}
+
+    def error_word(self, clear=True):
+        w = C.c_uint32(0)
+        F.check(F.lib().gzg_scene_error_word(self.handle, C.byref(w), 1 if clear else 0))
+        return w.value
+
+    def trace_closest(self, rays_d, hits_d, inst_d, options=None, stream=None):
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_trace_closest_instanced_device(self.handle, rays_d.data_ptr(), rays_d.shape[0],
+                                                           hits_d.data_ptr(), inst_d.data_ptr(), opt,
+                                                           _stream_handle(stream)))
+
+    def trace_any(self, rays_d, hit_prim_d, options=None, stream=None):
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_trace_any_device(self.handle, rays_d.data_ptr(), rays_d.shape[0], hit_prim_d.data_ptr(),
+                                             opt, _stream_handle(stream)))
+
+    def autotune(self, rays_d, any_hit=False, stream=None):
+        best = F.TraceOptions()
+        ms = C.c_float(0.0)
+        F.check(F.lib().gzg_scene_autotune(self.handle, rays_d.data_ptr(), rays_d.shape[0], 1 if any_hit else 0,
+                                           C.byref(best), C.byref(ms), _stream_handle(stream)))
+        return {k: getattr(best, k) for k in ("block_size", "blocks_per_sm", "stack_depth", "l1_carveout")}, ms.value
+
+
 class Renderer:
     """A wavefront renderer bound to one scene (gzg_renderer_*); renders into
     caller-owned device films (torch CUDA tensors)."""

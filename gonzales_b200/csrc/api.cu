@@ -109,6 +109,9 @@ struct gzg_scene {
         std::vector<void *> allocs;
         gzg_scene_info info{};
         TunedLaunch tuned_closest, tuned_any;
+        WideBvh host_wide;          // host copy of the wide tree (two-level assembly)
+        float root_bounds[6] = {0, 0, 0, 0, 0, 0};
+        bool instanced = false;
         std::mutex pool_mu;
         std::vector<std::unique_ptr<Staging>> pool;
 
@@ -175,6 +178,7 @@ LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o, bool any
         p.wide_depth = s->info.wide_depth;
         p.counters = o ? reinterpret_cast<unsigned long long *>(o->fetch_counters) : nullptr;
         p.n_dev = nullptr;
+        p.inst_out = nullptr;
         return p;
 }
 
@@ -208,6 +212,9 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
                       size_t out_bytes, int out_fmt, const gzg_trace_options *opt) {
         if (!s || count < 0 || (count > 0 && (!rays || !tmax || !results)))
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "batch call: null pointer or negative count");
+        if (s->instanced)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "batch call: two-level scenes take the device calls (gzg_trace_*_device)");
         gzg_status st = check_options(opt);
         if (st != GZG_OK) return st;
         if (count == 0) return clear_error();
@@ -478,6 +485,11 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         if (st != GZG_OK) return st;
         d.mesh_sizes = ms;
         d.mesh_count = mesh_count;
+        for (int a = 0; a < 3; ++a) {
+                scene->root_bounds[a] = bvh2_nodes[0].bounds_min[a];
+                scene->root_bounds[3 + a] = bvh2_nodes[0].bounds_max[a];
+        }
+        scene->host_wide = std::move(wide);
         *out_scene = scene.release();
         return clear_error();
 }
@@ -548,10 +560,6 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
         TunedLaunch cur;
         float cur_ms = 0;
         status = time_config(cur, &cur_ms);
-        const int carves[] = {1, 25, 50, 75, 100};
-        const int bps[] = {2, 3, 4, 5, 6, 7, 8};
-        const int blocks[] = {64, 256};
-        const int stacks[] = {16, 32};
         auto try_set = [&](TunedLaunch cand) {
                 if (status) return;
                 float ms = 0;
@@ -561,25 +569,26 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
                         cur_ms = ms;
                 }
         };
-        for (int c : carves) {
-                TunedLaunch t = cur;
-                t.l1_carveout = c;
-                try_set(t);
-        }
-        for (int b : bps) {
-                TunedLaunch t = cur;
-                t.blocks_per_sm = b;
-                try_set(t);
-        }
+        // Joint grid over the coupled knobs (shared stack size, resident
+        // blocks, L1/shared split), then block size around the winner.
+        const int stacks[] = {0, 16};
+        const int bps[] = {0, 4, 5, 6, 7, 8};
+        const int carves[] = {-1, 25, 50};
+        for (int sd : stacks)
+                for (int b : bps)
+                        for (int c : carves) {
+                                TunedLaunch t;
+                                t.stack_depth = sd;
+                                t.blocks_per_sm = b;
+                                t.l1_carveout = c;
+                                try_set(t);
+                        }
+        const int blocks[] = {64, 256};
+        const TunedLaunch base = cur;
         for (int bs : blocks) {
-                TunedLaunch t = cur;
+                TunedLaunch t = base;
                 t.block_size = bs;
-                t.blocks_per_sm = cur.blocks_per_sm ? std::max(1, cur.blocks_per_sm * 128 / bs) : 0;
-                try_set(t);
-        }
-        for (int s : stacks) {
-                TunedLaunch t = cur;
-                t.stack_depth = s;
+                t.blocks_per_sm = base.blocks_per_sm ? std::max(1, base.blocks_per_sm * 128 / bs) : 0;
                 try_set(t);
         }
         cudaEventDestroy(e0);
@@ -597,6 +606,167 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
                 best->l1_carveout = cur.l1_carveout;
         }
         if (best_ms) *best_ms = cur_ms;
+        return clear_error();
+}
+
+// transform * bound (Geometry/Bounds3.swift:61-69): the eight corners in the
+// order of Bounds3.points (:31-42) through Transform*Point, the first two
+// through Bounds3(first:second:), the rest through add(point:).
+static void instance_world_bounds(const float *lo_hi, const float *m, float *out6) {
+        float c[8][3];
+        for (int i = 0; i < 8; ++i) {
+                const float x = (i & 4) ? lo_hi[3] : lo_hi[0];
+                const float y = (i & 2) ? lo_hi[4] : lo_hi[1];
+                const float z = (i & 1) ? lo_hi[5] : lo_hi[2];
+                for (int r = 0; r < 3; ++r) {
+                        const float *row = m + 4 * r;
+                        float v = row[0] * x;
+                        v = v + row[1] * y;
+                        v = v + row[2] * z;
+                        c[i][r] = v + row[3];
+                }
+        }
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+                lo[a] = c[1][a] < c[0][a] ? c[1][a] : c[0][a];
+                hi[a] = c[1][a] >= c[0][a] ? c[1][a] : c[0][a];
+        }
+        for (int i = 2; i < 8; ++i)
+                for (int a = 0; a < 3; ++a) {
+                        if (c[i][a] < lo[a]) lo[a] = c[i][a];
+                        if (c[i][a] > hi[a]) hi[a] = c[i][a];
+                }
+        std::memcpy(out6, lo, 12);
+        std::memcpy(out6 + 3, hi, 12);
+}
+
+GZG_API gzg_status gzg_host_instance_bounds(const float *blas_bounds6, int64_t blas_count, const gzg_instance *inst,
+                                            int64_t instance_count, float *bounds6) {
+        if (blas_count < 0 || instance_count < 0 || (instance_count > 0 && (!blas_bounds6 || !inst || !bounds6)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_host_instance_bounds: bad arguments");
+        for (int64_t k = 0; k < instance_count; ++k) {
+                if (inst[k].blas < 0 || inst[k].blas >= blas_count)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_host_instance_bounds: instance " + std::to_string(k) +
+                                                                       " references a missing bottom-level scene");
+                instance_world_bounds(blas_bounds6 + 6 * inst[k].blas, inst[k].object_to_world, bounds6 + 6 * k);
+        }
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t blas_count, const gzg_instance *inst,
+                                              int64_t instance_count, const gzg_bvh2_node *tlas_nodes,
+                                              int64_t tlas_node_count, const int64_t *tlas_leaf_instance,
+                                              int64_t tlas_leaf_count, gzg_scene **out_scene) {
+        if (!out_scene) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_instanced_scene_create: out_scene is NULL");
+        *out_scene = nullptr;
+        if (blas_count <= 0 || !blas || instance_count <= 0 || !inst || tlas_node_count <= 0 || !tlas_nodes ||
+            tlas_leaf_count < 0 || (tlas_leaf_count > 0 && !tlas_leaf_instance))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_instanced_scene_create: bad arguments");
+        int device = -1;
+        std::vector<float> blas_bounds((size_t)blas_count * 6);
+        for (int64_t b = 0; b < blas_count; ++b) {
+                if (!blas[b] || blas[b]->instanced)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         "gzg_instanced_scene_create: bottom-level scene " + std::to_string(b) + " is NULL or two-level");
+                if (device >= 0 && blas[b]->device != device)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_instanced_scene_create: scenes on different devices");
+                device = blas[b]->device;
+                std::memcpy(&blas_bounds[6 * b], blas[b]->root_bounds, 24);
+        }
+        std::vector<float> ib((size_t)instance_count * 6);
+        gzg_status st = gzg_host_instance_bounds(blas_bounds.data(), blas_count, inst, instance_count, ib.data());
+        if (st) return st;
+        WideBvh tlas;
+        int32_t tlas_bvh2_depth = 0;
+        st = build_wide_tlas(tlas_nodes, tlas_node_count, tlas_leaf_instance, tlas_leaf_count, ib.data(), instance_count,
+                             &tlas, &tlas_bvh2_depth);
+        if (st) return st;
+
+        // One node array and one leaf-record array: top level first, then each
+        // bottom-level tree with its child and leaf bases moved by its offsets.
+        std::vector<WideNode> nodes = tlas.nodes;
+        std::vector<float4_> v0 = tlas.v0, v1 = tlas.v1, v2 = tlas.v2;
+        std::vector<uint32_t> root(blas_count);
+        int32_t max_blas_depth = 0;
+        for (int64_t b = 0; b < blas_count; ++b) {
+                const WideBvh &w = blas[b]->host_wide;
+                const uint32_t noff = (uint32_t)nodes.size(), toff = (uint32_t)v0.size();
+                root[b] = noff;
+                for (WideNode n : w.nodes) {
+                        n.child_base += noff;
+                        n.tri_base += toff;
+                        nodes.push_back(n);
+                }
+                v0.insert(v0.end(), w.v0.begin(), w.v0.end());
+                v1.insert(v1.end(), w.v1.begin(), w.v1.end());
+                v2.insert(v2.end(), w.v2.begin(), w.v2.end());
+                max_blas_depth = std::max(max_blas_depth, w.depth);
+        }
+        if (nodes.size() >= 0x7FFFFFFFu || v0.size() >= 0x7FFFFFFFu)
+                return set_error(GZG_ERR_LIMIT, "gzg_instanced_scene_create: more than 2^31 nodes or leaf records");
+        std::vector<float4_> table((size_t)instance_count * 4);
+        uint64_t steps = tlas.nodes.size();
+        for (int64_t k = 0; k < instance_count; ++k) {
+                const float *m = inst[k].world_to_object;
+                for (int r = 0; r < 3; ++r) table[4 * k + r] = float4_{m[4 * r], m[4 * r + 1], m[4 * r + 2], m[4 * r + 3]};
+                float rf, bf;
+                const int32_t rb = (int32_t)root[inst[k].blas], bb = inst[k].blas;
+                std::memcpy(&rf, &rb, 4);
+                std::memcpy(&bf, &bb, 4);
+                table[4 * k + 3] = float4_{rf, bf, 0.0f, 0.0f};
+                steps += blas[inst[k].blas]->host_wide.nodes.size();
+        }
+
+        auto scene = std::make_unique<gzg_scene>();
+        scene->device = device;
+        scene->instanced = true;
+        DeviceGuard g(device);
+        DevScene &d = scene->dev;
+        const uint4 *wn;
+        st = scene->upload(reinterpret_cast<const uint4 *>(nodes.data()), nodes.size() * 5, &wn, "wide nodes");
+        if (st) return st;
+        d.wide = wn;
+        const float4 *f;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(v0.data()), v0.size(), &f, "leaf records"))) return st;
+        d.tv0 = f;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(v1.data()), v1.size(), &f, "leaf records"))) return st;
+        d.tv1 = f;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(v2.data()), v2.size(), &f, "leaf records"))) return st;
+        d.tv2 = f;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(table.data()), table.size(), &f, "instance table")))
+                return st;
+        d.instances = f;
+        d.instance_count = instance_count;
+        const uint32_t zero = 0;
+        const uint32_t *ew;
+        if ((st = scene->upload(&zero, 1, &ew, "error word"))) return st;
+        d.err = const_cast<uint32_t *>(ew);
+        d.wide_count = (uint32_t)std::min<uint64_t>(steps, 0xFFFFFFFFull);
+        scene->info.wide_nodes = (int64_t)nodes.size();
+        scene->info.triangles = (int64_t)(v0.size() - tlas.v0.size());
+        scene->info.prims = instance_count;
+        scene->info.bvh2_nodes = tlas_node_count;
+        scene->info.bvh2_depth = tlas_bvh2_depth;
+        scene->info.wide_depth = tlas.depth + max_blas_depth + 2;
+        *out_scene = scene.release();
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_trace_closest_instanced_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
+                                                      gzg_hit_d *hits, int32_t *instance,
+                                                      const gzg_trace_options *options, void *stream) {
+        if (!scene || count < 0 || (count > 0 && (!rays || !hits || !instance)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_trace_closest_instanced_device: bad arguments");
+        if (!scene->instanced)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_trace_closest_instanced_device: not a two-level scene");
+        gzg_status st = check_options(options);
+        if (st != GZG_OK) return st;
+        DeviceGuard g(scene->device);
+        LaunchParams p = params_for(scene, options, false);
+        p.inst_out = instance;
+        GZG_CK(launch_trace(scene->dev, p, kRayDevice, kOutHit, rays, nullptr, count, hits,
+                            reinterpret_cast<cudaStream_t>(stream)),
+               "gzg_trace_closest_instanced_device launch");
         return clear_error();
 }
 

@@ -39,6 +39,11 @@ struct DevScene {
         const gzg_triangle_mesh *meshes;
         const int64_t *mesh_sizes;     // per mesh: point floats, vertex indices
         int64_t mesh_count;
+        // two-level scenes: per instance 4 x float4 (world_to_object rows,
+        // then bottom-level root node index and scene index as int bits)
+        const float4 *instances;
+        int64_t instance_count;
+        int32_t *inst_out;             // per-launch output of hit instances (optional)
 };
 
 // The launch's ray count: the device-side count when one is given.

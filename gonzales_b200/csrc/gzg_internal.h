@@ -67,6 +67,13 @@ gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const 
 #define GZG_HOST_DEVICE
 #endif
 
+// Converts a top-level BVH2 whose leaf prim k is instance leaf_instance[k]
+// (world bounds in inst_bounds, 6 floats per instance) into the wide layout;
+// its leaf records are instance entries (v0.w = -(instance + 1)).
+gzg_status build_wide_tlas(const gzg_bvh2_node *nodes, int64_t node_count, const int64_t *leaf_instance,
+                           int64_t leaf_count, const float *inst_bounds, int64_t inst_count, WideBvh *out,
+                           int32_t *bvh2_depth);
+
 // Decodes PrimId_C to (mesh, first vertex-index slot) as kernel.mojo:270-279;
 // returns false for prims the reference never intersects.
 GZG_HOST_DEVICE inline bool prim_triangle(const gzg_prim_id &p, int64_t *mesh, int64_t *base) {

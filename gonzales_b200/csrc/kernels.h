@@ -18,6 +18,7 @@ struct LaunchParams {
         int l1_carveout;    // preferred shared-memory carveout percent; <= 0 = driver default
         unsigned long long *counters;  // optional fetch counters (device)
         const uint32_t *n_dev;         // optional device-side ray count; n is then the capacity
+        int32_t *inst_out;             // two-level scenes: hit instance per ray (optional)
 };
 
 // ray_fmt: RayFormat; out_fmt: OutFormat.  Asynchronous on `st`.

@@ -338,6 +338,215 @@ __global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void 
         add_counters(s, n_nodes, n_tris, n_rays);
 }
 
+__device__ __forceinline__ void set_ray_dirs(WideRay &r) {
+        r.rdx = __fdiv_rn(1.0f, r.dx);
+        r.rdy = __fdiv_rn(1.0f, r.dy);
+        r.rdz = __fdiv_rn(1.0f, r.dz);
+        r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
+                ((__float_as_uint(r.rdz) >> 31) << 2);
+}
+
+// Transform*Point / Transform*Vector of Geometry/Transform.swift:31-65 with a
+// 3x4 affine matrix (w = 1, so the division is exact and omitted), each product
+// and sum rounded separately in the reference's order.
+__device__ __forceinline__ float xf_point(const float4 &row, float x, float y, float z) {
+        return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(row.x, x), __fmul_rn(row.y, y)), __fmul_rn(row.z, z)), row.w);
+}
+__device__ __forceinline__ float xf_vector(const float4 &row, float x, float y, float z) {
+        return __fadd_rn(__fadd_rn(__fmul_rn(row.x, x), __fmul_rn(row.y, y)), __fmul_rn(row.z, z));
+}
+
+// Two-level persistent traversal (TransformedPrimitive.intersect,
+// Primitive/TransformedPrimitive.swift:5-22).  The top-level tree's leaf
+// records are instances (v0.w = -(instance + 1)); reaching one pushes, in this
+// order, the rest of the current node's children, the rest of its leaf
+// records (0x80000000 | base, mask) and a return marker (0xFFFFFFFF), moves the
+// ray to object space and descends into the bottom-level root.  Popping the
+// marker restores the world ray.  Bottom-level trees are ordinary wide trees
+// stored after the top-level nodes in the same arrays.
+template <int OUTFMT, bool ANY, int STACK>
+__global__ void __launch_bounds__(256) k_wide_instanced(DevScene s, const void *__restrict__ rays,
+                                                        const float *__restrict__ tmaxs, int64_t n,
+                                                        void *__restrict__ out) {
+        extern __shared__ uint2 smem_stack[];
+        const unsigned FULL = 0xFFFFFFFFu;
+        n = ray_count(s, n);
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned lt_mask = (1u << lane) - 1u;
+        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+        int64_t chunk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        int64_t cursor = chunk * 32;
+        int64_t chunk_end = cursor + 32 < n ? cursor + 32 : n;
+
+        uint2 *stack = smem_stack + threadIdx.x;
+        const int stride = blockDim.x;
+        int64_t ray_i = -1;
+        WideRay r;
+        float wox = 0, woy = 0, woz = 0, wdx = 0, wdy = 0, wdz = 0;  // world ray
+        float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
+        int prim = -1, hit_inst = -1, cur_inst = -1, sp = 0;
+        uint2 group = make_uint2(0u, 0u);
+        uint32_t pend_base = 0, pend_mask = 0;
+        uint32_t steps = 0, n_nodes = 0, n_tris = 0, n_rays = 0;
+
+        for (;;) {
+                unsigned need = __ballot_sync(FULL, ray_i < 0);
+                while (need != 0u && cursor < n) {
+                        if (cursor >= chunk_end) {
+                                chunk += nwarps;
+                                cursor = chunk * 32;
+                                chunk_end = cursor + 32 < n ? cursor + 32 : n;
+                                if (cursor >= n) break;
+                        }
+                        const int avail = (int)(chunk_end - cursor);
+                        const int rank = __popc(need & lt_mask);
+                        if (ray_i < 0 && rank < avail) {
+                                ray_i = cursor + rank;
+                                const RayIn in = load_ray<kRayDevice>(rays, tmaxs, ray_i);
+                                wox = r.ox = in.ox;
+                                woy = r.oy = in.oy;
+                                woz = r.oz = in.oz;
+                                wdx = r.dx = in.dx;
+                                wdy = r.dy = in.dy;
+                                wdz = r.dz = in.dz;
+                                set_ray_dirs(r);
+                                tmax = thit = in.tmax;
+                                bu = bv = 0.0f;
+                                prim = hit_inst = cur_inst = -1;
+                                sp = 0;
+                                steps = 0;
+                                pend_mask = 0;
+                                group = make_uint2(0u, (1u << 24) | (1u << r.oct));
+                        }
+                        const int npop = __popc(need);
+                        cursor += npop < avail ? npop : avail;
+                        need = __ballot_sync(FULL, ray_i < 0);
+                }
+                if (__all_sync(FULL, ray_i < 0)) break;
+                if (ray_i < 0) continue;
+
+                bool finished = false, fault = false;
+                if (pend_mask == 0) {
+                        if ((group.y >> 24) == 0 && sp > 0) {
+                                --sp;
+                                const uint2 e = stack[sp * stride];
+                                if (e.x == 0xFFFFFFFFu) {
+                                        r.ox = wox;
+                                        r.oy = woy;
+                                        r.oz = woz;
+                                        r.dx = wdx;
+                                        r.dy = wdy;
+                                        r.dz = wdz;
+                                        set_ray_dirs(r);
+                                        cur_inst = -1;
+                                } else if (e.x & 0x80000000u) {
+                                        pend_base = e.x & 0x7FFFFFFFu;
+                                        pend_mask = e.y;
+                                } else {
+                                        group = e;
+                                }
+                        }
+                        uint32_t hits = group.y >> 24;
+                        if (pend_mask == 0 && hits) {
+                                const uint32_t key = __ffs(hits) - 1;
+                                hits &= hits - 1;
+                                const uint32_t im = group.y & 0xFFu;
+                                const uint32_t slot = key ^ r.oct;
+                                const uint32_t node = group.x + __popc(im & ((1u << slot) - 1u));
+                                if (hits) {
+                                        if (sp >= STACK) {
+                                                atomicOr(s.err, kErrStackOverflow);
+                                                fault = true;
+                                        } else {
+                                                stack[sp * stride] = make_uint2(group.x, (hits << 24) | im);
+                                                ++sp;
+                                        }
+                                }
+                                if (++steps > s.wide_count) {
+                                        atomicOr(s.err, kErrStepCap);
+                                        fault = true;
+                                }
+                                if (!fault) {
+                                        uint32_t nh, nim, cb;
+                                        open_node(s.wide + 5 * (size_t)node, r, thit, nh, nim, cb, pend_mask, pend_base);
+                                        ++n_nodes;
+                                        group = make_uint2(cb, (nh << 24) | nim);
+                                }
+                        }
+                }
+                while (!fault && pend_mask) {
+                        const uint32_t b = __ffs(pend_mask) - 1;
+                        pend_mask &= pend_mask - 1;
+                        const uint32_t ti = pend_base + b;
+                        const float4 a = __ldg(s.tv0 + ti);
+                        const int tag = __float_as_int(a.w);
+                        if (tag < 0) {
+                                // instance record: save the resume state and descend
+                                const int inst = -tag - 1;
+                                const int need_slots = ((group.y >> 24) ? 1 : 0) + (pend_mask ? 1 : 0) + 1;
+                                if (sp + need_slots > STACK || inst >= (int)s.instance_count) {
+                                        atomicOr(s.err, inst >= (int)s.instance_count ? kErrBadIndex : kErrStackOverflow);
+                                        fault = true;
+                                        break;
+                                }
+                                if (group.y >> 24) {
+                                        stack[sp * stride] = group;
+                                        ++sp;
+                                        group.y = 0u;
+                                }
+                                if (pend_mask) {
+                                        stack[sp * stride] = make_uint2(0x80000000u | pend_base, pend_mask);
+                                        ++sp;
+                                        pend_mask = 0;
+                                }
+                                stack[sp * stride] = make_uint2(0xFFFFFFFFu, 0u);
+                                ++sp;
+                                const float4 m0 = __ldg(s.instances + 4 * inst), m1 = __ldg(s.instances + 4 * inst + 1),
+                                             m2 = __ldg(s.instances + 4 * inst + 2), m3 = __ldg(s.instances + 4 * inst + 3);
+                                r.ox = xf_point(m0, wox, woy, woz);
+                                r.oy = xf_point(m1, wox, woy, woz);
+                                r.oz = xf_point(m2, wox, woy, woz);
+                                r.dx = xf_vector(m0, wdx, wdy, wdz);
+                                r.dy = xf_vector(m1, wdx, wdy, wdz);
+                                r.dz = xf_vector(m2, wdx, wdy, wdz);
+                                set_ray_dirs(r);
+                                cur_inst = inst;
+                                group = make_uint2((uint32_t)__float_as_int(m3.x), (1u << 24) | (1u << r.oct));
+                                break;
+                        }
+                        ++n_tris;
+                        const float4 bb = __ldg(s.tv1 + ti);
+                        const float4 c = __ldg(s.tv2 + ti);
+                        float t, u, v;
+                        if (mt_test(r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, a, bb, c, thit, t, u, v)) {
+                                thit = t;
+                                bu = u;
+                                bv = v;
+                                prim = tag;
+                                hit_inst = cur_inst;
+                                if (ANY) {
+                                        finished = true;
+                                        break;
+                                }
+                        }
+                }
+                if (fault || (!finished && pend_mask == 0 && (group.y >> 24) == 0 && sp == 0)) finished = true;
+                if (finished) {
+                        if (prim < 0) {
+                                thit = tmax;
+                                bu = 0.0f;
+                                bv = 0.0f;
+                                hit_inst = -1;
+                        }
+                        store_hit<OUTFMT>(s, out, ray_i, prim, thit, bu, bv);
+                        if (s.inst_out) s.inst_out[ray_i] = hit_inst;
+                        ray_i = -1;
+                        ++n_rays;
+                }
+        }
+        add_counters(s, n_nodes, n_tris, n_rays);
+}
+
 // The reference's slab test (kernel.mojo:171-206), separately rounded.
 __device__ __forceinline__ bool ref_aabb(const float4 &lo, const float4 &hi, const float rd[3], const float ord[3],
                                          const bool nm[3], float tmax, float &tnear_out) {
@@ -553,6 +762,28 @@ cudaError_t launch_trace(const DevScene &scene, const LaunchParams &p, int ray_f
         DevScene s = scene;
         s.counters = p.counters;
         s.n_dev = p.n_dev;
+        s.inst_out = p.inst_out;
+        if (s.instances) {
+                // two-level scenes: persistent wide traversal only
+                if (ray_fmt != kRayDevice || (out_fmt != kOutHit && out_fmt != kOutAnyPrim)) return cudaErrorNotSupported;
+                const int need = p.wide_depth > 1 ? p.wide_depth : 1;
+                const int want = p.stack_depth > need ? p.stack_depth : need;
+                LaunchParams q = p;
+                q.traversal = GZG_TRAVERSAL_WIDE;
+                TraceKernel k;
+                int stack;
+                if (want <= 16) {
+                        stack = 16;
+                        k = out_fmt == kOutHit ? k_wide_instanced<kOutHit, false, 16> : k_wide_instanced<kOutAnyPrim, true, 16>;
+                } else if (want <= 32) {
+                        stack = 32;
+                        k = out_fmt == kOutHit ? k_wide_instanced<kOutHit, false, 32> : k_wide_instanced<kOutAnyPrim, true, 32>;
+                } else {
+                        stack = 64;
+                        k = out_fmt == kOutHit ? k_wide_instanced<kOutHit, false, 64> : k_wide_instanced<kOutAnyPrim, true, 64>;
+                }
+                return launch_wide_kernel(k, stack, true, q, s, rays, tmax, n, out, st);
+        }
         if (ray_fmt == kRayDevice) {
                 switch (out_fmt) {
                 case kOutHit: return launch_fmt<kRayDevice, kOutHit, false>(s, p, rays, tmax, n, out, st);

@@ -38,8 +38,11 @@ struct BinNode {
         }
 };
 
+// A leaf entry: a triangle (prim >= 0, the prim index) or, in a top-level
+// tree, an instance (prim = -(instance + 1), vertices unused).
 struct Tri {
         float p0[3], p1[3], p2[3];
+        float lo[3], hi[3];
         int32_t prim;
 };
 
@@ -50,6 +53,14 @@ class Converter {
                   const int64_t *vi_counts)
             : nodes_(nodes), node_count_(node_count), prims_(prims), prim_count_(prim_count), meshes_(meshes),
               mesh_count_(mesh_count), pts_counts_(pts_counts), vi_counts_(vi_counts) {}
+
+        // Top-level mode: leaf prim k of the BVH2 is instance leaf_instance[k]
+        // with world bounds inst_bounds[6 * instance ...].
+        Converter(const gzg_bvh2_node *nodes, int64_t node_count, const int64_t *leaf_instance, int64_t leaf_count,
+                  const float *inst_bounds, int64_t inst_count)
+            : nodes_(nodes), node_count_(node_count), prims_(nullptr), prim_count_(leaf_count), meshes_(nullptr),
+              mesh_count_(0), pts_counts_(nullptr), vi_counts_(nullptr), leaf_instance_(leaf_instance),
+              inst_bounds_(inst_bounds), inst_count_(inst_count) {}
 
         gzg_status run(WideBvh *out, int32_t *bvh2_depth) {
                 gzg_status st = lift(bvh2_depth);
@@ -67,6 +78,9 @@ class Converter {
         int64_t mesh_count_;
         const int64_t *pts_counts_;
         const int64_t *vi_counts_;
+        const int64_t *leaf_instance_ = nullptr;
+        const float *inst_bounds_ = nullptr;
+        int64_t inst_count_ = 0;
 
         std::vector<BinNode> bin_;
         std::vector<Tri> tris_;
@@ -76,6 +90,21 @@ class Converter {
 
         // Reads prim k's triangle into tris_ (if it is one).  Returns false on a bad index.
         bool read_prim(int64_t k, bool *is_tri, std::string *why) {
+                if (leaf_instance_) {
+                        const int64_t inst = leaf_instance_[k];
+                        if (inst < 0 || inst >= inst_count_) {
+                                *why = "top-level leaf " + std::to_string(k) + " references instance " + std::to_string(inst);
+                                return false;
+                        }
+                        Tri t;
+                        std::memset(&t, 0, sizeof(t));
+                        std::memcpy(t.lo, inst_bounds_ + 6 * inst, 12);
+                        std::memcpy(t.hi, inst_bounds_ + 6 * inst + 3, 12);
+                        t.prim = -(int32_t)(inst + 1);
+                        tris_.push_back(t);
+                        *is_tri = true;
+                        return true;
+                }
                 int64_t mesh, base;
                 *is_tri = prim_triangle(prims_[k], &mesh, &base);
                 if (!*is_tri) return true;
@@ -99,6 +128,10 @@ class Converter {
                         dst[c][0] = m.points[v * 4 + 0];
                         dst[c][1] = m.points[v * 4 + 1];
                         dst[c][2] = m.points[v * 4 + 2];
+                }
+                for (int a = 0; a < 3; ++a) {
+                        t.lo[a] = std::min({t.p0[a], t.p1[a], t.p2[a]});
+                        t.hi[a] = std::max({t.p0[a], t.p1[a], t.p2[a]});
                 }
                 t.prim = (int32_t)k;
                 tris_.push_back(t);
@@ -124,8 +157,8 @@ class Converter {
                         for (int64_t i = first; i < first + count; ++i) {
                                 const Tri &t = tris_[i];
                                 for (int a = 0; a < 3; ++a) {
-                                        lo[a] = std::min({lo[a], t.p0[a], t.p1[a], t.p2[a]});
-                                        hi[a] = std::max({hi[a], t.p0[a], t.p1[a], t.p2[a]});
+                                        lo[a] = std::min(lo[a], t.lo[a]);
+                                        hi[a] = std::max(hi[a], t.hi[a]);
                                 }
                         }
                         int32_t id = new_bin(lo, hi);
@@ -406,6 +439,13 @@ gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const 
                           const int64_t *points_counts, const int64_t *vertex_index_counts, WideBvh *out,
                           int32_t *bvh2_depth) {
         Converter c(nodes, node_count, prims, prim_count, meshes, mesh_count, points_counts, vertex_index_counts);
+        return c.run(out, bvh2_depth);
+}
+
+gzg_status build_wide_tlas(const gzg_bvh2_node *nodes, int64_t node_count, const int64_t *leaf_instance,
+                           int64_t leaf_count, const float *inst_bounds, int64_t inst_count, WideBvh *out,
+                           int32_t *bvh2_depth) {
+        Converter c(nodes, node_count, leaf_instance, leaf_count, inst_bounds, inst_count);
         return c.run(out, bvh2_depth);
 }
 

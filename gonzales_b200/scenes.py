@@ -170,6 +170,81 @@ def raycast_rays(host_scene, n_coherent_w, n_coherent_h, n_incoherent, seed=0xC1
     return o, d, t
 
 
+# ---------------------------------------------------------------- instanced scene
+
+
+def grid_mesh(kind, n_u, n_v, seed, amplitude=0.05):
+    """A displaced tube (open cylinder, radius 0.3, height 1) or lat-long sphere
+    (radius 0.5) with n_u x n_v quads (2 * n_u * n_v triangles)."""
+    u = np.arange(n_u) / n_u * 2 * math.pi
+    if kind == "tube":
+        v = np.linspace(-0.5, 0.5, n_v + 1)
+        uu, vv = np.meshgrid(u, v, indexing="ij")
+        p = np.stack([0.3 * np.cos(uu), vv, 0.3 * np.sin(uu)], -1).reshape(-1, 3)
+        normal = np.stack([np.cos(uu), np.zeros_like(uu), np.sin(uu)], -1).reshape(-1, 3)
+    else:
+        v = np.linspace(0.02, math.pi - 0.02, n_v + 1)
+        uu, vv = np.meshgrid(u, v, indexing="ij")
+        normal = np.stack([np.sin(vv) * np.cos(uu), np.cos(vv), np.sin(vv) * np.sin(uu)], -1).reshape(-1, 3)
+        p = 0.5 * normal
+    p = p + normal * (amplitude * value_noise(p * 2.0, seed))[:, None]
+    i = np.arange(n_u)[:, None]
+    j = np.arange(n_v)[None, :]
+    a = i * (n_v + 1) + j
+    b = ((i + 1) % n_u) * (n_v + 1) + j
+    tris = np.stack([np.stack([a, b, a + 1], -1), np.stack([b, b + 1, a + 1], -1)], 2).reshape(-1, 3)
+    return p.astype(np.float32), tris.astype(np.int64)
+
+
+def random_instances(n, n_blas, seed, extent=20.0):
+    """Instances with seeded affine transforms: uniform random rotation, uniform
+    scale in [0.5, 2], translation uniform in [-extent, extent]^3."""
+    from ._ffi import INSTANCE_DTYPE
+
+    rng = np.random.default_rng(seed)
+    inst = np.zeros(n, INSTANCE_DTYPE)
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+    s = rng.uniform(0.5, 2.0, n)
+    t = rng.uniform(-extent, extent, (n, 3))
+    M = np.zeros((n, 4, 4))
+    M[:, :3, :3] = R * s[:, None, None]
+    M[:, :3, 3] = t
+    M[:, 3, 3] = 1.0
+    Minv = np.linalg.inv(M)
+    inst["object_to_world"] = M[:, :3, :].reshape(n, 12).astype(np.float32)
+    inst["world_to_object"] = Minv[:, :3, :].reshape(n, 12).astype(np.float32)
+    inst["blas"] = rng.integers(0, n_blas, n)
+    return inst
+
+
+def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0):
+    """Bottom-level scenes (one mesh each: tubes and spheres alternating) and
+    instances; 2 * n_u * n_v triangles per mesh (50,000 at the defaults)."""
+    blas = []
+    for k in range(n_meshes):
+        pts, tris = grid_mesh("tube" if k % 2 == 0 else "sphere", n_u, n_v, seed + k)
+        sb = SceneBuilder()
+        sb.add_mesh(pts, tris, sb.add_material((0.5, 0.5, 0.5)))
+        blas.append(sb.build())
+    return blas, random_instances(n_instances, n_meshes, seed, extent)
+
+
+def instanced_rays(n, extent, seed):
+    """Rays through the instance field: origins uniform in a box 1.2x the
+    instance extent, directions uniform on the sphere, tMax = infinity."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(-1.2 * extent, 1.2 * extent, (n, 3))
+    d = _normalize(rng.normal(size=(n, 3)))
+    return o.astype(np.float32), d.astype(np.float32), np.full(n, np.inf, np.float32)
+
+
 # ---------------------------------------------------------------- box scene
 
 

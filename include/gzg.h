@@ -273,6 +273,48 @@ GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays,
                                         int32_t *hit_prim, const gzg_trace_options *options,
                                         void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Two-level scenes (TransformedPrimitive, Primitive/TransformedPrimitive.swift:5-57) */
+/* ------------------------------------------------------------------------- */
+
+/* An instance of a bottom-level scene.  Matrices are row-major 3x4 affine
+ * transforms (the top three rows of the reference's 4x4 Transform); the ray is
+ * taken to object space as world_to_object * ray (Core/Transform+Ray.swift,
+ * Geometry/Transform.swift:31-65) without renormalising the direction, so the
+ * ray parameter t is shared between levels. */
+typedef struct gzg_instance {
+        float object_to_world[12];
+        float world_to_object[12];
+        int32_t blas;  /* index into the bottom-level scene list */
+        int32_t pad_;
+} gzg_instance;
+
+/* World bounds of each instance: the 8 corners of its bottom-level root box
+ * (blas_bounds6: minx..maxz per bottom-level scene) through object_to_world
+ * (Bounds3.swift:61-69), for building the top-level BVH on the host. */
+GZG_API gzg_status gzg_host_instance_bounds(const float *blas_bounds6, int64_t blas_count,
+                                            const gzg_instance *instances, int64_t instance_count,
+                                            float *bounds6);
+
+/* Creates a two-level scene from uploaded bottom-level scenes (each from
+ * gzg_gpu_upload_scene; they stay owned by the caller and must outlive the
+ * new scene), the instances, and a top-level BVH2 the host built over the
+ * instance bounds (leaf prim k is instance tlas_leaf_instance[k]).  Only the
+ * wide traversal runs on a two-level scene; hits report the bottom-level prim
+ * index and, through gzg_trace_closest_instanced_device, the instance. */
+GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t blas_count,
+                                              const gzg_instance *instances, int64_t instance_count,
+                                              const gzg_bvh2_node *tlas_nodes, int64_t tlas_node_count,
+                                              const int64_t *tlas_leaf_instance, int64_t tlas_leaf_count,
+                                              gzg_scene **out_scene);
+
+/* Closest hit on a two-level scene: hits as gzg_trace_closest_device (prim =
+ * index into the hit instance's bottom-level prim array) and instance[i] =
+ * the hit instance or -1. */
+GZG_API gzg_status gzg_trace_closest_instanced_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
+                                                      gzg_hit_d *hits, int32_t *instance,
+                                                      const gzg_trace_options *options, void *stream);
+
 /* Launch autotuner: times the persistent wide kernel on the caller's DEVICE
  * rays over L1 carveout, blocks per SM, block size and stack depth
  * (coordinate descent, CUDA events on `stream`), keeps the fastest as the

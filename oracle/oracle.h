@@ -127,6 +127,25 @@ typedef struct orc_path_state {
 void orc_shade_batch(orc_path_state *paths, int64_t n, const orc_isect *isects, const orc_mesh *meshes,
                      const orc_material *materials);
 
+/* --- two-level scenes --------------------------------------------------- */
+
+typedef struct orc_blas {
+        const orc_node *nodes;
+        const orc_prim_id *prims;
+        const orc_mesh *meshes;
+} orc_blas;
+
+/* Closest hit through a top-level BVH2 whose leaf prim k is instance
+ * leaf_instance[k]; instance i has world_to_object w2o[12 * i] (row-major
+ * 3x4) and bottom-level scene blas_of[i].  Restates TransformedPrimitive.
+ * intersect (Primitive/TransformedPrimitive.swift:5-22): ray = inverse * ray
+ * (Core/Transform+Ray.swift, Geometry/Transform.swift:31-65), bottom-level
+ * closest hit with the current tHit.  Outputs per ray: prim (bottom-level
+ * prim index or -1), instance (or -1), t (tMax on a miss), u, v. */
+void orc_traverse_instanced(const orc_node *tlas, const int64_t *leaf_instance, const float *w2o,
+                            const int32_t *blas_of, const orc_blas *blas, const orc_ray *rays, const float *tmax,
+                            int64_t n, int32_t *prim, int32_t *inst, float *t, float *u, float *v, int threads);
+
 /* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
 int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1,
                               const float *p2, float tmax, float *t, float *u, float *v);

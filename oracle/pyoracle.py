@@ -36,7 +36,7 @@ _lib = None
 
 
 def build():
-    src = [HERE / "oracle.cpp", HERE / "integrator.cpp", HERE / "shade.cpp", HERE / "oracle.h"]
+    src = list(HERE.glob("*.cpp")) + [HERE / "oracle.h", HERE / "Makefile"]
     if not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime for p in src):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -248,3 +248,47 @@ def shade_batch(hs, paths, isects):
     L.orc_shade_batch(_p(out), len(out), _p(np.ascontiguousarray(isects)), C.addressof(arr),
                       _p(np.ascontiguousarray(hs.materials)))
     return out
+
+
+class _Blas(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("prims", C.c_void_p), ("meshes", C.c_void_p)]
+
+
+def traverse_instanced(tlas_nodes, leaf_instance, w2o, blas_of, blas_scenes, rays6, tmax, threads=0):
+    """Two-level closest hit.  blas_scenes: HostScene list; w2o: (n_inst, 12)
+    float32; blas_of: (n_inst,) int32.  Returns prim, inst, t, u, v arrays."""
+    L = lib()
+    if not getattr(L, "_inst_bound", False):
+        L.orc_traverse_instanced.restype = None
+        L.orc_traverse_instanced.argtypes = [C.c_void_p] * 7 + [C.c_int64] + [C.c_void_p] * 5 + [C.c_int]
+        L._inst_bound = True
+    keep = []
+    blas = (_Blas * len(blas_scenes))()
+    for i, hs in enumerate(blas_scenes):
+        arr = (_Mesh * max(len(hs.meshes), 1))()
+        for k, m in enumerate(hs.meshes):
+            p4 = np.ascontiguousarray(m.points, np.float32)
+            vi = np.ascontiguousarray(m.vertex_indices, np.int64)
+            keep += [p4, vi]
+            arr[k] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+        nodes = np.ascontiguousarray(hs.nodes)
+        prims = np.ascontiguousarray(hs.prims)
+        keep += [arr, nodes, prims]
+        blas[i] = _Blas(nodes.ctypes.data, prims.ctypes.data, C.addressof(arr))
+    tlas_nodes = np.ascontiguousarray(tlas_nodes)
+    leaf_instance = np.ascontiguousarray(leaf_instance, np.int64)
+    w2o = np.ascontiguousarray(w2o, np.float32)
+    blas_of = np.ascontiguousarray(blas_of, np.int32)
+    rays6 = np.ascontiguousarray(rays6, np.float32).reshape(-1, 6)
+    tmax = np.ascontiguousarray(tmax, np.float32)
+    n = len(tmax)
+    prim = np.zeros(n, np.int32)
+    inst = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    u = np.zeros(n, np.float32)
+    v = np.zeros(n, np.float32)
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    L.orc_traverse_instanced(_p(tlas_nodes), _p(leaf_instance), _p(w2o), _p(blas_of), C.addressof(blas), _p(rays6),
+                             _p(tmax), n, _p(prim), _p(inst), _p(t), _p(u), _p(v), threads)
+    return prim, inst, t, u, v
