@@ -5,10 +5,10 @@ this package is its host-side mirror of the reference's Accelerator interface.
 There is no CPU fallback: without libgzg.so or a B200, calls raise GzgError.
 """
 from ._ffi import GzgError, LEAF_MOLLER_TRUMBORE, LEAF_WATERTIGHT, TRAVERSAL_BVH2, TRAVERSAL_WIDE, options
-from .accel import GpuAccelerator, InstancedAccelerator, Renderer, gpu_available, instance_bounds
+from .accel import BatchRenderer, GpuAccelerator, InstancedAccelerator, Renderer, gpu_available, instance_bounds
 from .scene import HostScene, SceneBuilder, build_bvh2, make_mesh, triangle_bounds
 
 __all__ = [
-    "GzgError", "GpuAccelerator", "HostScene", "Renderer", "SceneBuilder", "build_bvh2", "gpu_available", "make_mesh",
+    "BatchRenderer", "GzgError", "GpuAccelerator", "HostScene", "Renderer", "SceneBuilder", "build_bvh2", "gpu_available", "make_mesh",
     "options", "triangle_bounds", "LEAF_MOLLER_TRUMBORE", "LEAF_WATERTIGHT", "TRAVERSAL_BVH2", "TRAVERSAL_WIDE",
 ]

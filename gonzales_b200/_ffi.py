@@ -99,6 +99,19 @@ def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_correcte
                         first_sample, sampler_spp, wave_paths, use_graph)
 
 
+SORT_NONE, SORT_MATERIAL, SORT_SCENE = 0, 1, 2
+
+
+class TextureBinding(C.Structure):
+    _fields_ = [("material", C.c_int32), ("reserved", C.c_int32), ("origin", C.c_float * 3),
+                ("u_axis", C.c_float * 3), ("v_axis", C.c_float * 3)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("wave_paths", C.c_int32), ("use_graph", C.c_int32), ("sort_key", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 VP = C.c_void_p
 I64 = C.c_int64
 ST = C.c_int32
@@ -126,6 +139,13 @@ PROTOTYPES = {
     "gzg_renderer_destroy": (ST, [VP]),
     "gzg_renderer_render": (ST, [VP, VP, VP, VP, VP]),
     "gzg_renderer_stats": (ST, [VP, C.POINTER(RenderStats)]),
+    "gzg_batch_renderer_create": (ST, [VP, VP, I64, C.POINTER(BatchOptions), C.POINTER(VP)]),
+    "gzg_renderer_film_layout": (ST, [VP, VP]),
+    "gzg_renderer_autotune": (ST, [VP, C.POINTER(BatchOptions), C.POINTER(C.c_float), VP]),
+    "gzg_renderer_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int32]),
+    "gzg_renderer_set_textures": (ST, [VP, VP, C.c_int32, C.c_int32, VP, C.c_float]),
+    "gzg_renderer_render_f64": (ST, [VP, VP, VP, VP, VP]),
+    "gzg_renderer_adjoint": (ST, [VP, VP, VP, VP, VP, VP]),
     "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),
     "gzg_zsobol_fill_device": (ST, [I64, C.c_int32, C.c_int32, I64, VP, VP, VP, I64, VP, C.c_int32, VP, VP]),
     "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),

@@ -291,3 +291,53 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+
+class BatchRenderer(Renderer):
+    """One renderer over many scenes (gzg_batch_renderer_create).  Scene k's
+    image is the window film[offsets[k]:offsets[k+1]] of one batch film;
+    `split` cuts a batch film into per-scene (H, W, ...) views."""
+
+    def __init__(self, accels, params, wave_paths=0, use_graph=1, sort_key=F.SORT_NONE):
+        self.accels = list(accels)
+        self.params = list(params)
+        if len(self.accels) != len(self.params) or not self.accels:
+            raise ValueError("BatchRenderer: one params record per scene, at least one scene")
+        self.handle = C.c_void_p()
+        handles = (C.c_void_p * len(self.accels))(*[a.handle.value for a in self.accels])
+        prm = (F.RenderParams * len(self.params))(*self.params)
+        self.options = F.BatchOptions(wave_paths, use_graph, sort_key, 0)
+        h = C.c_void_p()
+        F.check(F.lib().gzg_batch_renderer_create(handles, prm, len(self.accels), C.byref(self.options),
+                                                  C.byref(h)))
+        self.handle = h
+        offs = (C.c_int64 * (len(self.accels) + 1))()
+        F.check(F.lib().gzg_renderer_film_layout(self.handle, offs))
+        self.offsets = list(offs)
+
+    @property
+    def pixels(self):
+        """Pixel count of the batch film."""
+        return self.offsets[-1]
+
+    def split(self, film):
+        """Per-scene (H, W, ...) views of a batch film (pixels first)."""
+        out = []
+        for k, p in enumerate(self.params):
+            part = film[self.offsets[k]:self.offsets[k + 1]]
+            out.append(part.reshape((p.height, p.width) + tuple(part.shape[1:])))
+        return out
+
+    def autotune(self, stream=None):
+        """Times renders over wave sizes and sort keys; keeps and returns the
+        fastest (options dict, ms per render)."""
+        best = F.BatchOptions()
+        ms = C.c_float()
+        F.check(F.lib().gzg_renderer_autotune(self.handle, C.byref(best), C.byref(ms), _stream_handle(stream)))
+        self.options = best
+        return {name: getattr(best, name) for name, _ in F.BatchOptions._fields_}, ms.value
+
+    def error_word(self, clear=True):
+        w = C.c_uint32()
+        F.check(F.lib().gzg_renderer_error_word(self.handle, C.byref(w), int(clear)))
+        return w.value

@@ -112,6 +112,8 @@ struct gzg_scene {
         WideBvh host_wide;          // host copy of the wide tree (two-level assembly)
         float root_bounds[6] = {0, 0, 0, 0, 0, 0};
         bool instanced = false;
+        // host copies of the shading arrays (batch assembly)
+        HostShading host_shading;
         std::mutex pool_mu;
         std::vector<std::unique_ptr<Staging>> pool;
 
@@ -490,6 +492,15 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
                 scene->root_bounds[3 + a] = bvh2_nodes[0].bounds_max[a];
         }
         scene->host_wide = std::move(wide);
+        HostShading &hsd = scene->host_shading;
+        hsd.pv0 = std::move(pv0);
+        hsd.pv1 = std::move(pv1);
+        hsd.pv2 = std::move(pv2);
+        hsd.prims.assign(prim_ids, prim_ids + prim_count);
+        hsd.materials = std::move(mats);
+        hsd.lights = std::move(lights);
+        hsd.light_cdf = std::move(cdf);
+        hsd.light_total = total;
         *out_scene = scene.release();
         return clear_error();
 }
@@ -835,5 +846,9 @@ void scene_view(const gzg_scene *scene, DevScene *view, int *device, int *wide_d
 namespace gzg {
 
 LaunchParams scene_launch(const gzg_scene *scene, bool any_hit) { return params_for(scene, nullptr, any_hit); }
+
+const WideBvh &scene_host_wide(const gzg_scene *scene) { return scene->host_wide; }
+const HostShading &scene_host_shading(const gzg_scene *scene) { return scene->host_shading; }
+bool scene_is_instanced(const gzg_scene *scene) { return scene->instanced; }
 
 }  // namespace gzg

@@ -44,6 +44,9 @@ struct DevScene {
         const float4 *instances;
         int64_t instance_count;
         int32_t *inst_out;             // per-launch output of hit instances (optional)
+        // batches of scenes: a device ray's spare lane (gzg_ray_d.pad_) holds
+        // the wide-node index its traversal starts at
+        int32_t per_ray_root;
 };
 
 // The launch's ray count: the device-side count when one is given.
@@ -163,6 +166,7 @@ enum RayFormat { kRayDevice = 0, kRayReference = 1 };
 
 struct RayIn {
         float ox, oy, oz, dx, dy, dz, tmax;
+        uint32_t root;  // device rays: bits of the spare lane (traversal root in batches)
 };
 
 template <int FMT>
@@ -178,6 +182,7 @@ __device__ __forceinline__ RayIn load_ray(const void *rays, const float *tmax, i
                 r.dx = b.x;
                 r.dy = b.y;
                 r.dz = b.z;
+                r.root = __float_as_uint(b.w);
         } else {
                 const float2 *p = reinterpret_cast<const float2 *>(reinterpret_cast<const char *>(rays) + 24 * i);
                 const float2 a = __ldcs(p), b = __ldcs(p + 1), c = __ldcs(p + 2);
@@ -188,6 +193,7 @@ __device__ __forceinline__ RayIn load_ray(const void *rays, const float *tmax, i
                 r.dy = c.x;
                 r.dz = c.y;
                 r.tmax = __ldcs(tmax + i);
+                r.root = 0u;
         }
         return r;
 }

@@ -54,6 +54,16 @@ struct WideBvh {
         int32_t depth = 0;
 };
 
+// Host copies of a scene's shading arrays, as uploaded (see DevScene).
+struct HostShading {
+        std::vector<float4_> pv0, pv1, pv2;  // triangles in prim order
+        std::vector<gzg_prim_id> prims;
+        std::vector<float4_> materials;      // 2 per material
+        std::vector<float4_> lights;         // 4 per light
+        std::vector<float> light_cdf;
+        float light_total = 0.0f;
+};
+
 // Converts a validated reference BVH2 + prims + meshes into the wide layout.
 // Returns GZG_OK or an error (with set_error called).
 gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const gzg_prim_id *prims,
@@ -66,6 +76,11 @@ gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const 
 #else
 #define GZG_HOST_DEVICE
 #endif
+
+// Host copies kept by an uploaded scene (batch assembly).
+const WideBvh &scene_host_wide(const gzg_scene *scene);
+const HostShading &scene_host_shading(const gzg_scene *scene);
+bool scene_is_instanced(const gzg_scene *scene);
 
 // Converts a top-level BVH2 whose leaf prim k is instance leaf_instance[k]
 // (world bounds in inst_bounds, 6 floats per instance) into the wide layout;

@@ -1,4 +1,5 @@
-// render.cu - the path integrator as a device-resident wavefront.
+// render.cu - the path integrator as a device-resident wavefront over a batch
+// of scenes.
 //
 // Gonzales runs its bounce loop on the host, one tile at a time, shipping rays
 // and path states to the plugin and back every bounce (Core/Tile.swift:66-209).
@@ -7,6 +8,7 @@
 //   generate   Z-Sobol camera sample, Gaussian filter sample, pinhole ray
 //   per bounce b = 0 .. max_depth-1:
 //     extend   closest hit of the extension queue (k_wide_persistent)
+//     [sort]   optional counting sort of the queue by material or scene
 //     shade    emission, light choice + light sample (-> shadow queue),
 //              MIS BSDF sample (-> probe queue, corrected MIS only),
 //              continuation sample, Russian roulette (-> next extension queue)
@@ -14,17 +16,27 @@
 //     probe    closest hit of the probe queue, then add emission it reaches
 //   accumulate film sums (radiance, its square, filter weight) with atomics
 //
-// Queue lengths live on the device; no stage waits for the host, so a whole
-// wave can be captured once as a CUDA graph and replayed.  The shading
-// arithmetic restates Integrator/VolumePathIntegrator.swift:67-463 and the
-// helpers it calls (same citations as the CPU oracle's integrator).  The
-// reference's last extension (bounce == max_depth) can only add environment
-// light to camera or specular paths; these scenes have neither, so it is not
-// traced.
+// A renderer serves a batch of scenes: each scene has its own camera, film
+// window, sampler, lights and BVH root in a per-scene constant table, every
+// path carries its scene index, and traversal starts at a per-ray root in one
+// concatenated node array.  A single scene is a batch of one that uses the
+// scene's own device arrays.  Queue lengths live on the device; no stage waits
+// for the host, so a whole wave can be captured as a CUDA graph and replayed.
+// The shading arithmetic restates Integrator/VolumePathIntegrator.swift:67-463
+// and the helpers it calls (same citations as the CPU oracle's integrator).
+// The reference's last extension (bounce == max_depth) can only add
+// environment light to camera or specular paths; these scenes have neither, so
+// it is not traced.
+//
+// Differentiable rendering: single-scene renderers may bind albedo textures
+// and an emission scale; gzg_renderer_adjoint replays each wave's paths
+// (primal pass, then replay with the same samples) and accumulates
+// dLoss/dtexel and dLoss/dscale.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -179,26 +191,42 @@ __device__ float gaussian(float x, float sigma) {
 
 // ------------------------------------------------------------ state
 
-struct RenderConst {
+// Per-scene constants of a batch.
+struct SceneConst {
         V3 eye, right, up, fwd;
         float tan_half, sx0, sx1, sy0, sy1;
-        int32_t width, height, spp, max_depth, rr_min, mis_corrected, first_sample;
         float filter_radius, filter_sigma;
+        int32_t width, height, spp, max_depth, rr_min, mis_corrected, first_sample;
+        int32_t light_begin, light_count;
+        float light_total;
+        int32_t material_begin;  // the scene's material 0 (area-light hits scatter with it)
+        int32_t material_count;
+        uint32_t root;            // wide-node root of the scene's tree
+        uint32_t film_offset;     // first pixel of the scene in the batch film
+        uint64_t path_begin;      // first batch-wide path index of the scene
         ZSobolConfig zs;
 };
 
 enum { kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4, kCountWords = 8 };
 enum { kStatCamera = 0, kStatExt = 1, kStatShadow = 2, kStatProbe = 3, kStatWaves = 4, kStatWords = 8 };
+enum SortKey { kSortNone = 0, kSortMaterial = 1, kSortScene = 2 };
+
+// kRender: film accumulation; kPrimal: keep each path's radiance in Ltot;
+// kReplay: path replay with gradients (Ltot from the primal pass of the wave).
+enum Mode { kRender = 0, kPrimal = 1, kReplay = 2 };
 
 struct Wave {
         uint32_t capacity;
         uint64_t total_paths;
+        const SceneConst *scenes;
+        int32_t scene_count;
         // path state, indexed by path slot in the wave
         uint64_t *zs_morton;
         int32_t *zs_dim;
         float4 *thr;
         float4 *L;
-        uint32_t *pixel;
+        uint32_t *pixel;  // batch film pixel
+        uint32_t *scene;
         float *weight;
         // queues
         float4 *q_ray[2];  // gzg_ray_d, 2 x float4 per entry
@@ -212,8 +240,25 @@ struct Wave {
         uint32_t *pr_id;
         float4 *pr_contrib;
         float4 *pr_hits;
-        uint32_t *counts;           // kCountWords words; wave base as 2 words at kCountWaveBase
+        // sort of the extension queue before shading
+        int32_t sort_key;
+        int32_t key_count;
+        uint32_t *key_hist;    // key_count counters, then key_count cursors
+        uint32_t *order;       // sorted entry order, capacity
+        uint32_t *counts;      // kCountWords words; wave base as 2 words at kCountWaveBase
         unsigned long long *stats;  // kStatWords
+        // differentiable rendering (single-scene renderers)
+        const float *tex;          // texels: count x tex_res x tex_res x 3 (row v, column u)
+        const int32_t *mat_tex;    // per material: texture index or -1 (null: no textures)
+        const float *tex_map;      // per texture: origin, u axis, v axis (9 floats)
+        int32_t tex_res;
+        float emission_scale;      // multiplies every emission
+        int32_t mode;              // Mode
+        float4 *Ltot;              // per path slot: radiance of the primal pass (replay input)
+        const float *adj_rgb;      // dLoss/dImage per film pixel (3 floats)
+        const float *adj_w;        // film weight sums per pixel (image = rgb / w)
+        float *d_tex;              // dLoss/dtexel (accumulated)
+        double *d_emission;        // dLoss/demission_scale (accumulated)
 };
 
 // Appends to a queue with one atomic per converged group of lanes.
@@ -227,9 +272,10 @@ __device__ __forceinline__ uint32_t queue_slot(uint32_t *count) {
         return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ void store_ray(float4 *q, uint32_t slot, V3 o, float tmax, V3 d) {
+// A queued ray; the spare lane carries the traversal root of the path's scene.
+__device__ __forceinline__ void store_ray(float4 *q, uint32_t slot, V3 o, float tmax, V3 d, uint32_t root) {
         q[2 * slot] = make_float4(o.x, o.y, o.z, tmax);
-        q[2 * slot + 1] = make_float4(d.x, d.y, d.z, 0.0f);
+        q[2 * slot + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(root));
 }
 
 __device__ __forceinline__ uint64_t wave_base(const Wave &w) {
@@ -250,18 +296,30 @@ __device__ __forceinline__ void prim_triangle_dev(const DevScene &s, int prim, V
 }
 
 // type byte and material index of a PrimId_C record.
-__device__ __forceinline__ void prim_info(const DevScene &s, int prim, int &type, int64_t &material, int64_t &id1) {
+__device__ __forceinline__ void prim_info(const DevScene &s, int prim, int &type, int64_t &material) {
         const long long *r = reinterpret_cast<const long long *>(s.prims + prim);
-        id1 = __ldg(r);
         material = __ldg(r + 2);
         type = (int)(signed char)(__ldg(reinterpret_cast<const unsigned char *>(r + 3)));
 }
 
+// Nearest texel of texture t at p (planar map), as a texel index.
+__device__ __forceinline__ int texel_at(const Wave &w, int t, V3 p) {
+        const float *mp = w.tex_map + 9 * t;
+        const V3 d = p - v3(__ldg(mp), __ldg(mp + 1), __ldg(mp + 2));
+        const float u = dot(d, v3(__ldg(mp + 3), __ldg(mp + 4), __ldg(mp + 5)));
+        const float v = dot(d, v3(__ldg(mp + 6), __ldg(mp + 7), __ldg(mp + 8)));
+        const int R = w.tex_res;
+        const int ix = (int)fminf(fmaxf(u * (float)R, 0.0f), (float)(R - 1));
+        const int iy = (int)fminf(fmaxf(v * (float)R, 0.0f), (float)(R - 1));
+        return (t * R + iy) * R + ix;
+}
+
 // ------------------------------------------------------------ kernels
 
-// generate: Tile.render phase 1 (Core/Tile.swift:27-59) for the paths
-// [base, base + count) of the render; path p is sample p % spp of pixel p / spp.
-__global__ void k_generate(RenderConst rc, Wave w) {
+// generate: Tile.render phase 1 (Core/Tile.swift:27-59).  Batch path p belongs
+// to the scene whose [path_begin, next path_begin) holds it; within the scene
+// path q is sample q % spp of pixel q / spp.
+__global__ void k_generate(Wave w) {
         const uint32_t count = wave_count(w);
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -271,46 +329,58 @@ __global__ void k_generate(RenderConst rc, Wave w) {
         }
         if (i >= count) return;
         const uint64_t path = wave_base(w) + i;
-        const uint32_t pixel = (uint32_t)(path / (uint64_t)rc.spp);
-        const uint32_t sample = (uint32_t)(path % (uint64_t)rc.spp) + (uint32_t)rc.first_sample;
-        const uint32_t px = pixel % (uint32_t)rc.width, py = pixel / (uint32_t)rc.width;
+        int lo = 0, hi = w.scene_count - 1;
+        while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (w.scenes[mid].path_begin <= path)
+                        lo = mid;
+                else
+                        hi = mid - 1;
+        }
+        const SceneConst &sc = w.scenes[lo];
+        const uint64_t q = path - sc.path_begin;
+        const uint32_t pixel = (uint32_t)(q / (uint64_t)sc.spp);
+        const uint32_t sample = (uint32_t)(q % (uint64_t)sc.spp) + (uint32_t)sc.first_sample;
+        const uint32_t px = pixel % (uint32_t)sc.width, py = pixel / (uint32_t)sc.width;
         ZSobol z;
-        zs_start(rc.zs, z, px, py, sample);
+        zs_start(sc.zs, z, px, py, sample);
         // getCameraSample (Sampler/Sampler.swift:69-82)
         float u0, u1;
-        zs_get2d(rc.zs, z, u0, u1);
+        zs_get2d(sc.zs, z, u0, u1);
         float dx, dy, denx, deny;
-        gaussian_sample_1d(u0, rc.filter_radius, rc.filter_sigma, dx, denx);
-        gaussian_sample_1d(u1, rc.filter_radius, rc.filter_sigma, dy, deny);
+        gaussian_sample_1d(u0, sc.filter_radius, sc.filter_sigma, dx, denx);
+        gaussian_sample_1d(u1, sc.filter_radius, sc.filter_sigma, dy, deny);
         const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
         float l0, l1;
-        zs_get2d(rc.zs, z, l0, l1);  // lens sample: drawn, unused by a pinhole
+        zs_get2d(sc.zs, z, l0, l1);  // lens sample: drawn, unused by a pinhole
         // raster -> screen -> camera -> world (pinhole)
-        const float scx = rc.sx0 + fx / (float)rc.width * (rc.sx1 - rc.sx0);
-        const float scy = rc.sy1 - fy / (float)rc.height * (rc.sy1 - rc.sy0);
-        const V3 dcam = normalize(v3(scx * rc.tan_half, scy * rc.tan_half, 1.0f));
-        const V3 dir = rc.right * dcam.x + rc.up * dcam.y + rc.fwd * dcam.z;
+        const float scx = sc.sx0 + fx / (float)sc.width * (sc.sx1 - sc.sx0);
+        const float scy = sc.sy1 - fy / (float)sc.height * (sc.sy1 - sc.sy0);
+        const V3 dcam = normalize(v3(scx * sc.tan_half, scy * sc.tan_half, 1.0f));
+        const V3 dir = sc.right * dcam.x + sc.up * dcam.y + sc.fwd * dcam.z;
         // rayWeight = filter value / filter pdf (Tile.swift:36-40)
         const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
-        const float fv = fmaxf(0.0f, gaussian(ddx, rc.filter_sigma)) * fmaxf(0.0f, gaussian(ddy, rc.filter_sigma));
+        const float fv = fmaxf(0.0f, gaussian(ddx, sc.filter_sigma)) * fmaxf(0.0f, gaussian(ddy, sc.filter_sigma));
         w.zs_morton[i] = z.morton;
         w.zs_dim[i] = z.dim;
         w.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         w.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.pixel[i] = pixel;
+        w.pixel[i] = sc.film_offset + pixel;
+        w.scene[i] = (uint32_t)lo;
         w.weight[i] = fv / (denx * deny);
-        store_ray(w.q_ray[0], i, rc.eye, kInf, dir);
+        store_ray(w.q_ray[0], i, sc.eye, kInf, dir, sc.root);
         w.q_id[0][i] = i;
 }
 
-// Power light sampler: lowerBound over the running power sum
-// (Light/PowerLightSampler.swift:4-48).
-__device__ int choose_light(const DevScene &s, float u, float &pdf) {
-        const float key = u * s.light_total_power;
-        int lo = 0, hi = s.light_count;
+// Power light sampler over the scene's lights: lowerBound over the running
+// power sum (Light/PowerLightSampler.swift:4-48).
+__device__ int choose_light(const DevScene &s, const SceneConst &sc, float u, float &pdf) {
+        const float key = u * sc.light_total;
+        int lo = 0, hi = sc.light_count;
+        const float *cdf = s.light_cdf + sc.light_begin;
         while (lo < hi) {
                 const int mid = lo + (hi - lo) / 2;
-                const float c = __ldg(s.light_cdf + mid);
+                const float c = __ldg(cdf + mid);
                 if (c == key) {
                         lo = mid;
                         break;
@@ -320,9 +390,10 @@ __device__ int choose_light(const DevScene &s, float u, float &pdf) {
                         hi = mid;
                 }
         }
-        if (lo >= s.light_count) lo = s.light_count - 1;
-        pdf = __ldg(s.lights + 4 * lo + 1).w / s.light_total_power;
-        return lo;
+        if (lo >= sc.light_count) lo = sc.light_count - 1;
+        const int li = sc.light_begin + lo;
+        pdf = __ldg(s.lights + 4 * li + 1).w / sc.light_total;
+        return li;
 }
 
 // offsetRayOrigin(point:normal:direction:) (Core/Interaction.swift:26-35).
@@ -331,18 +402,72 @@ __device__ __forceinline__ V3 offset_origin(V3 p, V3 n, V3 dir) {
         return dot(dir, n) > 0.0f ? p + off : p + neg(off);
 }
 
-// shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
-__global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur) {
+// Sort key of an extension-queue entry: the hit's material (batch-wide) or
+// the path's scene; misses get the last key.
+__device__ __forceinline__ int entry_key(const Wave &w, const DevScene &s, int cur, uint32_t i) {
+        const int prim = __float_as_int(w.hits[i].w);
+        if (prim < 0) return w.key_count - 1;
+        if (w.sort_key == kSortScene) return (int)w.scene[w.q_id[cur][i]];
+        int type;
+        int64_t m;
+        prim_info(s, prim, type, m);
+        if (type == 3) m = w.scenes[w.scene[w.q_id[cur][i]]].material_begin;
+        return m >= 0 && m < w.key_count - 1 ? (int)m : w.key_count - 1;
+}
+
+__global__ void k_sort_count(Wave w, DevScene s, int cur) {
         const uint32_t n = w.counts[cur];
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= n) return;
+        atomicAdd(w.key_hist + entry_key(w, s, cur, i), 1u);
+}
+
+// Exclusive scan of the key histogram into the cursors (one block of 1024).
+__global__ void k_sort_scan(Wave w) {
+        __shared__ uint32_t part[1024];
+        const int per = (w.key_count + blockDim.x - 1) / blockDim.x;
+        const int b0 = threadIdx.x * per;
+        uint32_t sum = 0;
+        for (int k = b0; k < b0 + per && k < w.key_count; ++k) sum += w.key_hist[k];
+        part[threadIdx.x] = sum;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+                const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+                __syncthreads();
+                part[threadIdx.x] += v;
+                __syncthreads();
+        }
+        uint32_t run = part[threadIdx.x] - sum;
+        for (int k = b0; k < b0 + per && k < w.key_count; ++k) {
+                const uint32_t c = w.key_hist[k];
+                w.key_hist[w.key_count + k] = run;
+                w.key_hist[k] = 0;  // ready for the next bounce
+                run += c;
+        }
+}
+
+__global__ void k_sort_scatter(Wave w, DevScene s, int cur) {
+        const uint32_t n = w.counts[cur];
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        const uint32_t pos = atomicAdd(w.key_hist + w.key_count + entry_key(w, s, cur, i), 1u);
+        w.order[pos] = i;
+}
+
+// shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
+__global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
+        const uint32_t n = w.counts[cur];
+        const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+        if (slot >= n) return;
+        const uint32_t i = sorted ? w.order[slot] : slot;
         const uint32_t path = w.q_id[cur][i];
         const float4 hit = w.hits[i];
         const int prim = __float_as_int(hit.w);
         if (prim < 0) return;  // miss: no environment light
+        const SceneConst &sc = w.scenes[w.scene[path]];
         V3 thr = v3(w.thr[path]);
         if (is_black(thr)) return;
-        if (bounce >= rc.max_depth) return;
+        if (bounce >= sc.max_depth) return;
         const float4 rd = w.q_ray[cur][2 * i + 1];
         const V3 d = v3(rd);
         V3 p0, p1, p2;
@@ -352,36 +477,54 @@ __global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur)
         const V3 ng = normalize(cross(p0 - p2, p1 - p2));
         const V3 wo = normalize(neg(d));
         int type;
-        int64_t mat_index, id1;
-        prim_info(s, prim, type, mat_index, id1);
+        int64_t mat_index;
+        prim_info(s, prim, type, mat_index);
         const bool is_light = type == 3;
-        float4 Lacc = w.L[path];
-        V3 L = v3(Lacc);
+        V3 L = v3(w.L[path]);
         if (bounce == 0 && is_light && mat_index >= 0 && mat_index < s.material_count) {
-                const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1));
+                const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
                 if (dot(ng, wo) > 0.0f) L = L + mulv(thr, le);
         }
-        // Area-light hits scatter with material 0 (their interaction keeps
-        // materialIndex 0, Core/SurfaceInteraction.swift:20).
-        const int64_t mi = is_light ? 0 : mat_index;
-        const V3 refl = (mi >= 0 && mi < s.material_count) ? v3(__ldg(s.materials + 2 * mi)) : v3(0.5f, 0.5f, 0.5f);
+        // Area-light hits scatter with the scene's material 0 (their interaction
+        // keeps materialIndex 0, Core/SurfaceInteraction.swift:20).
+        const int64_t mi = is_light ? (int64_t)sc.material_begin : mat_index;
+        V3 refl = (mi >= 0 && mi < s.material_count) ? v3(__ldg(s.materials + 2 * mi)) : v3(0.5f, 0.5f, 0.5f);
+        if (w.mat_tex && mi >= 0 && mi < s.material_count) {
+                const int t = __ldg(w.mat_tex + mi);
+                if (t >= 0) {
+                        const int texel = texel_at(w, t, pos);
+                        refl = v3(__ldg(w.tex + 3 * texel), __ldg(w.tex + 3 * texel + 1), __ldg(w.tex + 3 * texel + 2));
+                        if (w.mode == kReplay) {
+                                // Path replay: every contribution still to come passes
+                                // through this vertex's albedo once per channel, so
+                                // dL/dalbedo = (Ltot - L so far) / albedo.
+                                const V3 after = v3(w.Ltot[path]) - L;
+                                const uint32_t px = w.pixel[path];
+                                const float inv_w = 1.0f / w.adj_w[px];
+                                const float *adj = w.adj_rgb + 3 * (size_t)px;
+                                if (refl.x > 0.0f) atomicAdd(w.d_tex + 3 * texel, adj[0] * inv_w * (after.x / refl.x));
+                                if (refl.y > 0.0f) atomicAdd(w.d_tex + 3 * texel + 1, adj[1] * inv_w * (after.y / refl.y));
+                                if (refl.z > 0.0f) atomicAdd(w.d_tex + 3 * texel + 2, adj[2] * inv_w * (after.z / refl.z));
+                        }
+                }
+        }
         const V3 f_val = refl * (1.0f / kPi);
         Frame fr;
         ZSobol z;
         z.morton = w.zs_morton[path];
         z.dim = w.zs_dim[path];
         bool alive = make_frame(p0, p1, p2, ng, fr);
-        if (alive && s.light_count > 0) {
+        if (alive && sc.light_count > 0) {
                 const V3 wo_l = fr.to_local(wo);
                 // ---- light choice and light sample (sampleLightSource, :67-89)
                 float choose_pdf;
-                const int li = choose_light(s, zs_get1d(rc.zs, z), choose_pdf);
+                const int li = choose_light(s, sc, zs_get1d(sc.zs, z), choose_pdf);
                 const float4 l0 = __ldg(s.lights + 4 * li), l1 = __ldg(s.lights + 4 * li + 1),
                              l2 = __ldg(s.lights + 4 * li + 2), le4 = __ldg(s.lights + 4 * li + 3);
-                const V3 lp0 = v3(l0), lp1 = v3(l1), lp2 = v3(l2), le = v3(le4);
+                const V3 lp0 = v3(l0), lp1 = v3(l1), lp2 = v3(l2), le = v3(le4) * w.emission_scale;
                 const float area = l0.w;
                 float u0, u1;
-                zs_get2d(rc.zs, z, u0, u1);
+                zs_get2d(sc.zs, z, u0, u1);
                 const float su0 = sqrtf(u0);
                 const float lb0 = 1.0f - su0, lb1 = u1 * su0;
                 const V3 lp = lp0 * lb0 + lp1 * lb1 + lp2 * ((1.0f - lb0) - lb1);
@@ -409,15 +552,15 @@ __global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur)
                         const V3 so = pos + (lp - pos) * 0.0001f;
                         const V3 sd = lp - so;
                         const V3 c = mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf));
-                        const uint32_t slot = queue_slot(w.counts + kCountShadow);
-                        store_ray(w.sh_ray, slot, so, 1.0f - 0.00001f, sd);
-                        w.sh_id[slot] = path;
-                        w.sh_contrib[slot] = make_float4(c.x, c.y, c.z, 0.0f);
+                        const uint32_t q = queue_slot(w.counts + kCountShadow);
+                        store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
+                        w.sh_id[q] = path;
+                        w.sh_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
                 }
                 // ---- MIS BSDF sample (sampleDistributionFunction, :91-133)
                 float v0, v1, v2;
-                zs_get3d(rc.zs, z, v0, v1, v2);
-                if (rc.mis_corrected) {
+                zs_get3d(sc.zs, z, v0, v1, v2);
+                if (sc.mis_corrected) {
                         V3 wi_l = cosine_hemisphere(v0, v1);
                         if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
                         const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? fabsf(wi_l.z) / kPi : 0.0f;
@@ -428,7 +571,8 @@ __global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur)
                                 // light density of the chosen light along wi (Sampleable.swift:47-68 with tHit = inf)
                                 float light_density = 0.0f;
                                 float tl, lu, lv;
-                                const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f), b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
+                                const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f),
+                                             b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
                                              c4 = make_float4(lp2.x, lp2.y, lp2.z, 0.0f);
                                 if (watertight_test(po.x, po.y, po.z, wi.x, wi.y, wi.z, a4, b4, c4, kInf, tl, lu, lv)) {
                                         const V3 hp = po + wi * tl;
@@ -440,15 +584,15 @@ __global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur)
                                 const float bw = power_heuristic(pdf_b, light_density);
                                 if (bw > 0.0f) {
                                         const V3 c = mulv(thr, est * (bw / pdf_b) * (1.0f / choose_pdf));
-                                        const uint32_t slot = queue_slot(w.counts + kCountProbe);
-                                        store_ray(w.pr_ray, slot, po, kInf, wi);
-                                        w.pr_id[slot] = path;
-                                        w.pr_contrib[slot] = make_float4(c.x, c.y, c.z, 0.0f);
+                                        const uint32_t q = queue_slot(w.counts + kCountProbe);
+                                        store_ray(w.pr_ray, q, po, kInf, wi, sc.root);
+                                        w.pr_id[q] = path;
+                                        w.pr_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
                                 }
                         }
                 }
                 // ---- continuation (bsdf.sampleWorldSpace, :358-369)
-                zs_get3d(rc.zs, z, v0, v1, v2);
+                zs_get3d(sc.zs, z, v0, v1, v2);
                 V3 wi_l = cosine_hemisphere(v0, v1);
                 if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
                 const float pdf_c = (wo_l.z * wi_l.z > 0.0f) ? fabsf(wi_l.z) / kPi : 0.0f;
@@ -460,18 +604,18 @@ __global__ void k_shade(RenderConst rc, Wave w, DevScene s, int bounce, int cur)
                         const V3 o = offset_origin(pos, ng, wi);
                         // stopWithRussianRoulette (:269-283), roulette value from Z-Sobol
                         const float mv = fmaxf(thr.x, fmaxf(thr.y, thr.z));
-                        if (mv < 1.0f && bounce >= rc.rr_min) {
-                                const float q = fmaxf(0.0f, 1.0f - mv);
-                                if (zs_get1d(rc.zs, z) < q)
+                        if (mv < 1.0f && bounce >= sc.rr_min) {
+                                const float qq = fmaxf(0.0f, 1.0f - mv);
+                                if (zs_get1d(sc.zs, z) < qq)
                                         alive = false;
                                 else
-                                        thr = thr * (1.0f / (1.0f - q));
+                                        thr = thr * (1.0f / (1.0f - qq));
                         }
-                        if (alive && bounce + 1 < rc.max_depth) {
+                        if (alive && bounce + 1 < sc.max_depth) {
                                 const int nxt = cur ^ 1;
-                                const uint32_t slot = queue_slot(w.counts + nxt);
-                                store_ray(w.q_ray[nxt], slot, o, kInf, wi);
-                                w.q_id[nxt][slot] = path;
+                                const uint32_t q = queue_slot(w.counts + nxt);
+                                store_ray(w.q_ray[nxt], q, o, kInf, wi, sc.root);
+                                w.q_id[nxt][q] = path;
                         }
                 }
         }
@@ -505,15 +649,15 @@ __global__ void k_probe_resolve(Wave w, DevScene s) {
         const int prim = __float_as_int(h.w);
         if (prim < 0) return;
         int type;
-        int64_t mat_index, id1;
-        prim_info(s, prim, type, mat_index, id1);
+        int64_t mat_index;
+        prim_info(s, prim, type, mat_index);
         if (type != 3 || mat_index < 0 || mat_index >= s.material_count) return;
         V3 q0, q1, q2;
         prim_triangle_dev(s, prim, q0, q1, q2);
         const V3 qn = normalize(cross(q0 - q2, q1 - q2));
         const V3 wi = v3(w.pr_ray[2 * i + 1]);
         if (!(dot(qn, neg(wi)) > 0.0f)) return;
-        const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1));
+        const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
         const uint32_t path = w.pr_id[i];
         const float4 c = w.pr_contrib[i];
         float4 L = w.L[path];
@@ -523,14 +667,14 @@ __global__ void k_probe_resolve(Wave w, DevScene s) {
         w.L[path] = L;
 }
 
-// Per-bounce bookkeeping: ray statistics of this bounce, then the counters of
-// the queues the next stages fill are cleared.
+// Per-bounce bookkeeping: ray statistics of the bounce.
 __global__ void k_bounce_tally(Wave w, int cur) {
         atomicAdd(w.stats + kStatExt, (unsigned long long)w.counts[cur]);
         atomicAdd(w.stats + kStatShadow, (unsigned long long)w.counts[kCountShadow]);
         atomicAdd(w.stats + kStatProbe, (unsigned long long)w.counts[kCountProbe]);
 }
 
+// Clears the counters of the queues the next stages fill.
 __global__ void k_clear_counts(Wave w, int next) {
         w.counts[next] = 0;
         w.counts[kCountShadow] = 0;
@@ -538,23 +682,66 @@ __global__ void k_clear_counts(Wave w, int next) {
 }
 
 // Film sums (Core/Film.swift:107-119): radiance (iso 100 -> scale 1), its
-// square, and the filter weight, per pixel; then advance the wave base.
+// square, and the filter weight, per pixel of the batch film.
 __global__ void k_accumulate(Wave w, float *film_rgb, float *film_sq, float *film_w) {
         const uint32_t count = wave_count(w);
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count) return;
+        const uint32_t px = w.pixel[i];
+        const float4 L = w.L[i];
+        atomicAdd(film_rgb + 3 * (size_t)px, L.x);
+        atomicAdd(film_rgb + 3 * (size_t)px + 1, L.y);
+        atomicAdd(film_rgb + 3 * (size_t)px + 2, L.z);
+        if (film_sq) {
+                atomicAdd(film_sq + 3 * (size_t)px, L.x * L.x);
+                atomicAdd(film_sq + 3 * (size_t)px + 1, L.y * L.y);
+                atomicAdd(film_sq + 3 * (size_t)px + 2, L.z * L.z);
+        }
+        atomicAdd(film_w + px, w.weight[i]);
+}
+
+// Double-precision film sums (finite differences need sums whose rounding
+// does not depend on the order of the atomics).
+__global__ void k_accumulate_f64(Wave w, double *film_rgb, double *film_sq, double *film_w) {
+        const uint32_t count = wave_count(w);
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count) return;
+        const uint32_t px = w.pixel[i];
+        const float4 L = w.L[i];
+        atomicAdd(film_rgb + 3 * (size_t)px, (double)L.x);
+        atomicAdd(film_rgb + 3 * (size_t)px + 1, (double)L.y);
+        atomicAdd(film_rgb + 3 * (size_t)px + 2, (double)L.z);
+        if (film_sq) {
+                atomicAdd(film_sq + 3 * (size_t)px, (double)L.x * L.x);
+                atomicAdd(film_sq + 3 * (size_t)px + 1, (double)L.y * L.y);
+                atomicAdd(film_sq + 3 * (size_t)px + 2, (double)L.z * L.z);
+        }
+        atomicAdd(film_w + px, (double)w.weight[i]);
+}
+
+// Primal pass of a wave: keep each path's radiance for the replay.
+__global__ void k_store_total(Wave w) {
+        const uint32_t count = wave_count(w);
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count) return;
+        w.Ltot[i] = w.L[i];
+}
+
+// End of a replay: every emission is linear in the emission scale, so
+// dLoss/dscale = sum over paths of <dLoss/dL, Ltot> / scale.
+__global__ void k_emission_gradient(Wave w) {
+        const uint32_t count = wave_count(w);
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        double v = 0.0;
         if (i < count) {
                 const uint32_t px = w.pixel[i];
-                const float4 L = w.L[i];
-                atomicAdd(film_rgb + 3 * (size_t)px, L.x);
-                atomicAdd(film_rgb + 3 * (size_t)px + 1, L.y);
-                atomicAdd(film_rgb + 3 * (size_t)px + 2, L.z);
-                if (film_sq) {
-                        atomicAdd(film_sq + 3 * (size_t)px, L.x * L.x);
-                        atomicAdd(film_sq + 3 * (size_t)px + 1, L.y * L.y);
-                        atomicAdd(film_sq + 3 * (size_t)px + 2, L.z * L.z);
-                }
-                atomicAdd(film_w + px, w.weight[i]);
+                const float4 Lt = w.Ltot[i];
+                const float *adj = w.adj_rgb + 3 * (size_t)px;
+                const double g = (double)adj[0] * Lt.x + (double)adj[1] * Lt.y + (double)adj[2] * Lt.z;
+                v = g / ((double)w.adj_w[px] * (double)w.emission_scale);
         }
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
+        if ((threadIdx.x & 31u) == 0 && v != 0.0) atomicAdd(w.d_emission, v);
 }
 
 __global__ void k_advance_wave(Wave w) {
@@ -563,12 +750,17 @@ __global__ void k_advance_wave(Wave w) {
         w.counts[kCountWaveBase + 1] = (uint32_t)(next >> 32);
 }
 
-// Z-Sobol values for n pixel samples: the sequence of get1D/get2D/get3D
-// calls in `kinds` (1, 2 or 3 each), starting at dimension 0.
+__global__ void k_set_wave_base(Wave w, uint64_t base) {
+        w.counts[kCountWaveBase] = (uint32_t)(base & 0xFFFFFFFFull);
+        w.counts[kCountWaveBase + 1] = (uint32_t)(base >> 32);
+}
+
 struct KindList {
         int32_t k[64];
 };
 
+// Z-Sobol values for n pixel samples: the sequence of get1D/get2D/get3D
+// calls in `kinds` (1, 2 or 3 each), starting at dimension 0.
 __global__ void k_zsobol_fill(ZSobolConfig c, const int32_t *px, const int32_t *py, const int64_t *index, int64_t n,
                               KindList kinds, int nkinds, int per, float *out) {
         const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -588,11 +780,6 @@ __global__ void k_zsobol_fill(ZSobolConfig c, const int32_t *px, const int32_t *
                         o += 3;
                 }
         }
-}
-
-__global__ void k_set_wave_base(Wave w, uint64_t base) {
-        w.counts[kCountWaveBase] = (uint32_t)(base & 0xFFFFFFFFull);
-        w.counts[kCountWaveBase + 1] = (uint32_t)(base >> 32);
 }
 
 // ------------------------------------------------------------ host side
@@ -619,13 +806,72 @@ gzg_status device_sobol(int dev, const uint32_t **out) {
         return GZG_OK;
 }
 
-V3 hv3(float x, float y, float z) { return V3{x, y, z}; }
-V3 hsub(V3 a, V3 b) { return hv3(a.x - b.x, a.y - b.y, a.z - b.z); }
-V3 hcross(V3 a, V3 b) { return hv3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+// ZSobolSampler.init (ZSobolSampler.swift:114-122).
+ZSobolConfig make_zsobol(int64_t spp, int32_t res_x, int32_t res_y, int64_t seed, const uint32_t *matrices) {
+        ZSobolConfig c{};
+        c.matrices = matrices;
+        c.seed = (uint64_t)seed;
+        c.log2spp = __builtin_ctzll((uint64_t)spp);
+        int64_t res = std::max(res_x, res_y);
+        res -= 1;
+        res |= res >> 1;
+        res |= res >> 2;
+        res |= res >> 4;
+        res |= res >> 8;
+        res |= res >> 16;
+        res += 1;
+        c.n_base4_digits = __builtin_ctzll((uint64_t)res) + (c.log2spp + 1) / 2;
+        return c;
+}
+
+V3 hsub(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 hcross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
 V3 hnorm(V3 a) {
         const float l = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
-        return hv3(a.x / l, a.y / l, a.z / l);
+        return V3{a.x / l, a.y / l, a.z / l};
 }
+
+// Camera, film and sampler constants of one scene.
+SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices) {
+        SceneConst sc{};
+        const V3 eye{P.eye[0], P.eye[1], P.eye[2]};
+        const V3 fwd = hnorm(hsub(V3{P.target[0], P.target[1], P.target[2]}, eye));
+        const V3 right = hnorm(hcross(fwd, V3{P.up[0], P.up[1], P.up[2]}));
+        sc.eye = eye;
+        sc.fwd = fwd;
+        sc.right = right;
+        sc.up = hcross(right, fwd);
+        sc.tan_half = std::tan(P.fov_deg * 3.14159265358979323846f / 180.0f / 2.0f);
+        const float aspect = (float)P.width / (float)P.height;
+        sc.sx0 = aspect > 1.0f ? -aspect : -1.0f;
+        sc.sx1 = -sc.sx0;
+        sc.sy0 = aspect > 1.0f ? -1.0f : -1.0f / aspect;
+        sc.sy1 = -sc.sy0;
+        sc.filter_radius = P.filter_radius;
+        sc.filter_sigma = P.filter_sigma;
+        sc.width = P.width;
+        sc.height = P.height;
+        sc.spp = P.spp;
+        sc.max_depth = P.max_depth;
+        sc.rr_min = P.rr_min_bounce;
+        sc.mis_corrected = P.mis_corrected;
+        sc.first_sample = P.first_sample;
+        sc.zs = make_zsobol(P.sampler_spp > 0 ? P.sampler_spp : P.spp, P.width, P.height, P.seed, matrices);
+        return sc;
+}
+
+bool params_ok(const gzg_render_params &P) {
+        return P.width > 0 && P.height > 0 && P.spp > 0 && P.max_depth >= 0 && P.fov_deg > 0.0f &&
+               P.filter_sigma > 0.0f && P.filter_radius > 0.0f && P.first_sample >= 0 && P.sampler_spp >= 0;
+}
+
+gzg_status cuda_err(cudaError_t e, const char *what) {
+        if (e == cudaSuccess) return GZG_OK;
+        return set_error(e == cudaErrorMemoryAllocation ? GZG_ERR_OUT_OF_MEMORY : GZG_ERR_CUDA,
+                         std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+constexpr uint32_t kDefaultWave = 1u << 21;
 
 }  // namespace
 }  // namespace gzg
@@ -633,26 +879,39 @@ V3 hnorm(V3 a) {
 using namespace gzg;
 
 struct gzg_renderer {
-        gzg_scene *scene = nullptr;
         int device = 0;
-        gzg_render_params params{};
-        RenderConst rc{};
+        std::vector<gzg_scene *> scenes;
+        std::vector<gzg_render_params> params;
+        gzg_batch_options opts{};
+        std::vector<SceneConst> consts;
+        std::vector<int64_t> film_offsets;  // scene count + 1 pixel offsets
         Wave w{};
+        uint32_t max_capacity = 0;
         DevScene view{};
         int wide_depth = 0;
         std::vector<void *> allocs;
         cudaGraphExec_t graph = nullptr;
         cudaGraph_t graph_def = nullptr;
-        float *graph_film[3] = {nullptr, nullptr, nullptr};
+        const void *graph_key[6] = {};
+        // differentiable rendering
+        int32_t *d_mat_tex = nullptr;
+        float *d_tex_map = nullptr;
+        int tex_slots = 0;
 
         ~gzg_renderer() {
                 int prev = 0;
                 cudaGetDevice(&prev);
                 if (prev != device) cudaSetDevice(device);
-                if (graph) cudaGraphExecDestroy(graph);
-                if (graph_def) cudaGraphDestroy(graph_def);
+                drop_graph();
                 for (void *p : allocs) cudaFree(p);
                 if (prev != device) cudaSetDevice(prev);
+        }
+
+        void drop_graph() {
+                if (graph) cudaGraphExecDestroy(graph);
+                if (graph_def) cudaGraphDestroy(graph_def);
+                graph = nullptr;
+                graph_def = nullptr;
         }
 
         template <class T>
@@ -665,27 +924,70 @@ struct gzg_renderer {
                 return GZG_OK;
         }
 
-        // One wave: generate, bounces, accumulate, advance.  Enqueued on st.
-        cudaError_t enqueue_wave(float *film_rgb, float *film_sq, float *film_w, cudaStream_t st) {
+        // Copies a host vector to a new device buffer of element type D.
+        template <class D, class T>
+        gzg_status upload(const D **p, const std::vector<T> &v) {
+                static_assert(sizeof(T) % sizeof(D) == 0 || sizeof(D) % sizeof(T) == 0, "record size mismatch");
+                const size_t bytes = v.size() * sizeof(T);
+                D *d = nullptr;
+                gzg_status st = alloc(&d, (bytes + sizeof(D) - 1) / sizeof(D));
+                if (st) return st;
+                if (bytes) {
+                        st = cuda_err(cudaMemcpy(d, v.data(), bytes, cudaMemcpyHostToDevice), "batch upload");
+                        if (st) return st;
+                }
+                *p = d;
+                return GZG_OK;
+        }
+
+        // Film buffers of a pass: float sums, or double sums (d* set).
+        struct Films {
+                float *rgb, *sq, *w;
+                double *drgb, *dsq, *dw;
+        };
+
+        // One wave: generate, bounces, then by w.mode accumulate + advance,
+        // keep the primal radiance, or finish a replay + advance.  Enqueued on st.
+        cudaError_t enqueue_wave(const Films &film, cudaStream_t st) {
                 const int block = 128;
                 const unsigned grid = (w.capacity + block - 1) / block;
-                k_generate<<<grid, block, 0, st>>>(rc, w);
+                int max_depth = 0;
+                bool corrected = false;
+                for (const gzg_render_params &P : params) {
+                        max_depth = std::max(max_depth, (int)P.max_depth);
+                        corrected = corrected || P.mis_corrected;
+                }
+                // the first scene's tuned launches (gzg_scene_autotune), read at
+                // enqueue time so a later autotune takes effect
+                LaunchParams lp_closest = scene_launch(scenes[0], false);
+                LaunchParams lp_any = scene_launch(scenes[0], true);
+                lp_closest.wide_depth = lp_any.wide_depth = wide_depth;
+                // per-ray roots exist in the wide layout only
+                if (view.per_ray_root) {
+                        if (lp_closest.traversal == GZG_TRAVERSAL_BVH2) lp_closest.traversal = GZG_TRAVERSAL_WIDE;
+                        if (lp_any.traversal == GZG_TRAVERSAL_BVH2) lp_any.traversal = GZG_TRAVERSAL_WIDE;
+                }
+                k_generate<<<grid, block, 0, st>>>(w);
                 int cur = 0;
-                for (int b = 0; b < rc.max_depth; ++b) {
+                for (int b = 0; b < max_depth; ++b) {
                         k_clear_counts<<<1, 1, 0, st>>>(w, cur ^ 1);
-                        // the scene's tuned launches (gzg_scene_autotune)
-                        LaunchParams lp = scene_launch(scene, false);
-                        LaunchParams lpa = scene_launch(scene, true);
+                        LaunchParams lp = lp_closest, lpa = lp_any;
                         lp.n_dev = w.counts + cur;
                         cudaError_t e = launch_trace(view, lp, kRayDevice, kOutHit, w.q_ray[cur], nullptr, w.capacity,
                                                      w.hits, st);
                         if (e != cudaSuccess) return e;
-                        k_shade<<<grid, block, 0, st>>>(rc, w, view, b, cur);
+                        const int sorted = w.sort_key != kSortNone;
+                        if (sorted) {
+                                k_sort_count<<<grid, block, 0, st>>>(w, view, cur);
+                                k_sort_scan<<<1, 1024, 0, st>>>(w);
+                                k_sort_scatter<<<grid, block, 0, st>>>(w, view, cur);
+                        }
+                        k_shade<<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                         lpa.n_dev = w.counts + kCountShadow;
                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
-                        if (rc.mis_corrected) {
+                        if (corrected) {
                                 lp.n_dev = w.counts + kCountProbe;
                                 e = launch_trace(view, lp, kRayDevice, kOutHit, w.pr_ray, nullptr, w.capacity, w.pr_hits,
                                                  st);
@@ -695,38 +997,239 @@ struct gzg_renderer {
                         k_bounce_tally<<<1, 1, 0, st>>>(w, cur);
                         cur ^= 1;
                 }
-                k_accumulate<<<grid, block, 0, st>>>(w, film_rgb, film_sq, film_w);
+                if (w.mode == kPrimal) {
+                        k_store_total<<<grid, block, 0, st>>>(w);  // the replay runs the same paths
+                        return cudaGetLastError();
+                }
+                if (w.mode == kReplay) {
+                        if (w.d_emission) k_emission_gradient<<<grid, block, 0, st>>>(w);
+                } else if (film.drgb) {
+                        k_accumulate_f64<<<grid, block, 0, st>>>(w, film.drgb, film.dsq, film.dw);
+                } else {
+                        k_accumulate<<<grid, block, 0, st>>>(w, film.rgb, film.sq, film.w);
+                }
                 k_advance_wave<<<1, 1, 0, st>>>(w);
                 return cudaGetLastError();
+        }
+
+        // Sets the wave capacity (clamped to the allocation) and the sort key.
+        void configure(uint32_t capacity, int sort_key) {
+                w.capacity = std::max<uint32_t>(1, std::min<uint32_t>(capacity, max_capacity));
+                w.sort_key = sort_key;
+                w.key_count = (sort_key == kSortScene ? (int32_t)scenes.size() : view.material_count) + 1;
+                drop_graph();
+        }
+
+        uint64_t wave_total() const { return (w.total_paths + w.capacity - 1) / w.capacity; }
+
+        // Double-precision films, direct launches.
+        gzg_status render_f64(double *rgb, double *sq, double *wt, cudaStream_t st) {
+                w.mode = kRender;
+                k_set_wave_base<<<1, 1, 0, st>>>(w, 0ull);
+                const Films f{nullptr, nullptr, nullptr, rgb, sq, wt};
+                for (uint64_t k = 0; k < wave_total(); ++k) {
+                        gzg_status status = cuda_err(enqueue_wave(f, st), "wave launch");
+                        if (status) return status;
+                }
+                return GZG_OK;
+        }
+
+        // Path-replay adjoint: per wave a primal pass, then the replay.
+        gzg_status adjoint(const float *adj_rgb, const float *adj_w, float *d_tex, double *d_emission, cudaStream_t st) {
+                if (!w.Ltot) {
+                        gzg_status status = alloc(&w.Ltot, max_capacity);
+                        if (status) return status;
+                }
+                w.adj_rgb = adj_rgb;
+                w.adj_w = adj_w;
+                w.d_tex = d_tex;
+                w.d_emission = d_emission;
+                k_set_wave_base<<<1, 1, 0, st>>>(w, 0ull);
+                const Films none{};
+                gzg_status status = GZG_OK;
+                for (uint64_t k = 0; k < wave_total() && !status; ++k) {
+                        w.mode = kPrimal;
+                        status = cuda_err(enqueue_wave(none, st), "primal wave launch");
+                        if (status) break;
+                        w.mode = kReplay;
+                        status = cuda_err(enqueue_wave(none, st), "replay wave launch");
+                }
+                w.mode = kRender;
+                w.adj_rgb = w.adj_w = nullptr;
+                w.d_tex = nullptr;
+                w.d_emission = nullptr;
+                return status;
+        }
+
+        gzg_status render(float *film_rgb, float *film_sq, float *film_w, cudaStream_t st) {
+                const uint64_t waves = wave_total();
+                w.mode = kRender;
+                const Films film{film_rgb, film_sq, film_w, nullptr, nullptr, nullptr};
+                k_set_wave_base<<<1, 1, 0, st>>>(w, 0ull);
+                if (opts.use_graph) {
+                        const void *key[6] = {film_rgb, film_sq, film_w, (const void *)(uintptr_t)w.capacity,
+                                              (const void *)(uintptr_t)w.sort_key, (const void *)(uintptr_t)w.total_paths};
+                        if (!graph || !std::equal(key, key + 6, graph_key)) {
+                                drop_graph();
+                                cudaStream_t cap;
+                                gzg_status status = cuda_err(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
+                                if (status) return status;
+                                status = cuda_err(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
+                                if (!status) {
+                                        cudaError_t e = enqueue_wave(film, cap);
+                                        cudaError_t e2 = cudaStreamEndCapture(cap, &graph_def);
+                                        status = cuda_err(e != cudaSuccess ? e : e2, "graph capture of a wave");
+                                        if (!status) status = cuda_err(cudaGraphInstantiate(&graph, graph_def, 0), "graph instantiate");
+                                }
+                                cudaStreamDestroy(cap);
+                                if (status) return status;
+                                std::copy(key, key + 6, graph_key);
+                        }
+                        for (uint64_t k = 0; k < waves; ++k) {
+                                gzg_status status = cuda_err(cudaGraphLaunch(graph, st), "graph launch");
+                                if (status) return status;
+                        }
+                        return GZG_OK;
+                }
+                for (uint64_t k = 0; k < waves; ++k) {
+                        gzg_status status = cuda_err(enqueue_wave(film, st), "wave launch");
+                        if (status) return status;
+                }
+                return GZG_OK;
         }
 };
 
 namespace {
 
-gzg_status cuda_err(cudaError_t e, const char *what) {
-        if (e == cudaSuccess) return GZG_OK;
-        return set_error(e == cudaErrorMemoryAllocation ? GZG_ERR_OUT_OF_MEMORY : GZG_ERR_CUDA,
-                         std::string(what) + ": " + cudaGetErrorString(e));
+// Builds the batch: per-scene constants and, for more than one scene, one
+// concatenated scene (nodes, leaf records with batch-wide prim indices,
+// triangles, prim ids with batch-wide material indices, materials, lights).
+gzg_status build_batch(gzg_renderer *r) {
+        const size_t n = r->scenes.size();
+        const uint32_t *matrices = nullptr;
+        gzg_status st = device_sobol(r->device, &matrices);
+        if (st) return st;
+        r->consts.resize(n);
+        r->film_offsets.assign(n + 1, 0);
+        uint64_t paths = 0;
+        for (size_t k = 0; k < n; ++k) {
+                r->consts[k] = make_scene_const(r->params[k], matrices);
+                r->consts[k].path_begin = paths;
+                r->consts[k].film_offset = (uint32_t)r->film_offsets[k];
+                r->film_offsets[k + 1] = r->film_offsets[k] + (int64_t)r->params[k].width * r->params[k].height;
+                paths += (uint64_t)r->params[k].width * r->params[k].height * r->params[k].spp;
+        }
+        if (r->film_offsets[n] >= (int64_t)0xFFFFFFFFll)
+                return set_error(GZG_ERR_LIMIT, "renderer: more than 2^32 film pixels in a batch");
+        r->w.total_paths = paths;
+        int wide_depth = 0;
+        if (n == 1) {
+                scene_view(r->scenes[0], &r->view, &r->device, &wide_depth);
+                const HostShading &hs = scene_host_shading(r->scenes[0]);
+                SceneConst &sc = r->consts[0];
+                sc.root = 0;
+                sc.material_begin = 0;
+                sc.material_count = (int32_t)(hs.materials.size() / 2);
+                sc.light_begin = 0;
+                sc.light_count = (int32_t)(hs.lights.size() / 4);
+                sc.light_total = hs.light_total;
+                r->view.per_ray_root = 0;
+        } else {
+                std::vector<WideNode> nodes;
+                std::vector<float4_> v0, v1, v2, pv0, pv1, pv2, mats, lights;
+                std::vector<gzg_prim_id> prims;
+                std::vector<float> cdf;
+                uint64_t steps = 0;
+                for (size_t k = 0; k < n; ++k) {
+                        const WideBvh &wb = scene_host_wide(r->scenes[k]);
+                        const HostShading &hs = scene_host_shading(r->scenes[k]);
+                        const uint32_t noff = (uint32_t)nodes.size(), toff = (uint32_t)v0.size();
+                        const int32_t poff = (int32_t)prims.size(), moff = (int32_t)(mats.size() / 2),
+                                      loff = (int32_t)(lights.size() / 4);
+                        for (WideNode nd : wb.nodes) {
+                                nd.child_base += noff;
+                                nd.tri_base += toff;
+                                nodes.push_back(nd);
+                        }
+                        for (float4_ a : wb.v0) {
+                                int32_t p;
+                                std::memcpy(&p, &a.w, 4);
+                                p += poff;
+                                std::memcpy(&a.w, &p, 4);
+                                v0.push_back(a);
+                        }
+                        v1.insert(v1.end(), wb.v1.begin(), wb.v1.end());
+                        v2.insert(v2.end(), wb.v2.begin(), wb.v2.end());
+                        pv0.insert(pv0.end(), hs.pv0.begin(), hs.pv0.end());
+                        pv1.insert(pv1.end(), hs.pv1.begin(), hs.pv1.end());
+                        pv2.insert(pv2.end(), hs.pv2.begin(), hs.pv2.end());
+                        for (gzg_prim_id p : hs.prims) {
+                                p.material_index += moff;
+                                prims.push_back(p);
+                        }
+                        mats.insert(mats.end(), hs.materials.begin(), hs.materials.end());
+                        lights.insert(lights.end(), hs.lights.begin(), hs.lights.end());
+                        cdf.insert(cdf.end(), hs.light_cdf.begin(), hs.light_cdf.end());
+                        SceneConst &sc = r->consts[k];
+                        sc.root = noff;
+                        sc.material_begin = moff;
+                        sc.material_count = (int32_t)(hs.materials.size() / 2);
+                        sc.light_begin = loff;
+                        sc.light_count = (int32_t)(hs.lights.size() / 4);
+                        sc.light_total = hs.light_total;
+                        steps = std::max<uint64_t>(steps, wb.nodes.size());
+                        wide_depth = std::max(wide_depth, (int)wb.depth);
+                }
+                if (nodes.size() >= 0x7FFFFFFFu || v0.size() >= 0x7FFFFFFFu || prims.size() >= 0x7FFFFFFFu)
+                        return set_error(GZG_ERR_LIMIT, "renderer: batch exceeds 2^31 nodes, records or prims");
+                DevScene &d = r->view;
+                d = DevScene{};
+                if ((st = r->upload(&d.wide, nodes)) || (st = r->upload(&d.tv0, v0)) || (st = r->upload(&d.tv1, v1)) ||
+                    (st = r->upload(&d.tv2, v2)) || (st = r->upload(&d.pv0, pv0)) || (st = r->upload(&d.pv1, pv1)) ||
+                    (st = r->upload(&d.pv2, pv2)) || (st = r->upload(&d.prims, prims)) ||
+                    (st = r->upload(&d.materials, mats)) || (st = r->upload(&d.lights, lights)) ||
+                    (st = r->upload(&d.light_cdf, cdf)))
+                        return st;
+                uint32_t *err = nullptr;
+                if ((st = r->alloc(&err, 1))) return st;
+                if ((st = cuda_err(cudaMemset(err, 0, 4), "batch error word"))) return st;
+                d.err = err;
+                d.prim_count = (int64_t)prims.size();
+                d.wide_count = (uint32_t)std::min<uint64_t>(steps, 0xFFFFFFFFull);
+                d.material_count = (int32_t)(mats.size() / 2);
+                d.light_count = (int32_t)(lights.size() / 4);
+                d.per_ray_root = 1;
+        }
+        r->wide_depth = wide_depth;
+        return GZG_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-GZG_API gzg_status gzg_renderer_create(gzg_scene *scene, const gzg_render_params *params, gzg_renderer **out) {
-        if (!out) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_create: out is NULL");
+gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *params, int64_t n,
+                           const gzg_batch_options *opts, gzg_renderer **out) {
+        if (!out) return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: out is NULL");
         *out = nullptr;
-        if (!scene || !params) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_create: null argument");
-        const gzg_render_params &P = *params;
-        if (P.width <= 0 || P.height <= 0 || P.spp <= 0 || P.max_depth < 0 || P.fov_deg <= 0.0f ||
-            P.filter_sigma <= 0.0f || P.filter_radius <= 0.0f || P.first_sample < 0 || P.sampler_spp < 0)
-                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_create: bad render parameters");
+        if (n <= 0 || !scenes || !params) return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: no scenes");
         auto r = std::make_unique<gzg_renderer>();
-        r->scene = scene;
-        r->params = P;
-        scene_view(scene, &r->view, &r->device, &r->wide_depth);
-        if (r->view.material_count <= 0)
-                return set_error(GZG_ERR_BAD_SCENE, "gzg_renderer_create: the scene was uploaded without materials");
+        for (int64_t k = 0; k < n; ++k) {
+                if (!scenes[k] || scene_is_instanced(scenes[k]))
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: scene " + std::to_string(k) +
+                                                                       " is NULL or two-level (not rendered yet)");
+                if (!params_ok(params[k]))
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         "renderer: bad render parameters for scene " + std::to_string(k));
+                DevScene v;
+                int dev = 0, depth = 0;
+                scene_view(scenes[k], &v, &dev, &depth);
+                if (v.material_count <= 0)
+                        return set_error(GZG_ERR_BAD_SCENE,
+                                         "renderer: scene " + std::to_string(k) + " was uploaded without materials");
+                if (k > 0 && dev != r->device)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: scenes on different devices");
+                r->device = dev;
+                r->scenes.push_back(scenes[k]);
+                r->params.push_back(params[k]);
+        }
+        if (opts) r->opts = *opts;
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != r->device) cudaSetDevice(r->device);
@@ -736,103 +1239,63 @@ GZG_API gzg_status gzg_renderer_create(gzg_scene *scene, const gzg_render_params
                         if (prev != dev) cudaSetDevice(prev);
                 }
         } restore{prev, r->device};
-
-        RenderConst &rc = r->rc;
-        const V3 eye = hv3(P.eye[0], P.eye[1], P.eye[2]);
-        const V3 fwd = hnorm(hsub(hv3(P.target[0], P.target[1], P.target[2]), eye));
-        const V3 right = hnorm(hcross(fwd, hv3(P.up[0], P.up[1], P.up[2])));
-        rc.eye = eye;
-        rc.fwd = fwd;
-        rc.right = right;
-        rc.up = hcross(right, fwd);
-        rc.tan_half = std::tan(P.fov_deg * 3.14159265358979323846f / 180.0f / 2.0f);
-        const float aspect = (float)P.width / (float)P.height;
-        rc.sx0 = aspect > 1.0f ? -aspect : -1.0f;
-        rc.sx1 = -rc.sx0;
-        rc.sy0 = aspect > 1.0f ? -1.0f : -1.0f / aspect;
-        rc.sy1 = -rc.sy0;
-        rc.width = P.width;
-        rc.height = P.height;
-        rc.spp = P.spp;
-        rc.max_depth = P.max_depth;
-        rc.rr_min = P.rr_min_bounce;
-        rc.mis_corrected = P.mis_corrected;
-        rc.first_sample = P.first_sample;
-        rc.filter_radius = P.filter_radius;
-        rc.filter_sigma = P.filter_sigma;
-        // ZSobolSampler.init (ZSobolSampler.swift:114-122)
-        const int64_t sampler_spp = P.sampler_spp > 0 ? P.sampler_spp : P.spp;
-        rc.zs.seed = (uint64_t)P.seed;
-        rc.zs.log2spp = __builtin_ctzll((uint64_t)sampler_spp);
-        int64_t res = std::max(P.width, P.height);
-        res -= 1;
-        res |= res >> 1;
-        res |= res >> 2;
-        res |= res >> 4;
-        res |= res >> 8;
-        res |= res >> 16;
-        res += 1;
-        rc.zs.n_base4_digits = __builtin_ctzll((uint64_t)res) + (rc.zs.log2spp + 1) / 2;
-        gzg_status st = device_sobol(r->device, &rc.zs.matrices);
-        if (st != GZG_OK) return st;
-
+        gzg_status st = build_batch(r.get());
+        if (st) return st;
         Wave &w = r->w;
-        w.total_paths = (uint64_t)P.width * P.height * P.spp;
-        const uint64_t cap = P.wave_paths > 0 ? (uint64_t)P.wave_paths : (uint64_t)(1u << 21);
-        w.capacity = (uint32_t)std::min<uint64_t>(cap, w.total_paths);
-        const size_t C = w.capacity;
+        w.emission_scale = 1.0f;
+        const uint64_t want = r->opts.wave_paths > 0 ? (uint64_t)r->opts.wave_paths : (uint64_t)kDefaultWave;
+        r->max_capacity = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(std::max<uint64_t>(want, kDefaultWave * 2), w.total_paths));
+        const size_t C = r->max_capacity;
+        w.scene_count = (int32_t)n;
+        const size_t keys = (size_t)std::max<int64_t>(n, r->view.material_count) + 1;
+        if (keys > (1u << 20)) return set_error(GZG_ERR_LIMIT, "renderer: more than 2^20 sort keys");
+        const SceneConst *scd = nullptr;
+        if ((st = r->upload(&scd, r->consts))) return st;
+        w.scenes = scd;
         if ((st = r->alloc(&w.zs_morton, C)) || (st = r->alloc(&w.zs_dim, C)) || (st = r->alloc(&w.thr, C)) ||
-            (st = r->alloc(&w.L, C)) || (st = r->alloc(&w.pixel, C)) || (st = r->alloc(&w.weight, C)) ||
-            (st = r->alloc(&w.q_ray[0], 2 * C)) || (st = r->alloc(&w.q_ray[1], 2 * C)) ||
+            (st = r->alloc(&w.L, C)) || (st = r->alloc(&w.pixel, C)) || (st = r->alloc(&w.scene, C)) ||
+            (st = r->alloc(&w.weight, C)) || (st = r->alloc(&w.q_ray[0], 2 * C)) || (st = r->alloc(&w.q_ray[1], 2 * C)) ||
             (st = r->alloc(&w.q_id[0], C)) || (st = r->alloc(&w.q_id[1], C)) || (st = r->alloc(&w.hits, C)) ||
             (st = r->alloc(&w.sh_ray, 2 * C)) || (st = r->alloc(&w.sh_id, C)) || (st = r->alloc(&w.sh_contrib, C)) ||
             (st = r->alloc(&w.sh_occ, C)) || (st = r->alloc(&w.pr_ray, 2 * C)) || (st = r->alloc(&w.pr_id, C)) ||
-            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) ||
-            (st = r->alloc(&w.counts, kCountWords)) || (st = r->alloc(&w.stats, kStatWords)))
+            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) ||
+            (st = r->alloc(&w.key_hist, 2 * keys)) || (st = r->alloc(&w.counts, kCountWords)) ||
+            (st = r->alloc(&w.stats, kStatWords)))
                 return st;
-        st = cuda_err(cudaMemset(w.counts, 0, kCountWords * 4), "renderer counters");
-        if (st) return st;
-        st = cuda_err(cudaMemset(w.stats, 0, kStatWords * 8), "renderer statistics");
-        if (st) return st;
+        if ((st = cuda_err(cudaMemset(w.key_hist, 0, 2 * keys * sizeof(uint32_t)), "sort histogram"))) return st;
+        if ((st = cuda_err(cudaMemset(w.counts, 0, kCountWords * 4), "renderer counters"))) return st;
+        if ((st = cuda_err(cudaMemset(w.stats, 0, kStatWords * 8), "renderer statistics"))) return st;
+        r->configure((uint32_t)std::min<uint64_t>(want, w.total_paths), r->opts.sort_key);
         *out = r.release();
         return clear_error();
 }
 
-GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res_x, int32_t res_y, int64_t seed,
-                                          const int32_t *px, const int32_t *py, const int64_t *index, int64_t n,
-                                          const int32_t *kinds, int32_t nkinds, float *out, void *stream) {
-        if (samples_per_pixel <= 0 || res_x <= 0 || res_y <= 0 || n < 0 || nkinds < 0 || nkinds > 64 ||
-            (n > 0 && (!px || !py || !index || !out)) || (nkinds > 0 && !kinds))
-                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_zsobol_fill_device: bad arguments");
-        int per = 0;
-        for (int k = 0; k < nkinds; ++k) {
-                if (kinds[k] < 1 || kinds[k] > 3) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_zsobol_fill_device: kind not 1, 2 or 3");
-                per += kinds[k];
-        }
-        if (n == 0 || nkinds == 0) return clear_error();
-        int dev = 0;
-        cudaGetDevice(&dev);
-        ZSobolConfig c{};
-        gzg_status st = device_sobol(dev, &c.matrices);
-        if (st) return st;
-        c.seed = (uint64_t)seed;
-        c.log2spp = __builtin_ctzll((uint64_t)samples_per_pixel);
-        int64_t res = std::max(res_x, res_y);
-        res -= 1;
-        res |= res >> 1;
-        res |= res >> 2;
-        res |= res >> 4;
-        res |= res >> 8;
-        res |= res >> 16;
-        res += 1;
-        c.n_base4_digits = __builtin_ctzll((uint64_t)res) + (c.log2spp + 1) / 2;
-        KindList kl{};
-        for (int k = 0; k < nkinds; ++k) kl.k[k] = kinds[k];
-        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-        k_zsobol_fill<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(c, px, py, index, n, kl, nkinds, per, out);
-        st = cuda_err(cudaGetLastError(), "zsobol launch");
-        if (!st) clear_error();
-        return st;
+}  // namespace
+
+extern "C" {
+
+GZG_API gzg_status gzg_renderer_create(gzg_scene *scene, const gzg_render_params *params, gzg_renderer **out) {
+        if (!params) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_create: null argument");
+        gzg_batch_options o{};
+        o.wave_paths = params->wave_paths;
+        o.use_graph = params->use_graph;
+        o.sort_key = GZG_SORT_NONE;
+        return renderer_create(&scene, params, 1, &o, out);
+}
+
+GZG_API gzg_status gzg_batch_renderer_create(gzg_scene *const *scenes, const gzg_render_params *params,
+                                             int64_t scene_count, const gzg_batch_options *options,
+                                             gzg_renderer **out) {
+        if (options && (options->sort_key < 0 || options->sort_key > 2))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_batch_renderer_create: unknown sort key");
+        return renderer_create(scenes, params, scene_count, options, out);
+}
+
+GZG_API gzg_status gzg_renderer_film_layout(const gzg_renderer *r, int64_t *pixel_offsets) {
+        if (!r || !pixel_offsets) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_film_layout: null argument");
+        std::copy(r->film_offsets.begin(), r->film_offsets.end(), pixel_offsets);
+        return clear_error();
 }
 
 GZG_API gzg_status gzg_renderer_destroy(gzg_renderer *renderer) {
@@ -845,47 +1308,161 @@ GZG_API gzg_status gzg_renderer_render(gzg_renderer *r, float *film_rgb, float *
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != r->device) cudaSetDevice(r->device);
+        const gzg_status st = r->render(film_rgb, film_sq, film_w, reinterpret_cast<cudaStream_t>(stream));
+        if (prev != r->device) cudaSetDevice(prev);
+        if (!st) clear_error();
+        return st;
+}
+
+// Times whole renders over wave sizes and sort keys (into scratch films) and
+// keeps the fastest configuration.
+GZG_API gzg_status gzg_renderer_autotune(gzg_renderer *r, gzg_batch_options *best, float *best_ms, void *stream) {
+        if (!r) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_autotune: null argument");
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
         cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-        gzg_status status = GZG_OK;
-        const uint64_t waves = (r->w.total_paths + r->w.capacity - 1) / r->w.capacity;
-        k_set_wave_base<<<1, 1, 0, st>>>(r->w, 0ull);
-        if (r->params.use_graph) {
-                const bool same_films =
-                    r->graph && r->graph_film[0] == film_rgb && r->graph_film[1] == film_sq && r->graph_film[2] == film_w;
-                if (!same_films) {
-                        if (r->graph) cudaGraphExecDestroy(r->graph);
-                        if (r->graph_def) cudaGraphDestroy(r->graph_def);
-                        r->graph = nullptr;
-                        r->graph_def = nullptr;
-                        cudaStream_t cap;
-                        status = cuda_err(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
-                        if (!status) {
-                                status = cuda_err(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
-                                if (!status) {
-                                        cudaError_t e = r->enqueue_wave(film_rgb, film_sq, film_w, cap);
-                                        cudaError_t e2 = cudaStreamEndCapture(cap, &r->graph_def);
-                                        status = cuda_err(e != cudaSuccess ? e : e2, "graph capture of a wave");
-                                        if (!status)
-                                                status = cuda_err(cudaGraphInstantiate(&r->graph, r->graph_def, 0),
-                                                                  "graph instantiate");
-                                }
-                                cudaStreamDestroy(cap);
-                        }
-                        if (!status) {
-                                r->graph_film[0] = film_rgb;
-                                r->graph_film[1] = film_sq;
-                                r->graph_film[2] = film_w;
+        const int64_t pix = r->film_offsets.back();
+        float *rgb = nullptr, *wgt = nullptr;
+        gzg_status status = r->alloc(&rgb, 3 * (size_t)pix);
+        if (!status) status = r->alloc(&wgt, (size_t)pix);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        const uint32_t waves[] = {1u << 19, 1u << 20, 1u << 21, 1u << 22};
+        const int keys[] = {kSortNone, kSortMaterial, kSortScene};
+        uint32_t best_cap = r->w.capacity;
+        int best_key = r->w.sort_key;
+        float best_t = 1e30f;
+        const int saved_graph = r->opts.use_graph;
+        r->opts.use_graph = 1;
+        for (int key : keys)
+                for (uint32_t cap : waves) {
+                        if (status) break;
+                        if (cap > r->max_capacity && cap != waves[0]) continue;
+                        r->configure(cap, key);
+                        status = r->render(rgb, nullptr, wgt, st);  // warm-up and graph capture
+                        if (status) break;
+                        cudaEventRecord(e0, st);
+                        status = r->render(rgb, nullptr, wgt, st);
+                        cudaEventRecord(e1, st);
+                        if (!status) status = cuda_err(cudaEventSynchronize(e1), "renderer autotune");
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (!status && ms < best_t) {
+                                best_t = ms;
+                                best_cap = r->w.capacity;
+                                best_key = key;
                         }
                 }
-                for (uint64_t k = 0; k < waves && !status; ++k)
-                        status = cuda_err(cudaGraphLaunch(r->graph, st), "graph launch");
-        } else {
-                for (uint64_t k = 0; k < waves && !status; ++k)
-                        status = cuda_err(r->enqueue_wave(film_rgb, film_sq, film_w, st), "wave launch");
-        }
+        r->opts.use_graph = saved_graph;
+        if (!status) status = cuda_err(cudaMemsetAsync(r->w.stats, 0, kStatWords * 8, st), "renderer statistics");
+        r->configure(best_cap, best_key);
+        r->opts.wave_paths = (int32_t)best_cap;
+        r->opts.sort_key = best_key;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (!status && best) *best = r->opts;
+        if (!status && best_ms) *best_ms = best_t;
         if (prev != r->device) cudaSetDevice(prev);
         if (!status) clear_error();
         return status;
+}
+
+GZG_API gzg_status gzg_renderer_set_textures(gzg_renderer *r, const gzg_texture_binding *bindings, int32_t count,
+                                             int32_t resolution, const float *texels, float emission_scale) {
+        if (!r) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_set_textures: null renderer");
+        if (r->scenes.size() != 1)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "gzg_renderer_set_textures: textures need a single-scene renderer");
+        if (count < 0 || (count > 0 && (!bindings || !texels || resolution < 1 || resolution > 16384)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_set_textures: bad texture arguments");
+        if (!std::isfinite(emission_scale))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_set_textures: emission scale not finite");
+        if ((int64_t)count * resolution * resolution * 3 >= ((int64_t)1 << 31))
+                return set_error(GZG_ERR_LIMIT, "gzg_renderer_set_textures: more than 2^31 texel values");
+        const int32_t nm = r->view.material_count;
+        std::vector<int32_t> mat_tex(nm, -1);
+        std::vector<float> maps(9 * (size_t)count);
+        for (int32_t t = 0; t < count; ++t) {
+                const gzg_texture_binding &b = bindings[t];
+                if (b.material < 0 || b.material >= nm)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         "gzg_renderer_set_textures: binding " + std::to_string(t) + " names material " +
+                                             std::to_string(b.material) + " of " + std::to_string(nm));
+                mat_tex[b.material] = t;
+                std::copy(b.origin, b.origin + 3, maps.begin() + 9 * t);
+                std::copy(b.u_axis, b.u_axis + 3, maps.begin() + 9 * t + 3);
+                std::copy(b.v_axis, b.v_axis + 3, maps.begin() + 9 * t + 6);
+        }
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        gzg_status st = GZG_OK;
+        if (count > 0) {
+                if (!r->d_mat_tex) st = r->alloc(&r->d_mat_tex, (size_t)nm);
+                if (!st && count > r->tex_slots) {
+                        st = r->alloc(&r->d_tex_map, 9 * (size_t)count);
+                        if (!st) r->tex_slots = count;
+                }
+                if (!st)
+                        st = cuda_err(cudaMemcpy(r->d_mat_tex, mat_tex.data(), 4 * (size_t)nm, cudaMemcpyHostToDevice),
+                                      "texture bindings");
+                if (!st)
+                        st = cuda_err(cudaMemcpy(r->d_tex_map, maps.data(), 4 * maps.size(), cudaMemcpyHostToDevice),
+                                      "texture maps");
+        }
+        if (prev != r->device) cudaSetDevice(prev);
+        if (st) return st;
+        r->w.tex = count > 0 ? texels : nullptr;
+        r->w.mat_tex = count > 0 ? r->d_mat_tex : nullptr;
+        r->w.tex_map = count > 0 ? r->d_tex_map : nullptr;
+        r->w.tex_res = count > 0 ? resolution : 0;
+        r->w.emission_scale = emission_scale;
+        r->drop_graph();
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_renderer_render_f64(gzg_renderer *r, double *film_rgb, double *film_sq, double *film_w,
+                                           void *stream) {
+        if (!r || !film_rgb || !film_w)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_render_f64: null argument");
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        const gzg_status st = r->render_f64(film_rgb, film_sq, film_w, reinterpret_cast<cudaStream_t>(stream));
+        if (prev != r->device) cudaSetDevice(prev);
+        if (!st) clear_error();
+        return st;
+}
+
+GZG_API gzg_status gzg_renderer_adjoint(gzg_renderer *r, const float *adj_rgb, const float *film_w, float *d_texels,
+                                        double *d_emission, void *stream) {
+        if (!r || !adj_rgb || !film_w) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_adjoint: null argument");
+        if (r->w.mat_tex && !d_texels)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_adjoint: textures bound but no texel gradient");
+        if (d_emission && r->w.emission_scale == 0.0f)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "gzg_renderer_adjoint: emission gradient needs a nonzero scale");
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        const gzg_status st = r->adjoint(adj_rgb, film_w, d_texels, d_emission, reinterpret_cast<cudaStream_t>(stream));
+        if (prev != r->device) cudaSetDevice(prev);
+        if (!st) clear_error();
+        return st;
+}
+
+GZG_API gzg_status gzg_renderer_error_word(gzg_renderer *r, uint32_t *word, int32_t clear) {
+        if (!r || !word) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_error_word: null argument");
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        gzg_status st = cuda_err(cudaMemcpy(word, r->view.err, 4, cudaMemcpyDeviceToHost), "error word read");
+        if (!st && clear) st = cuda_err(cudaMemset(r->view.err, 0, 4), "error word clear");
+        if (prev != r->device) cudaSetDevice(prev);
+        if (!st) clear_error();
+        return st;
 }
 
 GZG_API gzg_status gzg_renderer_stats(const gzg_renderer *r, gzg_render_stats *out) {
@@ -899,6 +1476,34 @@ GZG_API gzg_status gzg_renderer_stats(const gzg_renderer *r, gzg_render_stats *o
         out->probe_rays = s[kStatProbe];
         out->waves = s[kStatWaves];
         return clear_error();
+}
+
+GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res_x, int32_t res_y, int64_t seed,
+                                          const int32_t *px, const int32_t *py, const int64_t *index, int64_t n,
+                                          const int32_t *kinds, int32_t nkinds, float *out, void *stream) {
+        if (samples_per_pixel <= 0 || res_x <= 0 || res_y <= 0 || n < 0 || nkinds < 0 || nkinds > 64 ||
+            (n > 0 && (!px || !py || !index || !out)) || (nkinds > 0 && !kinds))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_zsobol_fill_device: bad arguments");
+        int per = 0;
+        for (int k = 0; k < nkinds; ++k) {
+                if (kinds[k] < 1 || kinds[k] > 3)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_zsobol_fill_device: kind not 1, 2 or 3");
+                per += kinds[k];
+        }
+        if (n == 0 || nkinds == 0) return clear_error();
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const uint32_t *matrices = nullptr;
+        gzg_status st = device_sobol(dev, &matrices);
+        if (st) return st;
+        const ZSobolConfig c = make_zsobol(samples_per_pixel, res_x, res_y, seed, matrices);
+        KindList kl{};
+        for (int k = 0; k < nkinds; ++k) kl.k[k] = kinds[k];
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        k_zsobol_fill<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(c, px, py, index, n, kl, nkinds, per, out);
+        st = cuda_err(cudaGetLastError(), "zsobol launch");
+        if (!st) clear_error();
+        return st;
 }
 
 GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *params, float *film_rgb, float *film_sq,
@@ -920,7 +1525,7 @@ GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *p
                 if ((st = cuda_err(cudaMemset(d_rgb, 0, 3 * pix * 4), "film clear"))) break;
                 if ((st = cuda_err(cudaMemset(d_w, 0, pix * 4), "film clear"))) break;
                 if (d_sq && (st = cuda_err(cudaMemset(d_sq, 0, 3 * pix * 4), "film clear"))) break;
-                if ((st = gzg_renderer_render(r, d_rgb, d_sq, d_w, nullptr))) break;
+                if ((st = r->render(d_rgb, d_sq, d_w, nullptr))) break;
                 if ((st = cuda_err(cudaDeviceSynchronize(), "render"))) break;
                 if ((st = cuda_err(cudaMemcpy(film_rgb, d_rgb, 3 * pix * 4, cudaMemcpyDeviceToHost), "film copy"))) break;
                 if ((st = cuda_err(cudaMemcpy(film_w, d_w, pix * 4, cudaMemcpyDeviceToHost), "film copy"))) break;

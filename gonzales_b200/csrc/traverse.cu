@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
         int prim = -1;
         uint32_t steps = 0, n_nodes = 0, n_tris = 0;
         // The root is key 0 of a virtual parent whose only interior slot is oct.
-        uint2 group = make_uint2(0u, (1u << 24) | (1u << r.oct));
+        uint2 group = make_uint2(s.per_ray_root ? in.root : 0u, (1u << 24) | (1u << r.oct));
         for (;;) {
                 uint32_t tri_hits = 0, tri_base = 0;
                 uint32_t hits = group.y >> 24;
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void 
                                 prim = -1;
                                 sp = 0;
                                 steps = 0;
-                                group = make_uint2(0u, (1u << 24) | (1u << r.oct));
+                                group = make_uint2(s.per_ray_root ? in.root : 0u, (1u << 24) | (1u << r.oct));
                         }
                         const int npop = __popc(need);
                         cursor += npop < avail ? npop : avail;

@@ -287,3 +287,105 @@ def box_scene(seed=0xB0):
     lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
     sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
     return sb
+
+
+# ---------------------------------------------------------------- scene batches
+
+BATCH_SIDES = (64, 128, 256, 512)
+
+
+def _room(sb, rng):
+    """The box scene's five inward walls of the unit cube (10 triangles)."""
+    walls = [
+        _quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)),
+        _quad((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0)),
+        _quad((0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0)),
+        _quad((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0)),
+        _quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1)),
+    ]
+    pts = np.concatenate([w[0] for w in walls])
+    tris = np.concatenate([w[1] + 4 * i for i, w in enumerate(walls)])
+    sb.add_mesh(pts, tris, sb.add_material(rng.uniform(0.1, 0.8, 3)))
+
+
+def _icosphere_cluster(sb, rng, target):
+    """Displaced icospheres (20 * 4**s triangles each, s <= 7) whose triangle
+    counts add up to about `target`, scattered in the lower half of the room."""
+    left = int(target)
+    sizes = []
+    for s in range(7, 1, -1):
+        n = 20 * 4 ** s
+        while left >= n:
+            sizes.append(s)
+            left -= n
+    if not sizes:
+        sizes.append(2)
+    for k, s in enumerate(sizes):
+        pts, tris = displaced_icosphere(s, amplitude=0.08, seed=int(rng.integers(1 << 30)))
+        radius = 0.09 + 0.16 * rng.random() / math.sqrt(1 + k)
+        centre = (rng.uniform(0.2, 0.8), radius + 0.01 + rng.uniform(0.0, 0.3), rng.uniform(0.2, 0.8))
+        sb.add_mesh(pts * np.float32(radius) + np.asarray(centre, np.float32), tris,
+                    sb.add_material(rng.uniform(0.1, 0.8, 3)))
+
+
+def _box_stacks(sb, rng, target):
+    """About target / 12 small rotated boxes stacked in columns on the floor."""
+    n_boxes = max(1, int(target) // 12)
+    cols = max(1, int(math.ceil(math.sqrt(n_boxes / 6.0))))
+    per_col = int(math.ceil(n_boxes / float(cols * cols)))
+    pitch = 0.8 / cols
+    size = 0.8 * pitch
+    height = min(size, 0.7 / per_col)
+    pts_all, tris_all = [], []
+    k = 0
+    for i in range(cols):
+        for j in range(cols):
+            for h in range(per_col):
+                if k >= n_boxes:
+                    break
+                c = (0.1 + (i + 0.5) * pitch, (h + 0.5) * height + 1e-4, 0.1 + (j + 0.5) * pitch)
+                bp, bt = _box(1.0, rng.uniform(0, math.pi / 2), (0.0, 0.0, 0.0))
+                bp = bp * np.array([size * 0.9, height * 0.95, size * 0.9]) + np.asarray(c)
+                pts_all.append(bp)
+                tris_all.append(bt + 8 * k)
+                k += 1
+    sb.add_mesh(np.concatenate(pts_all).astype(np.float32), np.concatenate(tris_all),
+                sb.add_material(rng.uniform(0.1, 0.8, 3)))
+
+
+def _ceiling_lights(sb, rng, n_lights):
+    """n_lights emissive ceiling quads, wound to face down, total power about
+    that of the box scene's light."""
+    sides = rng.uniform(0.08, 0.2, n_lights)
+    scale = 0.09 / float(np.sum(sides ** 2))
+    for s in sides:
+        x, z = rng.uniform(0.05, 0.95 - s, 2)
+        lp, lt = _quad((x, 0.999, z), (x + s, 0.999, z), (x + s, 0.999, z + s), (x, 0.999, z + s))
+        colour = rng.uniform(0.5, 1.0, 3)
+        sb.add_area_light(lp, lt, tuple(15.0 * scale * colour / colour.max()))
+
+
+def batch_scene(seed, target_tris):
+    """One scene of the batched workload: the room, about `target_tris`
+    triangles of displaced icospheres or box stacks, 1-8 ceiling lights."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    _room(sb, rng)
+    if rng.random() < 0.5:
+        _icosphere_cluster(sb, rng, target_tris)
+    else:
+        _box_stacks(sb, rng, target_tris)
+    _ceiling_lights(sb, rng, int(rng.integers(1, 9)))
+    return sb
+
+
+def batch_workload(n_scenes=64, seed=0xC3, tri_lo=1_000, tri_hi=500_000, sides=BATCH_SIDES):
+    """The scene-batch workload: per scene (builder, image side).  Triangle
+    counts are log-uniform in [tri_lo, tri_hi]; sides uniform among `sides`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        target = math.exp(rng.uniform(math.log(tri_lo), math.log(tri_hi)))
+        side = int(rng.choice(sides))
+        out.append((batch_scene(int(rng.integers(1 << 62)), target), side))
+    return out

@@ -381,6 +381,87 @@ GZG_API gzg_status gzg_renderer_render(gzg_renderer *renderer, float *film_rgb, 
 
 GZG_API gzg_status gzg_renderer_stats(const gzg_renderer *renderer, gzg_render_stats *stats);
 
+/* Sort of the extension queue before shading. */
+typedef enum gzg_sort_key {
+        GZG_SORT_NONE = 0,
+        GZG_SORT_MATERIAL = 1,  /* by the hit's material (batch-wide index) */
+        GZG_SORT_SCENE = 2      /* by the path's scene */
+} gzg_sort_key;
+
+/* Options of a batch renderer (the per-scene wave_paths / use_graph of
+ * gzg_render_params are not used by a batch). */
+typedef struct gzg_batch_options {
+        int32_t wave_paths;  /* paths in flight per wave (0: library default) */
+        int32_t use_graph;   /* capture one wave as a CUDA graph and replay it */
+        int32_t sort_key;    /* gzg_sort_key */
+        int32_t reserved;
+} gzg_batch_options;
+
+/* Creates one renderer over many scenes (no reference counterpart: Gonzales
+ * renders one scene per process).  Scene k is rendered with params[k] into
+ * its window of one batch film: pixels [offset_k, offset_k + W_k*H_k) where
+ * the offsets come from gzg_renderer_film_layout.  Paths of all scenes share
+ * the waves; each path carries its scene and starts traversal at its scene's
+ * root of one concatenated wide tree.  All scenes live on one device and were
+ * uploaded with materials; two-level scenes are rejected. */
+GZG_API gzg_status gzg_batch_renderer_create(gzg_scene *const *scenes, const gzg_render_params *params,
+                                             int64_t scene_count, const gzg_batch_options *options,
+                                             gzg_renderer **out);
+
+/* Writes scene_count + 1 pixel offsets of the batch film (the last one is
+ * the film's total pixel count). */
+GZG_API gzg_status gzg_renderer_film_layout(const gzg_renderer *renderer, int64_t *pixel_offsets);
+
+/* Times whole renders (into scratch films) over wave sizes and sort keys,
+ * keeps the fastest configuration and returns it (and its time per render in
+ * ms).  Synchronous; resets the renderer's statistics. */
+GZG_API gzg_status gzg_renderer_autotune(gzg_renderer *renderer, gzg_batch_options *best, float *best_ms,
+                                         void *stream);
+
+/* Reads (and with clear != 0 resets) the device error word the renderer's
+ * traversals report to. */
+GZG_API gzg_status gzg_renderer_error_word(gzg_renderer *renderer, uint32_t *word, int32_t clear);
+
+/* ------------------------------------------------------------------------- */
+/* Differentiable rendering (path-replay adjoint)                             */
+/* ------------------------------------------------------------------------- */
+
+/* An albedo texture over material `material` (no reference counterpart: the
+ * reference's GPU path has no textures or derivatives).  Nearest texel of a
+ * resolution x resolution RGB grid laid over a plane through `origin`:
+ * u = dot(p - origin, u_axis), v = dot(p - origin, v_axis), texel
+ * (ix, iy) = (int)clamp((u, v) * resolution, 0, resolution - 1). */
+typedef struct gzg_texture_binding {
+        int32_t material;
+        int32_t reserved;
+        float origin[3], u_axis[3], v_axis[3];
+} gzg_texture_binding;
+
+/* Binds `count` textures (texture t uses bindings[t]) whose texels live in
+ * the DEVICE array texels[count][resolution][resolution][3] (row iy, column
+ * ix), borrowed and read at render time, and scales every emission by
+ * emission_scale.  count = 0 removes the textures.  Single-scene renderers
+ * only.  Russian roulette is not differentiated: adjoint renders should set
+ * rr_min_bounce >= max_depth. */
+GZG_API gzg_status gzg_renderer_set_textures(gzg_renderer *renderer, const gzg_texture_binding *bindings,
+                                             int32_t count, int32_t resolution, const float *texels,
+                                             float emission_scale);
+
+/* gzg_renderer_render with double-precision DEVICE films (each path's
+ * radiance is still computed in FP32; only the sums are FP64). */
+GZG_API gzg_status gzg_renderer_render_f64(gzg_renderer *renderer, double *film_rgb, double *film_sq,
+                                           double *film_w, void *stream);
+
+/* Path-replay adjoint of one render pass: given adj_rgb = dLoss/dImage per
+ * pixel (DEVICE, 3 floats per pixel, image = film_rgb / film_w) and the
+ * pass's film_w (DEVICE), ADDS dLoss/dtexel to d_texels (DEVICE, the texel
+ * layout) and dLoss/demission_scale to *d_emission (DEVICE, may be NULL).
+ * Each wave is traced twice: a primal pass keeps each path's radiance, then
+ * the replay draws the same samples and, at every textured vertex, adds
+ * adj * (radiance still to come) / albedo.  Asynchronous on `stream`. */
+GZG_API gzg_status gzg_renderer_adjoint(gzg_renderer *renderer, const float *adj_rgb, const float *film_w,
+                                        float *d_texels, double *d_emission, void *stream);
+
 /* Device Z-Sobol values (Sampler/ZSobolSampler.swift:6-280): for each of n
  * pixel samples (device arrays px, py, index) the values of the get1D / get2D /
  * get3D calls listed in the HOST array kinds (1, 2 or 3 each, at most 64),

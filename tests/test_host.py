@@ -168,3 +168,33 @@ def test_upload_valid_scene_without_device_reports_no_device():
         pytest.skip("device present")
     st, _ = _upload_status(scenes.raycast_scene(subdiv=1).build())
     assert st == 2
+
+
+def test_batch_renderer_rejects_bad_arguments_before_touching_a_device():
+    L = F.lib()
+    h = C.c_void_p()
+    p = F.render_params(8, 8, 1)
+    opts = F.BatchOptions(0, 0, 0, 0)
+    assert L.gzg_batch_renderer_create(None, C.byref(p), 1, C.byref(opts), C.byref(h)) == 1
+    assert L.gzg_batch_renderer_create(None, C.byref(p), 0, C.byref(opts), C.byref(h)) == 1
+    assert L.gzg_batch_renderer_create(None, C.byref(p), 1, C.byref(opts), None) == 1
+    bad = F.BatchOptions(0, 0, 9, 0)
+    assert L.gzg_batch_renderer_create(None, C.byref(p), 1, C.byref(bad), C.byref(h)) == 1
+    assert "sort key" in L.gzg_last_error().decode()
+    assert L.gzg_renderer_film_layout(None, None) == 1
+    assert L.gzg_renderer_autotune(None, None, None, None) == 1
+    assert L.gzg_renderer_error_word(None, None, 0) == 1
+    assert L.gzg_renderer_set_textures(None, None, 0, 0, None, 1.0) == 1
+    assert L.gzg_renderer_render_f64(None, None, None, None, None) == 1
+    assert L.gzg_renderer_adjoint(None, None, None, None, None, None) == 1
+    assert L.gzg_renderer_destroy(None) == 0
+
+
+def test_batch_workload_shapes():
+    work = scenes.batch_workload(n_scenes=6, seed=5, tri_lo=1_000, tri_hi=4_000)
+    assert len(work) == 6
+    for sb, side in work:
+        assert side in scenes.BATCH_SIDES
+        n = sum(m.triangle_count for m in sb.meshes)
+        assert 10 + 2 <= n <= 10 + 4_000 + 16
+        assert 1 <= len(sb._lights) // 2 <= 8
