@@ -202,7 +202,30 @@ struct Scene {
         std::vector<float> cumulative;
         float total_power = 0.0f;
         const orc_render_params *p;
+        const orc_textures *tex = nullptr;
+        float escale = 1.0f;
 };
+
+// Emission times the scene's emission scale (1 without textures: exact).
+V3 emitted(const Scene &sc, V3 e) { return v3(e.x * sc.escale, e.y * sc.escale, e.z * sc.escale); }
+
+// Albedo of material m at p: its texture's nearest texel, else its constant.
+V3 albedo_at(const Scene &sc, int64_t m, V3 p) {
+        const orc_material &mat = sc.materials[m];
+        if (sc.tex && sc.tex->material_texture[m] >= 0) {
+                const int t = sc.tex->material_texture[m];
+                const int R = sc.tex->resolution;
+                const float *mp = sc.tex->maps + 9 * t;
+                const V3 d = sub(p, v3(mp[0], mp[1], mp[2]));
+                const float u = dot(d, v3(mp[3], mp[4], mp[5])), v = dot(d, v3(mp[6], mp[7], mp[8]));
+                // fmax/fmin: a NaN coordinate lands on texel 0
+                const int ix = (int)std::fmin(std::fmax(u * (float)R, 0.0f), (float)(R - 1));
+                const int iy = (int)std::fmin(std::fmax(v * (float)R, 0.0f), (float)(R - 1));
+                const float *tx = sc.tex->texels + (((size_t)t * R + iy) * R + ix) * 3;
+                return v3(tx[0], tx[1], tx[2]);
+        }
+        return v3(mat.albedo[0], mat.albedo[1], mat.albedo[2]);
+}
 
 bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
         const orc_prim_id &pr = sc.prims[k];
@@ -305,12 +328,12 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 const bool is_light = pr.type == 3;
                 if (bounce == 0 && is_light) {
                         const orc_material &lm = sc.materials[pr.material_index];
-                        if (dot(ng, wo) > 0.0f) L = add(L, mulv(thr, v3(lm.emission[0], lm.emission[1], lm.emission[2])));
+                        if (dot(ng, wo) > 0.0f)
+                                L = add(L, mulv(thr, emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]))));
                 }
                 // Area lights have materialIndex 0 in their interaction
                 // (Core/SurfaceInteraction.swift:20).
-                const orc_material &mat = sc.materials[is_light ? 0 : pr.material_index];
-                const V3 refl = v3(mat.albedo[0], mat.albedo[1], mat.albedo[2]);
+                const V3 refl = albedo_at(sc, is_light ? 0 : pr.material_index, pos);
                 const V3 f_val = mul(refl, 1.0f / kPi);
                 Frame fr;
                 if (!make_frame(p0, p1, p2, ng, &fr)) break;
@@ -348,7 +371,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                         const bool reflect = dot(dir, ng) * dot(wo, ng) > 0.0f;
                                         const V3 f = reflect ? f_val : v3(0, 0, 0);
                                         const V3 scatter = mul(f, std::fabs(dot(dir, ng)));
-                                        light_est = mulv(scatter, lt.le);
+                                        light_est = mulv(scatter, emitted(sc, lt.le));
                                         light_dir = dir;
                                         light_pdf = pdf;
                                 }
@@ -383,7 +406,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                         const V3 qn = normalize(cross(sub(q0, q2), sub(q1, q2)));
                                         const orc_material &lm = sc.materials[sc.prims[ph.prim].material_index];
                                         if (dot(qn, neg(wi)) > 0.0f)
-                                                radiance = v3(lm.emission[0], lm.emission[1], lm.emission[2]);
+                                                radiance = emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]));
                                 }
                                 est = mulv(est, radiance);
                                 float light_density = 0.0f;
@@ -427,11 +450,13 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
 
 }  // namespace
 
-extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
-                           const orc_material *materials, int64_t n_materials, int64_t n_prims,
-                           const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
-                           uint64_t *counters, int threads) {
+extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                                    const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                                    const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
+                                    float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
         Scene sc;
+        sc.tex = textures;
+        sc.escale = textures ? textures->emission_scale : 1.0f;
         sc.nodes = nodes;
         sc.prims = prims;
         sc.meshes = meshes;
@@ -530,4 +555,12 @@ extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, cons
         if (counters)
                 for (int ti = 0; ti < threads; ++ti)
                         for (int k = 0; k < 4; ++k) counters[k] += cnt[4 * ti + k];
+}
+
+extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                           const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                           const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
+                           uint64_t *counters, int threads) {
+        orc_render_textured(nodes, prims, meshes, materials, n_materials, n_prims, params, nullptr, sum_rgb, sum_sq,
+                            sum_w, counters, threads);
 }

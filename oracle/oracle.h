@@ -110,6 +110,27 @@ void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh 
                 const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                 uint64_t *counters, int threads);
 
+/* Albedo textures and an emission scale for the differentiable renderer's
+ * scene: material m with material_texture[m] = t >= 0 takes its albedo from
+ * texture t, a res x res RGB grid (texels[((t * res + iy) * res + ix) * 3 + c])
+ * laid over a plane: u = dot(p - origin, u_axis), v = dot(p - origin, v_axis),
+ * ix = (int)clamp(u * res, 0, res - 1), iy likewise (nearest texel).  Every
+ * emission (emitted hits, light samples, probes) is multiplied by
+ * emission_scale.  Not part of the reference, whose scenes carry no textures
+ * on this path; the oracle's finite differences check the GPU adjoint. */
+typedef struct orc_textures {
+        int32_t count, resolution;
+        const int32_t *material_texture; /* n_materials entries */
+        const float *maps;               /* count x {origin[3], u_axis[3], v_axis[3]} */
+        const float *texels;
+        float emission_scale;
+} orc_textures;
+
+void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                         const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                         const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
+                         float *sum_sq, float *sum_w, uint64_t *counters, int threads);
+
 /* PathState_C (mojo_kernel.h:36-44). */
 typedef struct orc_path_state {
         orc_ray ray;

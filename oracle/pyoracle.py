@@ -196,14 +196,23 @@ def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_correcte
                         first_sample, sampler_spp)
 
 
-def render(hs, params, threads=0):
+class _Textures(C.Structure):
+    _fields_ = [("count", C.c_int32), ("resolution", C.c_int32), ("material_texture", C.c_void_p),
+                ("maps", C.c_void_p), ("texels", C.c_void_p), ("emission_scale", C.c_float)]
+
+
+def render(hs, params, threads=0, textures=None):
     """Film sums of the oracle integrator: (sum_rgb (H,W,3), sum_sq (H,W,3),
-    sum_w (H,W), counters {camera, extension, shadow, probe})."""
+    sum_w (H,W), counters {camera, extension, shadow, probe}).
+
+    textures (optional): dict with material_texture (int32 per material, -1
+    for none), maps (count x 9 float32: origin, u axis, v axis), texels
+    (count x R x R x 3 float32) and emission_scale (float)."""
     L = lib()
     if not getattr(L, "_render_bound", False):
-        L.orc_render.restype = None
-        L.orc_render.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.POINTER(RenderParams)] + \
-            [C.c_void_p] * 4 + [C.c_int]
+        L.orc_render_textured.restype = None
+        L.orc_render_textured.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.POINTER(RenderParams),
+                                                             C.c_void_p] + [C.c_void_p] * 4 + [C.c_int]
         L._render_bound = True
     keep = []
     arr = (_Mesh * max(len(hs.meshes), 1))()
@@ -220,8 +229,20 @@ def render(hs, params, threads=0):
     cnt = np.zeros(4, np.uint64)
     if threads <= 0:
         threads = os.cpu_count() or 1
-    L.orc_render(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr), _p(mats),
-                 len(mats), len(hs.prims), C.byref(params), _p(s), _p(s2), _p(sw), _p(cnt), threads)
+    tex = None
+    if textures is not None:
+        mt = np.ascontiguousarray(textures["material_texture"], np.int32)
+        maps = np.ascontiguousarray(textures["maps"], np.float32)
+        tx = np.ascontiguousarray(textures["texels"], np.float32)
+        if len(mt) != len(mats) or tx.ndim != 4 or tx.shape[1] != tx.shape[2] or tx.shape[3] != 3 \
+                or maps.shape != (tx.shape[0], 9):
+            raise ValueError("oracle render: inconsistent texture arrays")
+        keep += [mt, maps, tx]
+        tex = _Textures(tx.shape[0], tx.shape[1], mt.ctypes.data, maps.ctypes.data, tx.ctypes.data,
+                        float(textures.get("emission_scale", 1.0)))
+    L.orc_render_textured(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr),
+                          _p(mats), len(mats), len(hs.prims), C.byref(params),
+                          C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw), _p(cnt), threads)
     return s, s2, sw, {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
 
 
