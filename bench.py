@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="small case for profiler captures")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    ap.add_argument("--skip-batch", action="store_true", help="omit the scene-batch and adjoint legs")
     return ap.parse_args()
 
 
@@ -200,6 +201,147 @@ def render_leg(acc_box, args, stream, barrier):
                       % (W, H, RENDER["spp"], RENDER["max_depth"], RENDER["rr_min_bounce"]),
             "spp_per_s": spp / ms * 1000.0, "ms_per_frame": ms, "mrays_per_s": rays / ms / 1000.0,
             "rays_per_frame": rays, "steps": steps, "graph": True}
+
+
+BATCH = dict(n_scenes=64, seed=0xC3, spp=32, max_depth=6, rr_min_bounce=2, ref_spp=256)
+
+
+def batch_leg(args, stream, barrier):
+    """The scene batch: 64 scenes (triangles log-uniform in 1k-500k,
+    displaced icospheres or box stacks; image sides among 64-512; 1-8 ceiling
+    lights), 32 spp, depth 6.  Plain = one graph-captured renderer per scene,
+    run back to back; batched = one autotuned renderer over all scenes.  Both
+    compute the same per-path estimates, so their relMSE against a 256-spp
+    render of the same scenes is reported to show it is equal."""
+    import torch
+
+    from gonzales_b200 import BatchRenderer, GpuAccelerator, Renderer, scenes
+    from gonzales_b200 import _ffi as F
+
+    t0 = time.perf_counter()
+    work = scenes.batch_workload(BATCH["n_scenes"], BATCH["seed"])
+    hosts = [sb.build() for sb, _ in work]
+    accs = [GpuAccelerator(h) for h in hosts]
+    setup_s = time.perf_counter() - t0
+    params = [F.render_params(side, side, BATCH["spp"], max_depth=BATCH["max_depth"],
+                              rr_min_bounce=BATCH["rr_min_bounce"], use_graph=1) for _, side in work]
+    paths = sum(p.width * p.height * p.spp for p in params)
+    steps = max(3, min(args.steps, 5))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(max(1, min(args.warmup, 2))):
+            fn()
+        barrier()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    with BatchRenderer(accs, params) as br:
+        tuned, tuned_ms = br.autotune(stream)
+        pix = br.pixels
+        offs = br.offsets
+        rgb_b = torch.zeros((pix, 3), device="cuda")
+        w_b = torch.zeros((pix,), device="cuda")
+        rgb_p = torch.zeros((pix, 3), device="cuda")
+        w_p = torch.zeros((pix,), device="cuda")
+        plain_renderers = [Renderer(a, p) for a, p in zip(accs, params)]
+
+        def batched():
+            br.render(rgb_b, w_b, stream=stream)
+
+        def plain():
+            for k, r in enumerate(plain_renderers):
+                r.render(rgb_p[offs[k]:offs[k + 1]], w_p[offs[k]:offs[k + 1]], stream=stream)
+
+        ms_b = timed(batched)
+        ms_p = timed(plain)
+        for r in plain_renderers:
+            r.close()
+        err = br.error_word()
+    # reference images: the batch at ref_spp (an independent Z-Sobol sequence)
+    ref_params = [F.render_params(p.width, p.height, BATCH["ref_spp"], max_depth=BATCH["max_depth"],
+                                  rr_min_bounce=BATCH["rr_min_bounce"]) for p in params]
+    with BatchRenderer(accs, ref_params, use_graph=1, sort_key=tuned["sort_key"]) as rr:
+        rgb_r = torch.zeros((pix, 3), device="cuda")
+        w_r = torch.zeros((pix,), device="cuda")
+        rr.render(rgb_r, w_r, stream=stream)
+        torch.cuda.synchronize()
+        ref = (rgb_r / w_r[:, None]).cpu().numpy()
+    img_b = (rgb_b / w_b[:, None]).cpu().numpy()
+    img_p = (rgb_p / w_p[:, None]).cpu().numpy()
+
+    def relmse(img):
+        per = [float(np.mean((img[offs[k]:offs[k + 1]] - ref[offs[k]:offs[k + 1]]) ** 2 /
+                             (ref[offs[k]:offs[k + 1]] ** 2 + 1e-2))) for k in range(len(params))]
+        return float(np.mean(per))
+
+    for a in accs:
+        a.close()
+    tris = [h.triangle_count for h in hosts]
+    return {"config": "%d scenes, triangles %d-%d (total %d), sides %s, %d spp, depth %d, roulette from bounce %d"
+                      % (len(params), min(tris), max(tris), sum(tris), sorted(set(p.width for p in params)),
+                         BATCH["spp"], BATCH["max_depth"], BATCH["rr_min_bounce"]),
+            "paths_per_frame": paths, "steps": steps, "setup_s": setup_s,
+            "batched_spp_per_s": paths / ms_b * 1000.0, "batched_ms": ms_b,
+            "plain_spp_per_s": paths / ms_p * 1000.0, "plain_ms": ms_p,
+            "autotuned": {"wave_paths": tuned["wave_paths"],
+                          "sort_key": ["none", "material", "scene"][tuned["sort_key"]], "ms": tuned_ms},
+            "relmse_vs_%dspp" % BATCH["ref_spp"]: {"batched": relmse(img_b), "plain": relmse(img_p)},
+            "max_abs_diff_batched_vs_plain": float(np.nanmax(np.abs(img_b - img_p))),
+            "error_word": err}
+
+
+def adjoint_leg(args, stream, barrier):
+    """The differentiable box scene (floor and back-wall albedo textures
+    256 x 256 x 3 each, emission scale; 393,217 parameters): one step is a
+    256 x 256, 16-spp forward render plus the path-replay adjoint of an L2
+    loss against a 1024-spp target (depth 5, no roulette)."""
+    import torch
+
+    from gonzales_b200 import GpuAccelerator
+    from gonzales_b200 import _ffi as F
+    from gonzales_b200 import adjoint as A
+
+    sb, mats = A.adjoint_box_scene()
+    acc = GpuAccelerator(sb.build())
+    gt = torch.as_tensor(A.ground_truth_textures()).cuda()
+    depth = 5
+    with A.DifferentiableRenderer(acc, F.render_params(256, 256, 1024, max_depth=depth, rr_min_bounce=depth),
+                                  mats) as dt:
+        target, _ = dt.forward(gt, 1.0)
+    tex = torch.full_like(gt, 0.5)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    steps = max(3, min(args.steps, 10))
+    with A.DifferentiableRenderer(acc, F.render_params(256, 256, 16, max_depth=depth, rr_min_bounce=depth),
+                                  mats) as dr:
+        for _ in range(max(3, args.warmup)):
+            img, w = dr.forward(tex, 0.8, stream=stream)
+            dr.backward(2.0 * (img - target) / img.numel(), w, tex, 0.8, stream=stream)
+        barrier()
+        fwd_ms = bwd_ms = 0.0
+        for _ in range(steps):
+            e0.record(stream)
+            img, w = dr.forward(tex, 0.8, stream=stream)
+            e1.record(stream)
+            d_tex, d_em = dr.backward(2.0 * (img - target) / img.numel(), w, tex, 0.8, stream=stream)
+            e2.record(stream)
+            e2.synchronize()
+            fwd_ms += e0.elapsed_time(e1)
+            bwd_ms += e1.elapsed_time(e2)
+        barrier()
+    acc.close()
+    return {"config": "adjoint box scene, 2 x 256x256x3 albedo textures + emission scale (393,217 parameters), "
+                      "256x256, 16 spp, depth 5, no roulette, L2 loss vs 1024-spp target",
+            "forward_ms": fwd_ms / steps, "adjoint_ms": bwd_ms / steps, "step_ms": (fwd_ms + bwd_ms) / steps,
+            "gradient_nonzero": int((d_tex != 0).sum().item()), "d_emission": float(d_em.item()),
+            "paths_per_step": 256 * 256 * 16, "steps": steps}
 
 
 def cpu_render_baseline():
@@ -361,6 +503,8 @@ def run_ours(args):
         e2e_s = float(tt.item())
 
     render = render_leg(acc_box=None, args=args, stream=stream, barrier=barrier) if not args.small else None
+    batch = batch_leg(args, stream, barrier) if not (args.small or args.skip_batch) else None
+    adjoint = adjoint_leg(args, stream, barrier) if not (args.small or args.skip_batch) else None
 
     if rank == 0:
         ms_per_step = elapsed_ms / args.steps
@@ -398,6 +542,10 @@ def run_ours(args):
         }
         if render is not None:
             line["render"] = render
+        if batch is not None:
+            line["batch"] = batch
+        if adjoint is not None:
+            line["adjoint"] = adjoint
         if world == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(hs, o, d, t)
             if render is not None:
