@@ -121,13 +121,16 @@ def test_autograd_function_and_descent_step(setup):
     d_tex, d_em = _adjoint(dr, tex.detach(), 0.8, target)
     torch.testing.assert_close(tex.grad, d_tex, rtol=1e-3, atol=1e-9)
     assert abs(em.grad.item() - d_em) <= 1e-3 * abs(d_em)
-    # a small step against the gradient lowers the loss (same samples)
+    # small steps against the gradients lower the loss (same samples): the
+    # texels (largest change 5e-3) and, separately, the emission scale
     with torch.no_grad():
         l0 = _loss64(dr, tex.detach(), 0.8, target)
         step = 5e-3 / float(tex.grad.abs().max().item())
         new = (tex - step * tex.grad).clamp(0.0, 1.0).contiguous()
-        l1 = _loss64(dr, new, 0.8 - step * em.grad.item(), target)
+        l1 = _loss64(dr, new, 0.8, target)
+        l2 = _loss64(dr, tex.detach(), 0.8 - 1e-2 * float(np.sign(em.grad.item())), target)
     assert l1 < l0, (l0, l1)
+    assert l2 < l0, (l0, l2)
 
 
 def test_textured_forward_matches_oracle(setup):
