@@ -224,16 +224,56 @@ def random_instances(n, n_blas, seed, extent=20.0):
     return inst
 
 
-def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0):
+def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0, coloured=False):
     """Bottom-level scenes (one mesh each: tubes and spheres alternating) and
-    instances; 2 * n_u * n_v triangles per mesh (50,000 at the defaults)."""
+    instances; 2 * n_u * n_v triangles per mesh (50,000 at the defaults).
+    coloured: a seeded diffuse albedo in [0.1, 0.8]^3 per mesh (else 0.5)."""
+    rng = np.random.default_rng(seed + 101)
     blas = []
     for k in range(n_meshes):
         pts, tris = grid_mesh("tube" if k % 2 == 0 else "sphere", n_u, n_v, seed + k)
         sb = SceneBuilder()
-        sb.add_mesh(pts, tris, sb.add_material((0.5, 0.5, 0.5)))
+        albedo = rng.uniform(0.1, 0.8, 3) if coloured else (0.5, 0.5, 0.5)
+        sb.add_mesh(pts, tris, sb.add_material(albedo))
         blas.append(sb.build())
     return blas, random_instances(n_instances, n_meshes, seed, extent)
+
+
+def equal_area_square_to_sphere(u, v):
+    """numpy form of InfiniteLight.equalAreaSquareToSphere (for building maps)."""
+    ru, rv = 2 * u - 1, 2 * v - 1
+    au, av = np.abs(ru), np.abs(rv)
+    sd = 1 - (au + av)
+    r = 1 - np.abs(sd)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        phi = np.where(r == 0, 1.0, (av - au) / np.where(r == 0, 1.0, r) + 1) * (np.pi / 4)
+    z = np.copysign(np.maximum(0.0, 1 - r * r), sd)
+    return np.stack([np.copysign(r * np.cos(phi), ru), np.copysign(r * np.sin(phi), rv), z], -1)
+
+
+def sky_map(width=1024, height=512, seed=0xE1, sun_sigma_deg=3.0):
+    """Seeded environment map in the equal-area square layout the environment
+    light reads: a sky gradient over +y (horizon to zenith), a dim ground
+    below the horizon, and a Gaussian sun lobe at a seeded direction."""
+    rng = np.random.default_rng(seed)
+    v, u = np.meshgrid((np.arange(height) + 0.5) / height, (np.arange(width) + 0.5) / width, indexing="ij")
+    d = equal_area_square_to_sphere(u, v)
+    d = d / np.linalg.norm(d, axis=-1, keepdims=True)  # the light looks maps up by unit direction
+    up = d[..., 1]
+    zenith = np.array([0.25, 0.45, 0.9])
+    horizon = np.array([0.9, 0.95, 1.0])
+    ground = np.array([0.12, 0.1, 0.08])
+    t = np.clip(up, 0, 1)[..., None]
+    sky = horizon * (1 - t) + zenith * t
+    rgb = np.where(up[..., None] >= 0, sky, ground)
+    el = rng.uniform(0.35, 0.9)
+    az = rng.uniform(0, 2 * np.pi)
+    sun = np.array([np.cos(el) * np.cos(az), np.sin(el), np.cos(el) * np.sin(az)])
+    cosang = np.clip(d @ sun, -1, 1)
+    ang = np.arccos(cosang)
+    sigma = np.deg2rad(sun_sigma_deg)
+    rgb = rgb + np.array([60.0, 55.0, 45.0]) * np.exp(-(ang ** 2) / (2 * sigma ** 2))[..., None]
+    return rgb.astype(np.float32)
 
 
 def instanced_rays(n, extent, seed):

@@ -129,3 +129,18 @@ extern "C" void orc_traverse_instanced(const orc_node *tlas, const int64_t *leaf
                 });
         for (auto &th : pool) th.join();
 }
+
+// One ray through the two-level scene (the renderer's trace); returns 1 on a
+// hit.
+extern "C" int orc_trace_instanced_one(const orc_node *tlas, const int64_t *leaf_instance, const float *w2o,
+                                       const int32_t *blas_of, const orc_blas *blas, const orc_ray *ray, float tmax,
+                                       int32_t *prim, int32_t *inst, float *t, float *u, float *v) {
+        Best b;
+        traverse_top(tlas, leaf_instance, w2o, blas_of, blas, *ray, tmax, b);
+        *prim = b.prim;
+        *inst = b.inst;
+        *t = b.t;
+        *u = b.u;
+        *v = b.v;
+        return b.prim >= 0 ? 1 : 0;
+}

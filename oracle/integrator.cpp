@@ -112,7 +112,8 @@ struct Frame {
         V3 to_world(V3 v) const { return add(add(mul(x, v.x), mul(y, v.y)), mul(z, v.z)); }
 };
 
-bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame *f) {
+// The interaction's dpdu (shading tangent) of Triangle.computeSurfaceInteraction.
+bool shading_dpdu(V3 p0, V3 p1, V3 p2, V3 ns, V3 *dpdu_out) {
         V3 gn = cross(sub(p2, p0), sub(p1, p0));
         if (length_sq(gn) == 0.0f) return false;
         V3 dpdu, dpdv;
@@ -125,9 +126,23 @@ bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame *f) {
         } else {
                 coordinate_system(ns, &s, &t);
         }
-        f->y = normalize(s);
-        f->z = ns;
-        f->x = cross(f->y, f->z);
+        *dpdu_out = s;
+        return true;
+}
+
+// BsdfFrame from the interaction's dpdu and shading normal.
+Frame frame_from(V3 dpdu, V3 ns) {
+        Frame f;
+        f.y = normalize(dpdu);
+        f.z = ns;
+        f.x = cross(f.y, f.z);
+        return f;
+}
+
+bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame *f) {
+        V3 s;
+        if (!shading_dpdu(p0, p1, p2, ns, &s)) return false;
+        *f = frame_from(s, ns);
         return true;
 }
 
@@ -190,6 +205,7 @@ struct Light {
         V3 le;
         float area;
         float power;
+        bool is_env = false;
 };
 
 struct Scene {
@@ -204,15 +220,17 @@ struct Scene {
         const orc_render_params *p;
         const orc_textures *tex = nullptr;
         float escale = 1.0f;
+        const orc_render_instances *inst = nullptr;
+        const orc_env *env = nullptr;
 };
 
 // Emission times the scene's emission scale (1 without textures: exact).
 V3 emitted(const Scene &sc, V3 e) { return v3(e.x * sc.escale, e.y * sc.escale, e.z * sc.escale); }
 
 // Albedo of material m at p: its texture's nearest texel, else its constant.
-V3 albedo_at(const Scene &sc, int64_t m, V3 p) {
-        const orc_material &mat = sc.materials[m];
-        if (sc.tex && sc.tex->material_texture[m] >= 0) {
+V3 albedo_at(const Scene &sc, const orc_material *mats, int64_t m, V3 p) {
+        const orc_material &mat = mats[m];
+        if (sc.tex && !sc.inst && sc.tex->material_texture[m] >= 0) {
                 const int t = sc.tex->material_texture[m];
                 const int R = sc.tex->resolution;
                 const float *mp = sc.tex->maps + 9 * t;
@@ -227,8 +245,8 @@ V3 albedo_at(const Scene &sc, int64_t m, V3 p) {
         return v3(mat.albedo[0], mat.albedo[1], mat.albedo[2]);
 }
 
-bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
-        const orc_prim_id &pr = sc.prims[k];
+bool prim_tri_of(const orc_prim_id *prims, const orc_mesh *meshes, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
+        const orc_prim_id &pr = prims[k];
         int64_t mesh, base;
         if (pr.type == 0) {
                 mesh = pr.id1;
@@ -239,7 +257,7 @@ bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
         } else {
                 return false;
         }
-        const orc_mesh &m = sc.meshes[mesh];
+        const orc_mesh &m = meshes[mesh];
         const float *a = m.points + 4 * m.vertex_indices[base];
         const float *b = m.points + 4 * m.vertex_indices[base + 1];
         const float *c = m.points + 4 * m.vertex_indices[base + 2];
@@ -249,18 +267,94 @@ bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
         return true;
 }
 
+bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
+        return prim_tri_of(sc.prims, sc.meshes, k, p0, p1, p2);
+}
+
 struct Hit {
         bool hit;
-        int32_t prim;
+        int32_t prim, inst;
         float t, u, v;
 };
 
 Hit trace(const Scene &sc, V3 o, V3 d, float tmax) {
         orc_ray r{o.x, o.y, o.z, d.x, d.y, d.z};
+        if (sc.inst) {
+                Hit h;
+                const orc_render_instances &I = *sc.inst;
+                h.hit = orc_trace_instanced_one(I.tlas, I.leaf_instance, I.w2o, I.blas_of, I.blas, &r, tmax, &h.prim,
+                                                &h.inst, &h.t, &h.u, &h.v) != 0;
+                return h;
+        }
         orc_isect is;
         int32_t idx;
         orc_trace_one(sc.nodes, sc.prims, sc.meshes, &r, tmax, &is, &idx);
-        return Hit{is.hit != 0, idx, is.t, is.u, is.v};
+        return Hit{is.hit != 0, idx, -1, is.t, is.u, is.v};
+}
+
+// Transform * Point / Vector / Normal (Geometry/Transform.swift:31-65) for a
+// row-major 3x4 matrix m; the normal uses the inverse matrix's columns.
+V3 xf_point(const float *m, V3 p) {
+        return v3(((m[0] * p.x + m[1] * p.y) + m[2] * p.z) + m[3], ((m[4] * p.x + m[5] * p.y) + m[6] * p.z) + m[7],
+                  ((m[8] * p.x + m[9] * p.y) + m[10] * p.z) + m[11]);
+}
+V3 xf_vector(const float *m, V3 v) {
+        return v3((m[0] * v.x + m[1] * v.y) + m[2] * v.z, (m[4] * v.x + m[5] * v.y) + m[6] * v.z,
+                  (m[8] * v.x + m[9] * v.y) + m[10] * v.z);
+}
+V3 xf_normal(const float *inv, V3 n) {
+        return v3((inv[0] * n.x + inv[4] * n.y) + inv[8] * n.z, (inv[1] * n.x + inv[5] * n.y) + inv[9] * n.z,
+                  (inv[2] * n.x + inv[6] * n.y) + inv[10] * n.z);
+}
+
+// The surface interaction of a hit (Triangle.computeSurfaceInteraction,
+// Shape/Triangle.swift:363-474; for an instance in object space, then
+// Transform * SurfaceInteraction, Core/Transform+SurfaceInteraction.swift:3-14).
+struct Isect {
+        V3 pos, ng, wo;
+        Frame fr;
+        bool frame_ok;
+        const orc_prim_id *pr;
+        const orc_material *mats;
+};
+
+bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
+        V3 p0, p1, p2;
+        const float b0 = (1.0f - h.u) - h.v;
+        if (!sc.inst) {
+                if (!prim_tri(sc, h.prim, &p0, &p1, &p2)) return false;
+                is->pos = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
+                is->ng = normalize(cross(sub(p0, p2), sub(p1, p2)));
+                is->wo = normalize(neg(d));
+                is->frame_ok = make_frame(p0, p1, p2, is->ng, &is->fr);
+                is->pr = &sc.prims[h.prim];
+                is->mats = sc.materials;
+                return true;
+        }
+        const orc_render_instances &I = *sc.inst;
+        const int32_t b = I.blas_of[h.inst];
+        const orc_blas &B = I.blas[b];
+        if (!prim_tri_of(B.prims, B.meshes, h.prim, &p0, &p1, &p2)) return false;
+        const float *w2o = I.w2o + 12 * h.inst, *o2w = I.o2w + 12 * h.inst;
+        const V3 pos_o = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
+        const V3 n_o = normalize(cross(sub(p0, p2), sub(p1, p2)));
+        const V3 wo_o = normalize(neg(xf_vector(w2o, d)));
+        V3 s_o = v3(0, 0, 0);
+        is->frame_ok = shading_dpdu(p0, p1, p2, n_o, &s_o);
+        is->pos = xf_point(o2w, pos_o);
+        is->ng = normalize(xf_normal(w2o, n_o));
+        is->wo = normalize(xf_vector(o2w, wo_o));
+        if (is->frame_ok) is->fr = frame_from(xf_vector(o2w, s_o), is->ng);
+        is->pr = &B.prims[h.prim];
+        is->mats = I.blas_materials[b];
+        return true;
+}
+
+V3 env_radiance(const Scene &sc, V3 d) {
+        const float dd[3] = {d.x, d.y, d.z};
+        float c[3];
+        orc_env_radiance(sc.env, dd, c);
+        return v3(c[0], c[1], c[2]);
 }
 
 // offsetRayOrigin(point:normal:direction:) (Core/Interaction.swift:26-35).
@@ -315,28 +409,32 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
         for (int bounce = 0; bounce <= P.max_depth; ++bounce) {
                 Hit h = trace(sc, o, d, kInfF);
                 ++res.ext;
-                if (!h.hit) break;  // no environment light in these scenes
+                if (!h.hit) {
+                        // shadeBounce on a miss (:375-387): environment light on
+                        // camera rays (no specular bounces in these scenes)
+                        if (bounce == 0 && sc.env) L = add(L, mulv(thr, env_radiance(sc, d)));
+                        break;
+                }
                 if (is_black(thr)) break;
                 if (bounce >= P.max_depth) break;
-                V3 p0, p1, p2;
-                prim_tri(sc, h.prim, &p0, &p1, &p2);
-                const float b0 = (1.0f - h.u) - h.v;
-                const V3 pos = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
-                const V3 ng = normalize(cross(sub(p0, p2), sub(p1, p2)));
-                const V3 wo = normalize(neg(d));
-                const orc_prim_id &pr = sc.prims[h.prim];
+                Isect is;
+                if (!interaction(sc, h, d, &is)) break;
+                const V3 pos = is.pos, ng = is.ng, wo = is.wo;
+                const orc_prim_id &pr = *is.pr;
                 const bool is_light = pr.type == 3;
                 if (bounce == 0 && is_light) {
-                        const orc_material &lm = sc.materials[pr.material_index];
+                        const orc_material &lm = is.mats[pr.material_index];
                         if (dot(ng, wo) > 0.0f)
                                 L = add(L, mulv(thr, emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]))));
                 }
                 // Area lights have materialIndex 0 in their interaction
-                // (Core/SurfaceInteraction.swift:20).
-                const V3 refl = albedo_at(sc, is_light ? 0 : pr.material_index, pos);
+                // (Core/SurfaceInteraction.swift:20): the scene's first material.
+                const V3 refl = is_light ? albedo_at(sc, sc.inst ? sc.inst->blas_materials[0] : sc.materials, 0, pos)
+                                         : albedo_at(sc, is.mats, pr.material_index, pos);
                 const V3 f_val = mul(refl, 1.0f / kPi);
-                Frame fr;
-                if (!make_frame(p0, p1, p2, ng, &fr)) break;
+                if (!is.frame_ok) break;
+                if (sc.lights.empty()) break;
+                const Frame &fr = is.fr;
                 const V3 wo_l = fr.to_local(wo);
 
                 // ---- sampleOneLight -> estimateDirect -> sampleMultipleImportance
@@ -348,7 +446,26 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 V3 light_est = v3(0, 0, 0);
                 V3 light_dir = v3(0, 0, 0);
                 float light_pdf = 0.0f;
-                {
+                if (lt.is_env) {
+                        // InfiniteLight.sample (InfiniteLight.swift:38-64)
+                        float dir[3], rgb[3];
+                        const float pdf = orc_env_sample(sc.env, u2[0], u2[1], dir, rgb);
+                        const V3 dv = v3(dir[0], dir[1], dir[2]), rad = v3(rgb[0], rgb[1], rgb[2]);
+                        if (!is_black(rad) && !std::isinf(pdf)) {
+                                const V3 target = add(pos, mul(dv, 100.0f));  // sceneDiameter
+                                const V3 so = add(pos, mul(sub(target, pos), 0.0001f));
+                                const V3 sd = sub(target, so);
+                                Hit sh = trace(sc, so, sd, 1.0f - 0.00001f);
+                                ++res.shadow;
+                                if (!sh.hit) {
+                                        const bool reflect = dot(dv, ng) * dot(wo, ng) > 0.0f;
+                                        const V3 f = reflect ? f_val : v3(0, 0, 0);
+                                        light_est = mulv(mul(f, std::fabs(dot(dv, ng))), rad);
+                                        light_dir = dv;
+                                        light_pdf = pdf;
+                                }
+                        }
+                } else {
                         const float su0 = std::sqrt(u2[0]);
                         const float lb0 = 1.0f - su0, lb1 = u2[1] * su0;
                         const V3 lp = add(add(mul(lt.p0, lb0), mul(lt.p1, lb1)), mul(lt.p2, (1.0f - lb0) - lb1));
@@ -386,7 +503,10 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 const float light_w = power_heuristic(light_pdf, brdf_density);
                 V3 contrib = light_pdf == 0.0f ? v3(0, 0, 0) : mul(mul(light_est, light_w), 1.0f / light_pdf);
 
-                // sampleDistributionFunction (VolumePathIntegrator.swift:91-133)
+                // sampleDistributionFunction (VolumePathIntegrator.swift:91-133).
+                // The light density of the chosen light along the BSDF sample:
+                // an environment light answers from its map; an area light, as
+                // written, is queried with tHit = 0 and answers 0 (weight 0).
                 float u3[3];
                 orc_zsobol_get3d(smp, u3);
                 {
@@ -395,30 +515,38 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                         const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? std::fabs(wi_l.z) / kPi : 0.0f;
                         const V3 wi = fr.to_world(wi_l);
                         V3 est = mul(f_val, std::fabs(dot(wi, ng)));
-                        if (P.mis_corrected && !is_black(est) && pdf_b > 0.0f) {
+                        if ((P.mis_corrected || lt.is_env) && !is_black(est) && pdf_b > 0.0f) {
                                 const V3 po = offset_origin(pos, ng, wi);
                                 Hit ph = trace(sc, po, wi, kInfF);
                                 ++res.probe;
                                 V3 radiance = v3(0, 0, 0);
-                                if (ph.hit && sc.prims[ph.prim].type == 3) {
-                                        V3 q0, q1, q2;
-                                        prim_tri(sc, ph.prim, &q0, &q1, &q2);
-                                        const V3 qn = normalize(cross(sub(q0, q2), sub(q1, q2)));
-                                        const orc_material &lm = sc.materials[sc.prims[ph.prim].material_index];
-                                        if (dot(qn, neg(wi)) > 0.0f)
-                                                radiance = emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]));
+                                Isect pi;
+                                if (ph.hit) {
+                                        if (interaction(sc, ph, wi, &pi) && pi.pr->type == 3) {
+                                                const orc_material &lm = pi.mats[pi.pr->material_index];
+                                                if (dot(pi.ng, neg(wi)) > 0.0f)
+                                                        radiance = emitted(sc, v3(lm.emission[0], lm.emission[1],
+                                                                                  lm.emission[2]));
+                                        }
+                                } else if (sc.env) {
+                                        radiance = env_radiance(sc, wi);
                                 }
                                 est = mulv(est, radiance);
                                 float light_density = 0.0f;
-                                float tl;
-                                if (hit_light(lt, po, wi, &tl)) {
-                                        const V3 hp = add(po, mul(wi, tl));
-                                        const V3 dq = sub(pos, hp);
-                                        const float dd2 = dot(dq, dq);
-                                        const V3 lnn = normalize(cross(sub(lt.p0, lt.p2), sub(lt.p1, lt.p2)));
-                                        const float ang = std::fabs(dot(lnn, neg(wi)));
-                                        const float dens = dd2 / (ang * lt.area);
-                                        light_density = std::isinf(dens) ? 0.0f : dens;
+                                if (lt.is_env) {
+                                        const float dd[3] = {wi.x, wi.y, wi.z};
+                                        light_density = orc_env_pdf(sc.env, dd);
+                                } else {
+                                        float tl;
+                                        if (hit_light(lt, po, wi, &tl)) {
+                                                const V3 hp = add(po, mul(wi, tl));
+                                                const V3 dq = sub(pos, hp);
+                                                const float dd2 = dot(dq, dq);
+                                                const V3 lnn = normalize(cross(sub(lt.p0, lt.p2), sub(lt.p1, lt.p2)));
+                                                const float ang = std::fabs(dot(lnn, neg(wi)));
+                                                const float dens = dd2 / (ang * lt.area);
+                                                light_density = std::isinf(dens) ? 0.0f : dens;
+                                        }
                                 }
                                 const float bw = power_heuristic(pdf_b, light_density);
                                 contrib = add(contrib, mul(mul(est, bw), 1.0f / pdf_b));
@@ -450,11 +578,15 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
 
 }  // namespace
 
-extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
-                                    const orc_material *materials, int64_t n_materials, int64_t n_prims,
-                                    const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
-                                    float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
+extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                              const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                              const orc_render_instances *instances, const orc_env *env,
+                              const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
+                              float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
         Scene sc;
+        sc.inst = instances;
+        sc.env = env;
+        if (instances) n_prims = 0;  // instanced emitters are not lights (objects add none)
         sc.tex = textures;
         sc.escale = textures ? textures->emission_scale : 1.0f;
         sc.nodes = nodes;
@@ -477,6 +609,13 @@ extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *pr
                 l.area = 0.5f * std::sqrt(length_sq(cross(sub(l.p1, l.p0), sub(l.p2, l.p0))));
                 const float avg = (l.le.x + l.le.y + l.le.z) / 3.0f;
                 l.power = avg * l.area * kPi;
+                sc.lights.push_back(l);
+        }
+        if (env) {
+                // the environment light after the area lights
+                Light l{};
+                l.is_env = true;
+                l.power = orc_env_power(env);
                 sc.lights.push_back(l);
         }
         float run = 0.0f;
@@ -561,6 +700,14 @@ extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, cons
                            const orc_material *materials, int64_t n_materials, int64_t n_prims,
                            const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                            uint64_t *counters, int threads) {
-        orc_render_textured(nodes, prims, meshes, materials, n_materials, n_prims, params, nullptr, sum_rgb, sum_sq,
-                            sum_w, counters, threads);
+        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, nullptr,
+                      sum_rgb, sum_sq, sum_w, counters, threads);
+}
+
+extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                                    const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                                    const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
+                                    float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
+        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, textures,
+                      sum_rgb, sum_sq, sum_w, counters, threads);
 }

@@ -131,6 +131,19 @@ void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const 
                          const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
                          float *sum_sq, float *sum_w, uint64_t *counters, int threads);
 
+typedef struct orc_env orc_env;
+typedef struct orc_render_instances orc_render_instances;
+
+/* The general form: a flat scene (nodes .. n_prims) or, with `instances`, a
+ * two-level one (the flat arrays are then unused); an optional environment
+ * light (appended last to the light list; its power enters the light
+ * choice); optional textures (flat scenes). */
+void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
+                   const orc_material *materials, int64_t n_materials, int64_t n_prims,
+                   const orc_render_instances *instances, const orc_env *env, const orc_render_params *params,
+                   const orc_textures *textures, float *sum_rgb, float *sum_sq, float *sum_w, uint64_t *counters,
+                   int threads);
+
 /* PathState_C (mojo_kernel.h:36-44). */
 typedef struct orc_path_state {
         orc_ray ray;
@@ -167,6 +180,26 @@ void orc_traverse_instanced(const orc_node *tlas, const int64_t *leaf_instance, 
                             const int32_t *blas_of, const orc_blas *blas, const orc_ray *rays, const float *tmax,
                             int64_t n, int32_t *prim, int32_t *inst, float *t, float *u, float *v, int threads);
 
+/* One ray of the above (the renderer's trace); returns 1 on a hit. */
+int orc_trace_instanced_one(const orc_node *tlas, const int64_t *leaf_instance, const float *w2o,
+                            const int32_t *blas_of, const orc_blas *blas, const orc_ray *ray, float tmax,
+                            int32_t *prim, int32_t *inst, float *t, float *u, float *v);
+
+/* A two-level scene for the renderer: the traversal arrays above plus
+ * object_to_world o2w[12 * i] (row-major 3x4) and each bottom-level scene's
+ * materials.  Hits are shaded in object space and carried to world space as
+ * Transform * SurfaceInteraction does (Core/Transform+SurfaceInteraction.swift:3-14). */
+typedef struct orc_render_instances {
+        const orc_node *tlas;
+        const int64_t *leaf_instance;
+        const float *w2o, *o2w;
+        const int32_t *blas_of;
+        int64_t instance_count;
+        const orc_blas *blas;
+        const orc_material *const *blas_materials;
+        int64_t blas_count;
+} orc_render_instances;
+
 /* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
 int orc_intersect_triangle_mt(const float *o, const float *d, const float *p0, const float *p1,
                               const float *p2, float tmax, float *t, float *u, float *v);
@@ -182,6 +215,23 @@ int orc_bounds_intersects_swift(const float *mn, const float *mx, const float *o
                                 float thit);
 float orc_bounds_surface_area(const float *mn, const float *mx);
 int orc_bounds_maximum_extent(const float *mn, const float *mx);
+
+/* --- environment light (Light/InfiniteLight.swift) ----------------------- */
+
+/* Map rgb[h][w][3] (row v, column u); scale enters the light's power only. */
+orc_env *orc_env_create(const float *rgb, int32_t w, int32_t h, float scale);
+void orc_env_destroy(orc_env *env);
+float orc_env_power(const orc_env *env);
+/* Light sample for (u0, u1): writes direction and map value, returns the
+ * solid-angle pdf (0: no sample). */
+float orc_env_sample(const orc_env *env, float u0, float u1, float *dir, float *rgb);
+float orc_env_pdf(const orc_env *env, const float *dir);
+void orc_env_radiance(const orc_env *env, const float *dir, float *rgb);
+void orc_env_tables(const orc_env *env, float *func, float *cdf, float *row_integral, float *marg_func,
+                    float *marg_cdf, float *marg_integral);
+void orc_env_lookup(const float *rgb, int32_t w, int32_t h, float u, float v, float *out);
+void orc_equal_area_square_to_sphere(float u, float v, float *dir);
+void orc_equal_area_sphere_to_square(const float *d, float *uv);
 
 /* --- Z-Sobol ------------------------------------------------------------ */
 

@@ -201,20 +201,119 @@ class _Textures(C.Structure):
                 ("maps", C.c_void_p), ("texels", C.c_void_p), ("emission_scale", C.c_float)]
 
 
-def render(hs, params, threads=0, textures=None):
+class _RenderInstances(C.Structure):
+    _fields_ = [("tlas", C.c_void_p), ("leaf_instance", C.c_void_p), ("w2o", C.c_void_p), ("o2w", C.c_void_p),
+                ("blas_of", C.c_void_p), ("instance_count", C.c_int64), ("blas", C.c_void_p),
+                ("blas_materials", C.c_void_p), ("blas_count", C.c_int64)]
+
+
+class Environment:
+    """The oracle's environment light (orc_env): map rgb (H, W, 3) float32,
+    scale (enters the light's power only)."""
+
+    def __init__(self, rgb, scale=1.0):
+        L = lib()
+        if not getattr(L, "_env_bound", False):
+            L.orc_env_create.restype = C.c_void_p
+            L.orc_env_create.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_float]
+            L.orc_env_destroy.argtypes = [C.c_void_p]
+            L.orc_env_power.restype = C.c_float
+            L.orc_env_power.argtypes = [C.c_void_p]
+            L.orc_env_sample.restype = C.c_float
+            L.orc_env_sample.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+            L.orc_env_pdf.restype = C.c_float
+            L.orc_env_pdf.argtypes = [C.c_void_p, C.c_void_p]
+            L.orc_env_radiance.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+            L.orc_env_tables.argtypes = [C.c_void_p] * 7
+            L._env_bound = True
+        self.rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w = self.rgb.shape[:2]
+        self.handle = L.orc_env_create(self.rgb.ctypes.data, w, h, float(scale))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().orc_env_destroy(self.handle)
+            self.handle = None
+
+    def power(self):
+        return float(lib().orc_env_power(self.handle))
+
+    def sample(self, u0, u1):
+        d = np.zeros(3, np.float32)
+        c = np.zeros(3, np.float32)
+        pdf = lib().orc_env_sample(self.handle, u0, u1, d.ctypes.data, c.ctypes.data)
+        return d, c, float(pdf)
+
+    def pdf(self, d):
+        d = np.ascontiguousarray(d, np.float32)
+        return float(lib().orc_env_pdf(self.handle, d.ctypes.data))
+
+    def radiance(self, d):
+        d = np.ascontiguousarray(d, np.float32)
+        c = np.zeros(3, np.float32)
+        lib().orc_env_radiance(self.handle, d.ctypes.data, c.ctypes.data)
+        return c
+
+    def tables(self):
+        func = np.zeros((1024, 1024), np.float32)
+        cdf = np.zeros((1024, 1025), np.float32)
+        ri = np.zeros(1024, np.float32)
+        mf = np.zeros(1024, np.float32)
+        mc = np.zeros(1025, np.float32)
+        mi = np.zeros(1, np.float32)
+        lib().orc_env_tables(self.handle, func.ctypes.data, cdf.ctypes.data, ri.ctypes.data, mf.ctypes.data,
+                             mc.ctypes.data, mi.ctypes.data)
+        return dict(func=func, cdf=cdf, row_integral=ri, marginal_func=mf, marginal_cdf=mc,
+                    marginal_integral=float(mi[0]))
+
+
+def render(hs, params, threads=0, textures=None, env=None, instances=None):
     """Film sums of the oracle integrator: (sum_rgb (H,W,3), sum_sq (H,W,3),
     sum_w (H,W), counters {camera, extension, shadow, probe}).
 
     textures (optional): dict with material_texture (int32 per material, -1
     for none), maps (count x 9 float32: origin, u axis, v axis), texels
-    (count x R x R x 3 float32) and emission_scale (float)."""
+    (count x R x R x 3 float32) and emission_scale (float).
+    env (optional): an Environment.
+    instances (optional): dict with tlas_nodes, leaf_instance, instances
+    (INSTANCE_DTYPE) and blas (HostScene list); hs is then unused (None)."""
     L = lib()
     if not getattr(L, "_render_bound", False):
-        L.orc_render_textured.restype = None
-        L.orc_render_textured.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.POINTER(RenderParams),
-                                                             C.c_void_p] + [C.c_void_p] * 4 + [C.c_int]
+        L.orc_render_ex.restype = None
+        L.orc_render_ex.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                                       C.POINTER(RenderParams), C.c_void_p] + [C.c_void_p] * 4 + \
+            [C.c_int]
         L._render_bound = True
     keep = []
+    inst_struct = None
+    if instances is not None:
+        blas_scenes = instances["blas"]
+        blas = (_Blas * len(blas_scenes))()
+        mat_ptrs = (C.c_void_p * len(blas_scenes))()
+        for i, b in enumerate(blas_scenes):
+            marr = (_Mesh * max(len(b.meshes), 1))()
+            for k, m in enumerate(b.meshes):
+                p4 = np.ascontiguousarray(m.points, np.float32)
+                vi = np.ascontiguousarray(m.vertex_indices, np.int64)
+                keep += [p4, vi]
+                marr[k] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+            nodes_b = np.ascontiguousarray(b.nodes)
+            prims_b = np.ascontiguousarray(b.prims)
+            mats_b = np.ascontiguousarray(b.materials)
+            keep += [marr, nodes_b, prims_b, mats_b]
+            blas[i] = _Blas(nodes_b.ctypes.data, prims_b.ctypes.data, C.addressof(marr))
+            mat_ptrs[i] = mats_b.ctypes.data
+        inst = np.ascontiguousarray(instances["instances"])
+        w2o = np.ascontiguousarray(inst["world_to_object"], np.float32)
+        o2w = np.ascontiguousarray(inst["object_to_world"], np.float32)
+        blas_of = np.ascontiguousarray(inst["blas"], np.int32)
+        tlas = np.ascontiguousarray(instances["tlas_nodes"])
+        leaf = np.ascontiguousarray(instances["leaf_instance"], np.int64)
+        keep += [blas, mat_ptrs, w2o, o2w, blas_of, tlas, leaf]
+        inst_struct = _RenderInstances(tlas.ctypes.data, leaf.ctypes.data, w2o.ctypes.data, o2w.ctypes.data,
+                                       blas_of.ctypes.data, len(inst), C.addressof(blas), C.addressof(mat_ptrs),
+                                       len(blas_scenes))
+        hs = blas_scenes[0]  # flat arrays unused
     arr = (_Mesh * max(len(hs.meshes), 1))()
     for i, m in enumerate(hs.meshes):
         p4 = np.ascontiguousarray(m.points, np.float32)
@@ -240,9 +339,10 @@ def render(hs, params, threads=0, textures=None):
         keep += [mt, maps, tx]
         tex = _Textures(tx.shape[0], tx.shape[1], mt.ctypes.data, maps.ctypes.data, tx.ctypes.data,
                         float(textures.get("emission_scale", 1.0)))
-    L.orc_render_textured(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr),
-                          _p(mats), len(mats), len(hs.prims), C.byref(params),
-                          C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw), _p(cnt), threads)
+    L.orc_render_ex(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr),
+                    _p(mats), len(mats), len(hs.prims), C.byref(inst_struct) if inst_struct is not None else None,
+                    env.handle if env is not None else None, C.byref(params),
+                    C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw), _p(cnt), threads)
     return s, s2, sw, {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
 
 
