@@ -174,6 +174,12 @@ class GpuAccelerator:
                                          C.byref(stats)))
         return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
 
+    def set_environment(self, rgb, scale=1.0):
+        """Adds the environment light (gzg_scene_set_environment): rgb (H, W, 3)
+        float32 in the equal-area square layout."""
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        F.check(F.lib().gzg_scene_set_environment(self.handle, F.ptr(rgb), rgb.shape[1], rgb.shape[0], float(scale)))
+
 
 def instance_bounds(blas_hosts, instances):
     """World bounds per instance (gzg_host_instance_bounds) from the bottom-level
@@ -234,6 +240,9 @@ class InstancedAccelerator:
         w = C.c_uint32(0)
         F.check(F.lib().gzg_scene_error_word(self.handle, C.byref(w), 1 if clear else 0))
         return w.value
+
+    render = GpuAccelerator.render
+    set_environment = GpuAccelerator.set_environment
 
     def trace_closest(self, rays_d, hits_d, inst_d, options=None, stream=None):
         opt = C.byref(options) if options is not None else None

@@ -728,6 +728,32 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 steps += blas[inst[k].blas]->host_wide.nodes.size();
         }
 
+        // Shading arrays: the bottom-level scenes' prim-order triangles, prims
+        // (material indices moved by each scene's material offset) and
+        // materials, concatenated; per instance object_to_world rows.
+        HostShading hsd;
+        std::vector<int32_t> prim_base(blas_count);
+        for (int64_t b = 0; b < blas_count; ++b) {
+                const HostShading &bs = blas[b]->host_shading;
+                prim_base[b] = (int32_t)hsd.prims.size();
+                const int64_t moff = (int64_t)(hsd.materials.size() / 2);
+                hsd.pv0.insert(hsd.pv0.end(), bs.pv0.begin(), bs.pv0.end());
+                hsd.pv1.insert(hsd.pv1.end(), bs.pv1.begin(), bs.pv1.end());
+                hsd.pv2.insert(hsd.pv2.end(), bs.pv2.begin(), bs.pv2.end());
+                for (gzg_prim_id p : bs.prims) {
+                        p.material_index += moff;
+                        hsd.prims.push_back(p);
+                }
+                hsd.materials.insert(hsd.materials.end(), bs.materials.begin(), bs.materials.end());
+        }
+        if (hsd.prims.size() >= 0x7FFFFFFFu)
+                return set_error(GZG_ERR_LIMIT, "gzg_instanced_scene_create: more than 2^31 bottom-level prims");
+        std::vector<float4_> o2w((size_t)instance_count * 3);
+        for (int64_t k = 0; k < instance_count; ++k) {
+                const float *m = inst[k].object_to_world;
+                for (int r = 0; r < 3; ++r) o2w[3 * k + r] = float4_{m[4 * r], m[4 * r + 1], m[4 * r + 2], m[4 * r + 3]};
+        }
+
         auto scene = std::make_unique<gzg_scene>();
         scene->device = device;
         scene->instanced = true;
@@ -748,6 +774,35 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 return st;
         d.instances = f;
         d.instance_count = instance_count;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(o2w.data()), o2w.size(), &f, "instance transforms")))
+                return st;
+        d.inst_o2w = f;
+        if (!hsd.prims.empty()) {
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.pv0.data()), hsd.pv0.size(), &f, "triangles")))
+                        return st;
+                d.pv0 = f;
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.pv1.data()), hsd.pv1.size(), &f, "triangles")))
+                        return st;
+                d.pv1 = f;
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.pv2.data()), hsd.pv2.size(), &f, "triangles")))
+                        return st;
+                d.pv2 = f;
+                const gzg_prim_id *pd;
+                if ((st = scene->upload(hsd.prims.data(), hsd.prims.size(), &pd, "prim ids"))) return st;
+                d.prims = pd;
+                d.prim_count = (int64_t)hsd.prims.size();
+        }
+        if (!hsd.materials.empty()) {
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.materials.data()), hsd.materials.size(), &f,
+                                        "materials")))
+                        return st;
+                d.materials = f;
+                d.material_count = (int32_t)(hsd.materials.size() / 2);
+        }
+        const int32_t *pb;
+        if ((st = scene->upload(prim_base.data(), prim_base.size(), &pb, "prim bases"))) return st;
+        d.blas_prim_base = pb;
+        scene->host_shading = std::move(hsd);
         const uint32_t zero = 0;
         const uint32_t *ew;
         if ((st = scene->upload(&zero, 1, &ew, "error word"))) return st;
@@ -760,6 +815,55 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
         scene->info.bvh2_depth = tlas_bvh2_depth;
         scene->info.wide_depth = tlas.depth + max_blas_depth + 2;
         *out_scene = scene.release();
+        return clear_error();
+}
+
+// Environment light: the map, its sampling distribution (built on the host,
+// env.cpp) and its place after the area lights in the light list: the
+// running power sum gains one entry (Light/PowerLightSampler.swift) and the
+// total the light's power pi * 50^2 * average(scale)
+// (Light/InfiniteLight.swift:141-144).
+GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
+                                             float scale) {
+        if (!scene || !rgb || width <= 0 || height <= 0 || (int64_t)width * height > ((int64_t)1 << 28) ||
+            !std::isfinite(scale) || scale < 0.0f)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_environment: bad arguments");
+        if (scene->host_shading.has_env)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_environment: the scene has an environment");
+        EnvTables t;
+        build_env_tables(rgb, width, height, &t);
+        DeviceGuard g(scene->device);
+        DevScene &d = scene->dev;
+        gzg_status st;
+        const float *p;
+        if ((st = scene->upload(rgb, (size_t)width * height * 3, &p, "environment map"))) return st;
+        d.env_rgb = p;
+        if ((st = scene->upload(t.func.data(), t.func.size(), &p, "environment distribution"))) return st;
+        d.env_func = p;
+        if ((st = scene->upload(t.cdf.data(), t.cdf.size(), &p, "environment distribution"))) return st;
+        d.env_cdf = p;
+        if ((st = scene->upload(t.row_integral.data(), t.row_integral.size(), &p, "environment distribution")))
+                return st;
+        d.env_row_int = p;
+        if ((st = scene->upload(t.marg_func.data(), t.marg_func.size(), &p, "environment distribution"))) return st;
+        d.env_marg_func = p;
+        if ((st = scene->upload(t.marg_cdf.data(), t.marg_cdf.size(), &p, "environment distribution"))) return st;
+        d.env_marg_cdf = p;
+        d.env_marg_int = t.marg_integral;
+        d.env_w = width;
+        d.env_h = height;
+        const float pi = 3.14159265358979323846f, radius = 100.0f / 2.0f;
+        const float power = pi * (radius * radius) * ((scale + scale + scale) / 3.0f);
+        d.env_power = power;
+        HostShading &hs = scene->host_shading;
+        std::vector<float> cdf = hs.light_cdf;
+        cdf.push_back(cdf.empty() ? power : cdf.back() + power);
+        if ((st = scene->upload(cdf.data(), cdf.size(), &p, "light cdf"))) return st;
+        d.light_cdf = p;
+        hs.has_env = true;
+        hs.env_power = power;
+        hs.light_total_env = hs.light_total + power;
+        hs.light_cdf = std::move(cdf);
         return clear_error();
 }
 

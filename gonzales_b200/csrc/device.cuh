@@ -47,6 +47,19 @@ struct DevScene {
         // batches of scenes: a device ray's spare lane (gzg_ray_d.pad_) holds
         // the wide-node index its traversal starts at
         int32_t per_ray_root;
+        // two-level shading: per instance object_to_world rows (3 x float4),
+        // per bottom-level scene the first index of its prims in pv0/1/2 and
+        // prims (materials already offset)
+        const float4 *inst_o2w;
+        const int32_t *blas_prim_base;
+        // environment light (gzg_scene_set_environment): map env_w x env_h RGB,
+        // 1024 x 1024 distribution (function, cdf 1025 per row, row integrals),
+        // marginal function, cdf and integral, and the light's power
+        const float *env_rgb;
+        int32_t env_w, env_h;
+        const float *env_func, *env_cdf, *env_row_int, *env_marg_func, *env_marg_cdf;
+        float env_marg_int;
+        float env_power;
 };
 
 // The launch's ray count: the device-side count when one is given.

@@ -62,6 +62,10 @@ struct HostShading {
         std::vector<float4_> lights;         // 4 per light
         std::vector<float> light_cdf;
         float light_total = 0.0f;
+        // environment light, after the area lights in the light list
+        bool has_env = false;
+        float env_power = 0.0f;
+        float light_total_env = 0.0f;  // light_total + env_power
 };
 
 // Converts a validated reference BVH2 + prims + meshes into the wide layout.
@@ -76,6 +80,16 @@ gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const 
 #else
 #define GZG_HOST_DEVICE
 #endif
+
+// Environment light tables (env.cpp): kEnvDistSize x kEnvDistSize
+// piecewise-constant distribution over the equal-area square.
+constexpr int kEnvDistSize = 1024;
+struct EnvTables {
+        std::vector<float> func, cdf, row_integral, marg_func, marg_cdf;
+        float marg_integral = 0.0f;
+};
+void build_env_tables(const float *rgb, int w, int h, EnvTables *t);
+void env_lookup_host(const float *rgb, int w, int h, float u, float v, float *out);
 
 // Host copies kept by an uploaded scene (batch assembly).
 const WideBvh &scene_host_wide(const gzg_scene *scene);

@@ -120,9 +120,10 @@ struct Frame {
         __device__ V3 to_world(V3 v) const { return x * v.x + y * v.y + z * v.z; }
 };
 
-// Shading frame of a hit without UVs or vertex normals (Shape/Triangle.swift:
-// 395-452 with degenerate UVs, Reflection/BsdfFrame.swift:13-21).
-__device__ bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame &f) {
+// The interaction's dpdu of a hit without UVs or vertex normals
+// (Shape/Triangle.swift:395-452 with degenerate UVs): false for a degenerate
+// triangle.
+__device__ bool shading_dpdu(V3 p0, V3 p1, V3 p2, V3 ns, V3 &dpdu_out) {
         const V3 gn = cross(p2 - p0, p1 - p0);
         if (dot(gn, gn) == 0.0f) return false;
         V3 dpdu, dpdv;
@@ -135,10 +136,42 @@ __device__ bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame &f) {
         } else {
                 coordinate_system(ns, s, t);
         }
-        f.y = normalize(s);
+        dpdu_out = s;
+        return true;
+}
+
+// BsdfFrame from dpdu and the shading normal (Reflection/BsdfFrame.swift:13-21).
+__device__ Frame frame_from(V3 dpdu, V3 ns) {
+        Frame f;
+        f.y = normalize(dpdu);
         f.z = ns;
         f.x = cross(f.y, f.z);
+        return f;
+}
+
+__device__ bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame &f) {
+        V3 s;
+        if (!shading_dpdu(p0, p1, p2, ns, s)) return false;
+        f = frame_from(s, ns);
         return true;
+}
+
+// Transform * Point / Vector / Normal (Geometry/Transform.swift:31-65) with a
+// 3x4 matrix given as three float4 rows; the normal uses the inverse's columns.
+__device__ __forceinline__ V3 xf_pt(float4 a, float4 b, float4 c, V3 p) {
+        return v3(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, p.x), __fmul_rn(a.y, p.y)), __fmul_rn(a.z, p.z)), a.w),
+                  __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(b.x, p.x), __fmul_rn(b.y, p.y)), __fmul_rn(b.z, p.z)), b.w),
+                  __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, p.x), __fmul_rn(c.y, p.y)), __fmul_rn(c.z, p.z)), c.w));
+}
+__device__ __forceinline__ V3 xf_vec(float4 a, float4 b, float4 c, V3 p) {
+        return v3(__fadd_rn(__fadd_rn(__fmul_rn(a.x, p.x), __fmul_rn(a.y, p.y)), __fmul_rn(a.z, p.z)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(b.x, p.x), __fmul_rn(b.y, p.y)), __fmul_rn(b.z, p.z)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(c.x, p.x), __fmul_rn(c.y, p.y)), __fmul_rn(c.z, p.z)));
+}
+__device__ __forceinline__ V3 xf_nrm(float4 a, float4 b, float4 c, V3 n) {
+        return v3(__fadd_rn(__fadd_rn(__fmul_rn(a.x, n.x), __fmul_rn(b.x, n.y)), __fmul_rn(c.x, n.z)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(a.y, n.x), __fmul_rn(b.y, n.y)), __fmul_rn(c.y, n.z)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(a.z, n.x), __fmul_rn(b.z, n.y)), __fmul_rn(c.z, n.z)));
 }
 
 // erfinv of Filter/GaussianFilter.swift:27-91 (rational start, two Newton steps).
@@ -197,8 +230,10 @@ struct SceneConst {
         float tan_half, sx0, sx1, sy0, sy1;
         float filter_radius, filter_sigma;
         int32_t width, height, spp, max_depth, rr_min, mis_corrected, first_sample;
-        int32_t light_begin, light_count;
+        int32_t light_begin, light_count;  // light_count includes the environment light
         float light_total;
+        int32_t env_index;                 // scene-local index of the environment light or -1
+        float env_power;
         int32_t material_begin;  // the scene's material 0 (area-light hits scatter with it)
         int32_t material_count;
         uint32_t root;            // wide-node root of the scene's tree
@@ -259,6 +294,9 @@ struct Wave {
         const float *adj_w;        // film weight sums per pixel (image = rgb / w)
         float *d_tex;              // dLoss/dtexel (accumulated)
         double *d_emission;        // dLoss/demission_scale (accumulated)
+        // two-level scenes: the instance of each extension and probe hit
+        int32_t *hit_inst;
+        int32_t *pr_inst;
 };
 
 // Appends to a queue with one atomic per converged group of lanes.
@@ -302,6 +340,47 @@ __device__ __forceinline__ void prim_info(const DevScene &s, int prim, int &type
         type = (int)(signed char)(__ldg(reinterpret_cast<const unsigned char *>(r + 3)));
 }
 
+// The surface interaction of a hit: Triangle.computeSurfaceInteraction
+// (Shape/Triangle.swift:363-474); for an instance it is computed in object
+// space and carried to world space (Core/Transform+SurfaceInteraction.swift:
+// 3-14: position as a point, normals through the inverse, outgoing and dpdu
+// as vectors).  gprim is the prim's index in the scene's shading arrays.
+struct Surf {
+        V3 pos, ng, wo;
+        Frame fr;
+        bool frame_ok;
+        int gprim;
+};
+
+__device__ void surface(const DevScene &s, int prim, int inst, float bu, float bv, V3 d, Surf &o) {
+        V3 p0, p1, p2;
+        const float b0 = (1.0f - bu) - bv;
+        if (!s.instances) {
+                prim_triangle_dev(s, prim, p0, p1, p2);
+                o.pos = p0 * b0 + p1 * bu + p2 * bv;
+                o.ng = normalize(cross(p0 - p2, p1 - p2));
+                o.wo = normalize(neg(d));
+                o.frame_ok = make_frame(p0, p1, p2, o.ng, o.fr);
+                o.gprim = prim;
+                return;
+        }
+        const float4 w0 = __ldg(s.instances + 4 * inst), w1 = __ldg(s.instances + 4 * inst + 1),
+                     w2 = __ldg(s.instances + 4 * inst + 2), w3 = __ldg(s.instances + 4 * inst + 3);
+        const float4 o0 = __ldg(s.inst_o2w + 3 * inst), o1 = __ldg(s.inst_o2w + 3 * inst + 1),
+                     o2 = __ldg(s.inst_o2w + 3 * inst + 2);
+        o.gprim = __ldg(s.blas_prim_base + __float_as_int(w3.y)) + prim;
+        prim_triangle_dev(s, o.gprim, p0, p1, p2);
+        const V3 pos_o = p0 * b0 + p1 * bu + p2 * bv;
+        const V3 n_o = normalize(cross(p0 - p2, p1 - p2));
+        const V3 wo_o = normalize(neg(xf_vec(w0, w1, w2, d)));
+        V3 s_o = v3(0.0f, 0.0f, 0.0f);
+        o.frame_ok = shading_dpdu(p0, p1, p2, n_o, s_o);
+        o.pos = xf_pt(o0, o1, o2, pos_o);
+        o.ng = normalize(xf_nrm(w0, w1, w2, n_o));
+        o.wo = normalize(xf_vec(o0, o1, o2, wo_o));
+        if (o.frame_ok) o.fr = frame_from(xf_vec(o0, o1, o2, s_o), o.ng);
+}
+
 // Nearest texel of texture t at p (planar map), as a texel index.
 __device__ __forceinline__ int texel_at(const Wave &w, int t, V3 p) {
         const float *mp = w.tex_map + 9 * t;
@@ -312,6 +391,128 @@ __device__ __forceinline__ int texel_at(const Wave &w, int t, V3 p) {
         const int ix = (int)fminf(fmaxf(u * (float)R, 0.0f), (float)(R - 1));
         const int iy = (int)fminf(fmaxf(v * (float)R, 0.0f), (float)(R - 1));
         return (t * R + iy) * R + ix;
+}
+
+// ------------------------------------------------------------ environment light
+// Light/InfiniteLight.swift:7-160 with PiecewiseConstant1D/2D
+// (Core/Distribution1D.swift, Core/Distribution2D.swift).  The map lookup is
+// bilinear with clamped edges (the reference goes through OpenImageIO).
+
+__device__ V3 env_lookup(const DevScene &s, float u, float v) {
+        const float x = u * (float)s.env_w - 0.5f, y = v * (float)s.env_h - 0.5f;
+        const float fx = floorf(x), fy = floorf(y);
+        const float ax = x - fx, ay = y - fy;
+        const int x0 = min(max((int)fx, 0), s.env_w - 1), x1 = min(max((int)fx + 1, 0), s.env_w - 1);
+        const int y0 = min(max((int)fy, 0), s.env_h - 1), y1 = min(max((int)fy + 1, 0), s.env_h - 1);
+        float out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+                const float a = __ldg(s.env_rgb + ((size_t)y0 * s.env_w + x0) * 3 + c);
+                const float b = __ldg(s.env_rgb + ((size_t)y0 * s.env_w + x1) * 3 + c);
+                const float d = __ldg(s.env_rgb + ((size_t)y1 * s.env_w + x0) * 3 + c);
+                const float e = __ldg(s.env_rgb + ((size_t)y1 * s.env_w + x1) * 3 + c);
+                const float top = a + (b - a) * ax;
+                const float bot = d + (e - d) * ax;
+                out[c] = top + (bot - top) * ay;
+        }
+        return v3(out[0], out[1], out[2]);
+}
+
+// equalAreaSquareToSphere (InfiniteLight.swift:118-135): as in the reference,
+// x and y lack the sqrt(2 - r^2) factor, so the direction is not unit length.
+__device__ V3 env_square_to_sphere(float u, float v) {
+        const float ru = 2.0f * u - 1.0f, rv = 2.0f * v - 1.0f;
+        const float au = fabsf(ru), av = fabsf(rv);
+        const float sd = 1.0f - (au + av);
+        const float r = 1.0f - fabsf(sd);
+        const float phi = (r == 0.0f ? 1.0f : (av - au) / r + 1.0f) * (kPi / 4.0f);
+        const float z = copysignf(fmaxf(0.0f, 1.0f - r * r), sd);
+        return v3(copysignf(r * cosf(phi), ru), copysignf(r * sinf(phi), rv), z);
+}
+
+// equalAreaSphereToSquare (InfiniteLight.swift:92-116).
+__device__ void env_sphere_to_square(V3 d, float &u, float &v) {
+        const float x = fabsf(d.x), y = fabsf(d.y), z = fabsf(d.z);
+        const float radius = sqrtf(fmaxf(0.0f, 1.0f - z));
+        const float a = fmaxf(x, y);
+        float b = fminf(x, y);
+        b = a == 0.0f ? 0.0f : b / a;
+        float phi = atanf(b) * 2.0f / kPi;
+        if (x < y) phi = 1.0f - phi;
+        float vv = phi * radius;
+        float uu = radius - vv;
+        if (d.z < 0.0f) {
+                const float t = uu;
+                uu = 1.0f - vv;
+                vv = 1.0f - t;
+        }
+        u = 0.5f * (copysignf(uu, d.x) + 1.0f);
+        v = 0.5f * (copysignf(vv, d.y) + 1.0f);
+}
+
+// PiecewiseConstant1D.findInterval over cdf[0..n].
+__device__ int env_find_interval(const float *cdf, int n, float u) {
+        int lo = 0, hi = n;
+        while (lo < hi) {
+                const int mid = lo + (hi - lo) / 2;
+                if (__ldg(cdf + mid) <= u)
+                        lo = mid + 1;
+                else
+                        hi = mid;
+        }
+        return min(max(lo - 1, 0), n - 1);
+}
+
+// PiecewiseConstant1D.sampleContinuous: value, pdf(value), offset.
+__device__ float env_sample_1d(const float *func, const float *cdf, float integral, int n, float u, float &pdf,
+                               int &offset) {
+        const int o = env_find_interval(cdf, n, u);
+        float delta = u - __ldg(cdf + o);
+        const float dist = __ldg(cdf + o + 1) - __ldg(cdf + o);
+        if (dist > 0.0f) delta = delta / dist;
+        const float value = ((float)o + delta) / (float)n;
+        const int po = min(max((int)(value * (float)n), 0), n - 1);
+        pdf = __ldg(func + po) / integral;
+        offset = o;
+        return value;
+}
+
+// InfiniteLight.sample: direction and map value; returns the solid-angle pdf
+// (0: no sample).
+__device__ float env_sample(const DevScene &s, float u0, float u1, V3 &dir, V3 &rgb) {
+        constexpr int N = 1024;
+        float pdf1, pdf0;
+        int mo, co;
+        const float mv = env_sample_1d(s.env_marg_func, s.env_marg_cdf, s.env_marg_int, N, u1, pdf1, mo);
+        const float cv = env_sample_1d(s.env_func + (size_t)mo * N, s.env_cdf + (size_t)mo * (N + 1),
+                                       __ldg(s.env_row_int + mo), N, u0, pdf0, co);
+        const float map_pdf = pdf0 * pdf1;
+        if (map_pdf == 0.0f) {
+                dir = rgb = v3(0.0f, 0.0f, 0.0f);
+                return 0.0f;
+        }
+        dir = env_square_to_sphere(cv, mv);
+        rgb = env_lookup(s, cv, mv);
+        return map_pdf / (4.0f * kPi);
+}
+
+// InfiniteLight.probabilityDensityFor: the direction is not normalised.
+__device__ float env_pdf(const DevScene &s, V3 d) {
+        constexpr int N = 1024;
+        float u, v;
+        env_sphere_to_square(d, u, v);
+        const int col = min(max((int)(u * (float)N), 0), N - 1);
+        const int row = min(max((int)(v * (float)N), 0), N - 1);
+        return __ldg(s.env_func + (size_t)row * N + col) / s.env_marg_int / (4.0f * kPi);
+}
+
+// radianceFromInfinity: normalised direction (a zero vector stays as is).
+__device__ V3 env_radiance(const DevScene &s, V3 d) {
+        const float l = sqrtf(dot(d, d));
+        const V3 n = l != 0.0f ? v3(d.x / l, d.y / l, d.z / l) : d;
+        float u, v;
+        env_sphere_to_square(n, u, v);
+        return env_lookup(s, u, v);
 }
 
 // ------------------------------------------------------------ kernels
@@ -372,8 +573,9 @@ __global__ void k_generate(Wave w) {
         w.q_id[0][i] = i;
 }
 
-// Power light sampler over the scene's lights: lowerBound over the running
-// power sum (Light/PowerLightSampler.swift:4-48).
+// Power light sampler over the scene's lights (area lights, then the
+// environment light): lowerBound over the running power sum
+// (Light/PowerLightSampler.swift:4-48).  Returns the scene-local index.
 __device__ int choose_light(const DevScene &s, const SceneConst &sc, float u, float &pdf) {
         const float key = u * sc.light_total;
         int lo = 0, hi = sc.light_count;
@@ -391,9 +593,8 @@ __device__ int choose_light(const DevScene &s, const SceneConst &sc, float u, fl
                 }
         }
         if (lo >= sc.light_count) lo = sc.light_count - 1;
-        const int li = sc.light_begin + lo;
-        pdf = __ldg(s.lights + 4 * li + 1).w / sc.light_total;
-        return li;
+        pdf = (lo == sc.env_index ? sc.env_power : __ldg(s.lights + 4 * (sc.light_begin + lo) + 1).w) / sc.light_total;
+        return lo;
 }
 
 // offsetRayOrigin(point:normal:direction:) (Core/Interaction.swift:26-35).
@@ -408,9 +609,14 @@ __device__ __forceinline__ int entry_key(const Wave &w, const DevScene &s, int c
         const int prim = __float_as_int(w.hits[i].w);
         if (prim < 0) return w.key_count - 1;
         if (w.sort_key == kSortScene) return (int)w.scene[w.q_id[cur][i]];
+        int gp = prim;
+        if (s.instances) {
+                const float4 w3 = __ldg(s.instances + 4 * w.hit_inst[i] + 3);
+                gp = __ldg(s.blas_prim_base + __float_as_int(w3.y)) + prim;
+        }
         int type;
         int64_t m;
-        prim_info(s, prim, type, m);
+        prim_info(s, gp, type, m);
         if (type == 3) m = w.scenes[w.scene[w.q_id[cur][i]]].material_begin;
         return m >= 0 && m < w.key_count - 1 ? (int)m : w.key_count - 1;
 }
@@ -463,22 +669,32 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const uint32_t path = w.q_id[cur][i];
         const float4 hit = w.hits[i];
         const int prim = __float_as_int(hit.w);
-        if (prim < 0) return;  // miss: no environment light
+        const float4 rd = w.q_ray[cur][2 * i + 1];
+        const V3 d = v3(rd);
+        if (prim < 0) {
+                // shadeBounce on a miss (:375-387): the environment light on
+                // camera rays (no specular bounces in these scenes)
+                if (bounce == 0 && s.env_rgb) {
+                        const V3 thr = v3(w.thr[path]);
+                        const V3 le = env_radiance(s, d);
+                        float4 L = w.L[path];
+                        L.x += thr.x * le.x;
+                        L.y += thr.y * le.y;
+                        L.z += thr.z * le.z;
+                        w.L[path] = L;
+                }
+                return;
+        }
         const SceneConst &sc = w.scenes[w.scene[path]];
         V3 thr = v3(w.thr[path]);
         if (is_black(thr)) return;
         if (bounce >= sc.max_depth) return;
-        const float4 rd = w.q_ray[cur][2 * i + 1];
-        const V3 d = v3(rd);
-        V3 p0, p1, p2;
-        prim_triangle_dev(s, prim, p0, p1, p2);
-        const float b0 = (1.0f - hit.y) - hit.z;
-        const V3 pos = p0 * b0 + p1 * hit.y + p2 * hit.z;
-        const V3 ng = normalize(cross(p0 - p2, p1 - p2));
-        const V3 wo = normalize(neg(d));
+        Surf sf;
+        surface(s, prim, s.instances ? w.hit_inst[i] : -1, hit.y, hit.z, d, sf);
+        const V3 pos = sf.pos, ng = sf.ng, wo = sf.wo;
         int type;
         int64_t mat_index;
-        prim_info(s, prim, type, mat_index);
+        prim_info(s, sf.gprim, type, mat_index);
         const bool is_light = type == 3;
         V3 L = v3(w.L[path]);
         if (bounce == 0 && is_light && mat_index >= 0 && mat_index < s.material_count) {
@@ -509,37 +725,57 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                 }
         }
         const V3 f_val = refl * (1.0f / kPi);
-        Frame fr;
+        const Frame &fr = sf.fr;
         ZSobol z;
         z.morton = w.zs_morton[path];
         z.dim = w.zs_dim[path];
-        bool alive = make_frame(p0, p1, p2, ng, fr);
+        bool alive = sf.frame_ok;
         if (alive && sc.light_count > 0) {
                 const V3 wo_l = fr.to_local(wo);
                 // ---- light choice and light sample (sampleLightSource, :67-89)
                 float choose_pdf;
-                const int li = choose_light(s, sc, zs_get1d(sc.zs, z), choose_pdf);
-                const float4 l0 = __ldg(s.lights + 4 * li), l1 = __ldg(s.lights + 4 * li + 1),
-                             l2 = __ldg(s.lights + 4 * li + 2), le4 = __ldg(s.lights + 4 * li + 3);
-                const V3 lp0 = v3(l0), lp1 = v3(l1), lp2 = v3(l2), le = v3(le4) * w.emission_scale;
-                const float area = l0.w;
+                const int lo = choose_light(s, sc, zs_get1d(sc.zs, z), choose_pdf);
+                const bool chose_env = lo == sc.env_index;
+                const int li = sc.light_begin + lo;
                 float u0, u1;
                 zs_get2d(sc.zs, z, u0, u1);
-                const float su0 = sqrtf(u0);
-                const float lb0 = 1.0f - su0, lb1 = u1 * su0;
-                const V3 lp = lp0 * lb0 + lp1 * lb1 + lp2 * ((1.0f - lb0) - lb1);
-                const V3 ln = normalize(cross(lp1 - lp0, lp2 - lp0));
-                const V3 inc = normalize(lp - pos);
-                const V3 dl = pos - lp;
-                const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
-                float light_pdf = 0.0f;
-                V3 light_est = v3(0, 0, 0), light_dir = v3(0, 0, 0);
-                if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
-                        const bool reflect = dot(inc, ng) * dot(wo, ng) > 0.0f;
-                        const V3 f = reflect ? f_val : v3(0, 0, 0);
-                        light_est = mulv(f * fabsf(dot(inc, ng)), le);
-                        light_dir = inc;
-                        light_pdf = pdf;
+                float light_pdf = 0.0f, area = 0.0f;
+                V3 light_est = v3(0, 0, 0), light_dir = v3(0, 0, 0), lp0, lp1, lp2, target;
+                if (chose_env) {
+                        // InfiniteLight.sample (InfiniteLight.swift:38-64); the
+                        // shadow ray runs to a point 100 (sceneDiameter) away
+                        V3 dv, rad;
+                        const float pdf = env_sample(s, u0, u1, dv, rad);
+                        target = pos + dv * 100.0f;
+                        if (!is_black(rad) && !isinf(pdf)) {
+                                const bool reflect = dot(dv, ng) * dot(wo, ng) > 0.0f;
+                                const V3 f = reflect ? f_val : v3(0, 0, 0);
+                                light_est = mulv(f * fabsf(dot(dv, ng)), rad);
+                                light_dir = dv;
+                                light_pdf = pdf;
+                        }
+                } else {
+                        const float4 l0 = __ldg(s.lights + 4 * li), l1 = __ldg(s.lights + 4 * li + 1),
+                                     l2 = __ldg(s.lights + 4 * li + 2), le4 = __ldg(s.lights + 4 * li + 3);
+                        const V3 le = v3(le4) * w.emission_scale;
+                        lp0 = v3(l0);
+                        lp1 = v3(l1);
+                        lp2 = v3(l2);
+                        area = l0.w;
+                        const float su0 = sqrtf(u0);
+                        const float lb0 = 1.0f - su0, lb1 = u1 * su0;
+                        target = lp0 * lb0 + lp1 * lb1 + lp2 * ((1.0f - lb0) - lb1);
+                        const V3 ln = normalize(cross(lp1 - lp0, lp2 - lp0));
+                        const V3 inc = normalize(target - pos);
+                        const V3 dl = pos - target;
+                        const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
+                        if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
+                                const bool reflect = dot(inc, ng) * dot(wo, ng) > 0.0f;
+                                const V3 f = reflect ? f_val : v3(0, 0, 0);
+                                light_est = mulv(f * fabsf(dot(inc, ng)), le);
+                                light_dir = inc;
+                                light_pdf = pdf;
+                        }
                 }
                 float brdf_density = 0.0f;
                 {
@@ -549,18 +785,21 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                 const float light_w = power_heuristic(light_pdf, brdf_density);
                 if (light_pdf != 0.0f && !is_black(light_est)) {
                         // Visibility.occluded via spawnRay(from:target:) (Interaction.swift:15-24)
-                        const V3 so = pos + (lp - pos) * 0.0001f;
-                        const V3 sd = lp - so;
+                        const V3 so = pos + (target - pos) * 0.0001f;
+                        const V3 sd = target - so;
                         const V3 c = mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf));
                         const uint32_t q = queue_slot(w.counts + kCountShadow);
                         store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
                         w.sh_id[q] = path;
                         w.sh_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
                 }
-                // ---- MIS BSDF sample (sampleDistributionFunction, :91-133)
+                // ---- MIS BSDF sample (sampleDistributionFunction, :91-133).  The
+                // chosen light's density along it: an environment light answers
+                // from its map; an area light, as written, answers 0 (queried with
+                // tHit = 0), so that strategy is traced only for corrected MIS.
                 float v0, v1, v2;
                 zs_get3d(sc.zs, z, v0, v1, v2);
-                if (sc.mis_corrected) {
+                if (sc.mis_corrected || chose_env) {
                         V3 wi_l = cosine_hemisphere(v0, v1);
                         if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
                         const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? fabsf(wi_l.z) / kPi : 0.0f;
@@ -568,18 +807,23 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                         const V3 est = f_val * fabsf(dot(wi, ng));
                         if (!is_black(est) && pdf_b > 0.0f) {
                                 const V3 po = offset_origin(pos, ng, wi);
-                                // light density of the chosen light along wi (Sampleable.swift:47-68 with tHit = inf)
                                 float light_density = 0.0f;
-                                float tl, lu, lv;
-                                const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f),
-                                             b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
-                                             c4 = make_float4(lp2.x, lp2.y, lp2.z, 0.0f);
-                                if (watertight_test(po.x, po.y, po.z, wi.x, wi.y, wi.z, a4, b4, c4, kInf, tl, lu, lv)) {
-                                        const V3 hp = po + wi * tl;
-                                        const V3 dq = pos - hp;
-                                        const V3 lnn = normalize(cross(lp0 - lp2, lp1 - lp2));
-                                        const float dens = dot(dq, dq) / (fabsf(dot(lnn, neg(wi))) * area);
-                                        light_density = isinf(dens) ? 0.0f : dens;
+                                if (chose_env) {
+                                        light_density = env_pdf(s, wi);
+                                } else {
+                                        // Sampleable.swift:47-68 with tHit = inf
+                                        float tl, lu, lv;
+                                        const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f),
+                                                     b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
+                                                     c4 = make_float4(lp2.x, lp2.y, lp2.z, 0.0f);
+                                        if (watertight_test(po.x, po.y, po.z, wi.x, wi.y, wi.z, a4, b4, c4, kInf, tl, lu,
+                                                            lv)) {
+                                                const V3 hp = po + wi * tl;
+                                                const V3 dq = pos - hp;
+                                                const V3 lnn = normalize(cross(lp0 - lp2, lp1 - lp2));
+                                                const float dens = dot(dq, dq) / (fabsf(dot(lnn, neg(wi))) * area);
+                                                light_density = isinf(dens) ? 0.0f : dens;
+                                        }
                                 }
                                 const float bw = power_heuristic(pdf_b, light_density);
                                 if (bw > 0.0f) {
@@ -639,25 +883,29 @@ __global__ void k_shadow_resolve(Wave w) {
         w.L[path] = L;
 }
 
-// Adds the emission a BSDF probe reaches (corrected MIS): the probe's closest
-// hit must be an area light whose normal faces back along the probe.
+// Adds the radiance a BSDF probe reaches: the emission of an area light whose
+// normal faces back along the probe, or, on a miss, the environment light.
 __global__ void k_probe_resolve(Wave w, DevScene s) {
         const uint32_t n = w.counts[kCountProbe];
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= n) return;
         const float4 h = w.pr_hits[i];
         const int prim = __float_as_int(h.w);
-        if (prim < 0) return;
-        int type;
-        int64_t mat_index;
-        prim_info(s, prim, type, mat_index);
-        if (type != 3 || mat_index < 0 || mat_index >= s.material_count) return;
-        V3 q0, q1, q2;
-        prim_triangle_dev(s, prim, q0, q1, q2);
-        const V3 qn = normalize(cross(q0 - q2, q1 - q2));
         const V3 wi = v3(w.pr_ray[2 * i + 1]);
-        if (!(dot(qn, neg(wi)) > 0.0f)) return;
-        const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
+        V3 le;
+        if (prim < 0) {
+                if (!s.env_rgb) return;
+                le = env_radiance(s, wi);
+        } else {
+                Surf sf;
+                surface(s, prim, s.instances ? w.pr_inst[i] : -1, h.y, h.z, wi, sf);
+                int type;
+                int64_t mat_index;
+                prim_info(s, sf.gprim, type, mat_index);
+                if (type != 3 || mat_index < 0 || mat_index >= s.material_count) return;
+                if (!(dot(sf.ng, neg(wi)) > 0.0f)) return;
+                le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
+        }
         const uint32_t path = w.pr_id[i];
         const float4 c = w.pr_contrib[i];
         float4 L = w.L[path];
@@ -952,7 +1200,7 @@ struct gzg_renderer {
                 const int block = 128;
                 const unsigned grid = (w.capacity + block - 1) / block;
                 int max_depth = 0;
-                bool corrected = false;
+                bool corrected = view.env_rgb != nullptr;  // an environment light is probed as written too
                 for (const gzg_render_params &P : params) {
                         max_depth = std::max(max_depth, (int)P.max_depth);
                         corrected = corrected || P.mis_corrected;
@@ -973,6 +1221,7 @@ struct gzg_renderer {
                         k_clear_counts<<<1, 1, 0, st>>>(w, cur ^ 1);
                         LaunchParams lp = lp_closest, lpa = lp_any;
                         lp.n_dev = w.counts + cur;
+                        lp.inst_out = w.hit_inst;
                         cudaError_t e = launch_trace(view, lp, kRayDevice, kOutHit, w.q_ray[cur], nullptr, w.capacity,
                                                      w.hits, st);
                         if (e != cudaSuccess) return e;
@@ -989,6 +1238,7 @@ struct gzg_renderer {
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
                         if (corrected) {
                                 lp.n_dev = w.counts + kCountProbe;
+                                lp.inst_out = w.pr_inst;
                                 e = launch_trace(view, lp, kRayDevice, kOutHit, w.pr_ray, nullptr, w.capacity, w.pr_hits,
                                                  st);
                                 if (e != cudaSuccess) return e;
@@ -1131,8 +1381,10 @@ gzg_status build_batch(gzg_renderer *r) {
                 sc.material_begin = 0;
                 sc.material_count = (int32_t)(hs.materials.size() / 2);
                 sc.light_begin = 0;
-                sc.light_count = (int32_t)(hs.lights.size() / 4);
-                sc.light_total = hs.light_total;
+                sc.light_count = (int32_t)(hs.lights.size() / 4) + (hs.has_env ? 1 : 0);
+                sc.light_total = hs.has_env ? hs.light_total_env : hs.light_total;
+                sc.env_index = hs.has_env ? (int32_t)(hs.lights.size() / 4) : -1;
+                sc.env_power = hs.env_power;
                 r->view.per_ray_root = 0;
         } else {
                 std::vector<WideNode> nodes;
@@ -1177,6 +1429,7 @@ gzg_status build_batch(gzg_renderer *r) {
                         sc.light_begin = loff;
                         sc.light_count = (int32_t)(hs.lights.size() / 4);
                         sc.light_total = hs.light_total;
+                        sc.env_index = -1;
                         steps = std::max<uint64_t>(steps, wb.nodes.size());
                         wide_depth = std::max(wide_depth, (int)wb.depth);
                 }
@@ -1211,9 +1464,11 @@ gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *pa
         if (n <= 0 || !scenes || !params) return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: no scenes");
         auto r = std::make_unique<gzg_renderer>();
         for (int64_t k = 0; k < n; ++k) {
-                if (!scenes[k] || scene_is_instanced(scenes[k]))
-                        return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: scene " + std::to_string(k) +
-                                                                       " is NULL or two-level (not rendered yet)");
+                if (!scenes[k]) return set_error(GZG_ERR_INVALID_ARGUMENT, "renderer: scene " + std::to_string(k) + " is NULL");
+                if (n > 1 && (scene_is_instanced(scenes[k]) || scene_host_shading(scenes[k]).has_env))
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         "renderer: scene " + std::to_string(k) +
+                                             " is two-level or has an environment light (single-scene renderers only)");
                 if (!params_ok(params[k]))
                         return set_error(GZG_ERR_INVALID_ARGUMENT,
                                          "renderer: bad render parameters for scene " + std::to_string(k));
@@ -1263,6 +1518,7 @@ gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *pa
             (st = r->alloc(&w.key_hist, 2 * keys)) || (st = r->alloc(&w.counts, kCountWords)) ||
             (st = r->alloc(&w.stats, kStatWords)))
                 return st;
+        if (r->view.instances && ((st = r->alloc(&w.hit_inst, C)) || (st = r->alloc(&w.pr_inst, C)))) return st;
         if ((st = cuda_err(cudaMemset(w.key_hist, 0, 2 * keys * sizeof(uint32_t)), "sort histogram"))) return st;
         if ((st = cuda_err(cudaMemset(w.counts, 0, kCountWords * 4), "renderer counters"))) return st;
         if ((st = cuda_err(cudaMemset(w.stats, 0, kStatWords * 8), "renderer statistics"))) return st;

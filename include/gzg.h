@@ -327,6 +327,17 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
  * default for closest-hit (any_hit = 0) or any-hit queries. */
 GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const gzg_trace_options *config);
 
+/* Adds an environment light (Light/InfiniteLight.swift) to an uploaded scene
+ * (flat or two-level), after its area lights in the light list: the HOST map
+ * rgb[height][width][3] (row v, column u) in the equal-area square layout the
+ * reference reads, looked up bilinearly; its 1024 x 1024 sampling
+ * distribution is built from the green channel, as the reference's is, and
+ * `scale` enters only the light's power pi * 50^2 * scale (the light choice),
+ * as in the reference.  Once per scene; renderers created afterwards use it
+ * (single-scene renderers only). */
+GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
+                                             float scale);
+
 /* Expands device hits into reference Intersection_C records on the device
  * (prim-id lookup; the miss record of kernel.mojo:362-364). */
 GZG_API gzg_status gzg_hits_to_intersections_device(gzg_scene *scene, const gzg_hit_d *hits,
