@@ -25,6 +25,16 @@ __device__ __forceinline__ float qbyte(uint32_t word, uint32_t sel) {
         return __uint_as_float(__byte_perm(word, 0x4B000000u, sel)) - 8388608.0f;
 }
 
+// 1/d for the wide kernels' slab tests, kept finite: |d| <= 2^-64 (zero
+// included) gives +-2^64 with d's sign.  Finite reciprocals keep every plane
+// distance free of 0 * inf = NaN, which lets the slab test compare float bits
+// as integers (below).  A plane then appears at distance |dx| * 2^64 instead of
+// beyond it, still far past any hit distance of a scene with coordinates below
+// about 1e12, so the test stays conservative.
+__device__ __forceinline__ float wide_rcp(float d) {
+        return fabsf(d) > 5.42101086e-20f ? __fdiv_rn(1.0f, d) : copysignf(1.8446744e19f, d);
+}
+
 struct WideRay {
         float ox, oy, oz, dx, dy, dz;
         float rdx, rdy, rdz;
@@ -83,8 +93,13 @@ __device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const 
                 const float tfx = fmaf(qbyte(farx[w], sel), fsx, fax);
                 const float tfy = fmaf(qbyte(fary[w], sel), fsy, fay);
                 const float tfz = fmaf(qbyte(farz[w], sel), fsz, faz);
-                const float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-                const float tfar = fminf(fminf(tfx, tfy), fminf(tfz, thit_far));
+                // max(0, tn*) and min(tf*, thit) on the float bits as signed
+                // integers: order-preserving for non-negative floats; tnear is
+                // never negative, and a negative tfar (a negative integer)
+                // rejects the box either way.  No NaN occurs (finite rdir).
+                const int tnear = __vimax3_s32_relu(__float_as_int(tnx), __float_as_int(tny), __float_as_int(tnz));
+                const int tfar = __vimin3_s32(__float_as_int(tfx), __float_as_int(tfy),
+                                              min(__float_as_int(tfz), __float_as_int(thit_far)));
                 if (tnear <= tfar) {
                         const uint32_t m = (meta[w] >> (8 * (k & 3))) & 0xFFu;
                         if ((imask >> k) & 1u) {
@@ -114,9 +129,9 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
         r.dx = in.dx;
         r.dy = in.dy;
         r.dz = in.dz;
-        r.rdx = __fdiv_rn(1.0f, in.dx);
-        r.rdy = __fdiv_rn(1.0f, in.dy);
-        r.rdz = __fdiv_rn(1.0f, in.dz);
+        r.rdx = wide_rcp(in.dx);
+        r.rdy = wide_rcp(in.dy);
+        r.rdz = wide_rcp(in.dz);
         r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
                 ((__float_as_uint(r.rdz) >> 31) << 2);
 
@@ -242,9 +257,9 @@ __global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void 
                                 r.dx = in.dx;
                                 r.dy = in.dy;
                                 r.dz = in.dz;
-                                r.rdx = __fdiv_rn(1.0f, in.dx);
-                                r.rdy = __fdiv_rn(1.0f, in.dy);
-                                r.rdz = __fdiv_rn(1.0f, in.dz);
+                                r.rdx = wide_rcp(in.dx);
+                                r.rdy = wide_rcp(in.dy);
+                                r.rdz = wide_rcp(in.dz);
                                 r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
                                         ((__float_as_uint(r.rdz) >> 31) << 2);
                                 tmax = in.tmax;
@@ -339,9 +354,9 @@ __global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void 
 }
 
 __device__ __forceinline__ void set_ray_dirs(WideRay &r) {
-        r.rdx = __fdiv_rn(1.0f, r.dx);
-        r.rdy = __fdiv_rn(1.0f, r.dy);
-        r.rdz = __fdiv_rn(1.0f, r.dz);
+        r.rdx = wide_rcp(r.dx);
+        r.rdy = wide_rcp(r.dy);
+        r.rdz = wide_rcp(r.dz);
         r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
                 ((__float_as_uint(r.rdz) >> 31) << 2);
 }
