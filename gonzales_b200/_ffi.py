@@ -145,6 +145,8 @@ PROTOTYPES = {
     "gzg_renderer_autotune": (ST, [VP, C.POINTER(BatchOptions), C.POINTER(C.c_float), VP]),
     "gzg_renderer_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int32]),
     "gzg_renderer_set_textures": (ST, [VP, VP, C.c_int32, C.c_int32, VP, C.c_float]),
+    "gzg_renderer_set_film": (ST, [VP, C.c_float, C.c_float]),
+    "gzg_renderer_render_aov": (ST, [VP, VP, VP, VP, VP, VP, VP]),
     "gzg_renderer_render_f64": (ST, [VP, VP, VP, VP, VP]),
     "gzg_renderer_adjoint": (ST, [VP, VP, VP, VP, VP, VP]),
     "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),

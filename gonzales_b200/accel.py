@@ -274,10 +274,22 @@ class Renderer:
         F.check(F.lib().gzg_renderer_create(accel.handle, C.byref(params), C.byref(h)))
         self.handle = h
 
-    def render(self, film_rgb, film_w, film_sq=None, stream=None):
-        F.check(F.lib().gzg_renderer_render(self.handle, film_rgb.data_ptr(),
-                                            film_sq.data_ptr() if film_sq is not None else None,
-                                            film_w.data_ptr(), _stream_handle(stream)))
+    def render(self, film_rgb, film_w, film_sq=None, stream=None, film_albedo=None, film_normal=None):
+        if film_albedo is None and film_normal is None:
+            F.check(F.lib().gzg_renderer_render(self.handle, film_rgb.data_ptr(),
+                                                film_sq.data_ptr() if film_sq is not None else None,
+                                                film_w.data_ptr(), _stream_handle(stream)))
+            return
+        F.check(F.lib().gzg_renderer_render_aov(self.handle, film_rgb.data_ptr(),
+                                                film_sq.data_ptr() if film_sq is not None else None,
+                                                film_w.data_ptr(),
+                                                film_albedo.data_ptr() if film_albedo is not None else None,
+                                                film_normal.data_ptr() if film_normal is not None else None,
+                                                _stream_handle(stream)))
+
+    def set_film(self, iso=100.0, max_component=0.0):
+        """Film.add settings: light scaled by iso / 100, optional clamp."""
+        F.check(F.lib().gzg_renderer_set_film(self.handle, float(iso), float(max_component)))
 
     def stats(self):
         s = F.RenderStats()

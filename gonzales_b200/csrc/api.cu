@@ -558,14 +558,21 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
                 p.l1_carveout = t.l1_carveout;
                 const int fmt = any_hit ? kOutAnyPrim : kOutHit;
                 GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st), "autotune launch");
-                GZG_CK(cudaEventRecord(e0, st), "autotune event");
-                for (int k = 0; k < 3; ++k)
-                        GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st), "autotune launch");
-                GZG_CK(cudaEventRecord(e1, st), "autotune event");
-                GZG_CK(cudaEventSynchronize(e1), "autotune sync");
-                float el = 0;
-                cudaEventElapsedTime(&el, e0, e1);
-                *ms = el / 3.0f;
+                // the faster of two timed batches of three launches (a single
+                // batch let one noisy sample pick a slow configuration)
+                float best_el = 0.0f;
+                for (int rep = 0; rep < 2; ++rep) {
+                        GZG_CK(cudaEventRecord(e0, st), "autotune event");
+                        for (int k = 0; k < 3; ++k)
+                                GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st),
+                                       "autotune launch");
+                        GZG_CK(cudaEventRecord(e1, st), "autotune event");
+                        GZG_CK(cudaEventSynchronize(e1), "autotune sync");
+                        float el = 0;
+                        cudaEventElapsedTime(&el, e0, e1);
+                        if (rep == 0 || el < best_el) best_el = el;
+                }
+                *ms = best_el / 3.0f;
                 return GZG_OK;
         };
         TunedLaunch cur;

@@ -234,6 +234,8 @@ struct SceneConst {
         float light_total;
         int32_t env_index;                 // scene-local index of the environment light or -1
         float env_power;
+        float film_scale;                  // Film.add: iso / 100
+        float max_component;               // clamp of a sample's largest component (0: none)
         int32_t material_begin;  // the scene's material 0 (area-light hits scatter with it)
         int32_t material_count;
         uint32_t root;            // wide-node root of the scene's tree
@@ -297,6 +299,9 @@ struct Wave {
         // two-level scenes: the instance of each extension and probe hit
         int32_t *hit_inst;
         int32_t *pr_inst;
+        // first-hit AOVs per path slot: BSDF albedo and geometric normal
+        float4 *alb;
+        float4 *nrm;
 };
 
 // Appends to a queue with one atomic per converged group of lanes.
@@ -566,6 +571,8 @@ __global__ void k_generate(Wave w) {
         w.zs_dim[i] = z.dim;
         w.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         w.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.alb[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.nrm[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         w.pixel[i] = sc.film_offset + pixel;
         w.scene[i] = (uint32_t)lo;
         w.weight[i] = fv / (denx * deny);
@@ -725,6 +732,11 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                 }
         }
         const V3 f_val = refl * (1.0f / kPi);
+        if (bounce == 0) {
+                // surfaceEstimate (:341-344): state.albedo, state.firstNormal
+                w.alb[path] = make_float4(refl.x, refl.y, refl.z, 0.0f);
+                w.nrm[path] = make_float4(ng.x, ng.y, ng.z, 0.0f);
+        }
         const Frame &fr = sf.fr;
         ZSobol z;
         z.morton = w.zs_morton[path];
@@ -929,14 +941,35 @@ __global__ void k_clear_counts(Wave w, int next) {
         w.counts[kCountProbe] = 0;
 }
 
-// Film sums (Core/Film.swift:107-119): radiance (iso 100 -> scale 1), its
-// square, and the filter weight, per pixel of the batch film.
-__global__ void k_accumulate(Wave w, float *film_rgb, float *film_sq, float *film_w) {
+// Film.add (Core/Film.swift:107-119): the sample's light scaled by iso / 100
+// and, when a clamp is set, by max / its largest component.
+__device__ __forceinline__ float4 film_light(const Wave &w, uint32_t i) {
+        const SceneConst &sc = w.scenes[w.scene[i]];
+        float4 L = w.L[i];
+        L.x *= sc.film_scale;
+        L.y *= sc.film_scale;
+        L.z *= sc.film_scale;
+        if (sc.max_component > 0.0f) {
+                const float mv = fmaxf(L.x, fmaxf(L.y, L.z));
+                if (mv > sc.max_component) {
+                        const float k = sc.max_component / mv;
+                        L.x *= k;
+                        L.y *= k;
+                        L.z *= k;
+                }
+        }
+        return L;
+}
+
+// Film sums: radiance, its square, the filter weight and the first-hit AOVs
+// (albedo, normal: Tile.swift:157-205), per pixel of the batch film.
+__global__ void k_accumulate(Wave w, float *film_rgb, float *film_sq, float *film_w, float *film_alb,
+                             float *film_nrm) {
         const uint32_t count = wave_count(w);
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= count) return;
         const uint32_t px = w.pixel[i];
-        const float4 L = w.L[i];
+        const float4 L = film_light(w, i);
         atomicAdd(film_rgb + 3 * (size_t)px, L.x);
         atomicAdd(film_rgb + 3 * (size_t)px + 1, L.y);
         atomicAdd(film_rgb + 3 * (size_t)px + 2, L.z);
@@ -946,6 +979,18 @@ __global__ void k_accumulate(Wave w, float *film_rgb, float *film_sq, float *fil
                 atomicAdd(film_sq + 3 * (size_t)px + 2, L.z * L.z);
         }
         atomicAdd(film_w + px, w.weight[i]);
+        if (film_alb) {
+                const float4 a = w.alb[i];
+                atomicAdd(film_alb + 3 * (size_t)px, a.x);
+                atomicAdd(film_alb + 3 * (size_t)px + 1, a.y);
+                atomicAdd(film_alb + 3 * (size_t)px + 2, a.z);
+        }
+        if (film_nrm) {
+                const float4 nv = w.nrm[i];
+                atomicAdd(film_nrm + 3 * (size_t)px, nv.x);
+                atomicAdd(film_nrm + 3 * (size_t)px + 1, nv.y);
+                atomicAdd(film_nrm + 3 * (size_t)px + 2, nv.z);
+        }
 }
 
 // Double-precision film sums (finite differences need sums whose rounding
@@ -955,7 +1000,7 @@ __global__ void k_accumulate_f64(Wave w, double *film_rgb, double *film_sq, doub
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= count) return;
         const uint32_t px = w.pixel[i];
-        const float4 L = w.L[i];
+        const float4 L = film_light(w, i);
         atomicAdd(film_rgb + 3 * (size_t)px, (double)L.x);
         atomicAdd(film_rgb + 3 * (size_t)px + 1, (double)L.y);
         atomicAdd(film_rgb + 3 * (size_t)px + 2, (double)L.z);
@@ -1105,6 +1150,8 @@ SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices
         sc.mis_corrected = P.mis_corrected;
         sc.first_sample = P.first_sample;
         sc.zs = make_zsobol(P.sampler_spp > 0 ? P.sampler_spp : P.spp, P.width, P.height, P.seed, matrices);
+        sc.film_scale = 1.0f;  // iso 100
+        sc.max_component = 0.0f;
         return sc;
 }
 
@@ -1140,7 +1187,7 @@ struct gzg_renderer {
         std::vector<void *> allocs;
         cudaGraphExec_t graph = nullptr;
         cudaGraph_t graph_def = nullptr;
-        const void *graph_key[6] = {};
+        const void *graph_key[8] = {};
         // differentiable rendering
         int32_t *d_mat_tex = nullptr;
         float *d_tex_map = nullptr;
@@ -1192,6 +1239,7 @@ struct gzg_renderer {
         struct Films {
                 float *rgb, *sq, *w;
                 double *drgb, *dsq, *dw;
+                float *alb, *nrm;
         };
 
         // One wave: generate, bounces, then by w.mode accumulate + advance,
@@ -1256,7 +1304,7 @@ struct gzg_renderer {
                 } else if (film.drgb) {
                         k_accumulate_f64<<<grid, block, 0, st>>>(w, film.drgb, film.dsq, film.dw);
                 } else {
-                        k_accumulate<<<grid, block, 0, st>>>(w, film.rgb, film.sq, film.w);
+                        k_accumulate<<<grid, block, 0, st>>>(w, film.rgb, film.sq, film.w, film.alb, film.nrm);
                 }
                 k_advance_wave<<<1, 1, 0, st>>>(w);
                 return cudaGetLastError();
@@ -1276,7 +1324,7 @@ struct gzg_renderer {
         gzg_status render_f64(double *rgb, double *sq, double *wt, cudaStream_t st) {
                 w.mode = kRender;
                 k_set_wave_base<<<1, 1, 0, st>>>(w, 0ull);
-                const Films f{nullptr, nullptr, nullptr, rgb, sq, wt};
+                const Films f{nullptr, nullptr, nullptr, rgb, sq, wt, nullptr, nullptr};
                 for (uint64_t k = 0; k < wave_total(); ++k) {
                         gzg_status status = cuda_err(enqueue_wave(f, st), "wave launch");
                         if (status) return status;
@@ -1311,15 +1359,17 @@ struct gzg_renderer {
                 return status;
         }
 
-        gzg_status render(float *film_rgb, float *film_sq, float *film_w, cudaStream_t st) {
+        gzg_status render(float *film_rgb, float *film_sq, float *film_w, cudaStream_t st, float *film_alb = nullptr,
+                          float *film_nrm = nullptr) {
                 const uint64_t waves = wave_total();
                 w.mode = kRender;
-                const Films film{film_rgb, film_sq, film_w, nullptr, nullptr, nullptr};
+                const Films film{film_rgb, film_sq, film_w, nullptr, nullptr, nullptr, film_alb, film_nrm};
                 k_set_wave_base<<<1, 1, 0, st>>>(w, 0ull);
                 if (opts.use_graph) {
-                        const void *key[6] = {film_rgb, film_sq, film_w, (const void *)(uintptr_t)w.capacity,
-                                              (const void *)(uintptr_t)w.sort_key, (const void *)(uintptr_t)w.total_paths};
-                        if (!graph || !std::equal(key, key + 6, graph_key)) {
+                        const void *key[8] = {film_rgb, film_sq, film_w, (const void *)(uintptr_t)w.capacity,
+                                              (const void *)(uintptr_t)w.sort_key, (const void *)(uintptr_t)w.total_paths,
+                                              film_alb, film_nrm};
+                        if (!graph || !std::equal(key, key + 8, graph_key)) {
                                 drop_graph();
                                 cudaStream_t cap;
                                 gzg_status status = cuda_err(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
@@ -1333,7 +1383,7 @@ struct gzg_renderer {
                                 }
                                 cudaStreamDestroy(cap);
                                 if (status) return status;
-                                std::copy(key, key + 6, graph_key);
+                                std::copy(key, key + 8, graph_key);
                         }
                         for (uint64_t k = 0; k < waves; ++k) {
                                 gzg_status status = cuda_err(cudaGraphLaunch(graph, st), "graph launch");
@@ -1515,6 +1565,7 @@ gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *pa
             (st = r->alloc(&w.sh_ray, 2 * C)) || (st = r->alloc(&w.sh_id, C)) || (st = r->alloc(&w.sh_contrib, C)) ||
             (st = r->alloc(&w.sh_occ, C)) || (st = r->alloc(&w.pr_ray, 2 * C)) || (st = r->alloc(&w.pr_id, C)) ||
             (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) ||
+            (st = r->alloc(&w.alb, C)) || (st = r->alloc(&w.nrm, C)) ||
             (st = r->alloc(&w.key_hist, 2 * keys)) || (st = r->alloc(&w.counts, kCountWords)) ||
             (st = r->alloc(&w.stats, kStatWords)))
                 return st;
@@ -1623,6 +1674,39 @@ GZG_API gzg_status gzg_renderer_autotune(gzg_renderer *r, gzg_batch_options *bes
         if (prev != r->device) cudaSetDevice(prev);
         if (!status) clear_error();
         return status;
+}
+
+GZG_API gzg_status gzg_renderer_set_film(gzg_renderer *r, float iso, float max_component) {
+        if (!r || !(iso > 0.0f) || !std::isfinite(iso) || !(max_component >= 0.0f) || !std::isfinite(max_component))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_set_film: bad arguments");
+        for (SceneConst &sc : r->consts) {
+                sc.film_scale = iso / 100.0f;
+                sc.max_component = max_component;
+        }
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        const gzg_status st = cuda_err(cudaMemcpy(const_cast<SceneConst *>(r->w.scenes), r->consts.data(),
+                                                  r->consts.size() * sizeof(SceneConst), cudaMemcpyHostToDevice),
+                                       "film settings");
+        if (prev != r->device) cudaSetDevice(prev);
+        if (st) return st;
+        r->drop_graph();
+        return clear_error();
+}
+
+GZG_API gzg_status gzg_renderer_render_aov(gzg_renderer *r, float *film_rgb, float *film_sq, float *film_w,
+                                           float *film_albedo, float *film_normal, void *stream) {
+        if (!r || !film_rgb || !film_w)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_renderer_render_aov: null argument");
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != r->device) cudaSetDevice(r->device);
+        const gzg_status st = r->render(film_rgb, film_sq, film_w, reinterpret_cast<cudaStream_t>(stream), film_albedo,
+                                        film_normal);
+        if (prev != r->device) cudaSetDevice(prev);
+        if (!st) clear_error();
+        return st;
 }
 
 GZG_API gzg_status gzg_renderer_set_textures(gzg_renderer *r, const gzg_texture_binding *bindings, int32_t count,

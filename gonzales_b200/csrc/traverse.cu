@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
 // 32-ray batch finishes.  Each iteration opens one node and tests its
 // triangles.  No atomics or per-launch state: the assignment is static.
 template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
-__global__ void __launch_bounds__(256) k_wide_persistent(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void *__restrict__ rays,
                                                          const float *__restrict__ tmaxs, int64_t n,
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
@@ -698,7 +698,9 @@ using TraceKernel = void (*)(DevScene, const void *, const float *, int64_t, voi
 // ray.
 cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const LaunchParams &p, const DevScene &s,
                                const void *rays, const float *tmax, int64_t n, void *out, cudaStream_t st) {
-        const int block = (p.block_size == 64 || p.block_size == 256) ? p.block_size : 128;
+        // The persistent kernel is compiled for blocks of at most 128 threads
+        // (measured faster for any-hit queries than a 256-thread bound).
+        const int block = (p.block_size == 64 || (p.block_size == 256 && !persistent)) ? p.block_size : 128;
         const int blocks_per_sm = p.blocks_per_sm;
         const size_t smem = (size_t)stack * block * sizeof(uint2);
         if (smem > 48 * 1024) {

@@ -392,6 +392,18 @@ GZG_API gzg_status gzg_renderer_render(gzg_renderer *renderer, float *film_rgb, 
 
 GZG_API gzg_status gzg_renderer_stats(const gzg_renderer *renderer, gzg_render_stats *stats);
 
+/* Film settings of Film.add (Core/Film.swift:107-119): each sample's light is
+ * scaled by iso / 100 (default iso 100) and, when max_component > 0, scaled
+ * down so its largest component is at most max_component. */
+GZG_API gzg_status gzg_renderer_set_film(gzg_renderer *renderer, float iso, float max_component);
+
+/* gzg_renderer_render plus the first-hit AOVs of Tile.render (Tile.swift:
+ * 157-205): film_albedo[3*W*H] += the first hit's BSDF albedo, film_normal
+ * [3*W*H] += its geometric normal (zero for camera rays that miss); either may
+ * be NULL.  The AOV images are the sums / film_w, like the beauty image. */
+GZG_API gzg_status gzg_renderer_render_aov(gzg_renderer *renderer, float *film_rgb, float *film_sq, float *film_w,
+                                           float *film_albedo, float *film_normal, void *stream);
+
 /* Sort of the extension queue before shading. */
 typedef enum gzg_sort_key {
         GZG_SORT_NONE = 0,

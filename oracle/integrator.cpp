@@ -397,6 +397,7 @@ bool hit_light(const Light &l, V3 o, V3 d, float *t) {
 
 struct PathResult {
         V3 L;
+        V3 albedo{0.0f, 0.0f, 0.0f}, normal{0.0f, 0.0f, 0.0f};  // first hit's BSDF albedo and normal (AOVs)
         uint64_t ext = 0, shadow = 0, probe = 0;
 };
 
@@ -432,6 +433,11 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 const V3 refl = is_light ? albedo_at(sc, sc.inst ? sc.inst->blas_materials[0] : sc.materials, 0, pos)
                                          : albedo_at(sc, is.mats, pr.material_index, pos);
                 const V3 f_val = mul(refl, 1.0f / kPi);
+                if (bounce == 0) {
+                        // surfaceEstimate (:341-344): state.albedo, state.firstNormal
+                        res.albedo = refl;
+                        res.normal = ng;
+                }
                 if (!is.frame_ok) break;
                 if (sc.lights.empty()) break;
                 const Frame &fr = is.fr;
@@ -582,7 +588,8 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                               const orc_material *materials, int64_t n_materials, int64_t n_prims,
                               const orc_render_instances *instances, const orc_env *env,
                               const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
-                              float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
+                              float *sum_sq, float *sum_w, float *sum_albedo, float *sum_normal, uint64_t *counters,
+                              int threads) {
         Scene sc;
         sc.inst = instances;
         sc.env = env;
@@ -627,6 +634,7 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
         for (const Light &l : sc.lights) sc.total_power = sc.total_power + l.power;
 
         const orc_render_params &P = *params;
+        const float film_scale = (P.iso > 0.0f ? P.iso : 100.0f) / 100.0f;
         const int W = P.width, H = P.height;
         const int sampler_spp = P.sampler_spp > 0 ? P.sampler_spp : P.spp;
         // camera basis (right-handed: +x right, +y up in the image)
@@ -649,6 +657,7 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                 if (py >= H) break;
                                 for (int px = 0; px < W; ++px) {
                                         float acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0}, accw = 0.0f;
+                                        float acca[3] = {0, 0, 0}, accn[3] = {0, 0, 0};
                                         for (int si = 0; si < P.spp; ++si) {
                                                 orc_zsobol smp;
                                                 orc_zsobol_init(&smp, sampler_spp, W, H, P.seed);
@@ -674,10 +683,21 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                                 cnt[4 * ti + 1] += pr.ext;
                                                 cnt[4 * ti + 2] += pr.shadow;
                                                 cnt[4 * ti + 3] += pr.probe;
-                                                const float lv[3] = {pr.L.x, pr.L.y, pr.L.z};
+                                                // Film.add (Film.swift:107-119): iso scaling, then the
+                                                // optional clamp of the largest component
+                                                V3 sl = mul(pr.L, film_scale);
+                                                if (P.max_component > 0.0f) {
+                                                        const float mv = max_value(sl);
+                                                        if (mv > P.max_component) sl = mul(sl, P.max_component / mv);
+                                                }
+                                                const float lv[3] = {sl.x, sl.y, sl.z};
+                                                const float av[3] = {pr.albedo.x, pr.albedo.y, pr.albedo.z};
+                                                const float nv[3] = {pr.normal.x, pr.normal.y, pr.normal.z};
                                                 for (int c = 0; c < 3; ++c) {
                                                         acc[c] += lv[c];
                                                         acc2[c] += lv[c] * lv[c];
+                                                        acca[c] += av[c];
+                                                        accn[c] += nv[c];
                                                 }
                                                 accw += w;
                                         }
@@ -685,6 +705,8 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                         for (int c = 0; c < 3; ++c) {
                                                 sum_rgb[3 * pix + c] += acc[c];
                                                 if (sum_sq) sum_sq[3 * pix + c] += acc2[c];
+                                                if (sum_albedo) sum_albedo[3 * pix + c] += acca[c];
+                                                if (sum_normal) sum_normal[3 * pix + c] += accn[c];
                                         }
                                         sum_w[pix] += accw;
                                 }
@@ -701,7 +723,7 @@ extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, cons
                            const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                            uint64_t *counters, int threads) {
         orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, nullptr,
-                      sum_rgb, sum_sq, sum_w, counters, threads);
+                      sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
 }
 
 extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
@@ -709,5 +731,5 @@ extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *pr
                                     const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
                                     float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
         orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, textures,
-                      sum_rgb, sum_sq, sum_w, counters, threads);
+                      sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
 }

@@ -99,6 +99,8 @@ typedef struct orc_render_params {
         float filter_radius, filter_sigma;
         int32_t first_sample;   /* sample indices [first_sample, first_sample + spp) of a sampler */
         int32_t sampler_spp;    /* of sampler_spp samples per pixel (0: spp) */
+        float iso;              /* film sensitivity: light scaled by iso / 100 (0: 100) */
+        float max_component;    /* clamp of a sample's largest component (0: none) */
 } orc_render_params;
 
 /* Renders the scene; per pixel (row-major) accumulates the film sums of the
@@ -141,8 +143,8 @@ typedef struct orc_render_instances orc_render_instances;
 void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
                    const orc_material *materials, int64_t n_materials, int64_t n_prims,
                    const orc_render_instances *instances, const orc_env *env, const orc_render_params *params,
-                   const orc_textures *textures, float *sum_rgb, float *sum_sq, float *sum_w, uint64_t *counters,
-                   int threads);
+                   const orc_textures *textures, float *sum_rgb, float *sum_sq, float *sum_w, float *sum_albedo,
+                   float *sum_normal, uint64_t *counters, int threads);
 
 /* PathState_C (mojo_kernel.h:36-44). */
 typedef struct orc_path_state {

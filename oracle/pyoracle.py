@@ -185,15 +185,15 @@ class RenderParams(C.Structure):
                 ("rr_min_bounce", C.c_int32), ("mis_corrected", C.c_int32), ("seed", C.c_int64),
                 ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
                 ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
-                ("sampler_spp", C.c_int32)]
+                ("sampler_spp", C.c_int32), ("iso", C.c_float), ("max_component", C.c_float)]
 
 
 def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
                   eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
-                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0):
+                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, iso=100.0, max_component=0.0):
     return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
                         (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
-                        first_sample, sampler_spp)
+                        first_sample, sampler_spp, iso, max_component)
 
 
 class _Textures(C.Structure):
@@ -267,7 +267,7 @@ class Environment:
                     marginal_integral=float(mi[0]))
 
 
-def render(hs, params, threads=0, textures=None, env=None, instances=None):
+def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=False):
     """Film sums of the oracle integrator: (sum_rgb (H,W,3), sum_sq (H,W,3),
     sum_w (H,W), counters {camera, extension, shadow, probe}).
 
@@ -276,12 +276,14 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None):
     (count x R x R x 3 float32) and emission_scale (float).
     env (optional): an Environment.
     instances (optional): dict with tlas_nodes, leaf_instance, instances
-    (INSTANCE_DTYPE) and blas (HostScene list); hs is then unused (None)."""
+    (INSTANCE_DTYPE) and blas (HostScene list); hs is then unused (None).
+    aovs: also return the albedo and normal sums (H,W,3) (Tile.swift:157-205)
+    after the counters."""
     L = lib()
     if not getattr(L, "_render_bound", False):
         L.orc_render_ex.restype = None
         L.orc_render_ex.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
-                                                       C.POINTER(RenderParams), C.c_void_p] + [C.c_void_p] * 4 + \
+                                                       C.POINTER(RenderParams), C.c_void_p] + [C.c_void_p] * 6 + \
             [C.c_int]
         L._render_bound = True
     keep = []
@@ -326,6 +328,8 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None):
     s2 = np.zeros((H, W, 3), np.float32)
     sw = np.zeros((H, W), np.float32)
     cnt = np.zeros(4, np.uint64)
+    alb = np.zeros((H, W, 3), np.float32)
+    nrm = np.zeros((H, W, 3), np.float32)
     if threads <= 0:
         threads = os.cpu_count() or 1
     tex = None
@@ -342,8 +346,12 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None):
     L.orc_render_ex(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr),
                     _p(mats), len(mats), len(hs.prims), C.byref(inst_struct) if inst_struct is not None else None,
                     env.handle if env is not None else None, C.byref(params),
-                    C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw), _p(cnt), threads)
-    return s, s2, sw, {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
+                    C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw),
+                    _p(alb) if aovs else None, _p(nrm) if aovs else None, _p(cnt), threads)
+    counters = {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
+    if aovs:
+        return s, s2, sw, counters, alb, nrm
+    return s, s2, sw, counters
 
 
 PATH_DTYPE = np.dtype({"names": ["ray", "throughput", "estimate", "albedo", "pcg_state", "pcg_inc", "active"],
