@@ -132,6 +132,7 @@ PROTOTYPES = {
     "gzg_scene_autotune": (ST, [VP, VP, I64, C.c_int32, C.POINTER(TraceOptions), C.POINTER(C.c_float), VP]),
     "gzg_scene_set_launch": (ST, [VP, C.c_int32, C.POINTER(TraceOptions)]),
     "gzg_scene_set_environment": (ST, [VP, VP, C.c_int32, C.c_int32, C.c_float]),
+    "gzg_scene_set_material_params": (ST, [VP, VP, I64]),
     "gzg_host_instance_bounds": (ST, [VP, I64, VP, I64, VP]),
     "gzg_instanced_scene_create": (ST, [VP, I64, VP, I64, VP, I64, VP, I64, C.POINTER(VP)]),
     "gzg_trace_closest_instanced_device": (ST, [VP, VP, I64, VP, VP, C.POINTER(TraceOptions), VP]),

@@ -49,6 +49,12 @@ class GpuAccelerator:
             C.addressof(meshes), len(host_scene.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
             F.ptr(host_scene.materials), len(host_scene.materials), C.byref(handle)))
         self.handle = handle
+        if getattr(host_scene, "has_extended_materials", False) and host_scene.material_params is not None:
+            try:
+                self.set_material_params(host_scene.material_params)
+            except Exception:
+                self.close()
+                raise
 
     # ------------------------------------------------------------ lifetime
     def close(self):
@@ -173,6 +179,13 @@ class GpuAccelerator:
         F.check(F.lib().gzg_render_image(self.handle, C.byref(params), F.ptr(rgb), F.ptr(sq), F.ptr(w),
                                          C.byref(stats)))
         return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
+
+    def set_material_params(self, params):
+        """Dielectric / coated-diffuse parameters (gzg_scene_set_material_params):
+        (n_materials, 4) float32 rows of eta, roughness u, roughness v,
+        thickness.  A HostScene with such materials sets them on upload."""
+        params = np.ascontiguousarray(params, np.float32).reshape(-1, 4)
+        F.check(F.lib().gzg_scene_set_material_params(self.handle, F.ptr(params), len(params)))
 
     def set_environment(self, rgb, scale=1.0):
         """Adds the environment light (gzg_scene_set_environment): rgb (H, W, 3)

@@ -753,6 +753,17 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 }
                 hsd.materials.insert(hsd.materials.end(), bs.materials.begin(), bs.materials.end());
         }
+        bool any_params = false;
+        for (int64_t b = 0; b < blas_count; ++b) any_params = any_params || !blas[b]->host_shading.mat_params.empty();
+        if (any_params) {
+                for (int64_t b = 0; b < blas_count; ++b) {
+                        const HostShading &bs = blas[b]->host_shading;
+                        if (bs.mat_params.empty())
+                                hsd.mat_params.insert(hsd.mat_params.end(), bs.materials.size() / 2, float4_{1, 0, 0, 0});
+                        else
+                                hsd.mat_params.insert(hsd.mat_params.end(), bs.mat_params.begin(), bs.mat_params.end());
+                }
+        }
         if (hsd.prims.size() >= 0x7FFFFFFFu)
                 return set_error(GZG_ERR_LIMIT, "gzg_instanced_scene_create: more than 2^31 bottom-level prims");
         std::vector<float4_> o2w((size_t)instance_count * 3);
@@ -806,6 +817,12 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 d.materials = f;
                 d.material_count = (int32_t)(hsd.materials.size() / 2);
         }
+        if (!hsd.mat_params.empty()) {
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.mat_params.data()), hsd.mat_params.size(),
+                                        &f, "material parameters")))
+                        return st;
+                d.mat_params = f;
+        }
         const int32_t *pb;
         if ((st = scene->upload(prim_base.data(), prim_base.size(), &pb, "prim bases"))) return st;
         d.blas_prim_base = pb;
@@ -822,6 +839,47 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
         scene->info.bvh2_depth = tlas_bvh2_depth;
         scene->info.wide_depth = tlas.depth + max_blas_depth + 2;
         *out_scene = scene.release();
+        return clear_error();
+}
+
+// Parameters of dielectric (type 3) and coated-diffuse (type 4) materials, one
+// record per material: eta, roughness u, roughness v, thickness (Material/
+// Dielectric.swift:3-14, Material/CoatedDiffuse.swift:23-58; roughness is
+// remapped to alpha = sqrt(roughness) when shading).  Once per flat scene,
+// before it enters a two-level scene or a batch.
+GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const float *params, int64_t count) {
+        if (!scene || !params || count <= 0)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_material_params: bad arguments");
+        if (scene->instanced)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "gzg_scene_set_material_params: set them on the bottom-level scenes");
+        HostShading &hs = scene->host_shading;
+        if (!hs.mat_params.empty())
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_material_params: already set");
+        if ((size_t)count != hs.materials.size() / 2)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "gzg_scene_set_material_params: count differs from the scene's material count");
+        std::vector<float4_> mp((size_t)count);
+        for (int64_t k = 0; k < count; ++k) {
+                const float *q = params + 4 * k;
+                const int type = (int)hs.materials[2 * k].w;
+                if (type == 3 || type == 4) {
+                        const bool ok = std::isfinite(q[0]) && q[0] > 0.0f && std::isfinite(q[1]) && q[1] >= 0.0f &&
+                                        std::isfinite(q[2]) && q[2] >= 0.0f && std::isfinite(q[3]) && q[3] >= 0.0f;
+                        if (!ok)
+                                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                                 "gzg_scene_set_material_params: eta must be > 0, roughness and "
+                                                 "thickness finite and >= 0");
+                }
+                mp[k] = float4_{q[0], q[1], q[2], q[3]};
+        }
+        DeviceGuard g(scene->device);
+        const float4 *f;
+        gzg_status st;
+        if ((st = scene->upload(reinterpret_cast<const float4 *>(mp.data()), mp.size(), &f, "material parameters")))
+                return st;
+        scene->dev.mat_params = f;
+        hs.mat_params = std::move(mp);
         return clear_error();
 }
 

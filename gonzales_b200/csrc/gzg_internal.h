@@ -59,6 +59,9 @@ struct HostShading {
         std::vector<float4_> pv0, pv1, pv2;  // triangles in prim order
         std::vector<gzg_prim_id> prims;
         std::vector<float4_> materials;      // 2 per material
+        // per material: eta, roughness u, roughness v, thickness (types 3, 4);
+        // empty when none were set
+        std::vector<float4_> mat_params;
         std::vector<float4_> lights;         // 4 per light
         std::vector<float> light_cdf;
         float light_total = 0.0f;

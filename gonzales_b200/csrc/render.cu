@@ -222,6 +222,8 @@ __device__ float gaussian(float x, float sigma) {
         return 1.0f / sqrtf(2.0f * kPi * sigma * sigma) * expf(-(x * x) / (2.0f * sigma * sigma));
 }
 
+#include "bsdf.cuh"
+
 // ------------------------------------------------------------ state
 
 // Per-scene constants of a batch.
@@ -667,7 +669,145 @@ __global__ void k_sort_scatter(Wave w, DevScene s, int cur) {
         w.order[pos] = i;
 }
 
+// The general BSDF step of dielectric and coated-diffuse materials
+// (surfaceEstimate, VolumePathIntegrator.swift:325-371, with the material's
+// BSDF in place of the diffuse closed forms): the light sample is evaluated
+// through the BSDF in the shading frame, reflection only in world space
+// (FramedBsdf.swift:22-34); the BSDF strategy and the continuation sample it
+// from three Z-Sobol dimensions each.  The path's specular flag (thr.w)
+// records whether the continuation came from a specular BSDF.
+__device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst &sc, uint32_t path, int bounce,
+                              int cur, const BMat &bm, const Surf &sf, V3 thr, V3 L, ZSobol &z) {
+        const V3 pos = sf.pos, ng = sf.ng, wo = sf.wo;
+        const Frame &fr = sf.fr;
+        bool alive = sf.frame_ok;
+        bool specular = false;
+        if (alive && sc.light_count > 0) {
+                const V3 wo_l = fr.to_local(wo);
+                float choose_pdf;
+                const int lo = choose_light(s, sc, zs_get1d(sc.zs, z), choose_pdf);
+                const bool chose_env = lo == sc.env_index;
+                const int li = sc.light_begin + lo;
+                float u0, u1;
+                zs_get2d(sc.zs, z, u0, u1);
+                float light_pdf = 0.0f, area = 0.0f;
+                V3 rad = v3(0, 0, 0), light_dir = v3(0, 0, 0), lp0, lp1, lp2, target;
+                if (chose_env) {
+                        V3 dv, r;
+                        const float pdf = env_sample(s, u0, u1, dv, r);
+                        target = pos + dv * 100.0f;
+                        if (!is_black(r) && !isinf(pdf)) {
+                                rad = r;
+                                light_dir = dv;
+                                light_pdf = pdf;
+                        }
+                } else {
+                        const float4 l0 = __ldg(s.lights + 4 * li), l1 = __ldg(s.lights + 4 * li + 1),
+                                     l2 = __ldg(s.lights + 4 * li + 2), le4 = __ldg(s.lights + 4 * li + 3);
+                        lp0 = v3(l0);
+                        lp1 = v3(l1);
+                        lp2 = v3(l2);
+                        area = l0.w;
+                        const float su0 = sqrtf(u0);
+                        const float lb0 = 1.0f - su0, lb1 = u1 * su0;
+                        target = lp0 * lb0 + lp1 * lb1 + lp2 * ((1.0f - lb0) - lb1);
+                        const V3 ln = normalize(cross(lp1 - lp0, lp2 - lp0));
+                        const V3 inc = normalize(target - pos);
+                        const V3 dl = pos - target;
+                        const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
+                        if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
+                                rad = v3(le4) * w.emission_scale;
+                                light_dir = inc;
+                                light_pdf = pdf;
+                        }
+                }
+                if (light_pdf != 0.0f) {
+                        const V3 wl = fr.to_local(light_dir);
+                        const bool reflect = dot(light_dir, ng) * dot(wo, ng) > 0.0f;
+                        const V3 f = reflect ? bmat_f(bm, wo_l, wl) : v3(0, 0, 0);
+                        const V3 light_est = mulv(f * fabsf(dot(light_dir, ng)), rad);
+                        if (!is_black(light_est)) {
+                                const float brdf_density = wo_l.z == 0.0f ? 0.0f : bmat_pdf(bm, wo_l, wl);
+                                const float light_w = power_heuristic(light_pdf, brdf_density);
+                                const V3 so = pos + (target - pos) * 0.0001f;
+                                const V3 sd = target - so;
+                                const V3 c = mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf));
+                                const uint32_t q = queue_slot(w.counts + kCountShadow);
+                                store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
+                                w.sh_id[q] = path;
+                                w.sh_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
+                        }
+                }
+                float v0, v1, v2;
+                zs_get3d(sc.zs, z, v0, v1, v2);
+                if (sc.mis_corrected || chose_env) {
+                        const BsdfS bs = bmat_sample(bm, wo_l, v0, v1, v2);
+                        const float pdf_b = bs.pdf;
+                        const V3 wi = fr.to_world(bs.wi);
+                        const V3 est = bs.f * fabsf(dot(wi, ng));
+                        if (!is_black(est) && pdf_b > 0.0f) {
+                                const V3 po = offset_origin(pos, ng, wi);
+                                float light_density = 0.0f;
+                                if (chose_env) {
+                                        light_density = env_pdf(s, wi);
+                                } else {
+                                        float tl, lu, lv;
+                                        const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f),
+                                                     b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
+                                                     c4 = make_float4(lp2.x, lp2.y, lp2.z, 0.0f);
+                                        if (watertight_test(po.x, po.y, po.z, wi.x, wi.y, wi.z, a4, b4, c4, kInf, tl, lu,
+                                                            lv)) {
+                                                const V3 hp = po + wi * tl;
+                                                const V3 dq = pos - hp;
+                                                const V3 lnn = normalize(cross(lp0 - lp2, lp1 - lp2));
+                                                const float dens = dot(dq, dq) / (fabsf(dot(lnn, neg(wi))) * area);
+                                                light_density = isinf(dens) ? 0.0f : dens;
+                                        }
+                                }
+                                const float bw = power_heuristic(pdf_b, light_density);
+                                if (bw > 0.0f) {
+                                        const V3 c = mulv(thr, est * (bw / pdf_b) * (1.0f / choose_pdf));
+                                        const uint32_t q = queue_slot(w.counts + kCountProbe);
+                                        store_ray(w.pr_ray, q, po, kInf, wi, sc.root);
+                                        w.pr_id[q] = path;
+                                        w.pr_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
+                                }
+                        }
+                }
+                zs_get3d(sc.zs, z, v0, v1, v2);
+                const BsdfS bs = bmat_sample(bm, wo_l, v0, v1, v2);
+                const float pdf_c = bs.pdf;
+                if (pdf_c == 0.0f || isnan(pdf_c)) {
+                        alive = false;
+                } else {
+                        specular = bmat_specular(bm);
+                        const V3 wi = fr.to_world(bs.wi);
+                        thr = mulv(thr, bs.f * (fabsf(dot(wi, ng)) / pdf_c));
+                        const V3 o = offset_origin(pos, ng, wi);
+                        const float mv = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+                        if (mv < 1.0f && bounce >= sc.rr_min) {
+                                const float qq = fmaxf(0.0f, 1.0f - mv);
+                                if (zs_get1d(sc.zs, z) < qq)
+                                        alive = false;
+                                else
+                                        thr = thr * (1.0f / (1.0f - qq));
+                        }
+                        if (alive && bounce + 1 < sc.max_depth) {
+                                const int nxt = cur ^ 1;
+                                const uint32_t q = queue_slot(w.counts + nxt);
+                                store_ray(w.q_ray[nxt], q, o, kInf, wi, sc.root);
+                                w.q_id[nxt][q] = path;
+                        }
+                }
+        }
+        w.thr[path] = make_float4(thr.x, thr.y, thr.z, specular ? 1.0f : 0.0f);
+        w.L[path] = make_float4(L.x, L.y, L.z, 0.0f);
+        w.zs_dim[path] = z.dim;
+}
+
 // shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
+// kGeneric: the scene has dielectric or coated-diffuse materials.
+template <bool kGeneric>
 __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const uint32_t n = w.counts[cur];
         const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -680,9 +820,10 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const V3 d = v3(rd);
         if (prim < 0) {
                 // shadeBounce on a miss (:375-387): the environment light on
-                // camera rays (no specular bounces in these scenes)
-                if (bounce == 0 && s.env_rgb) {
-                        const V3 thr = v3(w.thr[path]);
+                // camera rays and after specular bounces
+                const float4 t4 = w.thr[path];
+                if ((bounce == 0 || t4.w != 0.0f) && s.env_rgb) {
+                        const V3 thr = v3(t4);
                         const V3 le = env_radiance(s, d);
                         float4 L = w.L[path];
                         L.x += thr.x * le.x;
@@ -693,7 +834,9 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                 return;
         }
         const SceneConst &sc = w.scenes[w.scene[path]];
-        V3 thr = v3(w.thr[path]);
+        const float4 t4 = w.thr[path];
+        V3 thr = v3(t4);
+        const bool after_specular = t4.w != 0.0f;
         if (is_black(thr)) return;
         if (bounce >= sc.max_depth) return;
         Surf sf;
@@ -704,13 +847,31 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         prim_info(s, sf.gprim, type, mat_index);
         const bool is_light = type == 3;
         V3 L = v3(w.L[path]);
-        if (bounce == 0 && is_light && mat_index >= 0 && mat_index < s.material_count) {
+        if ((bounce == 0 || after_specular) && is_light && mat_index >= 0 && mat_index < s.material_count) {
                 const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
                 if (dot(ng, wo) > 0.0f) L = L + mulv(thr, le);
         }
         // Area-light hits scatter with the scene's material 0 (their interaction
         // keeps materialIndex 0, Core/SurfaceInteraction.swift:20).
         const int64_t mi = is_light ? (int64_t)sc.material_begin : mat_index;
+        if (kGeneric && s.mat_params && mi >= 0 && mi < s.material_count) {
+                const float4 m0 = __ldg(s.materials + 2 * mi);
+                const int mt = (int)m0.w;
+                if (mt == 3 || mt == 4) {
+                        const V3 base = v3(m0);
+                        if (bounce == 0) {
+                                const V3 a = mt == 3 ? v3(1.0f, 1.0f, 1.0f) : base;
+                                w.alb[path] = make_float4(a.x, a.y, a.z, 0.0f);
+                                w.nrm[path] = make_float4(ng.x, ng.y, ng.z, 0.0f);
+                        }
+                        const BMat bm = make_bmat(mt, base, __ldg(s.mat_params + mi));
+                        ZSobol z;
+                        z.morton = w.zs_morton[path];
+                        z.dim = w.zs_dim[path];
+                        shade_generic(w, s, sc, path, bounce, cur, bm, sf, thr, L, z);
+                        return;
+                }
+        }
         V3 refl = (mi >= 0 && mi < s.material_count) ? v3(__ldg(s.materials + 2 * mi)) : v3(0.5f, 0.5f, 0.5f);
         if (w.mat_tex && mi >= 0 && mi < s.material_count) {
                 const int t = __ldg(w.mat_tex + mi);
@@ -1279,7 +1440,10 @@ struct gzg_renderer {
                                 k_sort_scan<<<1, 1024, 0, st>>>(w);
                                 k_sort_scatter<<<grid, block, 0, st>>>(w, view, cur);
                         }
-                        k_shade<<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                        if (view.mat_params)
+                                k_shade<true><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                        else
+                                k_shade<false><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                         lpa.n_dev = w.counts + kCountShadow;
                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
@@ -1438,7 +1602,9 @@ gzg_status build_batch(gzg_renderer *r) {
                 r->view.per_ray_root = 0;
         } else {
                 std::vector<WideNode> nodes;
-                std::vector<float4_> v0, v1, v2, pv0, pv1, pv2, mats, lights;
+                std::vector<float4_> v0, v1, v2, pv0, pv1, pv2, mats, lights, mparams;
+                bool any_params = false;
+                for (size_t k = 0; k < n; ++k) any_params = any_params || !scene_host_shading(r->scenes[k]).mat_params.empty();
                 std::vector<gzg_prim_id> prims;
                 std::vector<float> cdf;
                 uint64_t steps = 0;
@@ -1470,6 +1636,12 @@ gzg_status build_batch(gzg_renderer *r) {
                                 prims.push_back(p);
                         }
                         mats.insert(mats.end(), hs.materials.begin(), hs.materials.end());
+                        if (any_params) {
+                                if (hs.mat_params.empty())
+                                        mparams.insert(mparams.end(), hs.materials.size() / 2, float4_{1, 0, 0, 0});
+                                else
+                                        mparams.insert(mparams.end(), hs.mat_params.begin(), hs.mat_params.end());
+                        }
                         lights.insert(lights.end(), hs.lights.begin(), hs.lights.end());
                         cdf.insert(cdf.end(), hs.light_cdf.begin(), hs.light_cdf.end());
                         SceneConst &sc = r->consts[k];
@@ -1493,6 +1665,7 @@ gzg_status build_batch(gzg_renderer *r) {
                     (st = r->upload(&d.materials, mats)) || (st = r->upload(&d.lights, lights)) ||
                     (st = r->upload(&d.light_cdf, cdf)))
                         return st;
+                if (any_params && (st = r->upload(&d.mat_params, mparams))) return st;
                 uint32_t *err = nullptr;
                 if ((st = r->alloc(&err, 1))) return st;
                 if ((st = cuda_err(cudaMemset(err, 0, 4), "batch error word"))) return st;

@@ -26,6 +26,9 @@ PRIM_AREA_LIGHT = 3
 MATERIAL_NONE = 0
 MATERIAL_DIFFUSE = 1
 MATERIAL_AREA_LIGHT = 2
+# renderer extensions (Material_C.type values the reference's plugin never sees)
+MATERIAL_DIELECTRIC = 3      # Material/Dielectric.swift
+MATERIAL_COATED_DIFFUSE = 4  # Material/CoatedDiffuse.swift
 
 
 @dataclass
@@ -77,6 +80,11 @@ class HostScene:
     nodes: np.ndarray      # BVH2_NODE_DTYPE
     materials: np.ndarray  # MATERIAL_DTYPE
     prim_order: np.ndarray  # k-th leaf prim = input prim prim_order[k]
+    material_params: np.ndarray = None  # (n_materials, 4) float32: eta, roughness u, v, thickness
+
+    @property
+    def has_extended_materials(self):
+        return bool(np.isin(self.materials["type"], (MATERIAL_DIELECTRIC, MATERIAL_COATED_DIFFUSE)).any())
 
     def mesh_structs(self):
         arr = (F.TriangleMeshC * max(len(self.meshes), 1))()
@@ -111,11 +119,19 @@ class SceneBuilder:
         self.meshes = []
         self._prims = []       # list of (mesh, first_tri, ntri, type, material or light)
         self._materials = []   # (type, albedo, emission)
+        self._material_params = []  # (eta, roughness u, roughness v, thickness)
         self._lights = []      # emission per area light
         self._geometric = 0
 
-    def add_material(self, albedo=(0.5, 0.5, 0.5)):
-        self._materials.append((MATERIAL_DIFFUSE, tuple(albedo), (0.0, 0.0, 0.0)))
+    def add_material(self, albedo=(0.5, 0.5, 0.5), kind="diffuse", eta=1.5, roughness=0.0, thickness=0.01):
+        """kind: "diffuse" (albedo), "dielectric" (eta, roughness; albedo
+        unused) or "coateddiffuse" (reflectance = albedo, coating eta and
+        roughness, clear layer thickness).  Roughness is remapped to alpha =
+        sqrt(roughness) as the reference's remaproughness default does."""
+        t = {"diffuse": MATERIAL_DIFFUSE, "dielectric": MATERIAL_DIELECTRIC,
+             "coateddiffuse": MATERIAL_COATED_DIFFUSE}[kind]
+        self._materials.append((t, tuple(albedo), (0.0, 0.0, 0.0)))
+        self._material_params.append((eta, roughness, roughness, thickness))
         return len(self._materials) - 1
 
     def add_mesh(self, points, triangles, material=0):
@@ -165,5 +181,8 @@ class SceneBuilder:
         # leave the padding bytes undefined).
         raw = prims.view(np.uint8).reshape(-1, F.PRIM_ID_DTYPE.itemsize)[order]
         sorted_prims = np.ascontiguousarray(raw).view(F.PRIM_ID_DTYPE).reshape(-1)
+        params = np.zeros((len(mats), 4), np.float32)
+        if self._material_params:
+            params[:n_surface] = np.asarray(self._material_params, np.float32)
         return HostScene(meshes=self.meshes, prims=sorted_prims, nodes=nodes, materials=mats,
-                         prim_order=order)
+                         prim_order=order, material_params=params)

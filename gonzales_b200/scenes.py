@@ -224,17 +224,29 @@ def random_instances(n, n_blas, seed, extent=20.0):
     return inst
 
 
-def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0, coloured=False):
+MIXED_KINDS = ("diffuse", "coateddiffuse", "dielectric")
+
+
+def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0, coloured=False,
+                    mixed=False):
     """Bottom-level scenes (one mesh each: tubes and spheres alternating) and
     instances; 2 * n_u * n_v triangles per mesh (50,000 at the defaults).
-    coloured: a seeded diffuse albedo in [0.1, 0.8]^3 per mesh (else 0.5)."""
+    coloured: a seeded diffuse albedo in [0.1, 0.8]^3 per mesh (else 0.5).
+    mixed: mesh k is diffuse, coated diffuse or dielectric (k mod 3), eta 1.5,
+    roughness uniform in [0.05, 0.5], coating thickness 0.01 (implies
+    coloured)."""
     rng = np.random.default_rng(seed + 101)
     blas = []
     for k in range(n_meshes):
         pts, tris = grid_mesh("tube" if k % 2 == 0 else "sphere", n_u, n_v, seed + k)
         sb = SceneBuilder()
-        albedo = rng.uniform(0.1, 0.8, 3) if coloured else (0.5, 0.5, 0.5)
-        sb.add_mesh(pts, tris, sb.add_material(albedo))
+        albedo = rng.uniform(0.1, 0.8, 3) if (coloured or mixed) else (0.5, 0.5, 0.5)
+        if mixed:
+            rough = float(rng.uniform(0.05, 0.5))
+            m = sb.add_material(albedo, kind=MIXED_KINDS[k % 3], eta=1.5, roughness=rough, thickness=0.01)
+        else:
+            m = sb.add_material(albedo)
+        sb.add_mesh(pts, tris, m)
         blas.append(sb.build())
     return blas, random_instances(n_instances, n_meshes, seed, extent)
 
@@ -324,6 +336,29 @@ def box_scene(seed=0xB0):
         sb.add_mesh(bp, bt, sb.add_material(rng.uniform(0.1, 0.8, 3)))
     # wound so cross(p1 - p0, p2 - p0) points down (-y): area lights emit on
     # the side their geometric normal faces
+    lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
+    sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
+    return sb
+
+
+def materials_box_scene(seed=0xB1):
+    """The box scene with the renderer's other materials: a coated-diffuse box
+    (roughness 0.2), a rough dielectric box (0.1), a smooth dielectric sphere
+    (specular) and a rough coated sphere (0.4), diffuse walls, ceiling light."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    _room(sb, rng)
+    bp, bt = _box(0.25, 0.4, (0.3, 0.125 + 1e-4, 0.35))
+    sb.add_mesh(bp, bt, sb.add_material(rng.uniform(0.1, 0.8, 3), kind="coateddiffuse", roughness=0.2,
+                                        thickness=0.01))
+    bp, bt = _box(0.3, 1.1, (0.7, 0.15 + 1e-4, 0.6))
+    sb.add_mesh(bp, bt, sb.add_material(kind="dielectric", eta=1.5, roughness=0.1))
+    sp, st = icosphere(3)
+    sb.add_mesh(sp * 0.12 + np.array([0.62, 0.5, 0.75]), st, sb.add_material(kind="dielectric", eta=1.33,
+                                                                               roughness=0.0))
+    sb.add_mesh(sp * 0.1 + np.array([0.3, 0.36, 0.4]), st,
+                sb.add_material(rng.uniform(0.1, 0.8, 3), kind="coateddiffuse", eta=1.5, roughness=0.4,
+                                thickness=0.05))
     lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
     sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
     return sb

@@ -338,6 +338,16 @@ GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const
 GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
                                              float scale);
 
+/* Parameters of the renderer's dielectric (Material_C.type 3,
+ * Material/Dielectric.swift) and coated-diffuse (type 4,
+ * Material/CoatedDiffuse.swift, diffuse base = albedo) materials: HOST
+ * params[count][4] = eta, roughness u, roughness v, layer thickness, one
+ * record per material of the flat scene (count = its material count; records
+ * of other types are ignored).  Roughness is remapped to alpha =
+ * sqrt(roughness).  Once per scene, before the scene enters a two-level scene,
+ * a batch or a renderer; without it types 3 and 4 shade as diffuse. */
+GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const float *params, int64_t count);
+
 /* Expands device hits into reference Intersection_C records on the device
  * (prim-id lookup; the miss record of kernel.mojo:362-364). */
 GZG_API gzg_status gzg_hits_to_intersections_device(gzg_scene *scene, const gzg_hit_d *hits,

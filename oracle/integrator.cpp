@@ -222,6 +222,7 @@ struct Scene {
         float escale = 1.0f;
         const orc_render_instances *inst = nullptr;
         const orc_env *env = nullptr;
+        const float *mat_params = nullptr;  // 4 per material (eta, roughness u, v, thickness)
 };
 
 // Emission times the scene's emission scale (1 without textures: exact).
@@ -316,6 +317,7 @@ struct Isect {
         bool frame_ok;
         const orc_prim_id *pr;
         const orc_material *mats;
+        int blas;  // bottom-level scene of an instance hit, -1 for a flat scene
 };
 
 bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
@@ -329,6 +331,7 @@ bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
                 is->frame_ok = make_frame(p0, p1, p2, is->ng, &is->fr);
                 is->pr = &sc.prims[h.prim];
                 is->mats = sc.materials;
+                is->blas = -1;
                 return true;
         }
         const orc_render_instances &I = *sc.inst;
@@ -347,6 +350,7 @@ bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
         if (is->frame_ok) is->fr = frame_from(xf_vector(o2w, s_o), is->ng);
         is->pr = &B.prims[h.prim];
         is->mats = I.blas_materials[b];
+        is->blas = b;
         return true;
 }
 
@@ -401,19 +405,166 @@ struct PathResult {
         uint64_t ext = 0, shadow = 0, probe = 0;
 };
 
+// The surface step for the non-diffuse materials (dielectric, coated
+// diffuse): surfaceEstimate (VolumePathIntegrator.swift:325-371) through the
+// FramedBsdf wrappers (Reflection/FramedBsdf.swift:16-83): light sample with
+// MIS, BSDF sample with MIS, continuation.  Updates L, thr, the next ray and
+// the specular flag; false ends the path.
+bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, const Isect &is, int bounce, V3 &L,
+                   V3 &thr, V3 &o, V3 &d, bool &specular, PathResult &res) {
+        const orc_render_params &P = *sc.p;
+        const V3 pos = is.pos, ng = is.ng, wo = is.wo;
+        const Frame &fr = is.fr;
+        const V3 wo_l = fr.to_local(wo);
+        auto f_local = [&](V3 a, V3 b) {
+                const float wa[3] = {a.x, a.y, a.z}, wb[3] = {b.x, b.y, b.z};
+                float f[3], pdf;
+                orc_bsdf_eval(&bp, wa, wb, f, &pdf);
+                return v3(f[0], f[1], f[2]);
+        };
+        auto pdf_local = [&](V3 a, V3 b) {
+                const float wa[3] = {a.x, a.y, a.z}, wb[3] = {b.x, b.y, b.z};
+                float f[3], pdf;
+                orc_bsdf_eval(&bp, wa, wb, f, &pdf);
+                return pdf;
+        };
+        auto sample_local = [&](const float u[3], V3 &f, V3 &wi, float &pdf) {
+                const float wa[3] = {wo_l.x, wo_l.y, wo_l.z};
+                float fo[3], wio[3];
+                orc_bsdf_sample(&bp, wa, u, fo, wio, &pdf);
+                f = v3(fo[0], fo[1], fo[2]);
+                wi = v3(wio[0], wio[1], wio[2]);
+        };
+        // evaluateDistributionFunction: reflection only (no BSDF here is
+        // transmissive in world space), times |cos| with the shading normal
+        auto f_world = [&](V3 wi) {
+                const bool reflect = dot(wi, ng) * dot(wo, ng) > 0.0f;
+                return reflect ? f_local(wo_l, fr.to_local(wi)) : v3(0, 0, 0);
+        };
+
+        float choose_pdf;
+        const int li = choose_light(sc, orc_zsobol_get1d(smp), &choose_pdf);
+        const Light &lt = sc.lights[li];
+        float u2[2];
+        orc_zsobol_get2d(smp, u2);
+        V3 light_est = v3(0, 0, 0), light_dir = v3(0, 0, 0);
+        float light_pdf = 0.0f;
+        if (lt.is_env) {
+                float dir[3], rgb[3];
+                const float pdf = orc_env_sample(sc.env, u2[0], u2[1], dir, rgb);
+                const V3 dv = v3(dir[0], dir[1], dir[2]), rad = v3(rgb[0], rgb[1], rgb[2]);
+                if (!is_black(rad) && !std::isinf(pdf)) {
+                        const V3 target = add(pos, mul(dv, 100.0f));
+                        const V3 so = add(pos, mul(sub(target, pos), 0.0001f));
+                        Hit sh = trace(sc, so, sub(target, so), 1.0f - 0.00001f);
+                        ++res.shadow;
+                        if (!sh.hit) {
+                                light_est = mulv(mul(f_world(dv), std::fabs(dot(dv, ng))), rad);
+                                light_dir = dv;
+                                light_pdf = pdf;
+                        }
+                }
+        } else {
+                const float su0 = std::sqrt(u2[0]);
+                const float lb0 = 1.0f - su0, lb1 = u2[1] * su0;
+                const V3 lp = add(add(mul(lt.p0, lb0), mul(lt.p1, lb1)), mul(lt.p2, (1.0f - lb0) - lb1));
+                const V3 ln = normalize(cross(sub(lt.p1, lt.p0), sub(lt.p2, lt.p0)));
+                const V3 inc = normalize(sub(lp, pos));
+                const V3 dl = sub(pos, lp);
+                const float pdf = (1.0f / lt.area) * (dot(dl, dl) / std::fabs(dot(ln, neg(inc))));
+                if (dot(ln, neg(inc)) > 0.0f && !std::isinf(pdf)) {
+                        const V3 so = add(pos, mul(sub(lp, pos), 0.0001f));
+                        Hit sh = trace(sc, so, sub(lp, so), 1.0f - 0.00001f);
+                        ++res.shadow;
+                        if (!sh.hit) {
+                                light_est = mulv(mul(f_world(inc), std::fabs(dot(inc, ng))), emitted(sc, lt.le));
+                                light_dir = inc;
+                                light_pdf = pdf;
+                        }
+                }
+        }
+        const float brdf_density = wo_l.z == 0.0f ? 0.0f : pdf_local(wo_l, fr.to_local(light_dir));
+        const float light_w = power_heuristic(light_pdf, brdf_density);
+        V3 contrib = light_pdf == 0.0f ? v3(0, 0, 0) : mul(mul(light_est, light_w), 1.0f / light_pdf);
+
+        float u3[3];
+        orc_zsobol_get3d(smp, u3);
+        {
+                V3 fs, wi_l;
+                float pdf_b;
+                sample_local(u3, fs, wi_l, pdf_b);
+                const V3 wi = fr.to_world(wi_l);
+                V3 est = mul(fs, std::fabs(dot(wi, ng)));
+                if ((P.mis_corrected || lt.is_env) && !is_black(est) && pdf_b > 0.0f) {
+                        const V3 po = offset_origin(pos, ng, wi);
+                        Hit ph = trace(sc, po, wi, kInfF);
+                        ++res.probe;
+                        V3 radiance = v3(0, 0, 0);
+                        Isect pi;
+                        if (ph.hit) {
+                                if (interaction(sc, ph, wi, &pi) && pi.pr->type == 3) {
+                                        const orc_material &lm = pi.mats[pi.pr->material_index];
+                                        if (dot(pi.ng, neg(wi)) > 0.0f)
+                                                radiance = emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]));
+                                }
+                        } else if (sc.env) {
+                                radiance = env_radiance(sc, wi);
+                        }
+                        est = mulv(est, radiance);
+                        float light_density = 0.0f;
+                        if (lt.is_env) {
+                                const float dd[3] = {wi.x, wi.y, wi.z};
+                                light_density = orc_env_pdf(sc.env, dd);
+                        } else {
+                                float tl;
+                                if (hit_light(lt, po, wi, &tl)) {
+                                        const V3 hp = add(po, mul(wi, tl));
+                                        const V3 dq = sub(pos, hp);
+                                        const V3 lnn = normalize(cross(sub(lt.p0, lt.p2), sub(lt.p1, lt.p2)));
+                                        const float dens = dot(dq, dq) / (std::fabs(dot(lnn, neg(wi))) * lt.area);
+                                        light_density = std::isinf(dens) ? 0.0f : dens;
+                                }
+                        }
+                        const float bw = power_heuristic(pdf_b, light_density);
+                        contrib = add(contrib, mul(mul(est, bw), 1.0f / pdf_b));
+                }
+        }
+        L = add(L, mulv(thr, mul(contrib, 1.0f / choose_pdf)));
+
+        // continuation: bsdf.sampleWorldSpace + throughputWeight(normal:)
+        orc_zsobol_get3d(smp, u3);
+        V3 fs, wi_l;
+        float pdf_c;
+        sample_local(u3, fs, wi_l, pdf_c);
+        if (pdf_c == 0.0f || std::isnan(pdf_c)) return false;
+        specular = orc_bsdf_is_specular(&bp) != 0;
+        const V3 wi = fr.to_world(wi_l);
+        thr = mulv(thr, mul(fs, std::fabs(dot(wi, ng)) / pdf_c));
+        o = offset_origin(pos, ng, wi);
+        d = wi;
+        const float mv = max_value(thr);
+        if (mv < 1.0f && bounce >= P.rr_min_bounce) {
+                const float q = std::max(0.0f, 1.0f - mv);
+                if (orc_zsobol_get1d(smp) < q) return false;
+                thr = mul(thr, 1.0f / (1.0f - q));
+        }
+        return true;
+}
+
 // One path: VolumePathIntegrator.bounces (:448-463) with shadeBounce (:373-430)
 // and surfaceEstimate (:325-371).
 PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
         const orc_render_params &P = *sc.p;
         PathResult res;
         V3 L = v3(0, 0, 0), thr = v3(1, 1, 1);
+        bool specular = false;  // state.specularBounce
         for (int bounce = 0; bounce <= P.max_depth; ++bounce) {
                 Hit h = trace(sc, o, d, kInfF);
                 ++res.ext;
                 if (!h.hit) {
                         // shadeBounce on a miss (:375-387): environment light on
                         // camera rays (no specular bounces in these scenes)
-                        if (bounce == 0 && sc.env) L = add(L, mulv(thr, env_radiance(sc, d)));
+                        if ((bounce == 0 || specular) && sc.env) L = add(L, mulv(thr, env_radiance(sc, d)));
                         break;
                 }
                 if (is_black(thr)) break;
@@ -423,13 +574,39 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 const V3 pos = is.pos, ng = is.ng, wo = is.wo;
                 const orc_prim_id &pr = *is.pr;
                 const bool is_light = pr.type == 3;
-                if (bounce == 0 && is_light) {
+                if ((bounce == 0 || specular) && is_light) {
                         const orc_material &lm = is.mats[pr.material_index];
                         if (dot(ng, wo) > 0.0f)
                                 L = add(L, mulv(thr, emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]))));
                 }
                 // Area lights have materialIndex 0 in their interaction
                 // (Core/SurfaceInteraction.swift:20): the scene's first material.
+                // The material: a dielectric or coated diffuse takes the general
+                // BSDF step; diffuse keeps its closed forms below.
+                {
+                        const orc_material *mset = is_light ? (sc.inst ? sc.inst->blas_materials[0] : sc.materials) : is.mats;
+                        const int64_t mi = is_light ? 0 : pr.material_index;
+                        const float *mp = nullptr;
+                        if (sc.inst) {
+                                const int b = is_light ? 0 : is.blas;
+                                if (sc.inst->blas_material_params && sc.inst->blas_material_params[b])
+                                        mp = sc.inst->blas_material_params[b] + 4 * mi;
+                        } else if (sc.mat_params) {
+                                mp = sc.mat_params + 4 * mi;
+                        }
+                        const orc_material &mm = mset[mi];
+                        if ((mm.type == 3 || mm.type == 4) && mp) {
+                                orc_bsdf_params bp{mm.type, {mm.albedo[0], mm.albedo[1], mm.albedo[2]}, mp[0], mp[1], mp[2], mp[3]};
+                                if (bounce == 0) {
+                                        res.albedo = mm.type == 3 ? v3(1, 1, 1) : v3(mm.albedo[0], mm.albedo[1], mm.albedo[2]);
+                                        res.normal = ng;
+                                }
+                                if (!is.frame_ok || sc.lights.empty()) break;
+                                if (!shade_generic(sc, smp, bp, is, bounce, L, thr, o, d, specular, res)) break;
+                                continue;
+                        }
+                }
+                specular = false;
                 const V3 refl = is_light ? albedo_at(sc, sc.inst ? sc.inst->blas_materials[0] : sc.materials, 0, pos)
                                          : albedo_at(sc, is.mats, pr.material_index, pos);
                 const V3 f_val = mul(refl, 1.0f / kPi);
@@ -586,13 +763,14 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
 
 extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
                               const orc_material *materials, int64_t n_materials, int64_t n_prims,
-                              const orc_render_instances *instances, const orc_env *env,
+                              const orc_render_instances *instances, const orc_env *env, const float *material_params,
                               const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
                               float *sum_sq, float *sum_w, float *sum_albedo, float *sum_normal, uint64_t *counters,
                               int threads) {
         Scene sc;
         sc.inst = instances;
         sc.env = env;
+        sc.mat_params = material_params;
         if (instances) n_prims = 0;  // instanced emitters are not lights (objects add none)
         sc.tex = textures;
         sc.escale = textures ? textures->emission_scale : 1.0f;
@@ -722,14 +900,14 @@ extern "C" void orc_render(const orc_node *nodes, const orc_prim_id *prims, cons
                            const orc_material *materials, int64_t n_materials, int64_t n_prims,
                            const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                            uint64_t *counters, int threads) {
-        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, nullptr,
-                      sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
+        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, nullptr, params,
+                      nullptr, sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
 }
 
 extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
                                     const orc_material *materials, int64_t n_materials, int64_t n_prims,
                                     const orc_render_params *params, const orc_textures *textures, float *sum_rgb,
                                     float *sum_sq, float *sum_w, uint64_t *counters, int threads) {
-        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, params, textures,
-                      sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
+        orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, nullptr, params,
+                      textures, sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
 }

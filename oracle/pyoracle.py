@@ -204,7 +204,7 @@ class _Textures(C.Structure):
 class _RenderInstances(C.Structure):
     _fields_ = [("tlas", C.c_void_p), ("leaf_instance", C.c_void_p), ("w2o", C.c_void_p), ("o2w", C.c_void_p),
                 ("blas_of", C.c_void_p), ("instance_count", C.c_int64), ("blas", C.c_void_p),
-                ("blas_materials", C.c_void_p), ("blas_count", C.c_int64)]
+                ("blas_materials", C.c_void_p), ("blas_count", C.c_int64), ("blas_material_params", C.c_void_p)]
 
 
 class Environment:
@@ -282,7 +282,7 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
     L = lib()
     if not getattr(L, "_render_bound", False):
         L.orc_render_ex.restype = None
-        L.orc_render_ex.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+        L.orc_render_ex.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                                        C.POINTER(RenderParams), C.c_void_p] + [C.c_void_p] * 6 + \
             [C.c_int]
         L._render_bound = True
@@ -292,6 +292,7 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
         blas_scenes = instances["blas"]
         blas = (_Blas * len(blas_scenes))()
         mat_ptrs = (C.c_void_p * len(blas_scenes))()
+        par_ptrs = (C.c_void_p * len(blas_scenes))()
         for i, b in enumerate(blas_scenes):
             marr = (_Mesh * max(len(b.meshes), 1))()
             for k, m in enumerate(b.meshes):
@@ -305,16 +306,20 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
             keep += [marr, nodes_b, prims_b, mats_b]
             blas[i] = _Blas(nodes_b.ctypes.data, prims_b.ctypes.data, C.addressof(marr))
             mat_ptrs[i] = mats_b.ctypes.data
+            if getattr(b, "material_params", None) is not None:
+                par_b = np.ascontiguousarray(b.material_params, np.float32)
+                keep.append(par_b)
+                par_ptrs[i] = par_b.ctypes.data
         inst = np.ascontiguousarray(instances["instances"])
         w2o = np.ascontiguousarray(inst["world_to_object"], np.float32)
         o2w = np.ascontiguousarray(inst["object_to_world"], np.float32)
         blas_of = np.ascontiguousarray(inst["blas"], np.int32)
         tlas = np.ascontiguousarray(instances["tlas_nodes"])
         leaf = np.ascontiguousarray(instances["leaf_instance"], np.int64)
-        keep += [blas, mat_ptrs, w2o, o2w, blas_of, tlas, leaf]
+        keep += [blas, mat_ptrs, par_ptrs, w2o, o2w, blas_of, tlas, leaf]
         inst_struct = _RenderInstances(tlas.ctypes.data, leaf.ctypes.data, w2o.ctypes.data, o2w.ctypes.data,
                                        blas_of.ctypes.data, len(inst), C.addressof(blas), C.addressof(mat_ptrs),
-                                       len(blas_scenes))
+                                       len(blas_scenes), C.addressof(par_ptrs))
         hs = blas_scenes[0]  # flat arrays unused
     arr = (_Mesh * max(len(hs.meshes), 1))()
     for i, m in enumerate(hs.meshes):
@@ -323,6 +328,10 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
         keep += [p4, vi]
         arr[i] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
     mats = np.ascontiguousarray(hs.materials)
+    mparams = None
+    if instances is None and getattr(hs, "material_params", None) is not None:
+        mparams = np.ascontiguousarray(hs.material_params, np.float32)
+        keep.append(mparams)
     W, H = params.width, params.height
     s = np.zeros((H, W, 3), np.float32)
     s2 = np.zeros((H, W, 3), np.float32)
@@ -345,7 +354,8 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
                         float(textures.get("emission_scale", 1.0)))
     L.orc_render_ex(_p(np.ascontiguousarray(hs.nodes)), _p(np.ascontiguousarray(hs.prims)), C.addressof(arr),
                     _p(mats), len(mats), len(hs.prims), C.byref(inst_struct) if inst_struct is not None else None,
-                    env.handle if env is not None else None, C.byref(params),
+                    env.handle if env is not None else None, _p(mparams) if mparams is not None else None,
+                    C.byref(params),
                     C.byref(tex) if tex is not None else None, _p(s), _p(s2), _p(sw),
                     _p(alb) if aovs else None, _p(nrm) if aovs else None, _p(cnt), threads)
     counters = {"camera": int(cnt[0]), "extension": int(cnt[1]), "shadow": int(cnt[2]), "probe": int(cnt[3])}
@@ -421,3 +431,58 @@ def traverse_instanced(tlas_nodes, leaf_instance, w2o, blas_of, blas_scenes, ray
     L.orc_traverse_instanced(_p(tlas_nodes), _p(leaf_instance), _p(w2o), _p(blas_of), C.addressof(blas), _p(rays6),
                              _p(tmax), n, _p(prim), _p(inst), _p(t), _p(u), _p(v), threads)
     return prim, inst, t, u, v
+
+
+class BsdfParams(C.Structure):
+    _fields_ = [("type", C.c_int32), ("reflectance", C.c_float * 3), ("eta", C.c_float), ("roughness_u", C.c_float),
+                ("roughness_v", C.c_float), ("thickness", C.c_float)]
+
+
+def bsdf_params(kind, reflectance=(0.5, 0.5, 0.5), eta=1.5, roughness=0.0, thickness=0.01):
+    """kind: 1 diffuse, 3 dielectric, 4 coated diffuse (Material_C.type values)."""
+    p = BsdfParams()
+    p.type = int(kind)
+    for c in range(3):
+        p.reflectance[c] = float(reflectance[c])
+    p.eta, p.roughness_u, p.roughness_v, p.thickness = float(eta), float(roughness), float(roughness), float(thickness)
+    return p
+
+
+def _bsdf_lib():
+    L = lib()
+    if not getattr(L, "_bsdf_bound", False):
+        L.orc_bsdf_eval.restype = None
+        L.orc_bsdf_eval.argtypes = [C.POINTER(BsdfParams)] + [C.c_void_p] * 4
+        L.orc_bsdf_sample.restype = C.c_int
+        L.orc_bsdf_sample.argtypes = [C.POINTER(BsdfParams)] + [C.c_void_p] * 5
+        L.orc_bsdf_is_specular.restype = C.c_int
+        L.orc_bsdf_is_specular.argtypes = [C.POINTER(BsdfParams)]
+        L._bsdf_bound = True
+    return L
+
+
+def bsdf_eval(p, wo, wi):
+    """(f rgb, pdf) of directions in the shading frame."""
+    L = _bsdf_lib()
+    a = np.ascontiguousarray(wo, np.float32)
+    b = np.ascontiguousarray(wi, np.float32)
+    f = np.zeros(3, np.float32)
+    pdf = np.zeros(1, np.float32)
+    L.orc_bsdf_eval(C.byref(p), _p(a), _p(b), _p(f), _p(pdf))
+    return f, float(pdf[0])
+
+
+def bsdf_sample(p, wo, u):
+    """(valid, f rgb, wi, pdf) for three uniform numbers u."""
+    L = _bsdf_lib()
+    a = np.ascontiguousarray(wo, np.float32)
+    uu = np.ascontiguousarray(u, np.float32)
+    f = np.zeros(3, np.float32)
+    wi = np.zeros(3, np.float32)
+    pdf = np.zeros(1, np.float32)
+    ok = L.orc_bsdf_sample(C.byref(p), _p(a), _p(uu), _p(f), _p(wi), _p(pdf))
+    return bool(ok), f, wi, float(pdf[0])
+
+
+def bsdf_is_specular(p):
+    return bool(_bsdf_lib().orc_bsdf_is_specular(C.byref(p)))
