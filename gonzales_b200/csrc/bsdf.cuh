@@ -187,7 +187,7 @@ struct BDiel {
         BTR d;
         float eta;
         __device__ bool specular() const { return eta == 1.0f || d.smooth(); }
-        __device__ float f(V3 wo, V3 wi) const {
+        __device__ __noinline__ float f(V3 wo, V3 wi) const {
                 if (specular()) return 0.0f;
                 const float co = wo.z, ci = wi.z;
                 const bool reflect = ci * co > 0.0f;
@@ -205,7 +205,7 @@ struct BDiel {
                 num = num / b_sq(etap);
                 return num / den;
         }
-        __device__ BsdfS sample(V3 wo, float u0, float u1, float u2, bool radiance) const {
+        __device__ __noinline__ BsdfS sample(V3 wo, float u0, float u1, float u2, bool radiance) const {
                 if (specular()) {
                         const float r = b_fresnel(wo.z, eta), t = 1.0f - r;
                         const float pr = r / (r + t), pt = t / (r + t);
@@ -240,7 +240,7 @@ struct BDiel {
                 if (radiance) fv = fv / b_sq(etap);
                 return bs_scalar(fv, wi, pdf);
         }
-        __device__ float pdf(V3 wo, V3 wi) const {
+        __device__ __noinline__ float pdf(V3 wo, V3 wi) const {
                 if (eta == 1.0f || d.smooth()) return 0.0f;
                 const float co = wo.z, ci = wi.z;
                 const bool reflect = ci * co > 0.0f;
@@ -286,7 +286,7 @@ struct BCoated {
         float thickness;
         int max_depth, nsamples;
 
-        __device__ V3 f(V3 wo, V3 wi) const {
+        __device__ __noinline__ V3 f(V3 wo, V3 wi) const {
                 V3 res = v3(0, 0, 0);
                 if (wo.z < 0.0f) {
                         wo = neg(wo);
@@ -377,7 +377,7 @@ struct BCoated {
 
         // As written, the walk ends after its first interface sample (the
         // transmission test runs after the walk direction was replaced).
-        __device__ BsdfS sample(V3 wo, float u0, float u1, float u2) const {
+        __device__ __noinline__ BsdfS sample(V3 wo, float u0, float u1, float u2) const {
                 bool flip = false;
                 if (wo.z < 0.0f) {
                         wo = neg(wo);
@@ -416,7 +416,7 @@ struct BCoated {
                 return bs_none();
         }
 
-        __device__ float pdf(V3 wo, V3 wi) const {
+        __device__ __noinline__ float pdf(V3 wo, V3 wi) const {
                 if (wo.z < 0.0f) {
                         wo = neg(wo);
                         wi = neg(wi);
@@ -488,17 +488,24 @@ __device__ BMat make_bmat(int type, V3 R, float4 p) {
         return m;
 }
 
+// Kind-specific dispatch (K = 3 dielectric, 4 coated diffuse).
+template <int K>
 __device__ __forceinline__ V3 bmat_f(const BMat &m, V3 wo, V3 wi) {
-        if (m.type == 3) {
+        if (K == 3) {
                 const float f = m.diel.f(wo, wi);
                 return v3(f, f, f);
         }
         return m.coated.f(wo, wi);
 }
+template <int K>
 __device__ __forceinline__ float bmat_pdf(const BMat &m, V3 wo, V3 wi) {
-        return m.type == 3 ? m.diel.pdf(wo, wi) : m.coated.pdf(wo, wi);
+        return K == 3 ? m.diel.pdf(wo, wi) : m.coated.pdf(wo, wi);
 }
+template <int K>
 __device__ __forceinline__ BsdfS bmat_sample(const BMat &m, V3 wo, float u0, float u1, float u2) {
-        return m.type == 3 ? m.diel.sample(wo, u0, u1, u2, true) : m.coated.sample(wo, u0, u1, u2);
+        return K == 3 ? m.diel.sample(wo, u0, u1, u2, true) : m.coated.sample(wo, u0, u1, u2);
 }
-__device__ __forceinline__ bool bmat_specular(const BMat &m) { return m.type == 3 && m.diel.specular(); }
+template <int K>
+__device__ __forceinline__ bool bmat_specular(const BMat &m) {
+        return K == 3 && m.diel.specular();
+}

@@ -246,7 +246,10 @@ struct SceneConst {
         ZSobolConfig zs;
 };
 
-enum { kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4, kCountWords = 8 };
+enum {
+        kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4,
+        kCountDielectric = 6, kCountCoated = 7, kCountWords = 8
+};
 enum { kStatCamera = 0, kStatExt = 1, kStatShadow = 2, kStatProbe = 3, kStatWaves = 4, kStatWords = 8 };
 enum SortKey { kSortNone = 0, kSortMaterial = 1, kSortScene = 2 };
 
@@ -284,6 +287,9 @@ struct Wave {
         int32_t key_count;
         uint32_t *key_hist;    // key_count counters, then key_count cursors
         uint32_t *order;       // sorted entry order, capacity
+        // shade queues of the general BSDFs: extension-queue entries that hit a
+        // dielectric (from the front) or a coated diffuse (from the back)
+        uint32_t *gen_q;
         uint32_t *counts;      // kCountWords words; wave base as 2 words at kCountWaveBase
         unsigned long long *stats;  // kStatWords
         // differentiable rendering (single-scene renderers)
@@ -676,6 +682,7 @@ __global__ void k_sort_scatter(Wave w, DevScene s, int cur) {
 // (FramedBsdf.swift:22-34); the BSDF strategy and the continuation sample it
 // from three Z-Sobol dimensions each.  The path's specular flag (thr.w)
 // records whether the continuation came from a specular BSDF.
+template <int K>
 __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst &sc, uint32_t path, int bounce,
                               int cur, const BMat &bm, const Surf &sf, V3 thr, V3 L, ZSobol &z) {
         const V3 pos = sf.pos, ng = sf.ng, wo = sf.wo;
@@ -724,10 +731,10 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                 if (light_pdf != 0.0f) {
                         const V3 wl = fr.to_local(light_dir);
                         const bool reflect = dot(light_dir, ng) * dot(wo, ng) > 0.0f;
-                        const V3 f = reflect ? bmat_f(bm, wo_l, wl) : v3(0, 0, 0);
+                        const V3 f = reflect ? bmat_f<K>(bm, wo_l, wl) : v3(0, 0, 0);
                         const V3 light_est = mulv(f * fabsf(dot(light_dir, ng)), rad);
                         if (!is_black(light_est)) {
-                                const float brdf_density = wo_l.z == 0.0f ? 0.0f : bmat_pdf(bm, wo_l, wl);
+                                const float brdf_density = wo_l.z == 0.0f ? 0.0f : bmat_pdf<K>(bm, wo_l, wl);
                                 const float light_w = power_heuristic(light_pdf, brdf_density);
                                 const V3 so = pos + (target - pos) * 0.0001f;
                                 const V3 sd = target - so;
@@ -741,7 +748,7 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                 float v0, v1, v2;
                 zs_get3d(sc.zs, z, v0, v1, v2);
                 if (sc.mis_corrected || chose_env) {
-                        const BsdfS bs = bmat_sample(bm, wo_l, v0, v1, v2);
+                        const BsdfS bs = bmat_sample<K>(bm, wo_l, v0, v1, v2);
                         const float pdf_b = bs.pdf;
                         const V3 wi = fr.to_world(bs.wi);
                         const V3 est = bs.f * fabsf(dot(wi, ng));
@@ -775,12 +782,12 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                         }
                 }
                 zs_get3d(sc.zs, z, v0, v1, v2);
-                const BsdfS bs = bmat_sample(bm, wo_l, v0, v1, v2);
+                const BsdfS bs = bmat_sample<K>(bm, wo_l, v0, v1, v2);
                 const float pdf_c = bs.pdf;
                 if (pdf_c == 0.0f || isnan(pdf_c)) {
                         alive = false;
                 } else {
-                        specular = bmat_specular(bm);
+                        specular = bmat_specular<K>(bm);
                         const V3 wi = fr.to_world(bs.wi);
                         thr = mulv(thr, bs.f * (fabsf(dot(wi, ng)) / pdf_c));
                         const V3 o = offset_origin(pos, ng, wi);
@@ -805,14 +812,26 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
         w.zs_dim[path] = z.dim;
 }
 
+enum ShadeKind { kShadeDiffuse = 0, kShadeSplit = 1, kShadeDielectric = 3, kShadeCoated = 4 };
+
 // shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
-// kGeneric: the scene has dielectric or coated-diffuse materials.
-template <bool kGeneric>
+// kShadeDiffuse: a scene without general BSDFs.  kShadeSplit: shades diffuse
+// hits and misses and queues dielectric and coated-diffuse hits on their own
+// shade queues, which kShadeDielectric and kShadeCoated launches then shade
+// (one material kind per kernel: coherent warps, one BSDF's code).
+template <int kKind>
 __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
-        const uint32_t n = w.counts[cur];
         const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-        if (slot >= n) return;
-        const uint32_t i = sorted ? w.order[slot] : slot;
+        uint32_t i;
+        if (kKind == kShadeDielectric || kKind == kShadeCoated) {
+                const uint32_t n = w.counts[kKind == kShadeDielectric ? kCountDielectric : kCountCoated];
+                if (slot >= n) return;
+                i = kKind == kShadeDielectric ? w.gen_q[slot] : w.gen_q[w.capacity - 1u - slot];
+        } else {
+                const uint32_t n = w.counts[cur];
+                if (slot >= n) return;
+                i = sorted ? w.order[slot] : slot;
+        }
         const uint32_t path = w.q_id[cur][i];
         const float4 hit = w.hits[i];
         const int prim = __float_as_int(hit.w);
@@ -854,24 +873,35 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         // Area-light hits scatter with the scene's material 0 (their interaction
         // keeps materialIndex 0, Core/SurfaceInteraction.swift:20).
         const int64_t mi = is_light ? (int64_t)sc.material_begin : mat_index;
-        if (kGeneric && s.mat_params && mi >= 0 && mi < s.material_count) {
+        if (kKind != kShadeDiffuse && s.mat_params && mi >= 0 && mi < s.material_count) {
                 const float4 m0 = __ldg(s.materials + 2 * mi);
                 const int mt = (int)m0.w;
-                if (mt == 3 || mt == 4) {
+                if (kKind == kShadeSplit && (mt == 3 || mt == 4)) {
+                        if (mt == 3) {
+                                const uint32_t q = queue_slot(w.counts + kCountDielectric);
+                                w.gen_q[q] = i;
+                        } else {
+                                const uint32_t q = queue_slot(w.counts + kCountCoated);
+                                w.gen_q[w.capacity - 1u - q] = i;
+                        }
+                        return;
+                }
+                if (kKind == kShadeDielectric || kKind == kShadeCoated) {
                         const V3 base = v3(m0);
                         if (bounce == 0) {
                                 const V3 a = mt == 3 ? v3(1.0f, 1.0f, 1.0f) : base;
                                 w.alb[path] = make_float4(a.x, a.y, a.z, 0.0f);
                                 w.nrm[path] = make_float4(ng.x, ng.y, ng.z, 0.0f);
                         }
-                        const BMat bm = make_bmat(mt, base, __ldg(s.mat_params + mi));
+                        const BMat bm = make_bmat(kKind, base, __ldg(s.mat_params + mi));
                         ZSobol z;
                         z.morton = w.zs_morton[path];
                         z.dim = w.zs_dim[path];
-                        shade_generic(w, s, sc, path, bounce, cur, bm, sf, thr, L, z);
+                        shade_generic<kKind>(w, s, sc, path, bounce, cur, bm, sf, thr, L, z);
                         return;
                 }
         }
+        if (kKind == kShadeDielectric || kKind == kShadeCoated) return;  // not queued here
         V3 refl = (mi >= 0 && mi < s.material_count) ? v3(__ldg(s.materials + 2 * mi)) : v3(0.5f, 0.5f, 0.5f);
         if (w.mat_tex && mi >= 0 && mi < s.material_count) {
                 const int t = __ldg(w.mat_tex + mi);
@@ -1100,6 +1130,8 @@ __global__ void k_clear_counts(Wave w, int next) {
         w.counts[next] = 0;
         w.counts[kCountShadow] = 0;
         w.counts[kCountProbe] = 0;
+        w.counts[kCountDielectric] = 0;
+        w.counts[kCountCoated] = 0;
 }
 
 // Film.add (Core/Film.swift:107-119): the sample's light scaled by iso / 100
@@ -1440,10 +1472,13 @@ struct gzg_renderer {
                                 k_sort_scan<<<1, 1024, 0, st>>>(w);
                                 k_sort_scatter<<<grid, block, 0, st>>>(w, view, cur);
                         }
-                        if (view.mat_params)
-                                k_shade<true><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
-                        else
-                                k_shade<false><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                        if (view.mat_params) {
+                                k_shade<kShadeSplit><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                                k_shade<kShadeDielectric><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                                k_shade<kShadeCoated><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                        } else {
+                                k_shade<kShadeDiffuse><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                        }
                         lpa.n_dev = w.counts + kCountShadow;
                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
@@ -1737,7 +1772,7 @@ gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *pa
             (st = r->alloc(&w.q_id[0], C)) || (st = r->alloc(&w.q_id[1], C)) || (st = r->alloc(&w.hits, C)) ||
             (st = r->alloc(&w.sh_ray, 2 * C)) || (st = r->alloc(&w.sh_id, C)) || (st = r->alloc(&w.sh_contrib, C)) ||
             (st = r->alloc(&w.sh_occ, C)) || (st = r->alloc(&w.pr_ray, 2 * C)) || (st = r->alloc(&w.pr_id, C)) ||
-            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) ||
+            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) || (st = r->alloc(&w.gen_q, C)) ||
             (st = r->alloc(&w.alb, C)) || (st = r->alloc(&w.nrm, C)) ||
             (st = r->alloc(&w.key_hist, 2 * keys)) || (st = r->alloc(&w.counts, kCountWords)) ||
             (st = r->alloc(&w.stats, kStatWords)))
