@@ -181,10 +181,11 @@ class GpuAccelerator:
         return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
 
     def set_material_params(self, params):
-        """Dielectric / coated-diffuse parameters (gzg_scene_set_material_params):
-        (n_materials, 4) float32 rows of eta, roughness u, roughness v,
-        thickness.  A HostScene with such materials sets them on upload."""
-        params = np.ascontiguousarray(params, np.float32).reshape(-1, 4)
+        """Parameters of the dielectric, coated-diffuse, conductor and
+        coated-conductor materials (gzg_scene_set_material_params):
+        (n_materials, 12) float32 gzg_material_params rows.  A HostScene with
+        such materials sets them on upload."""
+        params = np.ascontiguousarray(params, np.float32).reshape(-1, 12)
         F.check(F.lib().gzg_scene_set_material_params(self.handle, F.ptr(params), len(params)))
 
     def set_environment(self, rgb, scale=1.0):

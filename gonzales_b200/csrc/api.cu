@@ -759,7 +759,8 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 for (int64_t b = 0; b < blas_count; ++b) {
                         const HostShading &bs = blas[b]->host_shading;
                         if (bs.mat_params.empty())
-                                hsd.mat_params.insert(hsd.mat_params.end(), bs.materials.size() / 2, float4_{1, 0, 0, 0});
+                                hsd.mat_params.insert(hsd.mat_params.end(), 3 * (bs.materials.size() / 2),
+                                                      float4_{1, 0, 0, 0});
                         else
                                 hsd.mat_params.insert(hsd.mat_params.end(), bs.mat_params.begin(), bs.mat_params.end());
                 }
@@ -842,12 +843,14 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
         return clear_error();
 }
 
-// Parameters of dielectric (type 3) and coated-diffuse (type 4) materials, one
-// record per material: eta, roughness u, roughness v, thickness (Material/
-// Dielectric.swift:3-14, Material/CoatedDiffuse.swift:23-58; roughness is
-// remapped to alpha = sqrt(roughness) when shading).  Once per flat scene,
-// before it enters a two-level scene or a batch.
-GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const float *params, int64_t count) {
+// Parameters of the general materials (types 3 to 6), one gzg_material_params
+// record per material, kept on the device as 3 float4 (Material/
+// Dielectric.swift:3-14, Material/CoatedDiffuse.swift:23-58,
+// Material/Conductor.swift:3-22, Material/CoatedConductor.swift:35-88; the
+// remapping of roughness to alpha happens when shading).  Once per flat
+// scene, before it enters a two-level scene or a batch.
+GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const gzg_material_params *params,
+                                                 int64_t count) {
         if (!scene || !params || count <= 0)
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_material_params: bad arguments");
         if (scene->instanced)
@@ -859,19 +862,28 @@ GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const float *
         if ((size_t)count != hs.materials.size() / 2)
                 return set_error(GZG_ERR_INVALID_ARGUMENT,
                                  "gzg_scene_set_material_params: count differs from the scene's material count");
-        std::vector<float4_> mp((size_t)count);
+        static_assert(sizeof(gzg_material_params) == 48, "gzg_material_params is 3 x float4");
+        auto fin = [](float x) { return std::isfinite(x) && x >= 0.0f; };
+        std::vector<float4_> mp((size_t)count * 3);
         for (int64_t k = 0; k < count; ++k) {
-                const float *q = params + 4 * k;
+                const gzg_material_params &q = params[k];
                 const int type = (int)hs.materials[2 * k].w;
-                if (type == 3 || type == 4) {
-                        const bool ok = std::isfinite(q[0]) && q[0] > 0.0f && std::isfinite(q[1]) && q[1] >= 0.0f &&
-                                        std::isfinite(q[2]) && q[2] >= 0.0f && std::isfinite(q[3]) && q[3] >= 0.0f;
-                        if (!ok)
-                                return set_error(GZG_ERR_INVALID_ARGUMENT,
-                                                 "gzg_scene_set_material_params: eta must be > 0, roughness and "
-                                                 "thickness finite and >= 0");
-                }
-                mp[k] = float4_{q[0], q[1], q[2], q[3]};
+                bool ok = true;
+                if (type == 3 || type == 4 || type == 6)
+                        ok = ok && fin(q.eta) && q.eta > 0.0f && fin(q.roughness_u) && fin(q.roughness_v) &&
+                             fin(q.thickness);
+                if (type == 5 || type == 6)
+                        for (int c = 0; c < 3; ++c)
+                                ok = ok && fin(q.conductor_eta[c]) && fin(q.conductor_k[c]) &&
+                                     fin(q.conductor_roughness_u) && fin(q.conductor_roughness_v);
+                if (!ok)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         "gzg_scene_set_material_params: eta must be > 0; roughness, thickness and "
+                                         "conductor eta / k finite and >= 0");
+                mp[3 * k] = float4_{q.eta, q.roughness_u, q.roughness_v, q.thickness};
+                mp[3 * k + 1] = float4_{q.conductor_eta[0], q.conductor_eta[1], q.conductor_eta[2],
+                                        q.conductor_roughness_u};
+                mp[3 * k + 2] = float4_{q.conductor_k[0], q.conductor_k[1], q.conductor_k[2], q.conductor_roughness_v};
         }
         DeviceGuard g(scene->device);
         const float4 *f;

@@ -1,6 +1,7 @@
-// bsdf.cuh - dielectric and coated-diffuse BSDFs on the device, in the
-// shading frame (z = normal).  Included by render.cu inside its anonymous
-// namespace, after its vector helpers (V3, dot, normalize, ...).
+// bsdf.cuh - dielectric, coated-diffuse, conductor and coated-conductor
+// BSDFs on the device, in the shading frame (z = normal).  Included by
+// render.cu inside its anonymous namespace, after its vector helpers (V3,
+// dot, normalize, ...).
 //
 //   Trowbridge-Reitz D, Lambda, G, visible-normal sample
 //       Reflection/TrowbridgeReitzDistribution.swift, Reflection/MicrofacetDistribution.swift
@@ -8,6 +9,9 @@
 //   DielectricBsdf                    Bsdf/DielectricBsdf.swift
 //   LayeredBsdf<Dielectric, Diffuse> with a clear layer (coated diffuse)
 //                                     Bsdf/LayeredBsdf.swift, Bsdf/CoatedDiffuseBsdf.swift
+//   conductor Fresnel, MicrofacetReflection, coated conductor
+//                                     Reflection/FresnelConductor.swift, Bsdf/MicrofacetReflection.swift,
+//                                     Bsdf/CoatedConductorBsdf.swift
 //
 // The layered walks draw from a PCG32 stream seeded by a hash of the call's
 // direction arguments (the reference seeds a RandomSampler from the system).
@@ -268,6 +272,58 @@ struct BDiff {
                 if (wo.z < 0.0f) wi.z = -wi.z;
                 return BsdfS{f(), wi, pdf(wo, wi)};
         }
+        // as a layer's base: the value ignores the directions
+        __device__ V3 f(V3, V3) const { return f(); }
+};
+
+// ---- conductor Fresnel term for one channel, etaI = 1 (Reflection/FresnelConductor.swift)
+__device__ float b_fresnel_conductor(float cos_theta, float eta, float etak) {
+        const float c = b_clamp(cos_theta, -1.0f, 1.0f);
+        const float cos2 = c * c;
+        const float sin2 = 1.0f - cos2;
+        const float eta2 = eta * eta;
+        const float etak2 = etak * etak;
+        const float t0 = eta2 - etak2 - sin2;
+        const float a2pb2 = sqrtf(t0 * t0 + 4.0f * eta2 * etak2);
+        const float t1 = a2pb2 + cos2;
+        const float a = sqrtf(0.5f * (a2pb2 + t0));
+        const float t2 = 2.0f * c * a;
+        const float rs = (t1 - t2) / (t1 + t2);
+        const float t3 = cos2 * a2pb2 + sin2 * sin2;
+        const float t4 = t2 * sin2;
+        const float rp = rs * (t3 - t4) / (t3 + t4);
+        return 0.5f * (rp + rs);
+}
+
+// ---- MicrofacetReflection with a conductor Fresnel term (Bsdf/MicrofacetReflection.swift)
+struct BCond {
+        BTR d;
+        V3 R, eta, k;
+        __device__ __noinline__ V3 f(V3 wo, V3 wi) const {
+                const float co = fabsf(wo.z), ci = fabsf(wi.z);
+                V3 h = wo + wi;
+                if (co == 0.0f || ci == 0.0f) return v3(0, 0, 0);
+                if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return v3(0, 0, 0);
+                h = b_norm0(h);
+                const float cf = fabsf(dot(wi, h));
+                const float area = d.D(h);
+                const float vis = d.G(wo, wi);
+                const float den = 4.0f * ci * co;
+                return v3(R.x * area * vis * b_fresnel_conductor(cf, eta.x, k.x) / den,
+                          R.y * area * vis * b_fresnel_conductor(cf, eta.y, k.y) / den,
+                          R.z * area * vis * b_fresnel_conductor(cf, eta.z, k.z) / den);
+        }
+        __device__ float pdf(V3 wo, V3 wi) const {
+                if (!b_same(wo, wi)) return 0.0f;
+                const V3 h = b_norm0(wo + wi);
+                return d.pdf(wo, h) / (4.0f * dot(wo, h));
+        }
+        __device__ __noinline__ BsdfS sample(V3 wo, float u0, float u1) const {
+                if (wo.z == 0.0f) return bs_none();
+                const V3 h = d.sample_wh(wo, u0, u1);
+                const V3 wi = neg(wo) + h * (2.0f * dot(wo, h));
+                return BsdfS{f(wo, wi), wi, pdf(wo, wi)};
+        }
 };
 
 __device__ __forceinline__ float b_tr(float dz, V3 w) {
@@ -279,10 +335,12 @@ __device__ __forceinline__ float b_ph(float f, float g) {
         return (f == 0.0f || g == 0.0f) ? 0.0f : (f * f) / (f * f + g * g);
 }
 
-// ---- LayeredBsdf<Dielectric, Diffuse>, clear layer, two-sided
-struct BCoated {
+// ---- LayeredBsdf<Dielectric, Bottom>, clear layer, two-sided: coated
+// diffuse (Bottom = BDiff) and coated conductor (Bottom = BCond)
+template <class Bottom>
+struct BLayered {
         BDiel top;
-        BDiff bottom;
+        Bottom bottom;
         float thickness;
         int max_depth, nsamples;
 
@@ -332,7 +390,7 @@ struct BCoated {
                                         V3 ne;
                                         float ne_pdf;
                                         if (z == 0.0f) {
-                                                ne = bottom.f();
+                                                ne = bottom.f(neg(w), neg(wis.wi));
                                                 ne_pdf = bottom.pdf(neg(w), neg(wis.wi));
                                         } else {
                                                 const float ft = top.f(neg(w), neg(wis.wi));
@@ -356,7 +414,7 @@ struct BCoated {
                                         V3 fe;
                                         float fe_pdf;
                                         if (exit_z == 0.0f) {
-                                                fe = bottom.f();
+                                                fe = bottom.f(neg(w), wi);
                                                 fe_pdf = bottom.pdf(neg(w), wi);
                                         } else {
                                                 const float ft = top.f(neg(w), wi);
@@ -459,51 +517,87 @@ struct BCoated {
         }
 };
 
-// A material's BSDF: type 3 dielectric, 4 coated diffuse (params: eta,
-// roughness u, v, thickness; roughness remapped to alpha = sqrt, the
-// coating's alpha at least 0.001: Material/Dielectric.swift:3-14,
-// Material/CoatedDiffuse.swift:23-58).
+// A material's BSDF: type 3 dielectric, 4 coated diffuse, 5 conductor, 6
+// coated conductor; p = the material's 3 parameter records (eta, roughness
+// u, v, thickness; conductor eta, roughness u; conductor k, roughness v).
+// Dielectric and coating roughness is remapped to alpha = sqrt (a coating's
+// alpha at least 0.001); a conductor's roughness is its alpha (at least
+// 1e-3), a coated conductor's is remapped (at least 0.001)
+// (Material/Dielectric.swift:3-14, Material/CoatedDiffuse.swift:23-58,
+// Material/Conductor.swift:3-22, Material/CoatedConductor.swift:35-88).
 struct BMat {
-        int type;
         BDiel diel;
-        BCoated coated;
+        BLayered<BDiff> coated;
+        BCond cond;
+        BLayered<BCond> coated_cond;
 };
 
-__device__ BMat make_bmat(int type, V3 R, float4 p) {
+template <int K>
+__device__ BMat make_bmat(V3 R, float4 p0, float4 p1, float4 p2) {
         BMat m;
-        m.type = type;
-        float ax = sqrtf(p.y), ay = sqrtf(p.z);
-        if (type == 4) {
+        float ax = sqrtf(p0.y), ay = sqrtf(p0.z);
+        if (K == 4 || K == 6) {
                 ax = fmaxf(ax, 0.001f);
                 ay = fmaxf(ay, 0.001f);
         }
         m.diel.d.ax = ax;
         m.diel.d.ay = ay;
-        m.diel.eta = p.x;
-        m.coated.top = m.diel;
-        m.coated.bottom.R = R;
-        m.coated.thickness = fmaxf(p.w, 1.17549435e-38f);
-        m.coated.max_depth = 10;
-        m.coated.nsamples = 1;
+        m.diel.eta = p0.x;
+        const float thick = fmaxf(p0.w, 1.17549435e-38f);
+        if (K == 4) {
+                m.coated.top = m.diel;
+                m.coated.bottom.R = R;
+                m.coated.thickness = thick;
+                m.coated.max_depth = 10;
+                m.coated.nsamples = 1;
+        }
+        if (K == 5 || K == 6) {
+                if (K == 6) {
+                        m.cond.d.ax = fmaxf(sqrtf(p1.w), 0.001f);
+                        m.cond.d.ay = fmaxf(sqrtf(p2.w), 0.001f);
+                        m.cond.R = R;
+                } else {
+                        m.cond.d.ax = fmaxf(p1.w, 1e-3f);
+                        m.cond.d.ay = fmaxf(p2.w, 1e-3f);
+                        m.cond.R = v3(1.0f, 1.0f, 1.0f);
+                }
+                m.cond.eta = v3(p1.x, p1.y, p1.z);
+                m.cond.k = v3(p2.x, p2.y, p2.z);
+        }
+        if (K == 6) {
+                m.coated_cond.top = m.diel;
+                m.coated_cond.bottom = m.cond;
+                m.coated_cond.thickness = thick;
+                m.coated_cond.max_depth = 10;
+                m.coated_cond.nsamples = 1;
+        }
         return m;
 }
 
-// Kind-specific dispatch (K = 3 dielectric, 4 coated diffuse).
+// Kind-specific dispatch (K = material type).
 template <int K>
 __device__ __forceinline__ V3 bmat_f(const BMat &m, V3 wo, V3 wi) {
         if (K == 3) {
                 const float f = m.diel.f(wo, wi);
                 return v3(f, f, f);
         }
-        return m.coated.f(wo, wi);
+        if (K == 4) return m.coated.f(wo, wi);
+        if (K == 5) return m.cond.f(wo, wi);
+        return m.coated_cond.f(wo, wi);
 }
 template <int K>
 __device__ __forceinline__ float bmat_pdf(const BMat &m, V3 wo, V3 wi) {
-        return K == 3 ? m.diel.pdf(wo, wi) : m.coated.pdf(wo, wi);
+        if (K == 3) return m.diel.pdf(wo, wi);
+        if (K == 4) return m.coated.pdf(wo, wi);
+        if (K == 5) return m.cond.pdf(wo, wi);
+        return m.coated_cond.pdf(wo, wi);
 }
 template <int K>
 __device__ __forceinline__ BsdfS bmat_sample(const BMat &m, V3 wo, float u0, float u1, float u2) {
-        return K == 3 ? m.diel.sample(wo, u0, u1, u2, true) : m.coated.sample(wo, u0, u1, u2);
+        if (K == 3) return m.diel.sample(wo, u0, u1, u2, true);
+        if (K == 4) return m.coated.sample(wo, u0, u1, u2);
+        if (K == 5) return m.cond.sample(wo, u0, u1);
+        return m.coated_cond.sample(wo, u0, u1, u2);
 }
 template <int K>
 __device__ __forceinline__ bool bmat_specular(const BMat &m) {

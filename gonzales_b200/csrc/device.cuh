@@ -30,7 +30,7 @@ struct DevScene {
         const uint32_t *n_dev;         // optional device-side ray count (overrides the launch's n)
         // shading data (path integrator)
         const float4 *materials;       // 2 x float4 per material: albedo + type, emission
-        const float4 *mat_params;      // per material: eta, roughness u, v, thickness (null: none)
+        const float4 *mat_params;      // per material 3 x float4 (gzg_material_params; null: none)
         const float4 *lights;          // 4 x float4 per area light: p0 + area, p1 + power, p2, emission
         const float *light_cdf;        // running sum of light powers
         int32_t material_count;

@@ -59,7 +59,8 @@ struct HostShading {
         std::vector<float4_> pv0, pv1, pv2;  // triangles in prim order
         std::vector<gzg_prim_id> prims;
         std::vector<float4_> materials;      // 2 per material
-        // per material: eta, roughness u, roughness v, thickness (types 3, 4);
+        // per material 3 records (gzg_material_params: eta, roughness u, v,
+        // thickness; conductor eta, roughness u; conductor k, roughness v);
         // empty when none were set
         std::vector<float4_> mat_params;
         std::vector<float4_> lights;         // 4 per light

@@ -248,7 +248,7 @@ struct SceneConst {
 
 enum {
         kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4,
-        kCountDielectric = 6, kCountCoated = 7, kCountWords = 8
+        kCountDielectric = 6, kCountCoated = 7, kCountConductor = 8, kCountCoatedConductor = 9, kCountWords = 12
 };
 enum { kStatCamera = 0, kStatExt = 1, kStatShadow = 2, kStatProbe = 3, kStatWaves = 4, kStatWords = 8 };
 enum SortKey { kSortNone = 0, kSortMaterial = 1, kSortScene = 2 };
@@ -287,8 +287,10 @@ struct Wave {
         int32_t key_count;
         uint32_t *key_hist;    // key_count counters, then key_count cursors
         uint32_t *order;       // sorted entry order, capacity
-        // shade queues of the general BSDFs: extension-queue entries that hit a
-        // dielectric (from the front) or a coated diffuse (from the back)
+        // shade queues of the general BSDFs (2 x capacity): extension-queue
+        // entries that hit a dielectric (from the front of the first half), a
+        // coated diffuse (from its back), a conductor (from the front of the
+        // second half) or a coated conductor (from its back)
         uint32_t *gen_q;
         uint32_t *counts;      // kCountWords words; wave base as 2 words at kCountWaveBase
         unsigned long long *stats;  // kStatWords
@@ -313,14 +315,18 @@ struct Wave {
 };
 
 // Appends to a queue with one atomic per converged group of lanes.
+// Lanes that reach this together may append to different queues (the shade
+// queues of several material kinds from one call site): each group of lanes
+// with the same counter takes one atomic and numbers its lanes in order.
 __device__ __forceinline__ uint32_t queue_slot(uint32_t *count) {
         const unsigned mask = __activemask();
+        const unsigned peers = __match_any_sync(mask, reinterpret_cast<unsigned long long>(count));
         const unsigned lane = threadIdx.x & 31u;
-        const int leader = __ffs(mask) - 1;
+        const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
+        if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(peers));
         base = __shfl_sync(mask, base, leader);
-        return base + __popc(mask & ((1u << lane) - 1u));
+        return base + __popc(peers & ((1u << lane) - 1u));
 }
 
 // A queued ray; the spare lane carries the traversal root of the path's scene.
@@ -812,21 +818,32 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
         w.zs_dim[path] = z.dim;
 }
 
-enum ShadeKind { kShadeDiffuse = 0, kShadeSplit = 1, kShadeDielectric = 3, kShadeCoated = 4 };
+enum ShadeKind {
+        kShadeDiffuse = 0, kShadeSplit = 1, kShadeDielectric = 3, kShadeCoated = 4, kShadeConductor = 5,
+        kShadeCoatedConductor = 6
+};
+
+// The shade queue of a general material kind: its counter and the gen_q
+// position of its entry `slot` (two kinds share each half, from either end).
+__device__ __forceinline__ uint32_t gen_counter(int kind) { return (uint32_t)(kCountDielectric + kind - 3); }
+__device__ __forceinline__ uint32_t gen_pos(const Wave &w, int kind, uint32_t slot) {
+        const uint32_t half = kind >= 5 ? w.capacity : 0u;
+        return (kind == 3 || kind == 5) ? half + slot : half + w.capacity - 1u - slot;
+}
 
 // shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
 // kShadeDiffuse: a scene without general BSDFs.  kShadeSplit: shades diffuse
-// hits and misses and queues dielectric and coated-diffuse hits on their own
-// shade queues, which kShadeDielectric and kShadeCoated launches then shade
-// (one material kind per kernel: coherent warps, one BSDF's code).
+// hits and misses and queues hits on the general materials on their kind's
+// shade queue, which the kShadeDielectric .. kShadeCoatedConductor launches
+// then shade (one material kind per kernel: coherent warps, one BSDF's code).
 template <int kKind>
 __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
         uint32_t i;
-        if (kKind == kShadeDielectric || kKind == kShadeCoated) {
-                const uint32_t n = w.counts[kKind == kShadeDielectric ? kCountDielectric : kCountCoated];
+        if (kKind >= kShadeDielectric) {
+                const uint32_t n = w.counts[gen_counter(kKind)];
                 if (slot >= n) return;
-                i = kKind == kShadeDielectric ? w.gen_q[slot] : w.gen_q[w.capacity - 1u - slot];
+                i = w.gen_q[gen_pos(w, kKind, slot)];
         } else {
                 const uint32_t n = w.counts[cur];
                 if (slot >= n) return;
@@ -876,24 +893,22 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         if (kKind != kShadeDiffuse && s.mat_params && mi >= 0 && mi < s.material_count) {
                 const float4 m0 = __ldg(s.materials + 2 * mi);
                 const int mt = (int)m0.w;
-                if (kKind == kShadeSplit && (mt == 3 || mt == 4)) {
-                        if (mt == 3) {
-                                const uint32_t q = queue_slot(w.counts + kCountDielectric);
-                                w.gen_q[q] = i;
-                        } else {
-                                const uint32_t q = queue_slot(w.counts + kCountCoated);
-                                w.gen_q[w.capacity - 1u - q] = i;
-                        }
+                if (kKind == kShadeSplit && mt >= 3 && mt <= 6) {
+                        const uint32_t q = queue_slot(w.counts + gen_counter(mt));
+                        w.gen_q[gen_pos(w, mt, q)] = i;
                         return;
                 }
-                if (kKind == kShadeDielectric || kKind == kShadeCoated) {
+                if (kKind >= kShadeDielectric) {
                         const V3 base = v3(m0);
                         if (bounce == 0) {
-                                const V3 a = mt == 3 ? v3(1.0f, 1.0f, 1.0f) : base;
+                                // Bsdf.albedo(): the base reflectance of a coated diffuse,
+                                // white for the dielectric and the conductors
+                                const V3 a = kKind == kShadeCoated ? base : v3(1.0f, 1.0f, 1.0f);
                                 w.alb[path] = make_float4(a.x, a.y, a.z, 0.0f);
                                 w.nrm[path] = make_float4(ng.x, ng.y, ng.z, 0.0f);
                         }
-                        const BMat bm = make_bmat(kKind, base, __ldg(s.mat_params + mi));
+                        const BMat bm = make_bmat<kKind>(base, __ldg(s.mat_params + 3 * mi), __ldg(s.mat_params + 3 * mi + 1),
+                                                         __ldg(s.mat_params + 3 * mi + 2));
                         ZSobol z;
                         z.morton = w.zs_morton[path];
                         z.dim = w.zs_dim[path];
@@ -901,7 +916,7 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                         return;
                 }
         }
-        if (kKind == kShadeDielectric || kKind == kShadeCoated) return;  // not queued here
+        if (kKind >= kShadeDielectric) return;  // not queued here
         V3 refl = (mi >= 0 && mi < s.material_count) ? v3(__ldg(s.materials + 2 * mi)) : v3(0.5f, 0.5f, 0.5f);
         if (w.mat_tex && mi >= 0 && mi < s.material_count) {
                 const int t = __ldg(w.mat_tex + mi);
@@ -1132,6 +1147,8 @@ __global__ void k_clear_counts(Wave w, int next) {
         w.counts[kCountProbe] = 0;
         w.counts[kCountDielectric] = 0;
         w.counts[kCountCoated] = 0;
+        w.counts[kCountConductor] = 0;
+        w.counts[kCountCoatedConductor] = 0;
 }
 
 // Film.add (Core/Film.swift:107-119): the sample's light scaled by iso / 100
@@ -1476,6 +1493,8 @@ struct gzg_renderer {
                                 k_shade<kShadeSplit><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                                 k_shade<kShadeDielectric><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                                 k_shade<kShadeCoated><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                                k_shade<kShadeConductor><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
+                                k_shade<kShadeCoatedConductor><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                         } else {
                                 k_shade<kShadeDiffuse><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                         }
@@ -1673,7 +1692,7 @@ gzg_status build_batch(gzg_renderer *r) {
                         mats.insert(mats.end(), hs.materials.begin(), hs.materials.end());
                         if (any_params) {
                                 if (hs.mat_params.empty())
-                                        mparams.insert(mparams.end(), hs.materials.size() / 2, float4_{1, 0, 0, 0});
+                                        mparams.insert(mparams.end(), 3 * (hs.materials.size() / 2), float4_{1, 0, 0, 0});
                                 else
                                         mparams.insert(mparams.end(), hs.mat_params.begin(), hs.mat_params.end());
                         }
@@ -1772,7 +1791,7 @@ gzg_status renderer_create(gzg_scene *const *scenes, const gzg_render_params *pa
             (st = r->alloc(&w.q_id[0], C)) || (st = r->alloc(&w.q_id[1], C)) || (st = r->alloc(&w.hits, C)) ||
             (st = r->alloc(&w.sh_ray, 2 * C)) || (st = r->alloc(&w.sh_id, C)) || (st = r->alloc(&w.sh_contrib, C)) ||
             (st = r->alloc(&w.sh_occ, C)) || (st = r->alloc(&w.pr_ray, 2 * C)) || (st = r->alloc(&w.pr_id, C)) ||
-            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) || (st = r->alloc(&w.gen_q, C)) ||
+            (st = r->alloc(&w.pr_contrib, C)) || (st = r->alloc(&w.pr_hits, C)) || (st = r->alloc(&w.order, C)) || (st = r->alloc(&w.gen_q, 2 * C)) ||
             (st = r->alloc(&w.alb, C)) || (st = r->alloc(&w.nrm, C)) ||
             (st = r->alloc(&w.key_hist, 2 * keys)) || (st = r->alloc(&w.counts, kCountWords)) ||
             (st = r->alloc(&w.stats, kStatWords)))

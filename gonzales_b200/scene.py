@@ -27,8 +27,17 @@ MATERIAL_NONE = 0
 MATERIAL_DIFFUSE = 1
 MATERIAL_AREA_LIGHT = 2
 # renderer extensions (Material_C.type values the reference's plugin never sees)
-MATERIAL_DIELECTRIC = 3      # Material/Dielectric.swift
-MATERIAL_COATED_DIFFUSE = 4  # Material/CoatedDiffuse.swift
+MATERIAL_DIELECTRIC = 3         # Material/Dielectric.swift
+MATERIAL_COATED_DIFFUSE = 4     # Material/CoatedDiffuse.swift
+MATERIAL_CONDUCTOR = 5          # Material/Conductor.swift
+MATERIAL_COATED_CONDUCTOR = 6   # Material/CoatedConductor.swift
+EXTENDED_MATERIALS = (MATERIAL_DIELECTRIC, MATERIAL_COATED_DIFFUSE, MATERIAL_CONDUCTOR, MATERIAL_COATED_CONDUCTOR)
+# gzg_material_params: eta, roughness u, v, thickness, conductor eta (3),
+# conductor roughness u, conductor k (3), conductor roughness v
+MATERIAL_PARAMS_WIDTH = 12
+# copper's refractive index and extinction at the RGB primaries (approximate)
+COPPER_ETA = (0.2, 0.92, 1.1)
+COPPER_K = (3.9, 2.45, 2.14)
 
 
 @dataclass
@@ -80,11 +89,11 @@ class HostScene:
     nodes: np.ndarray      # BVH2_NODE_DTYPE
     materials: np.ndarray  # MATERIAL_DTYPE
     prim_order: np.ndarray  # k-th leaf prim = input prim prim_order[k]
-    material_params: np.ndarray = None  # (n_materials, 4) float32: eta, roughness u, v, thickness
+    material_params: np.ndarray = None  # (n_materials, MATERIAL_PARAMS_WIDTH) float32
 
     @property
     def has_extended_materials(self):
-        return bool(np.isin(self.materials["type"], (MATERIAL_DIELECTRIC, MATERIAL_COATED_DIFFUSE)).any())
+        return bool(np.isin(self.materials["type"], EXTENDED_MATERIALS).any())
 
     def mesh_structs(self):
         arr = (F.TriangleMeshC * max(len(self.meshes), 1))()
@@ -119,19 +128,27 @@ class SceneBuilder:
         self.meshes = []
         self._prims = []       # list of (mesh, first_tri, ntri, type, material or light)
         self._materials = []   # (type, albedo, emission)
-        self._material_params = []  # (eta, roughness u, roughness v, thickness)
+        self._material_params = []  # MATERIAL_PARAMS_WIDTH floats per material
         self._lights = []      # emission per area light
         self._geometric = 0
 
-    def add_material(self, albedo=(0.5, 0.5, 0.5), kind="diffuse", eta=1.5, roughness=0.0, thickness=0.01):
+    def add_material(self, albedo=(0.5, 0.5, 0.5), kind="diffuse", eta=1.5, roughness=0.0, thickness=0.01,
+                     conductor_eta=COPPER_ETA, conductor_k=COPPER_K, conductor_roughness=0.0):
         """kind: "diffuse" (albedo), "dielectric" (eta, roughness; albedo
-        unused) or "coateddiffuse" (reflectance = albedo, coating eta and
-        roughness, clear layer thickness).  Roughness is remapped to alpha =
+        unused), "coateddiffuse" (reflectance = albedo, coating eta and
+        roughness, clear layer thickness), "conductor" (conductor eta / k per
+        channel, conductor roughness used as alpha) or "coatedconductor"
+        (coating eta and roughness over a conductor of reflectance = albedo,
+        conductor eta / k / roughness, layer thickness).  Dielectric and
+        coating roughness (and a coated conductor's) is remapped to alpha =
         sqrt(roughness) as the reference's remaproughness default does."""
         t = {"diffuse": MATERIAL_DIFFUSE, "dielectric": MATERIAL_DIELECTRIC,
-             "coateddiffuse": MATERIAL_COATED_DIFFUSE}[kind]
+             "coateddiffuse": MATERIAL_COATED_DIFFUSE, "conductor": MATERIAL_CONDUCTOR,
+             "coatedconductor": MATERIAL_COATED_CONDUCTOR}[kind]
         self._materials.append((t, tuple(albedo), (0.0, 0.0, 0.0)))
-        self._material_params.append((eta, roughness, roughness, thickness))
+        ce, ck = tuple(conductor_eta), tuple(conductor_k)
+        self._material_params.append((eta, roughness, roughness, thickness) + ce + (conductor_roughness,) + ck +
+                                     (conductor_roughness,))
         return len(self._materials) - 1
 
     def add_mesh(self, points, triangles, material=0):
@@ -181,7 +198,7 @@ class SceneBuilder:
         # leave the padding bytes undefined).
         raw = prims.view(np.uint8).reshape(-1, F.PRIM_ID_DTYPE.itemsize)[order]
         sorted_prims = np.ascontiguousarray(raw).view(F.PRIM_ID_DTYPE).reshape(-1)
-        params = np.zeros((len(mats), 4), np.float32)
+        params = np.zeros((len(mats), MATERIAL_PARAMS_WIDTH), np.float32)
         if self._material_params:
             params[:n_surface] = np.asarray(self._material_params, np.float32)
         return HostScene(meshes=self.meshes, prims=sorted_prims, nodes=nodes, materials=mats,

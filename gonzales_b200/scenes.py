@@ -224,7 +224,7 @@ def random_instances(n, n_blas, seed, extent=20.0):
     return inst
 
 
-MIXED_KINDS = ("diffuse", "coateddiffuse", "dielectric")
+MIXED_KINDS = ("diffuse", "coateddiffuse", "dielectric", "conductor", "coatedconductor")
 
 
 def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, extent=20.0, coloured=False,
@@ -232,8 +232,9 @@ def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, 
     """Bottom-level scenes (one mesh each: tubes and spheres alternating) and
     instances; 2 * n_u * n_v triangles per mesh (50,000 at the defaults).
     coloured: a seeded diffuse albedo in [0.1, 0.8]^3 per mesh (else 0.5).
-    mixed: mesh k is diffuse, coated diffuse or dielectric (k mod 3), eta 1.5,
-    roughness uniform in [0.05, 0.5], coating thickness 0.01 (implies
+    mixed: mesh k is diffuse, coated diffuse, dielectric, conductor (copper)
+    or coated conductor (k mod 5), eta 1.5, roughness uniform in [0.05, 0.5]
+    (coating and conductor alike), coating thickness 0.01 (implies
     coloured)."""
     rng = np.random.default_rng(seed + 101)
     blas = []
@@ -243,7 +244,8 @@ def instanced_scene(n_meshes=16, n_u=125, n_v=200, n_instances=4096, seed=0xC2, 
         albedo = rng.uniform(0.1, 0.8, 3) if (coloured or mixed) else (0.5, 0.5, 0.5)
         if mixed:
             rough = float(rng.uniform(0.05, 0.5))
-            m = sb.add_material(albedo, kind=MIXED_KINDS[k % 3], eta=1.5, roughness=rough, thickness=0.01)
+            m = sb.add_material(albedo, kind=MIXED_KINDS[k % len(MIXED_KINDS)], eta=1.5, roughness=rough,
+                                thickness=0.01, conductor_roughness=rough)
         else:
             m = sb.add_material(albedo)
         sb.add_mesh(pts, tris, m)
@@ -344,7 +346,9 @@ def box_scene(seed=0xB0):
 def materials_box_scene(seed=0xB1):
     """The box scene with the renderer's other materials: a coated-diffuse box
     (roughness 0.2), a rough dielectric box (0.1), a smooth dielectric sphere
-    (specular) and a rough coated sphere (0.4), diffuse walls, ceiling light."""
+    (specular), a rough coated sphere (0.4), a copper sphere (alpha 0.15) and
+    a coated-conductor box (coating 0.05, conductor 0.3), diffuse walls,
+    ceiling light."""
     rng = np.random.default_rng(seed)
     sb = SceneBuilder()
     _room(sb, rng)
@@ -359,6 +363,11 @@ def materials_box_scene(seed=0xB1):
     sb.add_mesh(sp * 0.1 + np.array([0.3, 0.36, 0.4]), st,
                 sb.add_material(rng.uniform(0.1, 0.8, 3), kind="coateddiffuse", eta=1.5, roughness=0.4,
                                 thickness=0.05))
+    sb.add_mesh(sp * 0.09 + np.array([0.18, 0.09, 0.75]), st,
+                sb.add_material(kind="conductor", conductor_roughness=0.15))
+    bp, bt = _box(0.14, 0.7, (0.82, 0.07 + 1e-4, 0.25))
+    sb.add_mesh(bp, bt, sb.add_material((0.9, 0.8, 0.5), kind="coatedconductor", eta=1.5, roughness=0.05,
+                                        thickness=0.02, conductor_roughness=0.3))
     lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
     sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
     return sb

@@ -338,15 +338,29 @@ GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const
 GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
                                              float scale);
 
-/* Parameters of the renderer's dielectric (Material_C.type 3,
- * Material/Dielectric.swift) and coated-diffuse (type 4,
- * Material/CoatedDiffuse.swift, diffuse base = albedo) materials: HOST
- * params[count][4] = eta, roughness u, roughness v, layer thickness, one
- * record per material of the flat scene (count = its material count; records
- * of other types are ignored).  Roughness is remapped to alpha =
- * sqrt(roughness).  Once per scene, before the scene enters a two-level scene,
- * a batch or a renderer; without it types 3 and 4 shade as diffuse. */
-GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const float *params, int64_t count);
+/* Parameters of the renderer's general materials, by Material_C.type:
+ *   3 dielectric        (Material/Dielectric.swift): eta, roughness u/v;
+ *   4 coated diffuse    (Material/CoatedDiffuse.swift, base = albedo): eta,
+ *                       roughness u/v of the coating, thickness;
+ *   5 conductor         (Material/Conductor.swift): conductor eta/k per RGB
+ *                       channel, conductor roughness u/v (used as alpha);
+ *   6 coated conductor  (Material/CoatedConductor.swift, base reflectance =
+ *                       albedo): coating eta, roughness u/v, thickness,
+ *                       conductor eta/k and roughness.
+ * Dielectric and coating roughness, and a coated conductor's conductor
+ * roughness, are remapped to alpha = sqrt(roughness). */
+typedef struct gzg_material_params {
+        float eta, roughness_u, roughness_v, thickness;
+        float conductor_eta[3], conductor_roughness_u;
+        float conductor_k[3], conductor_roughness_v;
+} gzg_material_params;
+
+/* One HOST record per material of the flat scene (count = its material
+ * count; records of other types are ignored).  Once per scene, before the
+ * scene enters a two-level scene, a batch or a renderer; without it types 3
+ * to 6 shade as diffuse. */
+GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const gzg_material_params *params,
+                                                 int64_t count);
 
 /* Expands device hits into reference Intersection_C records on the device
  * (prim-id lookup; the miss record of kernel.mojo:362-364). */

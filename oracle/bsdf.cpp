@@ -1,4 +1,5 @@
-// bsdf.cpp - CPU restatement of Gonzales' dielectric and coated-diffuse BSDFs
+// bsdf.cpp - CPU restatement of Gonzales' dielectric, coated-diffuse,
+// conductor and coated-conductor BSDFs
 // (test infrastructure: checker and CPU baseline).  -ffp-contract=off.
 //
 // Restated from (paths relative to Sources/libgonzales):
@@ -9,6 +10,8 @@
 //   LayeredBsdf (coated diffuse: dielectric top, Bsdf/LayeredBsdf.swift:55-520, 847-855;
 //     diffuse bottom, no medium)                 Bsdf/CoatedDiffuseBsdf.swift; Material/CoatedDiffuse.swift
 //   diffuse, default cosine sampling              Bsdf/DiffuseBsdf.swift; Reflection/Bsdf.swift:20-60
+//   conductor Fresnel, microfacet reflection      Reflection/FresnelConductor.swift, Bsdf/MicrofacetReflection.swift
+//   coated conductor (dielectric over conductor)  Bsdf/CoatedConductorBsdf.swift; Material/CoatedConductor.swift
 //
 // The layered BSDF's random walks draw from a RandomSampler the reference
 // seeds from the system (non-reproducible).  Here each evaluate / sample /
@@ -342,6 +345,65 @@ struct Diffuse {
                 s.pdf = pdf(wo, wi);
                 return s;
         }
+        // as a layer's base: the value ignores the directions (DiffuseBsdf.evaluate)
+        void f(V, V, float out[3]) const { f(out); }
+};
+
+// FresnelConductor.fresnelConductor for one channel, etaI = 1
+// (Reflection/FresnelConductor.swift:4-28).
+float fresnel_conductor(float cos_theta, float eta, float etak) {
+        const float c = clampf(cos_theta, -1.0f, 1.0f);
+        const float cos2 = c * c;
+        const float sin2 = 1.0f - cos2;
+        const float eta2 = eta * eta;
+        const float etak2 = etak * etak;
+        const float t0 = eta2 - etak2 - sin2;
+        const float a2pb2 = std::sqrt(t0 * t0 + 4.0f * eta2 * etak2);
+        const float t1 = a2pb2 + cos2;
+        const float a = std::sqrt(0.5f * (a2pb2 + t0));
+        const float t2 = 2.0f * c * a;
+        const float rs = (t1 - t2) / (t1 + t2);
+        const float t3 = cos2 * a2pb2 + sin2 * sin2;
+        const float t4 = t2 * sin2;
+        const float rp = rs * (t3 - t4) / (t3 + t4);
+        return 0.5f * (rp + rs);
+}
+
+// MicrofacetReflection with a conductor Fresnel term
+// (Bsdf/MicrofacetReflection.swift:1-42): Conductor (reflectance white) and
+// the base of CoatedConductor (reflectance from the material).
+struct Conductor {
+        TR d;
+        float R[3];
+        float eta[3], k[3];
+        void f(V wo, V wi, float out[3]) const {
+                out[0] = out[1] = out[2] = 0.0f;
+                const float co = std::fabs(wo.z), ci = std::fabs(wi.z);
+                V h = add(wo, wi);
+                if (co == 0.0f || ci == 0.0f) return;
+                if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return;
+                h = normalize(h);
+                const float cf = std::fabs(dot(wi, h));
+                const float area = d.D(h);
+                const float vis = d.G(wo, wi);
+                const float den = 4.0f * ci * co;
+                for (int c = 0; c < 3; ++c) out[c] = R[c] * area * vis * fresnel_conductor(cf, eta[c], k[c]) / den;
+        }
+        float pdf(V wo, V wi) const {
+                if (!same_hemisphere(wo, wi)) return 0.0f;
+                const V h = normalize(add(wo, wi));
+                return d.pdf(wo, h) / (4.0f * dot(wo, h));
+        }
+        Sample sample(V wo, float u0, float u1) const {
+                if (wo.z == 0.0f) return no_sample();
+                const V h = d.sample_wh(wo, u0, u1);
+                const V wi = add(neg(wo), mul(h, 2.0f * dot(wo, h)));
+                Sample s;
+                f(wo, wi, s.f);
+                s.wi = wi;
+                s.pdf = pdf(wo, wi);
+                return s;
+        }
 };
 
 inline float transmittance(float dz, V w) {
@@ -355,11 +417,14 @@ inline float max3(const float a[3]) { return std::max(a[0], std::max(a[1], a[2])
 
 namespace {
 
-// LayeredBsdf<DielectricBsdf, DiffuseBsdf> with a clear coating (albedo 0),
-// two-sided (Bsdf/LayeredBsdf.swift).
-struct Coated {
+// LayeredBsdf<DielectricBsdf, Bottom> with a clear layer (albedo 0),
+// two-sided (Bsdf/LayeredBsdf.swift): coated diffuse (Bottom = Diffuse,
+// Bsdf/CoatedDiffuseBsdf.swift) and coated conductor (Bottom = Conductor,
+// Bsdf/CoatedConductorBsdf.swift).
+template <class Bottom>
+struct Layered {
         Dielectric top;
-        Diffuse bottom;
+        Bottom bottom;
         float thickness;
         int max_depth, nsamples;
 
@@ -411,7 +476,7 @@ struct Coated {
                                         float ne[3];
                                         float ne_pdf;
                                         if (z == 0.0f) {
-                                                bottom.f(ne);
+                                                bottom.f(neg(w), neg(wis.wi), ne);
                                                 ne_pdf = bottom.pdf(neg(w), neg(wis.wi));
                                         } else {
                                                 const float ft = top.f(neg(w), neg(wis.wi));
@@ -437,7 +502,7 @@ struct Coated {
                                         float fe[3];
                                         float fe_pdf;
                                         if (exit_z == 0.0f) {
-                                                bottom.f(fe);
+                                                bottom.f(neg(w), wi, fe);
                                                 fe_pdf = bottom.pdf(neg(w), wi);
                                         } else {
                                                 const float ft = top.f(neg(w), wi);
@@ -564,33 +629,59 @@ struct Coated {
 // ---------------------------------------------------------------- materials
 
 struct OrcMat {
-        int type;  // 1 diffuse, 3 dielectric, 4 coated diffuse
+        int type;  // 1 diffuse, 3 dielectric, 4 coated diffuse, 5 conductor, 6 coated conductor
         Diffuse diffuse;
         Dielectric diel;
-        Coated coated;
+        Layered<Diffuse> coated;
+        Conductor conductor;
+        Layered<Conductor> coated_conductor;
 };
 
 namespace {
 
-// Dielectric.getBsdf / CoatedDiffuse.getBsdf (Material/Dielectric.swift:3-14,
-// Material/CoatedDiffuse.swift:23-58): roughness remapped to alpha = sqrt;
-// the coating's alpha is at least 0.001; thickness, depth 10, one sample.
+// Dielectric.getBsdf, CoatedDiffuse.getBsdf, Conductor.getBsdf and
+// CoatedConductor.getBsdf (Material/Dielectric.swift:3-14,
+// Material/CoatedDiffuse.swift:23-58, Material/Conductor.swift:3-22,
+// Material/CoatedConductor.swift:35-88): dielectric and coating roughness
+// remapped to alpha = sqrt (a coating's alpha at least 0.001); a plain
+// conductor's roughness is its alpha (at least 1e-3), a coated conductor's
+// is remapped (at least 0.001); layers: thickness, depth 10, one sample.
 OrcMat make_mat(const orc_bsdf_params &p) {
         OrcMat m;
         m.type = p.type;
         for (int c = 0; c < 3; ++c) m.diffuse.R[c] = p.reflectance[c];
         float ax = std::sqrt(p.roughness_u), ay = std::sqrt(p.roughness_v);
-        if (p.type == 4) {
+        if (p.type == 4 || p.type == 6) {
                 ax = std::max(ax, 0.001f);
                 ay = std::max(ay, 0.001f);
         }
         m.diel.d = TR{ax, ay};
         m.diel.eta = p.eta;
+        const float thick = std::max(p.thickness, 1.17549435e-38f);
         m.coated.top = m.diel;
         m.coated.bottom = m.diffuse;
-        m.coated.thickness = std::max(p.thickness, 1.17549435e-38f);
+        m.coated.thickness = thick;
         m.coated.max_depth = 10;
         m.coated.nsamples = 1;
+        float cx, cy;
+        if (p.type == 6) {
+                cx = std::max(std::sqrt(p.conductor_roughness_u), 0.001f);
+                cy = std::max(std::sqrt(p.conductor_roughness_v), 0.001f);
+        } else {
+                cx = std::max(p.conductor_roughness_u, 1e-3f);
+                cy = std::max(p.conductor_roughness_v, 1e-3f);
+        }
+        m.conductor.d = TR{cx, cy};
+        for (int c = 0; c < 3; ++c) {
+                m.conductor.R[c] = p.type == 6 ? p.reflectance[c] : 1.0f;
+                m.conductor.eta[c] = p.conductor_eta[c];
+                m.conductor.k[c] = p.conductor_k[c];
+        }
+        m.coated_conductor.top = m.diel;
+        m.coated_conductor.bottom = m.conductor;
+        m.coated_conductor.thickness = thick;
+        m.coated_conductor.max_depth = 10;
+        m.coated_conductor.nsamples = 1;
         return m;
 }
 
@@ -599,6 +690,10 @@ void mat_f(const OrcMat &m, V wo, V wi, float out[3]) {
                 out[0] = out[1] = out[2] = m.diel.f(wo, wi);
         } else if (m.type == 4) {
                 m.coated.f(wo, wi, out);
+        } else if (m.type == 5) {
+                m.conductor.f(wo, wi, out);
+        } else if (m.type == 6) {
+                m.coated_conductor.f(wo, wi, out);
         } else {
                 m.diffuse.f(out);
         }
@@ -607,12 +702,16 @@ void mat_f(const OrcMat &m, V wo, V wi, float out[3]) {
 float mat_pdf(const OrcMat &m, V wo, V wi) {
         if (m.type == 3) return m.diel.pdf(wo, wi);
         if (m.type == 4) return m.coated.pdf(wo, wi);
+        if (m.type == 5) return m.conductor.pdf(wo, wi);
+        if (m.type == 6) return m.coated_conductor.pdf(wo, wi);
         return m.diffuse.pdf(wo, wi);
 }
 
 Sample mat_sample(const OrcMat &m, V wo, float u0, float u1, float u2) {
         if (m.type == 3) return m.diel.sample(wo, u0, u1, u2, true);
         if (m.type == 4) return m.coated.sample(wo, u0, u1, u2);
+        if (m.type == 5) return m.conductor.sample(wo, u0, u1);
+        if (m.type == 6) return m.coated_conductor.sample(wo, u0, u1, u2);
         return m.diffuse.sample(wo, u0, u1);
 }
 

@@ -222,7 +222,7 @@ struct Scene {
         float escale = 1.0f;
         const orc_render_instances *inst = nullptr;
         const orc_env *env = nullptr;
-        const float *mat_params = nullptr;  // 4 per material (eta, roughness u, v, thickness)
+        const float *mat_params = nullptr;  // 12 per material (orc_bsdf_params order from eta on)
 };
 
 // Emission times the scene's emission scale (1 without textures: exact).
@@ -590,15 +590,29 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                         if (sc.inst) {
                                 const int b = is_light ? 0 : is.blas;
                                 if (sc.inst->blas_material_params && sc.inst->blas_material_params[b])
-                                        mp = sc.inst->blas_material_params[b] + 4 * mi;
+                                        mp = sc.inst->blas_material_params[b] + 12 * mi;
                         } else if (sc.mat_params) {
-                                mp = sc.mat_params + 4 * mi;
+                                mp = sc.mat_params + 12 * mi;
                         }
                         const orc_material &mm = mset[mi];
-                        if ((mm.type == 3 || mm.type == 4) && mp) {
-                                orc_bsdf_params bp{mm.type, {mm.albedo[0], mm.albedo[1], mm.albedo[2]}, mp[0], mp[1], mp[2], mp[3]};
+                        if (mm.type >= 3 && mm.type <= 6 && mp) {
+                                // mp: eta, roughness u, v, thickness, conductor eta[3],
+                                // conductor roughness u, conductor k[3], conductor roughness v
+                                const orc_bsdf_params bp{mm.type,
+                                                         {mm.albedo[0], mm.albedo[1], mm.albedo[2]},
+                                                         mp[0],
+                                                         mp[1],
+                                                         mp[2],
+                                                         mp[3],
+                                                         {mp[4], mp[5], mp[6]},
+                                                         {mp[8], mp[9], mp[10]},
+                                                         mp[7],
+                                                         mp[11]};
                                 if (bounce == 0) {
-                                        res.albedo = mm.type == 3 ? v3(1, 1, 1) : v3(mm.albedo[0], mm.albedo[1], mm.albedo[2]);
+                                        // Bsdf.albedo(): the diffuse base's reflectance for a coated
+                                        // diffuse; white for the dielectric and for both conductors
+                                        // (MicrofacetReflection.albedo)
+                                        res.albedo = mm.type == 4 ? v3(mm.albedo[0], mm.albedo[1], mm.albedo[2]) : v3(1, 1, 1);
                                         res.normal = ng;
                                 }
                                 if (!is.frame_ok || sc.lights.empty()) break;

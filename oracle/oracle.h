@@ -139,9 +139,10 @@ typedef struct orc_render_instances orc_render_instances;
 /* The general form: a flat scene (nodes .. n_prims) or, with `instances`, a
  * two-level one (the flat arrays are then unused); an optional environment
  * light (appended last to the light list; its power enters the light
- * choice); optional material parameters (4 floats per material: eta,
- * roughness u, v, thickness) for materials of type 3 (dielectric) and 4
- * (coated diffuse); optional textures (flat scenes). */
+ * choice); optional material parameters (per material: eta, roughness u,
+ * v, thickness, conductor eta[3], conductor roughness u,
+ * conductor k[3], conductor roughness v: 12 floats) for materials of types 3
+ * to 6; optional textures (flat scenes). */
 void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh *meshes,
                    const orc_material *materials, int64_t n_materials, int64_t n_prims,
                    const orc_render_instances *instances, const orc_env *env, const float *material_params,
@@ -203,7 +204,7 @@ typedef struct orc_render_instances {
         const orc_blas *blas;
         const orc_material *const *blas_materials;
         int64_t blas_count;
-        const float *const *blas_material_params; /* per bottom-level scene: 4 floats per material, or NULL */
+        const float *const *blas_material_params; /* per bottom-level scene: 12 floats per material, or NULL */
 } orc_render_instances;
 
 /* The MT leaf test alone (kernel.mojo:122-156); returns 1 on a hit. */
@@ -227,11 +228,16 @@ int orc_bounds_maximum_extent(const float *mn, const float *mx);
 /* type 1 diffuse (reflectance), 3 dielectric (eta, roughness u/v remapped to
  * alpha = sqrt), 4 coated diffuse (dielectric coating eta / roughness over a
  * diffuse base of `reflectance`, clear layer of `thickness`, depth 10, one
- * sample).  Directions are in the shading frame (z = normal). */
+ * sample), 5 conductor (conductor eta / k per channel, conductor roughness
+ * as alpha), 6 coated conductor (the coating over a conductor of
+ * `reflectance`, its roughness remapped).  Directions are in the shading
+ * frame (z = normal). */
 typedef struct orc_bsdf_params {
         int32_t type;
         float reflectance[3];
         float eta, roughness_u, roughness_v, thickness;
+        float conductor_eta[3], conductor_k[3];
+        float conductor_roughness_u, conductor_roughness_v;
 } orc_bsdf_params;
 
 void orc_bsdf_eval(const orc_bsdf_params *p, const float *wo, const float *wi, float *f, float *pdf);

@@ -435,16 +435,23 @@ def traverse_instanced(tlas_nodes, leaf_instance, w2o, blas_of, blas_scenes, ray
 
 class BsdfParams(C.Structure):
     _fields_ = [("type", C.c_int32), ("reflectance", C.c_float * 3), ("eta", C.c_float), ("roughness_u", C.c_float),
-                ("roughness_v", C.c_float), ("thickness", C.c_float)]
+                ("roughness_v", C.c_float), ("thickness", C.c_float), ("conductor_eta", C.c_float * 3),
+                ("conductor_k", C.c_float * 3), ("conductor_roughness_u", C.c_float),
+                ("conductor_roughness_v", C.c_float)]
 
 
-def bsdf_params(kind, reflectance=(0.5, 0.5, 0.5), eta=1.5, roughness=0.0, thickness=0.01):
-    """kind: 1 diffuse, 3 dielectric, 4 coated diffuse (Material_C.type values)."""
+def bsdf_params(kind, reflectance=(0.5, 0.5, 0.5), eta=1.5, roughness=0.0, thickness=0.01,
+                conductor_eta=(0.2, 0.92, 1.1), conductor_k=(3.9, 2.45, 2.14), conductor_roughness=0.0):
+    """kind: 1 diffuse, 3 dielectric, 4 coated diffuse, 5 conductor, 6 coated
+    conductor (Material_C.type values)."""
     p = BsdfParams()
     p.type = int(kind)
     for c in range(3):
         p.reflectance[c] = float(reflectance[c])
+        p.conductor_eta[c] = float(conductor_eta[c])
+        p.conductor_k[c] = float(conductor_k[c])
     p.eta, p.roughness_u, p.roughness_v, p.thickness = float(eta), float(roughness), float(roughness), float(thickness)
+    p.conductor_roughness_u = p.conductor_roughness_v = float(conductor_roughness)
     return p
 
 

@@ -4,14 +4,16 @@ the surface estimate of VolumePathIntegrator.swift:325-371 with a general
 BSDF), at equal Z-Sobol indices:
 
   - the box scene with a coated box, a rough dielectric box, a smooth
-    (specular) dielectric sphere and a coated sphere, MIS as written and
-    corrected, with and without the sky map (specular paths reach the
-    emitter and the environment);
-  - a two-level scene of diffuse, coated and dielectric meshes (roughness
-    uniform in [0.05, 0.5]) under the sky map;
+    (specular) dielectric sphere, a coated sphere, a copper sphere and a
+    coated-conductor box, MIS as written and corrected, with and without the
+    sky map (specular paths reach the emitter and the environment);
+  - a two-level scene of diffuse, coated-diffuse, dielectric, conductor and
+    coated-conductor meshes (roughness uniform in [0.05, 0.5]) under the sky
+    map;
   - a batch mixing the material scene with the diffuse box scene equals the
     solo renders;
-  - first-hit albedo: white for a dielectric, the base for a coated diffuse.
+  - first-hit albedo: white for a dielectric and the conductors, the base for
+    a coated diffuse.
 
 Per pixel, GPU and oracle means agree within 3 combined standard errors on
 >= 99 % of pixels and image means agree to 1.5 %.  The coated BSDF's
@@ -85,7 +87,7 @@ def test_material_box_with_environment_matches_oracle(mat_box, sky):
 
 
 def test_mixed_instanced_scene_matches_oracle(sky):
-    blas_hosts, inst = scenes.instanced_scene(n_meshes=6, n_u=30, n_v=20, n_instances=96, extent=5.0, mixed=True)
+    blas_hosts, inst = scenes.instanced_scene(n_meshes=10, n_u=30, n_v=20, n_instances=128, extent=5.0, mixed=True)
     assert any(b.has_extended_materials for b in blas_hosts)
     p = dict(width=64, height=48, spp=32, max_depth=5, rr_min_bounce=2, eye=(0.0, 2.0, 16.0),
              target=(0.0, 0.0, 0.0))
@@ -164,3 +166,15 @@ def test_material_params_are_validated(mat_box):
     bad.material_params[1, 0] = -1.0  # eta of a coated material
     with pytest.raises(GzgError):
         GpuAccelerator(bad)
+
+
+def test_material_render_is_repeatable(mat_box):
+    # every material kind in one scene: lanes of one warp append to the
+    # queues of different kinds at once; a repeat differs only by the order of
+    # the film's atomic additions
+    p = dict(width=48, height=48, spp=16, max_depth=5, rr_min_bounce=3)
+    with GpuAccelerator(mat_box) as acc:
+        a = acc.render(F.render_params(**p))
+        b = acc.render(F.render_params(**p))
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-5, atol=1e-6)
+    assert a[3] == b[3]
