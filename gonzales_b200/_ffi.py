@@ -70,6 +70,10 @@ class TraceOptions(C.Structure):
                 ("fetch_counters", C.c_void_p)]
 
 
+class BuildOptions(C.Structure):
+    _fields_ = [("leaf_size", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
 class SceneInfo(C.Structure):
     _fields_ = [("bvh2_nodes", C.c_int64), ("prims", C.c_int64), ("triangles", C.c_int64),
                 ("wide_nodes", C.c_int64), ("wide_depth", C.c_int32), ("bvh2_depth", C.c_int32),
@@ -133,6 +137,9 @@ PROTOTYPES = {
     "gzg_scene_set_launch": (ST, [VP, C.c_int32, C.POINTER(TraceOptions)]),
     "gzg_scene_set_environment": (ST, [VP, VP, C.c_int32, C.c_int32, C.c_float]),
     "gzg_scene_set_material_params": (ST, [VP, VP, I64]),
+    "gzg_gpu_build_scene": (ST, [VP, I64, VP, I64, VP, VP, VP, VP, I64, VP, C.POINTER(VP)]),
+    "gzg_scene_build_time": (ST, [VP, C.POINTER(C.c_float)]),
+    "gzg_scene_tree_cost": (ST, [VP, C.POINTER(C.c_double)]),
     "gzg_host_instance_bounds": (ST, [VP, I64, VP, I64, VP]),
     "gzg_instanced_scene_create": (ST, [VP, I64, VP, I64, VP, I64, VP, I64, C.POINTER(VP)]),
     "gzg_trace_closest_instanced_device": (ST, [VP, VP, I64, VP, VP, C.POINTER(TraceOptions), VP]),

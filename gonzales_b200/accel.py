@@ -39,15 +39,29 @@ def _stream_handle(stream):
 
 
 class GpuAccelerator:
-    def __init__(self, host_scene: HostScene):
+    def __init__(self, host_scene: HostScene, device_build=None, leaf_size=0):
+        """Uploads the scene with the host's BVH2 (gzg_gpu_upload_scene), or
+        builds its tree on the device (gzg_gpu_build_scene) when device_build
+        is true or the scene has no BVH2 (SceneBuilder.build(host_bvh=False))."""
         self.host = host_scene
         meshes = host_scene.mesh_structs()
         pts, fi, vi = host_scene.counts()
         handle = C.c_void_p()
-        F.check(F.lib().gzg_gpu_upload_scene(
-            F.ptr(host_scene.nodes), len(host_scene.nodes), F.ptr(host_scene.prims), len(host_scene.prims),
-            C.addressof(meshes), len(host_scene.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
-            F.ptr(host_scene.materials), len(host_scene.materials), C.byref(handle)))
+        if device_build is None:
+            device_build = host_scene.nodes is None
+        self.device_built = bool(device_build)
+        if self.device_built:
+            opt = F.BuildOptions()
+            opt.leaf_size = int(leaf_size)
+            F.check(F.lib().gzg_gpu_build_scene(
+                F.ptr(host_scene.prims), len(host_scene.prims), C.addressof(meshes), len(host_scene.meshes),
+                F.ptr(pts), F.ptr(fi), F.ptr(vi), F.ptr(host_scene.materials), len(host_scene.materials),
+                C.byref(opt), C.byref(handle)))
+        else:
+            F.check(F.lib().gzg_gpu_upload_scene(
+                F.ptr(host_scene.nodes), len(host_scene.nodes), F.ptr(host_scene.prims), len(host_scene.prims),
+                C.addressof(meshes), len(host_scene.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
+                F.ptr(host_scene.materials), len(host_scene.materials), C.byref(handle)))
         self.handle = handle
         if getattr(host_scene, "has_extended_materials", False) and host_scene.material_params is not None:
             try:
@@ -84,6 +98,18 @@ class GpuAccelerator:
         w = C.c_uint32(0)
         F.check(F.lib().gzg_scene_error_word(self.handle, C.byref(w), 1 if clear else 0))
         return w.value
+
+    def build_time_ms(self):
+        """Device time of the tree build (gzg_scene_build_time); -1 if uploaded."""
+        ms = C.c_float(0.0)
+        F.check(F.lib().gzg_scene_build_time(self.handle, C.byref(ms)))
+        return ms.value
+
+    def tree_cost(self):
+        """Surface-area cost of the wide tree (gzg_scene_tree_cost)."""
+        c = C.c_double(0.0)
+        F.check(F.lib().gzg_scene_tree_cost(self.handle, C.byref(c)))
+        return c.value
 
     def intersect_batch(self, rays, tmax, options=None, out=None):
         """Closest hit for host rays; returns INTERSECTION_DTYPE records."""
@@ -200,8 +226,7 @@ def instance_bounds(blas_hosts, instances):
     BVH2 root boxes."""
     bb = np.zeros((len(blas_hosts), 6), np.float32)
     for i, hs in enumerate(blas_hosts):
-        bb[i, :3] = hs.nodes[0]["bounds_min"]
-        bb[i, 3:] = hs.nodes[0]["bounds_max"]
+        bb[i, :3], bb[i, 3:] = hs.root_bounds()
     instances = np.ascontiguousarray(instances, F.INSTANCE_DTYPE)
     out = np.zeros((len(instances), 6), np.float32)
     F.check(F.lib().gzg_host_instance_bounds(F.ptr(bb), len(bb), F.ptr(instances), len(instances), F.ptr(out)))

@@ -38,8 +38,13 @@ def build(force=False, verbose=False):
         return OUT
     BUILD.mkdir(exist_ok=True)
     objs = []
+    headers = [p for p in CSRC.glob("*") if p.suffix in (".h", ".cuh")] + list(INCLUDE.glob("*.h")) + [Path(__file__)]
+    newest_header = max(p.stat().st_mtime for p in headers)
     for src in _sources():
         obj = BUILD / (src.name + ".o")
+        objs.append(str(obj))
+        if not force and obj.exists() and obj.stat().st_mtime > max(src.stat().st_mtime, newest_header):
+            continue  # up to date
         cmd = [NVCC, "-c", str(src), "-o", str(obj)] + COMMON
         if src.suffix == ".cu":
             cmd += CUDA_FLAGS
@@ -49,7 +54,6 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-        objs.append(str(obj))
     tmp = OUT.with_suffix(".so.tmp")
     link = [NVCC, "-shared", "-o", str(tmp)] + ARCH + [*objs, "-lpthread"]
     if verbose:

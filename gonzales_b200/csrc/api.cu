@@ -112,6 +112,7 @@ struct gzg_scene {
         WideBvh host_wide;          // host copy of the wide tree (two-level assembly)
         float root_bounds[6] = {0, 0, 0, 0, 0, 0};
         bool instanced = false;
+        float build_ms = -1.0f;     // device time of gzg_gpu_build_scene's tree build
         // host copies of the shading arrays (batch assembly)
         HostShading host_shading;
         std::mutex pool_mu;
@@ -295,28 +296,52 @@ GZG_API bool gzg_gpu_available(void) {
 
 GZG_API const char *gzg_last_error(void) { return g_last_error.c_str(); }
 
-GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count,
-                                        const gzg_prim_id *prim_ids, int64_t prim_count,
-                                        const gzg_triangle_mesh *meshes, int64_t mesh_count,
-                                        const int64_t *mesh_points_counts, const int64_t *mesh_face_indices_counts,
-                                        const int64_t *mesh_vertex_indices_counts, const gzg_material *materials,
-                                        int64_t material_count, gzg_scene **out_scene) {
-        (void)mesh_face_indices_counts;
-        if (!out_scene) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_gpu_upload_scene: out_scene is NULL");
+namespace {
+
+// gzg_gpu_upload_scene (bvh2_nodes given: the host's tree, converted on the
+// host) and gzg_gpu_build_scene (build given: the tree built on the device).
+gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count, const gzg_prim_id *prim_ids,
+                        int64_t prim_count, const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                        const int64_t *mesh_points_counts, const int64_t *mesh_vertex_indices_counts,
+                        const gzg_material *materials, int64_t material_count, const gzg_build_options *build,
+                        gzg_scene **out_scene, const char *fn) {
+        const std::string name(fn);
+        if (!out_scene) return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": out_scene is NULL");
         *out_scene = nullptr;
-        if (bvh2_node_count <= 0 || !bvh2_nodes || prim_count < 0 || (prim_count > 0 && !prim_ids) || mesh_count < 0 ||
-            (mesh_count > 0 && (!meshes || !mesh_points_counts || !mesh_vertex_indices_counts)) || material_count < 0 ||
-            (material_count > 0 && !materials))
-                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_gpu_upload_scene: bad arguments");
-        if (prim_count > INT32_MAX || bvh2_node_count > INT32_MAX)
-                return set_error(GZG_ERR_LIMIT, "gzg_gpu_upload_scene: more than 2^31 prims or nodes");
+        if ((!build && (bvh2_node_count <= 0 || !bvh2_nodes)) || prim_count < 0 || (prim_count > 0 && !prim_ids) ||
+            mesh_count < 0 || (mesh_count > 0 && (!meshes || !mesh_points_counts || !mesh_vertex_indices_counts)) ||
+            material_count < 0 || (material_count > 0 && !materials))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": bad arguments");
+        if (build && (build->leaf_size < 0 || build->leaf_size > 4))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": leaf_size must be 0 (default 4) to 4");
+        if (prim_count > INT32_MAX - 1 || bvh2_node_count > INT32_MAX)
+                return set_error(GZG_ERR_LIMIT, name + ": more than 2^31 prims or nodes");
         // Host-side validation and conversion first: a malformed scene is
         // reported as GZG_ERR_BAD_SCENE whether or not a device is present.
         WideBvh wide;
         int32_t bvh2_depth = 0;
-        gzg_status st = build_wide_bvh(bvh2_nodes, bvh2_node_count, prim_ids, prim_count, meshes, mesh_count,
-                                       mesh_points_counts, mesh_vertex_indices_counts, &wide, &bvh2_depth);
-        if (st != GZG_OK) return st;
+        gzg_status st;
+        if (!build) {
+                st = build_wide_bvh(bvh2_nodes, bvh2_node_count, prim_ids, prim_count, meshes, mesh_count,
+                                    mesh_points_counts, mesh_vertex_indices_counts, &wide, &bvh2_depth);
+                if (st != GZG_OK) return st;
+        } else {
+                // every triangle prim must resolve (no tree limits which ones are read)
+                for (int64_t k = 0; k < prim_count; ++k) {
+                        int64_t mesh, base;
+                        if (!prim_triangle(prim_ids[k], &mesh, &base)) continue;
+                        bool ok = mesh >= 0 && mesh < mesh_count && base >= 0 &&
+                                  base + 2 < mesh_vertex_indices_counts[mesh] && meshes[mesh].vertex_indices &&
+                                  meshes[mesh].points;
+                        for (int c = 0; ok && c < 3; ++c) {
+                                const int64_t v = meshes[mesh].vertex_indices[base + c];
+                                ok = v >= 0 && v * 4 + 3 <= mesh_points_counts[mesh];
+                        }
+                        if (!ok)
+                                return set_error(GZG_ERR_BAD_SCENE,
+                                                 name + ": prim " + std::to_string(k) + " has a mesh or vertex index out of range");
+                }
+        }
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
                 cudaGetLastError();
@@ -358,23 +383,27 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         auto scene = std::make_unique<gzg_scene>();
         cudaGetDevice(&scene->device);
         DevScene &d = scene->dev;
-        const uint4 *wn;
-        st = scene->upload(reinterpret_cast<const uint4 *>(wide.nodes.data()), wide.nodes.size() * 5, &wn, "wide nodes");
-        if (st != GZG_OK) return st;
-        d.wide = wn;
         const float4 *f;
-        st = scene->upload(reinterpret_cast<const float4 *>(wide.v0.data()), wide.v0.size(), &f, "triangles");
-        if (st != GZG_OK) return st;
-        d.tv0 = f;
-        st = scene->upload(reinterpret_cast<const float4 *>(wide.v1.data()), wide.v1.size(), &f, "triangles");
-        if (st != GZG_OK) return st;
-        d.tv1 = f;
-        st = scene->upload(reinterpret_cast<const float4 *>(wide.v2.data()), wide.v2.size(), &f, "triangles");
-        if (st != GZG_OK) return st;
-        d.tv2 = f;
-        st = scene->upload(reinterpret_cast<const float4 *>(bvh2_nodes), (size_t)bvh2_node_count * 2, &f, "bvh2 nodes");
-        if (st != GZG_OK) return st;
-        d.bvh2 = f;
+        if (!build) {
+                const uint4 *wn;
+                st = scene->upload(reinterpret_cast<const uint4 *>(wide.nodes.data()), wide.nodes.size() * 5, &wn,
+                                   "wide nodes");
+                if (st != GZG_OK) return st;
+                d.wide = wn;
+                st = scene->upload(reinterpret_cast<const float4 *>(wide.v0.data()), wide.v0.size(), &f, "triangles");
+                if (st != GZG_OK) return st;
+                d.tv0 = f;
+                st = scene->upload(reinterpret_cast<const float4 *>(wide.v1.data()), wide.v1.size(), &f, "triangles");
+                if (st != GZG_OK) return st;
+                d.tv1 = f;
+                st = scene->upload(reinterpret_cast<const float4 *>(wide.v2.data()), wide.v2.size(), &f, "triangles");
+                if (st != GZG_OK) return st;
+                d.tv2 = f;
+                st = scene->upload(reinterpret_cast<const float4 *>(bvh2_nodes), (size_t)bvh2_node_count * 2, &f,
+                                   "bvh2 nodes");
+                if (st != GZG_OK) return st;
+                d.bvh2 = f;
+        }
         st = scene->upload(reinterpret_cast<const float4 *>(pv0.data()), pv0.size(), &f, "prim triangles");
         if (st != GZG_OK) return st;
         d.pv0 = f;
@@ -393,12 +422,42 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         st = scene->upload(&zero, 1, &ew, "error word");
         if (st != GZG_OK) return st;
         d.err = const_cast<uint32_t *>(ew);
-        d.bvh2_count = bvh2_node_count;
+        if (build) {
+                // the tree, built on the device from the prim-order triangles
+                GpuWide gw;
+                float ms = 0.0f;
+                st = gpu_build_wide(reinterpret_cast<const float4_ *>(d.pv0), reinterpret_cast<const float4_ *>(d.pv1),
+                                    reinterpret_cast<const float4_ *>(d.pv2), prim_count, build->leaf_size, &gw, &ms);
+                for (void *p : {gw.nodes, gw.tv0, gw.tv1, gw.tv2})
+                        if (p) scene->allocs.push_back(p);
+                if (st != GZG_OK) return st;
+                d.wide = reinterpret_cast<const uint4 *>(gw.nodes);
+                d.tv0 = reinterpret_cast<const float4 *>(gw.tv0);
+                d.tv1 = reinterpret_cast<const float4 *>(gw.tv1);
+                d.tv2 = reinterpret_cast<const float4 *>(gw.tv2);
+                scene->info.device_bytes += (int64_t)gw.node_count * (int64_t)sizeof(WideNode) + 48 * (int64_t)gw.tri_count;
+                scene->build_ms = ms;
+                // host copy (two-level and batch assembly read it)
+                wide.nodes.resize(gw.node_count);
+                wide.v0.resize(gw.tri_count);
+                wide.v1.resize(gw.tri_count);
+                wide.v2.resize(gw.tri_count);
+                wide.depth = gw.depth;
+                GZG_CK(cudaMemcpy(wide.nodes.data(), gw.nodes, gw.node_count * sizeof(WideNode), cudaMemcpyDeviceToHost),
+                       "gzg_gpu_build_scene: tree download");
+                GZG_CK(cudaMemcpy(wide.v0.data(), gw.tv0, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost),
+                       "gzg_gpu_build_scene: tree download");
+                GZG_CK(cudaMemcpy(wide.v1.data(), gw.tv1, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost),
+                       "gzg_gpu_build_scene: tree download");
+                GZG_CK(cudaMemcpy(wide.v2.data(), gw.tv2, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost),
+                       "gzg_gpu_build_scene: tree download");
+        }
+        d.bvh2_count = build ? 0 : bvh2_node_count;
         d.prim_count = prim_count;
         d.wide_count = (uint32_t)wide.nodes.size();
 
         gzg_scene_info &info = scene->info;
-        info.bvh2_nodes = bvh2_node_count;
+        info.bvh2_nodes = build ? 0 : bvh2_node_count;
         info.prims = prim_count;
         info.triangles = (int64_t)wide.v0.size();
         info.wide_nodes = (int64_t)wide.nodes.size();
@@ -487,9 +546,30 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         if (st != GZG_OK) return st;
         d.mesh_sizes = ms;
         d.mesh_count = mesh_count;
-        for (int a = 0; a < 3; ++a) {
-                scene->root_bounds[a] = bvh2_nodes[0].bounds_min[a];
-                scene->root_bounds[3 + a] = bvh2_nodes[0].bounds_max[a];
+        if (!build) {
+                for (int a = 0; a < 3; ++a) {
+                        scene->root_bounds[a] = bvh2_nodes[0].bounds_min[a];
+                        scene->root_bounds[3 + a] = bvh2_nodes[0].bounds_max[a];
+                }
+        } else {
+                float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                for (int64_t k = 0; k < prim_count; ++k) {
+                        int flag;
+                        std::memcpy(&flag, &pv0[k].w, 4);
+                        if (flag != 1) continue;
+                        const float4_ *v[3] = {&pv0[k], &pv1[k], &pv2[k]};
+                        for (int c = 0; c < 3; ++c) {
+                                const float xyz[3] = {v[c]->x, v[c]->y, v[c]->z};
+                                for (int a = 0; a < 3; ++a) {
+                                        lo[a] = std::min(lo[a], xyz[a]);
+                                        hi[a] = std::max(hi[a], xyz[a]);
+                                }
+                        }
+                }
+                for (int a = 0; a < 3; ++a) {
+                        scene->root_bounds[a] = lo[a];
+                        scene->root_bounds[3 + a] = hi[a];
+                }
         }
         scene->host_wide = std::move(wide);
         HostShading &hsd = scene->host_shading;
@@ -502,6 +582,74 @@ GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t
         hsd.light_cdf = std::move(cdf);
         hsd.light_total = total;
         *out_scene = scene.release();
+        return clear_error();
+}
+
+}  // namespace
+
+GZG_API gzg_status gzg_gpu_upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count,
+                                        const gzg_prim_id *prim_ids, int64_t prim_count,
+                                        const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                                        const int64_t *mesh_points_counts, const int64_t *mesh_face_indices_counts,
+                                        const int64_t *mesh_vertex_indices_counts, const gzg_material *materials,
+                                        int64_t material_count, gzg_scene **out_scene) {
+        (void)mesh_face_indices_counts;
+        return upload_scene(bvh2_nodes, bvh2_node_count, prim_ids, prim_count, meshes, mesh_count, mesh_points_counts,
+                            mesh_vertex_indices_counts, materials, material_count, nullptr, out_scene,
+                            "gzg_gpu_upload_scene");
+}
+
+GZG_API gzg_status gzg_gpu_build_scene(const gzg_prim_id *prim_ids, int64_t prim_count,
+                                       const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                                       const int64_t *mesh_points_counts, const int64_t *mesh_face_indices_counts,
+                                       const int64_t *mesh_vertex_indices_counts, const gzg_material *materials,
+                                       int64_t material_count, const gzg_build_options *options,
+                                       gzg_scene **out_scene) {
+        (void)mesh_face_indices_counts;
+        const gzg_build_options defaults{};
+        return upload_scene(nullptr, 0, prim_ids, prim_count, meshes, mesh_count, mesh_points_counts,
+                            mesh_vertex_indices_counts, materials, material_count, options ? options : &defaults,
+                            out_scene, "gzg_gpu_build_scene");
+}
+
+GZG_API gzg_status gzg_scene_build_time(const gzg_scene *scene, float *device_ms) {
+        if (!scene || !device_ms) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_build_time: null argument");
+        *device_ms = scene->build_ms;
+        return clear_error();
+}
+
+// Surface-area cost of the wide tree (quantised boxes, relative to the
+// root's box): interior children cost 1 per unit area, leaf triangles 1 each.
+GZG_API gzg_status gzg_scene_tree_cost(const gzg_scene *scene, double *cost) {
+        if (!scene || !cost) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_tree_cost: null argument");
+        const WideBvh &w = scene->host_wide;
+        double root_area = 0.0, sum = 0.0;
+        for (size_t i = 0; i < w.nodes.size(); ++i) {
+                const WideNode &nd = w.nodes[i];
+                const float p[3] = {nd.px, nd.py, nd.pz};
+                const int e[3] = {nd.ex, nd.ey, nd.ez};
+                double nlo[3] = {INFINITY, INFINITY, INFINITY}, nhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                for (int s = 0; s < 8; ++s) {
+                        const bool interior = (nd.imask >> s) & 1u, leaf = (nd.meta[s] & 0x80u) != 0;
+                        if (!interior && !leaf) continue;
+                        double lo[3], hi[3];
+                        for (int a = 0; a < 3; ++a) {
+                                const double step = std::ldexp(1.0, e[a] - 127);
+                                lo[a] = p[a] + step * nd.qlo[a][s];
+                                hi[a] = p[a] + step * nd.qhi[a][s];
+                                nlo[a] = std::min(nlo[a], lo[a]);
+                                nhi[a] = std::max(nhi[a], hi[a]);
+                        }
+                        const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+                        const double area = 2.0 * (dx * dy + dx * dz + dy * dz);
+                        sum += interior ? area : area * (double)(((nd.meta[s] >> 5) & 3u) + 1u);
+                }
+                if (i == 0) {
+                        const double dx = nhi[0] - nlo[0], dy = nhi[1] - nlo[1], dz = nhi[2] - nlo[2];
+                        root_area = 2.0 * (dx * dy + dx * dz + dy * dz);
+                }
+        }
+        *cost = root_area > 0.0 ? 1.0 + sum / root_area : 0.0;
         return clear_error();
 }
 

@@ -1,0 +1,548 @@
+// gpu_build.cu - builds a scene's 8-wide quantised tree on the device.
+//
+// The reference builds its BVH2 on the host with a binned SAH
+// (Accelerators/BoundingHierarchyBuilder.swift:199-339); this is the device
+// alternative for scenes that arrive without one (a linear BVH):
+//   1. per prim: bounds, centroid, and the scene's centroid bounds
+//      (order-preserving integer atomics);
+//   2. a 64-bit key per intersectable prim: 30-bit Morton code of the
+//      centroid in the upper half, the prim index in the lower half (unique
+//      keys, a deterministic order); other prims sort last;
+//   3. a radix sort of the keys (CUB);
+//   4. the binary radix tree over the sorted keys (Karras 2012: one thread
+//      per internal node finds its range and split from common-prefix
+//      lengths);
+//   5. node bounds bottom-up (one thread per leaf; the second of two
+//      children to arrive at a node computes it);
+//   6. collapse into wide nodes level by level, as the host converter does
+//      (wide_bvh.cpp): a wide node opens the interior child of largest
+//      surface area until it has 8 children; a binary node covering at most
+//      leaf_size prims is a leaf; children go to octant slots and their
+//      boxes are quantised outward to 8 bits per plane.
+// The result uses the host converter's layout exactly (WideNode, leaf-order
+// triangle records with the prim index in v0.w), so every traversal kernel
+// runs on it unchanged.
+#include <cub/cub.cuh>
+#include <math_constants.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "device.cuh"
+#include "gzg_internal.h"
+
+namespace gzg {
+namespace {
+
+gzg_status build_fail(cudaError_t e, const char *what) {
+        const gzg_status code = (e == cudaErrorMemoryAllocation) ? GZG_ERR_OUT_OF_MEMORY : GZG_ERR_CUDA;
+        return set_error(code, std::string("gzg_gpu_build_scene: ") + what + ": " + cudaGetErrorString(e));
+}
+
+#define GZG_CK(call, what)                                   \
+        do {                                                 \
+                cudaError_t e_ = (call);                     \
+                if (e_ != cudaSuccess) return build_fail(e_, what); \
+        } while (0)
+
+constexpr uint64_t kInvalidKey = ~0ull;
+
+// float <-> int keeping the order of all non-NaN floats
+__device__ __forceinline__ int ord_int(float f) {
+        const int i = __float_as_int(f);
+        return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float ord_float(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF); }
+
+__device__ __forceinline__ bool prim_valid(const float4 &a) { return __float_as_int(a.w) == 1; }
+
+// Prim bounds (lo in .xyz of box[2k], hi in box[2k+1]) and the centroid
+// bounds (6 ordered ints: lo xyz, -hi xyz ... stored as min of lo and min of
+// -hi so one atomicMin serves both).
+__global__ void k_prim_bounds(const float4 *__restrict__ pv0, const float4 *__restrict__ pv1,
+                              const float4 *__restrict__ pv2, int64_t n, float4 *__restrict__ box,
+                              int *__restrict__ cb, unsigned long long *__restrict__ n_valid) {
+        const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        float c[3] = {0, 0, 0};
+        bool ok = false;
+        if (k < n) {
+                const float4 a = pv0[k], b = pv1[k], d = pv2[k];
+                ok = prim_valid(a);
+                const float lo[3] = {fminf(a.x, fminf(b.x, d.x)), fminf(a.y, fminf(b.y, d.y)), fminf(a.z, fminf(b.z, d.z))};
+                const float hi[3] = {fmaxf(a.x, fmaxf(b.x, d.x)), fmaxf(a.y, fmaxf(b.y, d.y)), fmaxf(a.z, fmaxf(b.z, d.z))};
+                box[2 * k] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+                box[2 * k + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+                for (int i = 0; i < 3; ++i) c[i] = 0.5f * lo[i] + 0.5f * hi[i];
+        }
+        // block reduction of the centroid bounds of valid prims
+        typedef cub::BlockReduce<int, 256> Reduce;
+        __shared__ typename Reduce::TempStorage tmp;
+        __shared__ int res[6];
+        unsigned cnt = __syncthreads_count(ok ? 1 : 0);
+        for (int i = 0; i < 6; ++i) {
+                const int v = ok ? (i < 3 ? ord_int(c[i]) : ord_int(-c[i - 3])) : INT_MAX;
+                const int r = Reduce(tmp).Reduce(v, cub::Min());
+                if (threadIdx.x == 0) res[i] = r;
+                __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+                for (int i = 0; i < 6; ++i)
+                        if (res[i] != INT_MAX) atomicMin(cb + i, res[i]);
+                if (cnt) atomicAdd(n_valid, (unsigned long long)cnt);
+        }
+}
+
+// Spreads the low 10 bits of v to every third bit.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+        v &= 0x3FFu;
+        v = (v | (v << 16)) & 0x030000FFu;
+        v = (v | (v << 8)) & 0x0300F00Fu;
+        v = (v | (v << 4)) & 0x030C30C3u;
+        v = (v | (v << 2)) & 0x09249249u;
+        return v;
+}
+
+__global__ void k_keys(const float4 *__restrict__ pv0, const float4 *__restrict__ box, int64_t n,
+                       const int *__restrict__ cb, uint64_t *__restrict__ keys) {
+        const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (k >= n) return;
+        if (!prim_valid(pv0[k])) {
+                keys[k] = kInvalidKey;
+                return;
+        }
+        const float4 lo = box[2 * k], hi = box[2 * k + 1];
+        const float c[3] = {0.5f * lo.x + 0.5f * hi.x, 0.5f * lo.y + 0.5f * hi.y, 0.5f * lo.z + 0.5f * hi.z};
+        uint32_t q[3];
+        for (int i = 0; i < 3; ++i) {
+                const float a = ord_float(cb[i]), b = -ord_float(cb[3 + i]);
+                const float ext = b - a;
+                float t = ext > 0.0f ? (c[i] - a) / ext : 0.0f;
+                t = fminf(fmaxf(t, 0.0f), 1.0f);
+                q[i] = (uint32_t)fminf(t * 1024.0f, 1023.0f);
+        }
+        const uint32_t m = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+        keys[k] = ((uint64_t)m << 32) | (uint64_t)(uint32_t)k;
+}
+
+// Common-prefix length of sorted keys i and j (-1 outside [0, m)).
+__device__ __forceinline__ int prefix(const uint64_t *__restrict__ k, int m, int i, int j) {
+        if (j < 0 || j >= m) return -1;
+        return __clzll(k[i] ^ k[j]);
+}
+
+// Binary radix tree: internal node i (0 .. m-2) gets children (>= 0:
+// internal node, < 0: ~leaf) and its sorted range [first, last].
+__global__ void k_radix_tree(const uint64_t *__restrict__ keys, int m, int2 *__restrict__ child,
+                             int2 *__restrict__ range, int *__restrict__ parent_int, int *__restrict__ parent_leaf) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= m - 1) return;
+        const int d = prefix(keys, m, i, i + 1) - prefix(keys, m, i, i - 1) >= 0 ? 1 : -1;
+        const int dmin = prefix(keys, m, i, i - d);
+        int lmax = 2;
+        while (prefix(keys, m, i, i + lmax * d) > dmin) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+                if (prefix(keys, m, i, i + (l + t) * d) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = prefix(keys, m, i, j);
+        int s = 0, t = l;
+        do {
+                t = (t + 1) >> 1;
+                if (prefix(keys, m, i, i + (s + t) * d) > dnode) s += t;
+        } while (t > 1);
+        const int gamma = i + s * d + min(d, 0);
+        const int first = min(i, j), last = max(i, j);
+        const int left = first == gamma ? ~gamma : gamma;
+        const int right = last == gamma + 1 ? ~(gamma + 1) : gamma + 1;
+        child[i] = make_int2(left, right);
+        range[i] = make_int2(first, last);
+        if (left >= 0)
+                parent_int[left] = i;
+        else
+                parent_leaf[~left] = i;
+        if (right >= 0)
+                parent_int[right] = i;
+        else
+                parent_leaf[~right] = i;
+}
+
+__device__ __forceinline__ void code_box(int code, const float4 *__restrict__ nbox, const float4 *__restrict__ pbox,
+                                         const uint64_t *__restrict__ keys, float4 &lo, float4 &hi) {
+        if (code >= 0) {
+                lo = __ldcg(nbox + 2 * code);
+                hi = __ldcg(nbox + 2 * code + 1);
+        } else {
+                const uint32_t p = (uint32_t)(keys[~code] & 0xFFFFFFFFu);
+                lo = pbox[2 * (size_t)p];
+                hi = pbox[2 * (size_t)p + 1];
+        }
+}
+
+// Bottom-up node bounds: one thread per leaf climbs while it is the second
+// child to arrive.  Every climb ends (each node admits one second arrival).
+__global__ void k_refit(const uint64_t *__restrict__ keys, int m, const int2 *__restrict__ child,
+                        const int *__restrict__ parent_int, const int *__restrict__ parent_leaf,
+                        const float4 *__restrict__ pbox, float4 *__restrict__ nbox, int *__restrict__ arrivals) {
+        const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+        if (leaf >= m || m < 2) return;
+        int node = parent_leaf[leaf];
+        for (int guard = 0; guard < m && node >= 0; ++guard) {
+                __threadfence();
+                if (atomicAdd(arrivals + node, 1) == 0) return;
+                const int2 c = child[node];
+                float4 l0, h0, l1, h1;
+                code_box(c.x, nbox, pbox, keys, l0, h0);
+                code_box(c.y, nbox, pbox, keys, l1, h1);
+                nbox[2 * node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+                nbox[2 * node + 1] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+                node = node == 0 ? -1 : parent_int[node];
+        }
+}
+
+struct Tree {
+        const uint64_t *keys;
+        int m;
+        const int2 *child, *range;
+        const float4 *nbox, *pbox;
+        const float4 *pv0, *pv1, *pv2;
+        int leaf_size;
+};
+
+__device__ __forceinline__ int code_count(const Tree &t, int code) {
+        if (code < 0) return 1;
+        const int2 r = t.range[code];
+        return r.y - r.x + 1;
+}
+__device__ __forceinline__ int code_first(const Tree &t, int code) { return code < 0 ? ~code : t.range[code].x; }
+__device__ __forceinline__ bool code_leaf(const Tree &t, int code) { return code_count(t, code) <= t.leaf_size; }
+__device__ __forceinline__ void code_bounds(const Tree &t, int code, double lo[3], double hi[3]) {
+        float4 l, h;
+        code_box(code, t.nbox, t.pbox, t.keys, l, h);
+        lo[0] = l.x;
+        lo[1] = l.y;
+        lo[2] = l.z;
+        hi[0] = h.x;
+        hi[1] = h.y;
+        hi[2] = h.z;
+}
+__device__ __forceinline__ double code_area(const Tree &t, int code) {
+        double lo[3], hi[3];
+        code_bounds(t, code, lo, hi);
+        const double x = hi[0] - lo[0], y = hi[1] - lo[1], z = hi[2] - lo[2];
+        return 2.0 * (x * y + x * z + y * z);
+}
+
+// quantise_axis of wide_bvh.cpp on the device (same arithmetic in double).
+__device__ void quantise_axis_dev(const double *clo, const double *chi, int n, float *p_out, uint8_t *e_out,
+                                  uint8_t *qlo, uint8_t *qhi) {
+        double lo = CUDART_INF, hi = -CUDART_INF;
+        for (int i = 0; i < n; ++i) {
+                lo = fmin(lo, clo[i]);
+                hi = fmax(hi, chi[i]);
+        }
+        const double mag = fmax(fabs(lo), fabs(hi));
+        double margin = ldexp(fmax(mag, hi - lo), -18);
+        if (!(margin > 0)) margin = 1e-30;
+        float p = (float)(lo - margin);
+        while ((double)p > lo - margin) p = nextafterf(p, -CUDART_INF_F);
+        const double span = (hi + margin) - (double)p;
+        int k = (int)ceil(log2(span / 255.0));
+        k = max(k, -126);
+        while (ldexp(255.0, k) < span) ++k;
+        k = min(k, 127);
+        const double s = ldexp(1.0, k);
+        *p_out = p;
+        *e_out = (uint8_t)(k + 127);
+        for (int i = 0; i < n; ++i) {
+                const double a = floor((clo[i] - margin - (double)p) / s);
+                const double b = ceil((chi[i] + margin - (double)p) / s);
+                qlo[i] = (uint8_t)fmin(255.0, fmax(0.0, a));
+                qhi[i] = (uint8_t)fmin(255.0, fmax(0.0, b));
+        }
+}
+
+// One level of the collapse: item = (binary code, wide node index).
+__global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_t *__restrict__ n_items,
+                           int2 *__restrict__ next, uint32_t *__restrict__ n_next, uint32_t *__restrict__ counters,
+                           WideNode *__restrict__ nodes, float4 *__restrict__ tv0, float4 *__restrict__ tv1,
+                           float4 *__restrict__ tv2, uint32_t node_cap, uint32_t tri_cap, uint32_t *__restrict__ err) {
+        const uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+        if (it >= *n_items) return;
+        const int2 item = items[it];
+        int kids[8];
+        int n = 0;
+        if (t.m == 0) {
+                n = 0;
+        } else if (code_leaf(t, item.x)) {
+                kids[n++] = item.x;
+        } else {
+                const int2 c = t.child[item.x];
+                kids[n++] = c.x;
+                kids[n++] = c.y;
+                while (n < 8) {
+                        int best = -1;
+                        double best_a = -1.0;
+                        for (int i = 0; i < n; ++i)
+                                if (!code_leaf(t, kids[i])) {
+                                        const double a = code_area(t, kids[i]);
+                                        if (a > best_a) {
+                                                best_a = a;
+                                                best = i;
+                                        }
+                                }
+                        if (best < 0) break;
+                        const int2 c2 = t.child[kids[best]];
+                        for (int i = n; i > best + 1; --i) kids[i] = kids[i - 1];
+                        kids[best] = c2.x;
+                        kids[best + 1] = c2.y;
+                        ++n;
+                }
+        }
+        // child boxes and octant slots (assign_slots of wide_bvh.cpp)
+        double clo[8][3], chi[8][3], cc[8][3], pc[3] = {0, 0, 0};
+        for (int k = 0; k < n; ++k) {
+                code_bounds(t, kids[k], clo[k], chi[k]);
+                for (int a = 0; a < 3; ++a) {
+                        cc[k][a] = 0.5 * (clo[k][a] + chi[k][a]);
+                        pc[a] += cc[k][a] / n;
+                }
+        }
+        int kid_in_slot[8];
+        bool kdone[8], sdone[8];
+        for (int i = 0; i < 8; ++i) {
+                kid_in_slot[i] = -1;
+                kdone[i] = sdone[i] = false;
+        }
+        for (int round = 0; round < n; ++round) {
+                // the smallest cost -d over free pairs, ties to the lowest (k, s)
+                // index as the host's stable sort does
+                double best = CUDART_INF;
+                int bk = -1, bs = -1;
+                for (int k = 0; k < n; ++k) {
+                        if (kdone[k]) continue;
+                        for (int s = 0; s < 8; ++s) {
+                                if (sdone[s]) continue;
+                                double d = 0;
+                                for (int a = 0; a < 3; ++a) d += (cc[k][a] - pc[a]) * ((s >> a) & 1 ? 1.0 : -1.0);
+                                if (-d < best) {
+                                        best = -d;
+                                        bk = k;
+                                        bs = s;
+                                }
+                        }
+                }
+                kdone[bk] = sdone[bs] = true;
+                kid_in_slot[bs] = bk;
+        }
+        WideNode w;
+        memset(&w, 0, sizeof(w));
+        int m = 0, order[8];
+        double ql[3][8], qh[3][8];
+        for (int s = 0; s < 8; ++s)
+                if (kid_in_slot[s] >= 0) {
+                        const int k = kid_in_slot[s];
+                        for (int a = 0; a < 3; ++a) {
+                                ql[a][m] = clo[k][a];
+                                qh[a][m] = chi[k][a];
+                        }
+                        order[m++] = s;
+                }
+        float pxyz[3] = {0, 0, 0};
+        uint8_t ee[3] = {127, 127, 127};
+        for (int a = 0; a < 3; ++a) {
+                uint8_t qlo8[8], qhi8[8];
+                if (m > 0) quantise_axis_dev(ql[a], qh[a], m, &pxyz[a], &ee[a], qlo8, qhi8);
+                for (int s = 0; s < 8; ++s) {
+                        w.qlo[a][s] = 255;
+                        w.qhi[a][s] = 0;
+                }
+                for (int i = 0; i < m; ++i) {
+                        w.qlo[a][order[i]] = qlo8[i];
+                        w.qhi[a][order[i]] = qhi8[i];
+                }
+        }
+        w.px = pxyz[0];
+        w.py = pxyz[1];
+        w.pz = pxyz[2];
+        w.ex = ee[0];
+        w.ey = ee[1];
+        w.ez = ee[2];
+        int n_int = 0, n_tri = 0;
+        for (int k = 0; k < n; ++k) {
+                if (code_leaf(t, kids[k]))
+                        n_tri += code_count(t, kids[k]);
+                else
+                        ++n_int;
+        }
+        const uint32_t cbase = n_int ? atomicAdd(counters + 0, (uint32_t)n_int) : 0u;
+        const uint32_t tbase = n_tri ? atomicAdd(counters + 1, (uint32_t)n_tri) : 0u;
+        if (cbase + (uint32_t)n_int > node_cap || tbase + (uint32_t)n_tri > tri_cap) {
+                atomicOr(err, kErrBadIndex);
+                return;
+        }
+        w.child_base = cbase;
+        w.tri_base = tbase;
+        uint32_t tri_off = 0, int_rank = 0;
+        for (int s = 0; s < 8; ++s) {
+                const int k = kid_in_slot[s];
+                if (k < 0) continue;
+                const int code = kids[k];
+                if (!code_leaf(t, code)) {
+                        w.imask |= (uint8_t)(1u << s);
+                        const uint32_t q = atomicAdd(n_next, 1u);
+                        next[q] = make_int2(code, (int)(cbase + int_rank));
+                        ++int_rank;
+                } else {
+                        const int cnt = code_count(t, code), first = code_first(t, code);
+                        w.meta[s] = (uint8_t)(0x80u | ((uint32_t)(cnt - 1) << 5) | tri_off);
+                        for (int j = 0; j < cnt; ++j) {
+                                const uint32_t p = (uint32_t)(t.keys[first + j] & 0xFFFFFFFFu);
+                                float4 a = t.pv0[p];
+                                a.w = __int_as_float((int)p);
+                                float4 b = t.pv1[p], c = t.pv2[p];
+                                b.w = 0.0f;
+                                c.w = 0.0f;
+                                tv0[tbase + tri_off + j] = a;
+                                tv1[tbase + tri_off + j] = b;
+                                tv2[tbase + tri_off + j] = c;
+                        }
+                        tri_off += (uint32_t)cnt;
+                }
+        }
+        nodes[item.y] = w;
+}
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count, std::vector<void *> &tmp) {
+        void *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, std::max<size_t>(count * sizeof(T), 16));
+        if (e == cudaSuccess) tmp.push_back(d);
+        *p = reinterpret_cast<T *>(d);
+        return e;
+}
+
+}  // namespace
+
+gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ *pv2, int64_t n, int leaf_size,
+                          GpuWide *out, float *device_ms) {
+        std::vector<void *> tmp;
+        struct Free {
+                std::vector<void *> &v;
+                ~Free() {
+                        for (void *p : v) cudaFree(p);
+                }
+        } free_tmp{tmp};
+        *out = GpuWide{};
+        if (n < 0 || n >= INT32_MAX) return set_error(GZG_ERR_LIMIT, "gzg_gpu_build_scene: prim count out of range");
+        if (leaf_size < 1 || leaf_size > 4) leaf_size = 4;
+        cudaStream_t st = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        struct Ev {
+                cudaEvent_t a, b;
+                ~Ev() {
+                        if (a) cudaEventDestroy(a);
+                        if (b) cudaEventDestroy(b);
+                }
+        } ev{e0, e1};
+        const float4 *d0 = reinterpret_cast<const float4 *>(pv0), *d1 = reinterpret_cast<const float4 *>(pv1),
+                     *d2 = reinterpret_cast<const float4 *>(pv2);
+        float4 *pbox;
+        int *cb;
+        unsigned long long *nvalid;
+        uint64_t *keys, *sorted;
+        GZG_CK(dalloc(&pbox, 2 * (size_t)n, tmp), "build: prim bounds");
+        GZG_CK(dalloc(&cb, 6, tmp), "build: centroid bounds");
+        GZG_CK(dalloc(&nvalid, 1, tmp), "build: prim count");
+        GZG_CK(dalloc(&keys, (size_t)n, tmp), "build: keys");
+        GZG_CK(dalloc(&sorted, (size_t)n, tmp), "build: keys");
+        cudaEventRecord(e0, st);
+        const int B = 256;
+        const unsigned grid = (unsigned)((n + B - 1) / B);
+        GZG_CK(cudaMemsetAsync(cb, 0x7F, 6 * sizeof(int), st), "build: reset");
+        GZG_CK(cudaMemsetAsync(nvalid, 0, sizeof(unsigned long long), st), "build: reset");
+        if (n > 0) {
+                k_prim_bounds<<<grid, B, 0, st>>>(d0, d1, d2, n, pbox, cb, nvalid);
+                k_keys<<<grid, B, 0, st>>>(d0, pbox, n, cb, keys);
+                size_t temp_bytes = 0;
+                cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys, sorted, (int)n, 0, 64, st);
+                void *temp;
+                GZG_CK(dalloc(reinterpret_cast<uint8_t **>(&temp), temp_bytes, tmp), "build: sort scratch");
+                GZG_CK(cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys, sorted, (int)n, 0, 64, st), "build: sort");
+        }
+        unsigned long long hv = 0;
+        GZG_CK(cudaMemcpyAsync(&hv, nvalid, sizeof(hv), cudaMemcpyDeviceToHost, st), "build: prim count");
+        GZG_CK(cudaStreamSynchronize(st), "build: prim count");
+        const int m = (int)hv;
+        int2 *child, *range;
+        int *parent_int, *parent_leaf, *arrivals;
+        float4 *nbox;
+        const size_t ni = (size_t)std::max(m - 1, 1);
+        GZG_CK(dalloc(&child, ni, tmp), "build: radix tree");
+        GZG_CK(dalloc(&range, ni, tmp), "build: radix tree");
+        GZG_CK(dalloc(&parent_int, ni, tmp), "build: radix tree");
+        GZG_CK(dalloc(&parent_leaf, (size_t)std::max(m, 1), tmp), "build: radix tree");
+        GZG_CK(dalloc(&arrivals, ni, tmp), "build: radix tree");
+        GZG_CK(dalloc(&nbox, 2 * ni, tmp), "build: node bounds");
+        GZG_CK(cudaMemsetAsync(arrivals, 0, ni * sizeof(int), st), "build: reset");
+        if (m >= 2) {
+                k_radix_tree<<<(unsigned)((m - 1 + B - 1) / B), B, 0, st>>>(sorted, m, child, range, parent_int,
+                                                                            parent_leaf);
+                k_refit<<<(unsigned)((m + B - 1) / B), B, 0, st>>>(sorted, m, child, parent_int, parent_leaf, pbox,
+                                                                   nbox, arrivals);
+        }
+        // wide nodes: at most one per binary internal node (and one root)
+        const uint32_t node_cap = (uint32_t)std::max(m, 1), tri_cap = (uint32_t)std::max(m, 1);
+        WideNode *nodes;
+        float4 *tv0, *tv1, *tv2;
+        int2 *qa, *qb;
+        uint32_t *counts;  // [0] nodes used, [1] tris used, [2] items in, [3] items out
+        uint32_t *err;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&nodes), (size_t)node_cap * sizeof(WideNode)), "build: wide nodes");
+        out->nodes = nodes;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv0), (size_t)tri_cap * sizeof(float4)), "build: triangles");
+        out->tv0 = tv0;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv1), (size_t)tri_cap * sizeof(float4)), "build: triangles");
+        out->tv1 = tv1;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv2), (size_t)tri_cap * sizeof(float4)), "build: triangles");
+        out->tv2 = tv2;
+        GZG_CK(dalloc(&qa, node_cap, tmp), "build: queue");
+        GZG_CK(dalloc(&qb, node_cap, tmp), "build: queue");
+        GZG_CK(dalloc(&counts, 4, tmp), "build: counters");
+        GZG_CK(dalloc(&err, 1, tmp), "build: error word");
+        const uint32_t init[4] = {1u, 0u, 1u, 0u};  // the root is node 0
+        GZG_CK(cudaMemcpyAsync(counts, init, sizeof(init), cudaMemcpyHostToDevice, st), "build: counters");
+        GZG_CK(cudaMemsetAsync(err, 0, 4, st), "build: error word");
+        const int2 root = make_int2(m >= 2 ? 0 : ~0, 0);
+        GZG_CK(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st), "build: queue");
+        Tree t{sorted, m, child, range, nbox, pbox, d0, d1, d2, leaf_size};
+        uint32_t level_items = 1;
+        int depth = 0;
+        while (level_items > 0) {
+                if (++depth > 64) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: tree deeper than 64 levels");
+                GZG_CK(cudaMemsetAsync(counts + 3, 0, 4, st), "build: counters");
+                k_collapse<<<(level_items + 127) / 128, 128, 0, st>>>(t, qa, counts + 2, qb, counts + 3, counts, nodes,
+                                                                     tv0, tv1, tv2, node_cap, tri_cap, err);
+                GZG_CK(cudaMemcpyAsync(counts + 2, counts + 3, 4, cudaMemcpyDeviceToDevice, st), "build: counters");
+                GZG_CK(cudaMemcpyAsync(&level_items, counts + 3, 4, cudaMemcpyDeviceToHost, st), "build: counters");
+                GZG_CK(cudaStreamSynchronize(st), "build: collapse");
+                std::swap(qa, qb);
+        }
+        cudaEventRecord(e1, st);
+        uint32_t hc[2], herr = 0;
+        GZG_CK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, st), "build: counters");
+        GZG_CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st), "build: error word");
+        GZG_CK(cudaStreamSynchronize(st), "build");
+        if (herr) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: collapse ran out of node or triangle slots");
+        if (hc[1] != (uint32_t)m)
+                return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: leaves do not cover every prim");
+        out->node_count = hc[0];
+        out->tri_count = hc[1];
+        out->depth = depth;
+        cudaEventElapsedTime(device_ms, e0, e1);
+        return clear_error();
+}
+
+}  // namespace gzg

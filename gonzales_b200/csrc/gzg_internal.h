@@ -72,6 +72,22 @@ struct HostShading {
         float light_total_env = 0.0f;  // light_total + env_power
 };
 
+// A wide tree built on the device (gpu_build.cu): device arrays the caller
+// takes ownership of (cudaFree), in the WideBvh layout.
+struct GpuWide {
+        void *nodes = nullptr;                      // node_count WideNode records
+        void *tv0 = nullptr, *tv1 = nullptr, *tv2 = nullptr;  // tri_count leaf-order records
+        uint32_t node_count = 0, tri_count = 0;
+        int32_t depth = 0;
+};
+
+// Builds the wide tree over device prim-order triangles pv0/pv1/pv2 (pv0.w =
+// int 1 for prims the traversal tests) with at most leaf_size (1..4) prims
+// per leaf; device_ms = the build's device time.  On an error the arrays
+// already allocated are in *out.
+gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ *pv2, int64_t n, int leaf_size,
+                          GpuWide *out, float *device_ms);
+
 // Converts a validated reference BVH2 + prims + meshes into the wide layout.
 // Returns GZG_OK or an error (with set_error called).
 gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const gzg_prim_id *prims,

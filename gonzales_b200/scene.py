@@ -91,6 +91,21 @@ class HostScene:
     prim_order: np.ndarray  # k-th leaf prim = input prim prim_order[k]
     material_params: np.ndarray = None  # (n_materials, MATERIAL_PARAMS_WIDTH) float32
 
+    def root_bounds(self):
+        """(lo[3], hi[3]) of the scene: the BVH2 root's box, or the
+        triangles' bounds when the tree is built on the device."""
+        if self.nodes is not None:
+            return self.nodes[0]["bounds_min"], self.nodes[0]["bounds_max"]
+        lo = np.full(3, np.inf, np.float32)
+        hi = np.full(3, -np.inf, np.float32)
+        for m in self.meshes:
+            p = np.asarray(m.points, np.float32).reshape(-1, 4)[:, :3]
+            used = p[np.asarray(m.vertex_indices, np.int64).reshape(-1)]
+            if len(used):
+                lo = np.minimum(lo, used.min(0))
+                hi = np.maximum(hi, used.max(0))
+        return lo, hi
+
     @property
     def has_extended_materials(self):
         return bool(np.isin(self.materials["type"], EXTENDED_MATERIALS).any())
@@ -169,7 +184,10 @@ class SceneBuilder:
         self._prims.append((idx, mesh.triangle_count, PRIM_AREA_LIGHT, None, first_light))
         return idx
 
-    def build(self, threads=0):
+    def build(self, threads=0, host_bvh=True):
+        """The HostScene.  host_bvh=False skips the host's SAH build: prims
+        stay in input order and nodes is None, for the device build
+        (GpuAccelerator builds the tree with gzg_gpu_build_scene)."""
         n_surface = len(self._materials)
         mats = np.zeros(n_surface + len(self._lights), F.MATERIAL_DTYPE)
         for i, (t, a, e) in enumerate(self._materials):
@@ -193,11 +211,14 @@ class SceneBuilder:
                 prims["material_index"][sl] = material
             bounds[sl] = triangle_bounds(self.meshes[mesh_idx])
             k += ntri
-        nodes, order = build_bvh2(bounds, threads)
-        # Reorder whole 32-byte records (a field-wise structured copy would
-        # leave the padding bytes undefined).
-        raw = prims.view(np.uint8).reshape(-1, F.PRIM_ID_DTYPE.itemsize)[order]
-        sorted_prims = np.ascontiguousarray(raw).view(F.PRIM_ID_DTYPE).reshape(-1)
+        if host_bvh:
+            nodes, order = build_bvh2(bounds, threads)
+            # Reorder whole 32-byte records (a field-wise structured copy would
+            # leave the padding bytes undefined).
+            raw = prims.view(np.uint8).reshape(-1, F.PRIM_ID_DTYPE.itemsize)[order]
+            sorted_prims = np.ascontiguousarray(raw).view(F.PRIM_ID_DTYPE).reshape(-1)
+        else:
+            nodes, order, sorted_prims = None, np.arange(total, dtype=np.int64), prims
         params = np.zeros((len(mats), MATERIAL_PARAMS_WIDTH), np.float32)
         if self._material_params:
             params[:n_surface] = np.asarray(self._material_params, np.float32)

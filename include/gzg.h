@@ -338,6 +338,39 @@ GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const
 GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
                                              float scale);
 
+/* Options of gzg_gpu_build_scene. */
+typedef struct gzg_build_options {
+        int32_t leaf_size;   /* prims per leaf, 1..4; 0 = 4 */
+        int32_t reserved[3]; /* zero */
+} gzg_build_options;
+
+/* Builds the scene's tree on the device instead of taking the host's BVH2
+ * (the replacement of BoundingHierarchyBuilder.swift:66-339 for hosts that
+ * would otherwise build it): the arguments of gzg_gpu_upload_scene without
+ * the BVH2, prims in any order.  A linear BVH (30-bit Morton codes of the
+ * prim centroids, radix tree, bottom-up bounds) collapsed on the device into
+ * the same 8-wide quantised tree the upload path makes; every query and
+ * renderer call accepts the scene, except traversal = GZG_TRAVERSAL_BVH2
+ * (there is no reference BVH2: the call fails).  Hit prim ids index
+ * prim_ids as given.  Every triangle prim must resolve to valid mesh and
+ * vertex indices (GZG_ERR_BAD_SCENE otherwise).  options may be NULL. */
+GZG_API gzg_status gzg_gpu_build_scene(const gzg_prim_id *prim_ids, int64_t prim_count,
+                                       const gzg_triangle_mesh *meshes, int64_t mesh_count,
+                                       const int64_t *mesh_points_counts, const int64_t *mesh_face_indices_counts,
+                                       const int64_t *mesh_vertex_indices_counts, const gzg_material *materials,
+                                       int64_t material_count, const gzg_build_options *options,
+                                       gzg_scene **out_scene);
+
+/* Device time in ms of the tree build of a gzg_gpu_build_scene scene (keys,
+ * sort, radix tree, bounds, collapse); -1 for an uploaded scene. */
+GZG_API gzg_status gzg_scene_build_time(const gzg_scene *scene, float *device_ms);
+
+/* Surface-area cost of the scene's wide tree: 1 + sum over interior
+ * children of their box area + sum over leaf children of area x triangles,
+ * relative to the root's area (quantised boxes).  Compares trees built by
+ * different builders over the same prims. */
+GZG_API gzg_status gzg_scene_tree_cost(const gzg_scene *scene, double *cost);
+
 /* Parameters of the renderer's general materials, by Material_C.type:
  *   3 dielectric        (Material/Dielectric.swift): eta, roughness u/v;
  *   4 coated diffuse    (Material/CoatedDiffuse.swift, base = albedo): eta,

@@ -1,0 +1,173 @@
+"""The device tree build (gzg_gpu_build_scene: linear BVH over Morton codes,
+radix tree, bottom-up bounds, collapse into the wide layout) against the
+oracle's traversal of the host's SAH tree on the same rays.
+
+Closest hits do not depend on the tree: every ray is exact, a counted
+equal-t tie or a counted reference-culled hit (the parity classes of the
+traversal tests), never a miss or a farther hit.  Prim ids index the prims as
+given (any order).  Edge cases: one triangle, no intersectable prim, many
+coincident centroids (equal Morton codes), leaves of 1 to 4 prims.  A
+render of a device-built scene equals the render of the uploaded one.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gonzales_b200 import GpuAccelerator, scenes
+from gonzales_b200 import _ffi as F
+from gonzales_b200.scene import SceneBuilder
+from tests import helpers as H
+from tests.test_gpu_traversal import device_any, device_closest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    hs, o, d, t = H.small_raycast(subdiv=5, n_side=64, n_incoherent=16384)
+    isect, idx, _ = H.oracle_closest(hs, o, d, t)
+    return hs, o, d, t, isect, idx
+
+
+@pytest.mark.parametrize("leaf_size", [1, 2, 4])
+def test_device_built_tree_matches_oracle(small, leaf_size):
+    hs, o, d, t, isect, idx = small
+    with GpuAccelerator(hs, device_build=True, leaf_size=leaf_size) as acc:
+        assert acc.device_built
+        info = acc.info()
+        assert info["bvh2_nodes"] == 0 and info["triangles"] == len(hs.prims)
+        gpu = device_closest(acc, o, d, t)
+        counts, fails = H.classify(hs, o, d, t, *gpu, idx, isect["t_hit"], isect["u"], isect["v"])
+        assert counts["fail"] == 0, (counts, fails[:10])
+        assert counts["exact"] >= 0.999 * counts["rays"], counts
+        anyp = device_any(acc, o, d, t)
+        assert np.all(anyp[idx >= 0] >= 0)
+        assert acc.build_time_ms() > 0.0
+        cost = acc.tree_cost()
+        assert np.isfinite(cost) and cost > 1.0
+        assert acc.error_word() == 0
+        # no reference BVH2: the reference-order kernel is refused
+        from gonzales_b200 import GzgError, options
+
+        with pytest.raises(GzgError):
+            device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
+
+
+def _identity(hs, prim):
+    """A triangle's identity independent of prim order: (mesh << 32 | tri)."""
+    prim = np.asarray(prim, np.int64)
+    out = np.full(len(prim), -1, np.int64)
+    ok = prim >= 0
+    out[ok] = hs.prims["id2"][prim[ok]]
+    return out
+
+
+def test_prims_in_input_order(small):
+    hs_sorted, o, d, t, isect, idx = small
+    hs = scenes.raycast_scene(subdiv=5).build(host_bvh=False)
+    with GpuAccelerator(hs) as acc:
+        assert acc.device_built
+        prim, tt, u, v = device_closest(acc, o, d, t)
+    same_t = H.bits(tt) == H.bits(np.where(idx >= 0, isect["t_hit"], t))
+    same_tri = _identity(hs, prim) == _identity(hs_sorted, idx)
+    # equal t everywhere but where the oracle's slab test culled a nearer hit
+    culled = (~same_t) & (tt < np.where(idx >= 0, isect["t_hit"], np.inf)) & (prim >= 0)
+    assert np.all(same_t | culled)
+    assert same_tri[same_t].mean() > 0.999
+
+
+def _tri_builder(tris):
+    sb = SceneBuilder()
+    m = sb.add_material((0.5, 0.5, 0.5))
+    pts = np.asarray(tris, np.float32).reshape(-1, 3)
+    sb.add_mesh(pts, np.arange(len(pts)).reshape(-1, 3), m)
+    return sb
+
+
+def _tri_scene(tris):
+    return _tri_builder(tris).build(host_bvh=False)
+
+
+def test_single_triangle_and_coincident_centroids():
+    hs = _tri_scene([[[-1, -1, 0], [1, -1, 0], [0, 1, 0]]])
+    o = np.array([[0, 0, 2], [5, 5, 2]], np.float32)
+    d = np.array([[0, 0, -1], [0, 0, -1]], np.float32)
+    t = np.full(2, np.inf, np.float32)
+    with GpuAccelerator(hs) as acc:
+        prim, tt, _, _ = device_closest(acc, o, d, t)
+    assert prim.tolist() == [0, -1] and tt[0] == 2.0
+    # 300 triangles tilted about the y axis by different amounts, all with
+    # the box centre (0, 0, 0): the centroid bounds are a point, every Morton
+    # code is 0, and the keys are ordered by prim index alone
+    tris = []
+    for h in np.linspace(-0.3, 0.3, 300):
+        tris.append([[-1.0, -1.0, -h], [1.0, -1.0, h], [0.0, 1.0, 0.0]])
+    sb = _tri_builder(tris)
+    rng = np.random.default_rng(3)
+    o = np.concatenate([rng.uniform(-1, 1, (2000, 2)), np.full((2000, 1), 1.0)], 1).astype(np.float32)
+    d = np.tile(np.array([[0, 0, -1]], np.float32), (2000, 1))
+    t = np.full(2000, np.inf, np.float32)
+    isect, idx, _ = H.oracle_closest(sb.build(), o, d, t)
+    with GpuAccelerator(sb.build(host_bvh=False)) as acc:
+        prim, tt, _, _ = device_closest(acc, o, d, t)
+        assert acc.error_word() == 0
+    hit = idx >= 0
+    assert hit.any()
+    assert np.array_equal(prim >= 0, hit)
+    assert np.array_equal(H.bits(tt[hit]), H.bits(isect["t_hit"][hit]))
+
+
+def test_no_intersectable_prim():
+    # a transformed-primitive record (type 2) is never intersected
+    hs = _tri_scene([[[-1, -1, 0], [1, -1, 0], [0, 1, 0]]])
+    hs.prims["type"][0] = 2
+    hs.prims["id2"][0] = -1
+    o = np.array([[0, 0, 2]], np.float32)
+    d = np.array([[0, 0, -1]], np.float32)
+    t = np.full(1, np.inf, np.float32)
+    with GpuAccelerator(hs) as acc:
+        assert acc.info()["triangles"] == 0
+        prim, tt, _, _ = device_closest(acc, o, d, t)
+    assert prim[0] == -1
+
+
+def test_device_built_render_equals_uploaded():
+    sb = scenes.box_scene()
+    hs_up, hs_dev = sb.build(), sb.build(host_bvh=False)
+    p = F.render_params(64, 64, 16, max_depth=5, rr_min_bounce=3)
+    with GpuAccelerator(hs_up) as a, GpuAccelerator(hs_dev) as b:
+        ra = a.render(p)
+        rb = b.render(p)
+    np.testing.assert_allclose(ra[0], rb[0], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(ra[2], rb[2], rtol=1e-6)
+    assert ra[3]["extension_rays"] == rb[3]["extension_rays"]
+
+
+def test_full_size_device_build():
+    """The ray-cast mesh (1,310,720 triangles): the device-built tree gives
+    the host-built tree's closest-hit distances on all 16,777,216 rays."""
+    torch = pytest.importorskip("torch")
+    sb = scenes.raycast_scene(subdiv=8)
+    hs = sb.build()
+    o, d, t = scenes.raycast_rays(hs, 4096, 2048, 8388608)
+    with GpuAccelerator(hs) as up:
+        g_up = device_closest(up, o, d, t)
+        cost_up = up.tree_cost()
+    with GpuAccelerator(hs, device_build=True) as dev:
+        g_dev = device_closest(dev, o, d, t)
+        build_ms = dev.build_time_ms()
+        cost_dev = dev.tree_cost()
+        info = dev.info()
+        assert dev.error_word() == 0
+    same_t = H.bits(g_up[1]) == H.bits(g_dev[1])
+    assert same_t.all(), int((~same_t).sum())
+    same_prim = g_up[0] == g_dev[0]
+    assert same_prim.mean() > 0.99999
+    out = Path(__file__).resolve().parent.parent / "gpurun_out"
+    if out.is_dir():
+        (out / "device_build_full.json").write_text(json.dumps(
+            {"build_ms": build_ms, "tree_cost_device": cost_dev, "tree_cost_host": cost_up,
+             "prim_mismatch_equal_t": int((~same_prim).sum()), "info": info}))
+    assert build_ms > 0

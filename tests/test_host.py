@@ -198,3 +198,50 @@ def test_batch_workload_shapes():
         n = sum(m.triangle_count for m in sb.meshes)
         assert 10 + 2 <= n <= 10 + 4_000 + 16
         assert 1 <= len(sb._lights) // 2 <= 8
+
+
+def _build_status(hs, leaf_size=0):
+    meshes = hs.mesh_structs()
+    pts, fi, vi = hs.counts()
+    h = C.c_void_p()
+    opt = F.BuildOptions()
+    opt.leaf_size = leaf_size
+    st = F.lib().gzg_gpu_build_scene(F.ptr(hs.prims), len(hs.prims), C.addressof(meshes), len(hs.meshes),
+                                     F.ptr(pts), F.ptr(fi), F.ptr(vi), F.ptr(hs.materials), len(hs.materials),
+                                     C.byref(opt), C.byref(h))
+    if st == 0:
+        F.lib().gzg_gpu_free_scene(h)
+    return st, F.lib().gzg_last_error().decode()
+
+
+def test_device_build_rejects_bad_input_before_touching_a_device():
+    L = F.lib()
+    h = C.c_void_p()
+    assert L.gzg_gpu_build_scene(None, 1, None, 0, None, None, None, None, 0, None, C.byref(h)) == 1
+    assert L.gzg_gpu_build_scene(None, 0, None, 0, None, None, None, None, 0, None, None) == 1
+    hs = scenes.raycast_scene(subdiv=1).build(host_bvh=False)
+    assert hs.nodes is None and np.array_equal(hs.prim_order, np.arange(len(hs.prims)))
+    st, msg = _build_status(hs, leaf_size=5)
+    assert st == 1 and "leaf_size" in msg
+    # every triangle prim is validated (no tree limits which are read)
+    hs.meshes[0].vertex_indices[7] = 10 ** 9
+    st, msg = _build_status(hs)
+    assert st == 5 and "prim 2" in msg
+
+
+def test_device_build_without_device_reports_no_device():
+    from tests.conftest import HAS_GPU
+
+    if HAS_GPU:
+        pytest.skip("device present")
+    st, _ = _build_status(scenes.raycast_scene(subdiv=1).build(host_bvh=False))
+    assert st == 2
+
+
+def test_root_bounds_without_a_host_tree():
+    a = scenes.box_scene().build()
+    b = scenes.box_scene().build(host_bvh=False)
+    lo_a, hi_a = a.root_bounds()
+    lo_b, hi_b = b.root_bounds()
+    np.testing.assert_allclose(lo_a, lo_b, atol=1e-6)
+    np.testing.assert_allclose(hi_a, hi_b, atol=1e-6)
