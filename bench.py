@@ -19,6 +19,10 @@ outputs (256 MiB of hits) are larger than the 126 MB L2, so no flush is done.
             bandwidth
   cpu_baseline  the oracle (CPU restatement of the reference traversal) on the
             host cores
+  render, batch, adjoint, instanced, device_build
+            the renderer legs (box scene, 64-scene batch, adjoint step,
+            two-level scene with the general materials) and the device tree
+            build against the host's SAH build, each described in its entry
 
 --impl reference times that CPU implementation alone (the reference's own
 Swift/Mojo build cannot run here).  Multi-GPU (torchrun): every rank traces
@@ -300,9 +304,9 @@ def instanced_leg(args, stream, barrier):
     """The two-level scene lit by an environment map: 16 displaced tubes and
     spheres of 50,000 triangles each, 4096 instances under seeded affine
     transforms, a 1024 x 512 sky map with a sun lobe, materials mixed per
-    mesh (diffuse, coated diffuse, dielectric; roughness uniform in
-    [0.05, 0.5]), 1920 x 1080, 64 spp, depth 8 (MIS as written; roulette
-    from bounce 2).  One frame per step through a graph-captured renderer."""
+    mesh (diffuse, coated diffuse, dielectric, conductor, coated conductor;
+    roughness uniform in [0.05, 0.5]), 1920 x 1080, 64 spp, depth 8 (MIS as
+    written; roulette from bounce 2).  One frame per step through a graph-captured renderer."""
     import torch
 
     from gonzales_b200 import GpuAccelerator, InstancedAccelerator, Renderer, scenes
@@ -339,12 +343,68 @@ def instanced_leg(args, stream, barrier):
     ms = e0.elapsed_time(e1) / steps
     rays = sum(s1[k] - s0[k] for k in ("camera_rays", "extension_rays", "shadow_rays", "probe_rays")) / steps
     return {"config": "16 x 50k-triangle meshes, 4096 instances, sky map 1024x512 + sun lobe, diffuse / "
-                      "coated diffuse / dielectric meshes (roughness U[0.05,0.5]), %dx%d, %d spp, depth 8, "
-                      "roulette from bounce 2" % (W, H, spp),
+                      "coated diffuse / dielectric / conductor / coated conductor meshes (roughness "
+                      "U[0.05,0.5]), %dx%d, %d spp, depth 8, roulette from bounce 2" % (W, H, spp),
             "spp_per_s": W * H * spp / ms * 1000.0, "ms_per_frame": ms, "mrays_per_s": rays / ms / 1000.0,
             "rays_per_frame": rays, "steps": steps, "setup_s": setup_s, "error_word": err,
             "not_built": "the homogeneous medium box (never sampled by the reference's integrator, whose "
                          "interface material throws)"}
+
+
+def build_leg(hs, rays_d, args, stream, barrier):
+    """The ray-cast mesh's tree built on the device (gzg_gpu_build_scene)
+    against the host's SAH build: build times, surface-area costs of the two
+    wide trees, and closest-hit Mrays/s on each (same rays)."""
+    import os
+
+    import torch
+
+    from gonzales_b200 import GpuAccelerator, scene as S
+
+    n = rays_d.shape[0]
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    bounds = np.concatenate([S.triangle_bounds(m) for m in hs.meshes])
+    S.build_bvh2(bounds, threads)
+    host_sah_s = time.perf_counter() - t0
+
+    def timed(acc):
+        for _ in range(3):
+            acc.trace_closest(rays_d, hits)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        steps = max(3, min(args.steps, 10))
+        e0.record(stream)
+        for _ in range(steps):
+            acc.trace_closest(rays_d, hits)
+        e1.record(stream)
+        barrier()
+        return n / (e0.elapsed_time(e1) / steps) / 1e3
+
+    t0 = time.perf_counter()
+    up = GpuAccelerator(hs)
+    upload_s = time.perf_counter() - t0
+    host_rate, host_cost = timed(up), up.tree_cost()
+    up.close()
+    ms = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        dev = GpuAccelerator(hs, device_build=True)
+        wall = time.perf_counter() - t0
+        ms.append(dev.build_time_ms())
+        if len(ms) < 3:
+            dev.close()
+    dev_rate, dev_cost, info = timed(dev), dev.tree_cost(), dev.info()
+    err = dev.error_word()
+    dev.close()
+    return {"config": "ray-cast mesh, %d triangles; closest hit on the %d bench rays" % (hs.triangle_count, n),
+            "device_build_ms": min(ms), "device_build_wall_s": wall, "host_sah_build_s": host_sah_s,
+            "host_sah_threads": threads, "upload_with_host_tree_s": upload_s,
+            "tree_cost_device": dev_cost, "tree_cost_host_sah": host_cost,
+            "closest_mrays_device_tree": dev_rate, "closest_mrays_host_tree": host_rate,
+            "device_wide_nodes": info["wide_nodes"], "error_word": err}
 
 
 def adjoint_leg(args, stream, barrier):
@@ -554,6 +614,7 @@ def run_ours(args):
         e2e_s = float(tt.item())
 
     render = render_leg(acc_box=None, args=args, stream=stream, barrier=barrier) if not args.small else None
+    build = build_leg(hs, rays_d, args, stream, barrier) if not (args.small or args.skip_batch) else None
     batch = batch_leg(args, stream, barrier) if not (args.small or args.skip_batch) else None
     adjoint = adjoint_leg(args, stream, barrier) if not (args.small or args.skip_batch) else None
     instanced = instanced_leg(args, stream, barrier) if not (args.small or args.skip_batch) else None
@@ -600,6 +661,8 @@ def run_ours(args):
             line["adjoint"] = adjoint
         if instanced is not None:
             line["instanced"] = instanced
+        if build is not None:
+            line["device_build"] = build
         if world == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(hs, o, d, t)
             if render is not None:
