@@ -74,6 +74,17 @@ class BuildOptions(C.Structure):
     _fields_ = [("leaf_size", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
+class MeshArrays(C.Structure):
+    _fields_ = [("points", C.c_void_p), ("vertex_count", C.c_int64), ("indices", C.c_void_p),
+                ("triangle_count", C.c_int64), ("material", C.c_int64)]
+
+
+class PlyMesh(C.Structure):
+    _fields_ = [("vertex_count", C.c_int64), ("face_count", C.c_int64), ("points", C.POINTER(C.c_float)),
+                ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
+                ("indices", C.POINTER(C.c_int32)), ("face_indices", C.POINTER(C.c_int32)), ("owner", C.c_void_p)]
+
+
 class SceneInfo(C.Structure):
     _fields_ = [("bvh2_nodes", C.c_int64), ("prims", C.c_int64), ("triangles", C.c_int64),
                 ("wide_nodes", C.c_int64), ("wide_depth", C.c_int32), ("bvh2_depth", C.c_int32),
@@ -139,6 +150,10 @@ PROTOTYPES = {
     "gzg_scene_set_material_params": (ST, [VP, VP, I64]),
     "gzg_gpu_build_scene": (ST, [VP, I64, VP, I64, VP, VP, VP, VP, I64, VP, C.POINTER(VP)]),
     "gzg_scene_build_time": (ST, [VP, C.POINTER(C.c_float)]),
+    "gzg_gpu_build_mesh_scene": (ST, [VP, I64, VP, I64, VP, C.POINTER(VP)]),
+    "gzg_ply_read": (ST, [C.c_char_p, C.POINTER(C.POINTER(PlyMesh))]),
+    "gzg_ply_parse": (ST, [VP, I64, C.POINTER(C.POINTER(PlyMesh))]),
+    "gzg_ply_free": (ST, [C.POINTER(PlyMesh)]),
     "gzg_scene_tree_cost": (ST, [VP, C.POINTER(C.c_double)]),
     "gzg_host_instance_bounds": (ST, [VP, I64, VP, I64, VP]),
     "gzg_instanced_scene_create": (ST, [VP, I64, VP, I64, VP, I64, VP, I64, C.POINTER(VP)]),

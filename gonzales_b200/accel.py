@@ -70,6 +70,32 @@ class GpuAccelerator:
                 self.close()
                 raise
 
+    @classmethod
+    def from_mesh_arrays(cls, meshes, materials, leaf_size=0):
+        """The ingestion fast path (gzg_gpu_build_mesh_scene): meshes is a list
+        of (points (n, 3) float32, indices (m, 3) int32, material index);
+        materials a MATERIAL_DTYPE array.  Prim k of the scene is triangle k
+        in mesh order (id2 = mesh << 32 | triangle)."""
+        self = cls.__new__(cls)
+        keep = []
+        arr = (F.MeshArrays * max(len(meshes), 1))()
+        for k, (pts, idx, mat) in enumerate(meshes):
+            pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+            idx = np.ascontiguousarray(idx, np.int32).reshape(-1, 3)
+            keep += [pts, idx]
+            arr[k] = F.MeshArrays(pts.ctypes.data if len(pts) else None, len(pts),
+                                  idx.ctypes.data if len(idx) else None, len(idx), int(mat))
+        materials = np.ascontiguousarray(materials)
+        opt = F.BuildOptions()
+        opt.leaf_size = int(leaf_size)
+        handle = C.c_void_p()
+        F.check(F.lib().gzg_gpu_build_mesh_scene(C.addressof(arr), len(meshes), F.ptr(materials), len(materials),
+                                                 C.byref(opt), C.byref(handle)))
+        self.handle = handle
+        self.device_built = True
+        self.host = _ArraysHost(meshes, materials)
+        return self
+
     # ------------------------------------------------------------ lifetime
     def close(self):
         if self.handle:
@@ -219,6 +245,22 @@ class GpuAccelerator:
         float32 in the equal-area square layout."""
         rgb = np.ascontiguousarray(rgb, np.float32)
         F.check(F.lib().gzg_scene_set_environment(self.handle, F.ptr(rgb), rgb.shape[1], rgb.shape[0], float(scale)))
+
+
+class _ArraysHost:
+    """What the Python side reads of a scene built from mesh arrays."""
+
+    def __init__(self, meshes, materials):
+        pts = [np.asarray(p, np.float32).reshape(-1, 3)[np.asarray(i, np.int64).reshape(-1)] for p, i, _ in meshes]
+        pts = np.concatenate(pts) if pts else np.zeros((0, 3), np.float32)
+        self._lo = pts.min(0) if len(pts) else np.zeros(3, np.float32)
+        self._hi = pts.max(0) if len(pts) else np.zeros(3, np.float32)
+        self.materials = materials
+        self.nodes = None
+        self.has_extended_materials = False
+
+    def root_bounds(self):
+        return self._lo, self._hi
 
 
 def instance_bounds(blas_hosts, instances):

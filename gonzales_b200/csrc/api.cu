@@ -136,6 +136,18 @@ struct gzg_scene {
                 return GZG_OK;
         }
 
+        // A device array the scene owns, left uninitialised.
+        template <class T>
+        gzg_status alloc(T **dst, size_t count, const char *what) {
+                void *d = nullptr;
+                const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+                GZG_CK(cudaMalloc(&d, bytes), what);
+                allocs.push_back(d);
+                info.device_bytes += (int64_t)bytes;
+                *dst = reinterpret_cast<T *>(d);
+                return GZG_OK;
+        }
+
         gzg_status acquire(std::unique_ptr<Staging> *out) {
                 {
                         std::lock_guard<std::mutex> lk(pool_mu);
@@ -297,6 +309,82 @@ GZG_API bool gzg_gpu_available(void) {
 GZG_API const char *gzg_last_error(void) { return g_last_error.c_str(); }
 
 namespace {
+
+// Materials, area lights (from the prim-order triangles) and the host copies
+// of a scene's shading arrays; the wide tree and pv0..2 move into the scene.
+gzg_status attach_shading(gzg_scene *scene, WideBvh &&wide, const gzg_prim_id *prim_ids, int64_t prim_count,
+                          std::vector<float4_> &&pv0, std::vector<float4_> &&pv1, std::vector<float4_> &&pv2,
+                          const gzg_material *materials, int64_t material_count) {
+        DevScene &d = scene->dev;
+        const float4 *f;
+        gzg_status st;
+        // Shading data for the path integrator.  Materials: albedo + type,
+        // emission (Material_C, mojo_kernel.h:11-15).  Lights: one per
+        // area-light triangle prim, in light-index order (SceneDescription
+        // creates one AreaLight per triangle), power = average radiance x area
+        // x pi (AreaLight.swift:47-49), with the running power sum the power
+        // light sampler searches (PowerLightSampler.swift:20-38).
+        std::vector<float4_> mats((size_t)std::max<int64_t>(material_count, 0) * 2);
+        for (int64_t k = 0; k < material_count; ++k) {
+                const gzg_material &m = materials[k];
+                mats[2 * k] = float4_{m.albedo[0], m.albedo[1], m.albedo[2], (float)m.type};
+                mats[2 * k + 1] = float4_{m.emission[0], m.emission[1], m.emission[2], 0.0f};
+        }
+        std::vector<std::pair<int64_t, int64_t>> light_prims;
+        for (int64_t k = 0; k < prim_count; ++k) {
+                int64_t mesh, base;
+                if (prim_ids[k].type == 3 && prim_triangle(prim_ids[k], &mesh, &base)) light_prims.push_back({prim_ids[k].id1, k});
+        }
+        std::sort(light_prims.begin(), light_prims.end());
+        std::vector<float4_> lights;
+        std::vector<float> cdf;
+        float total = 0.0f, run = 0.0f;
+        for (size_t i = 0; i < light_prims.size(); ++i) {
+                const int64_t k = light_prims[i].second;
+                const float4_ a = pv0[k], b = pv1[k], c = pv2[k];
+                const float e1[3] = {b.x - a.x, b.y - a.y, b.z - a.z}, e2[3] = {c.x - a.x, c.y - a.y, c.z - a.z};
+                const float cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                            cz = e1[0] * e2[1] - e1[1] * e2[0];
+                const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
+                float le[3] = {0, 0, 0};
+                const int64_t mi = prim_ids[k].material_index;
+                if (mi >= 0 && mi < material_count)
+                        for (int j = 0; j < 3; ++j) le[j] = materials[mi].emission[j];
+                const float power = (le[0] + le[1] + le[2]) / 3.0f * area * 3.14159265358979323846f;
+                lights.push_back(float4_{a.x, a.y, a.z, area});
+                lights.push_back(float4_{b.x, b.y, b.z, power});
+                lights.push_back(float4_{c.x, c.y, c.z, 0.0f});
+                lights.push_back(float4_{le[0], le[1], le[2], 0.0f});
+                run = i == 0 ? power : run + power;
+                cdf.push_back(run);
+                total = total + power;
+        }
+        st = scene->upload(reinterpret_cast<const float4 *>(mats.data()), mats.size(), &f, "materials");
+        if (st != GZG_OK) return st;
+        d.materials = f;
+        st = scene->upload(reinterpret_cast<const float4 *>(lights.data()), lights.size(), &f, "lights");
+        if (st != GZG_OK) return st;
+        d.lights = f;
+        const float *cdf_d;
+        st = scene->upload(cdf.data(), cdf.size(), &cdf_d, "light cdf");
+        if (st != GZG_OK) return st;
+        d.light_cdf = cdf_d;
+        d.material_count = (int32_t)material_count;
+        d.light_count = (int32_t)light_prims.size();
+        d.light_total_power = total;
+
+        scene->host_wide = std::move(wide);
+        HostShading &hsd = scene->host_shading;
+        hsd.pv0 = std::move(pv0);
+        hsd.pv1 = std::move(pv1);
+        hsd.pv2 = std::move(pv2);
+        hsd.prims.assign(prim_ids, prim_ids + prim_count);
+        hsd.materials = std::move(mats);
+        hsd.lights = std::move(lights);
+        hsd.light_cdf = std::move(cdf);
+        hsd.light_total = total;
+        return GZG_OK;
+}
 
 // gzg_gpu_upload_scene (bvh2_nodes given: the host's tree, converted on the
 // host) and gzg_gpu_build_scene (build given: the tree built on the device).
@@ -464,61 +552,6 @@ gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count
         info.wide_depth = wide.depth;
         info.bvh2_depth = bvh2_depth;
 
-        // Shading data for the path integrator.  Materials: albedo + type,
-        // emission (Material_C, mojo_kernel.h:11-15).  Lights: one per
-        // area-light triangle prim, in light-index order (SceneDescription
-        // creates one AreaLight per triangle), power = average radiance x area
-        // x pi (AreaLight.swift:47-49), with the running power sum the power
-        // light sampler searches (PowerLightSampler.swift:20-38).
-        std::vector<float4_> mats((size_t)std::max<int64_t>(material_count, 0) * 2);
-        for (int64_t k = 0; k < material_count; ++k) {
-                const gzg_material &m = materials[k];
-                mats[2 * k] = float4_{m.albedo[0], m.albedo[1], m.albedo[2], (float)m.type};
-                mats[2 * k + 1] = float4_{m.emission[0], m.emission[1], m.emission[2], 0.0f};
-        }
-        std::vector<std::pair<int64_t, int64_t>> light_prims;
-        for (int64_t k = 0; k < prim_count; ++k) {
-                int64_t mesh, base;
-                if (prim_ids[k].type == 3 && prim_triangle(prim_ids[k], &mesh, &base)) light_prims.push_back({prim_ids[k].id1, k});
-        }
-        std::sort(light_prims.begin(), light_prims.end());
-        std::vector<float4_> lights;
-        std::vector<float> cdf;
-        float total = 0.0f, run = 0.0f;
-        for (size_t i = 0; i < light_prims.size(); ++i) {
-                const int64_t k = light_prims[i].second;
-                const float4_ a = pv0[k], b = pv1[k], c = pv2[k];
-                const float e1[3] = {b.x - a.x, b.y - a.y, b.z - a.z}, e2[3] = {c.x - a.x, c.y - a.y, c.z - a.z};
-                const float cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
-                            cz = e1[0] * e2[1] - e1[1] * e2[0];
-                const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
-                float le[3] = {0, 0, 0};
-                const int64_t mi = prim_ids[k].material_index;
-                if (mi >= 0 && mi < material_count)
-                        for (int j = 0; j < 3; ++j) le[j] = materials[mi].emission[j];
-                const float power = (le[0] + le[1] + le[2]) / 3.0f * area * 3.14159265358979323846f;
-                lights.push_back(float4_{a.x, a.y, a.z, area});
-                lights.push_back(float4_{b.x, b.y, b.z, power});
-                lights.push_back(float4_{c.x, c.y, c.z, 0.0f});
-                lights.push_back(float4_{le[0], le[1], le[2], 0.0f});
-                run = i == 0 ? power : run + power;
-                cdf.push_back(run);
-                total = total + power;
-        }
-        st = scene->upload(reinterpret_cast<const float4 *>(mats.data()), mats.size(), &f, "materials");
-        if (st != GZG_OK) return st;
-        d.materials = f;
-        st = scene->upload(reinterpret_cast<const float4 *>(lights.data()), lights.size(), &f, "lights");
-        if (st != GZG_OK) return st;
-        d.lights = f;
-        const float *cdf_d;
-        st = scene->upload(cdf.data(), cdf.size(), &cdf_d, "light cdf");
-        if (st != GZG_OK) return st;
-        d.light_cdf = cdf_d;
-        d.material_count = (int32_t)material_count;
-        d.light_count = (int32_t)light_prims.size();
-        d.light_total_power = total;
-
         // Device copies of the meshes, for calls that take reference
         // Intersection_C records and decode (mesh, triangle) from the prim id
         // the way shade_core does (kernel.mojo:705-721).
@@ -571,16 +604,9 @@ gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count
                         scene->root_bounds[3 + a] = hi[a];
                 }
         }
-        scene->host_wide = std::move(wide);
-        HostShading &hsd = scene->host_shading;
-        hsd.pv0 = std::move(pv0);
-        hsd.pv1 = std::move(pv1);
-        hsd.pv2 = std::move(pv2);
-        hsd.prims.assign(prim_ids, prim_ids + prim_count);
-        hsd.materials = std::move(mats);
-        hsd.lights = std::move(lights);
-        hsd.light_cdf = std::move(cdf);
-        hsd.light_total = total;
+        st = attach_shading(scene.get(), std::move(wide), prim_ids, prim_count, std::move(pv0), std::move(pv1),
+                            std::move(pv2), materials, material_count);
+        if (st != GZG_OK) return st;
         *out_scene = scene.release();
         return clear_error();
 }
@@ -610,6 +636,168 @@ GZG_API gzg_status gzg_gpu_build_scene(const gzg_prim_id *prim_ids, int64_t prim
         return upload_scene(nullptr, 0, prim_ids, prim_count, meshes, mesh_count, mesh_points_counts,
                             mesh_vertex_indices_counts, materials, material_count, options ? options : &defaults,
                             out_scene, "gzg_gpu_build_scene");
+}
+
+GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64_t mesh_count,
+                                            const gzg_material *materials, int64_t material_count,
+                                            const gzg_build_options *options, gzg_scene **out_scene) {
+        const char *fn = "gzg_gpu_build_mesh_scene";
+        if (!out_scene) return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": out_scene is NULL");
+        *out_scene = nullptr;
+        if (mesh_count < 0 || (mesh_count > 0 && !meshes) || material_count < 0 || (material_count > 0 && !materials))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": bad arguments");
+        const gzg_build_options defaults{};
+        const gzg_build_options &opt = options ? *options : defaults;
+        if (opt.leaf_size < 0 || opt.leaf_size > 4)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": leaf_size must be 0 (default 4) to 4");
+        std::vector<MeshRange> ranges((size_t)mesh_count);
+        int64_t nv = 0, nt = 0, lights = 0;
+        for (int64_t k = 0; k < mesh_count; ++k) {
+                const gzg_mesh_arrays &m = meshes[k];
+                if (m.vertex_count < 0 || m.triangle_count < 0 || (m.vertex_count > 0 && !m.points) ||
+                    (m.triangle_count > 0 && !m.indices) || m.material < 0 || m.material >= material_count)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                         std::string(fn) + ": bad arrays or material index for mesh " + std::to_string(k));
+                const bool is_light = materials[m.material].type == 2;
+                ranges[k] = MeshRange{nv, nt, m.vertex_count, m.triangle_count, m.material, is_light ? lights : -1};
+                if (is_light) lights += m.triangle_count;
+                nv += m.vertex_count;
+                nt += m.triangle_count;
+        }
+        if (nt > INT32_MAX - 1 || nv > INT32_MAX) return set_error(GZG_ERR_LIMIT, std::string(fn) + ": more than 2^31 triangles or vertices");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+                cudaGetLastError();
+                return set_error(GZG_ERR_NO_DEVICE, std::string(fn) + ": no CUDA device");
+        }
+        auto scene = std::make_unique<gzg_scene>();
+        cudaGetDevice(&scene->device);
+        DevScene &d = scene->dev;
+        gzg_status st;
+        // staging: the packed arrays as they are, then the device expansion
+        float *p3 = nullptr;
+        int32_t *i3 = nullptr;
+        MeshRange *rd = nullptr;
+        struct Tmp {
+                std::vector<void *> v;
+                ~Tmp() {
+                        for (void *p : v) cudaFree(p);
+                }
+        } tmp;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&p3), std::max<size_t>(12 * (size_t)nv, 16)), "gzg_gpu_build_mesh_scene: staging");
+        tmp.v.push_back(p3);
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&i3), std::max<size_t>(12 * (size_t)nt, 16)), "gzg_gpu_build_mesh_scene: staging");
+        tmp.v.push_back(i3);
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&rd), std::max<size_t>(sizeof(MeshRange) * ranges.size(), 16)),
+               "gzg_gpu_build_mesh_scene: staging");
+        tmp.v.push_back(rd);
+        for (int64_t k = 0; k < mesh_count; ++k) {
+                const gzg_mesh_arrays &m = meshes[k];
+                if (m.vertex_count)
+                        GZG_CK(cudaMemcpy(p3 + 3 * ranges[k].vert_off, m.points, 12 * (size_t)m.vertex_count, cudaMemcpyHostToDevice),
+                               "gzg_gpu_build_mesh_scene: points");
+                if (m.triangle_count)
+                        GZG_CK(cudaMemcpy(i3 + 3 * ranges[k].tri_off, m.indices, 12 * (size_t)m.triangle_count,
+                                          cudaMemcpyHostToDevice),
+                               "gzg_gpu_build_mesh_scene: indices");
+        }
+        if (mesh_count)
+                GZG_CK(cudaMemcpy(rd, ranges.data(), sizeof(MeshRange) * ranges.size(), cudaMemcpyHostToDevice),
+                       "gzg_gpu_build_mesh_scene: mesh table");
+        float *p4;
+        int64_t *v64;
+        gzg_prim_id *prims;
+        float4_ *pv[3];
+        if ((st = scene->alloc(&p4, 4 * (size_t)nv, "mesh points")) || (st = scene->alloc(&v64, 3 * (size_t)nt, "mesh vertex indices")) ||
+            (st = scene->alloc(&prims, (size_t)nt, "prim ids")) || (st = scene->alloc(&pv[0], (size_t)nt, "prim triangles")) ||
+            (st = scene->alloc(&pv[1], (size_t)nt, "prim triangles")) || (st = scene->alloc(&pv[2], (size_t)nt, "prim triangles")))
+                return st;
+        bool bad = false;
+        if ((st = gpu_expand_meshes(p3, i3, rd, (int)mesh_count, nv, nt, p4, v64, prims, pv[0], pv[1], pv[2], &bad)))
+                return st;
+        if (bad) return set_error(GZG_ERR_BAD_SCENE, std::string(fn) + ": a triangle index is out of its mesh's vertices");
+        d.pv0 = reinterpret_cast<const float4 *>(pv[0]);
+        d.pv1 = reinterpret_cast<const float4 *>(pv[1]);
+        d.pv2 = reinterpret_cast<const float4 *>(pv[2]);
+        d.prims = prims;
+        const uint32_t zero = 0;
+        const uint32_t *ew;
+        if ((st = scene->upload(&zero, 1, &ew, "error word"))) return st;
+        d.err = const_cast<uint32_t *>(ew);
+        GpuWide gw;
+        float ms = 0.0f;
+        st = gpu_build_wide(pv[0], pv[1], pv[2], nt, opt.leaf_size, &gw, &ms);
+        for (void *p : {gw.nodes, gw.tv0, gw.tv1, gw.tv2})
+                if (p) scene->allocs.push_back(p);
+        if (st != GZG_OK) return st;
+        d.wide = reinterpret_cast<const uint4 *>(gw.nodes);
+        d.tv0 = reinterpret_cast<const float4 *>(gw.tv0);
+        d.tv1 = reinterpret_cast<const float4 *>(gw.tv1);
+        d.tv2 = reinterpret_cast<const float4 *>(gw.tv2);
+        scene->info.device_bytes += (int64_t)gw.node_count * (int64_t)sizeof(WideNode) + 48 * (int64_t)gw.tri_count;
+        scene->build_ms = ms;
+        // host copies: the tree and the shading arrays (batches, two-level
+        // scenes and the light list read them)
+        WideBvh wide;
+        wide.nodes.resize(gw.node_count);
+        wide.v0.resize(gw.tri_count);
+        wide.v1.resize(gw.tri_count);
+        wide.v2.resize(gw.tri_count);
+        wide.depth = gw.depth;
+        std::vector<float4_> h0((size_t)nt), h1((size_t)nt), h2((size_t)nt);
+        std::vector<gzg_prim_id> hp((size_t)nt);
+        GZG_CK(cudaMemcpy(wide.nodes.data(), gw.nodes, gw.node_count * sizeof(WideNode), cudaMemcpyDeviceToHost), "tree download");
+        GZG_CK(cudaMemcpy(wide.v0.data(), gw.tv0, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost), "tree download");
+        GZG_CK(cudaMemcpy(wide.v1.data(), gw.tv1, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost), "tree download");
+        GZG_CK(cudaMemcpy(wide.v2.data(), gw.tv2, gw.tri_count * sizeof(float4_), cudaMemcpyDeviceToHost), "tree download");
+        GZG_CK(cudaMemcpy(h0.data(), pv[0], nt * sizeof(float4_), cudaMemcpyDeviceToHost), "shading download");
+        GZG_CK(cudaMemcpy(h1.data(), pv[1], nt * sizeof(float4_), cudaMemcpyDeviceToHost), "shading download");
+        GZG_CK(cudaMemcpy(h2.data(), pv[2], nt * sizeof(float4_), cudaMemcpyDeviceToHost), "shading download");
+        GZG_CK(cudaMemcpy(hp.data(), prims, nt * sizeof(gzg_prim_id), cudaMemcpyDeviceToHost), "shading download");
+        // the device mesh table (reference layout) over the expanded arrays
+        std::vector<gzg_triangle_mesh> dev_meshes((size_t)mesh_count);
+        std::vector<int64_t> sizes((size_t)mesh_count * 2);
+        for (int64_t k = 0; k < mesh_count; ++k) {
+                dev_meshes[k] = gzg_triangle_mesh{p4 + 4 * ranges[k].vert_off, nullptr, v64 + 3 * ranges[k].tri_off};
+                sizes[2 * k] = 4 * ranges[k].vcount;
+                sizes[2 * k + 1] = 3 * ranges[k].tcount;
+        }
+        const gzg_triangle_mesh *dm;
+        if ((st = scene->upload(dev_meshes.data(), dev_meshes.size(), &dm, "mesh table"))) return st;
+        d.meshes = dm;
+        const int64_t *msz;
+        if ((st = scene->upload(sizes.data(), sizes.size(), &msz, "mesh sizes"))) return st;
+        d.mesh_sizes = msz;
+        d.mesh_count = mesh_count;
+        d.bvh2_count = 0;
+        d.prim_count = nt;
+        d.wide_count = (uint32_t)wide.nodes.size();
+        gzg_scene_info &info = scene->info;
+        info.bvh2_nodes = 0;
+        info.prims = nt;
+        info.triangles = (int64_t)wide.v0.size();
+        info.wide_nodes = (int64_t)wide.nodes.size();
+        info.wide_depth = wide.depth;
+        info.bvh2_depth = 0;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (const std::vector<float4_> *v : {&h0, &h1, &h2})
+                for (const float4_ &q : *v) {
+                        lo[0] = std::min(lo[0], q.x);
+                        lo[1] = std::min(lo[1], q.y);
+                        lo[2] = std::min(lo[2], q.z);
+                        hi[0] = std::max(hi[0], q.x);
+                        hi[1] = std::max(hi[1], q.y);
+                        hi[2] = std::max(hi[2], q.z);
+                }
+        for (int a = 0; a < 3; ++a) {
+                scene->root_bounds[a] = lo[a];
+                scene->root_bounds[3 + a] = hi[a];
+        }
+        st = attach_shading(scene.get(), std::move(wide), hp.data(), nt, std::move(h0), std::move(h1), std::move(h2),
+                            materials, material_count);
+        if (st != GZG_OK) return st;
+        *out_scene = scene.release();
+        return clear_error();
 }
 
 GZG_API gzg_status gzg_scene_build_time(const gzg_scene *scene, float *device_ms) {

@@ -546,3 +546,89 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
 }
 
 }  // namespace gzg
+
+namespace gzg {
+namespace {
+
+__global__ void k_expand_points(const float *__restrict__ p3, int64_t n, float4 *__restrict__ p4) {
+        const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (v >= n) return;
+        p4[v] = make_float4(p3[3 * v], p3[3 * v + 1], p3[3 * v + 2], 0.0f);
+}
+
+__global__ void k_expand_tris(const float4 *__restrict__ p4, const int32_t *__restrict__ idx3,
+                              const MeshRange *__restrict__ ranges, int mesh_count, int64_t n,
+                              long long *__restrict__ vidx64, gzg_prim_id *__restrict__ prims, float4 *__restrict__ pv0,
+                              float4 *__restrict__ pv1, float4 *__restrict__ pv2, uint32_t *__restrict__ bad) {
+        const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= n) return;
+        int lo = 0, hi = mesh_count - 1;
+        while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (ranges[mid].tri_off <= t)
+                        lo = mid;
+                else
+                        hi = mid - 1;
+        }
+        const MeshRange r = ranges[lo];
+        const int64_t lt = t - r.tri_off;
+        bool ok = true;
+        int32_t ix[3];
+        for (int c = 0; c < 3; ++c) {
+                ix[c] = idx3[3 * t + c];
+                ok = ok && ix[c] >= 0 && (int64_t)ix[c] < r.vcount;
+                vidx64[3 * t + c] = ok ? (long long)ix[c] : 0ll;
+        }
+        gzg_prim_id p;
+        memset(&p, 0, sizeof(p));
+        p.material_index = r.material;
+        if (r.light_base >= 0) {
+                p.type = 3;
+                p.id1 = r.light_base + lt;
+        } else {
+                p.type = 1;
+                p.id1 = 0;
+        }
+        p.id2 = ((int64_t)lo << 32) | lt;
+        prims[t] = p;
+        if (!ok) {
+                atomicOr(bad, 1u);
+                pv0[t] = pv1[t] = pv2[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                return;
+        }
+        float4 a = p4[r.vert_off + ix[0]];
+        a.w = __int_as_float(1);
+        pv0[t] = a;
+        pv1[t] = p4[r.vert_off + ix[1]];
+        pv2[t] = p4[r.vert_off + ix[2]];
+}
+
+}  // namespace
+
+gzg_status gpu_expand_meshes(const float *points3, const int32_t *idx3, const MeshRange *ranges_dev, int mesh_count,
+                             int64_t total_verts, int64_t total_tris, float *points4, int64_t *vidx64,
+                             gzg_prim_id *prims, float4_ *pv0, float4_ *pv1, float4_ *pv2, bool *bad) {
+        uint32_t *flag = nullptr;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&flag), 4), "expand: flag");
+        struct F {
+                uint32_t *p;
+                ~F() { cudaFree(p); }
+        } fr{flag};
+        GZG_CK(cudaMemset(flag, 0, 4), "expand: flag");
+        const int B = 256;
+        if (total_verts > 0)
+                k_expand_points<<<(unsigned)((total_verts + B - 1) / B), B>>>(points3, total_verts,
+                                                                             reinterpret_cast<float4 *>(points4));
+        if (total_tris > 0)
+                k_expand_tris<<<(unsigned)((total_tris + B - 1) / B), B>>>(
+                    reinterpret_cast<const float4 *>(points4), idx3, ranges_dev, mesh_count, total_tris,
+                    reinterpret_cast<long long *>(vidx64), prims, reinterpret_cast<float4 *>(pv0),
+                    reinterpret_cast<float4 *>(pv1), reinterpret_cast<float4 *>(pv2), flag);
+        GZG_CK(cudaGetLastError(), "expand: launch");
+        uint32_t h = 0;
+        GZG_CK(cudaMemcpy(&h, flag, 4, cudaMemcpyDeviceToHost), "expand: flag");
+        *bad = h != 0;
+        return clear_error();
+}
+
+}  // namespace gzg

@@ -88,6 +88,20 @@ struct GpuWide {
 gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ *pv2, int64_t n, int leaf_size,
                           GpuWide *out, float *device_ms);
 
+// Device expansion of packed meshes (gpu_build.cu): per mesh its first
+// vertex and triangle in the concatenated arrays, counts, material and,
+// for an area-light mesh, the light index of its first triangle (else -1).
+struct MeshRange {
+        int64_t vert_off, tri_off, vcount, tcount, material;
+        int64_t light_base;
+};
+// points3 / idx3: concatenated packed arrays on the device; writes points4
+// (x, y, z, 0), vidx64, prims (PrimId_C) and pv0/pv1/pv2 (pv0.w = int 1).
+// Sets *bad when an index is out of range (that triangle is left inert).
+gzg_status gpu_expand_meshes(const float *points3, const int32_t *idx3, const MeshRange *ranges_dev, int mesh_count,
+                             int64_t total_verts, int64_t total_tris, float *points4, int64_t *vidx64,
+                             gzg_prim_id *prims, float4_ *pv0, float4_ *pv1, float4_ *pv2, bool *bad);
+
 // Converts a validated reference BVH2 + prims + meshes into the wide layout.
 // Returns GZG_OK or an error (with set_error called).
 gzg_status build_wide_bvh(const gzg_bvh2_node *nodes, int64_t node_count, const gzg_prim_id *prims,

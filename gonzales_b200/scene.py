@@ -224,3 +224,79 @@ class SceneBuilder:
             params[:n_surface] = np.asarray(self._material_params, np.float32)
         return HostScene(meshes=self.meshes, prims=sorted_prims, nodes=nodes, materials=mats,
                          prim_order=order, material_params=params)
+
+
+def _ply_arrays(mesh_p):
+    m = mesh_p.contents
+    nv, nf = m.vertex_count, m.face_count
+
+    def arr(ptr, n, cols, dtype):
+        if not ptr or n == 0:
+            return None if not ptr else np.zeros((0, cols), dtype)
+        return np.ctypeslib.as_array(ptr, shape=(n * cols,)).reshape(n, cols).astype(dtype, copy=True)
+
+    out = {"points": arr(m.points, nv, 3, np.float32), "indices": arr(m.indices, nf, 3, np.int32),
+           "normals": arr(m.normals, nv, 3, np.float32), "uvs": arr(m.uvs, nv, 2, np.float32),
+           "face_indices": None}
+    if m.face_indices:
+        out["face_indices"] = np.ctypeslib.as_array(m.face_indices, shape=(nf,)).astype(np.int32, copy=True)
+    if out["points"] is None:
+        out["points"] = np.zeros((0, 3), np.float32)
+    if out["indices"] is None:
+        out["indices"] = np.zeros((0, 3), np.int32)
+    return out
+
+
+def read_ply(path=None, data=None):
+    """A PLY mesh (gzg_ply_read / gzg_ply_parse, the format of
+    Shape/PlyMesh.swift) as numpy arrays: points (n, 3) float32, indices
+    (m, 3) int32, normals / uvs / face_indices or None."""
+    L = F.lib()
+    mp = F.C.POINTER(F.PlyMesh)()
+    if path is not None:
+        F.check(L.gzg_ply_read(str(path).encode(), F.C.byref(mp)))
+    else:
+        buf = np.frombuffer(bytes(data), np.uint8)
+        F.check(L.gzg_ply_parse(F.ptr(buf) if len(buf) else None, len(buf), F.C.byref(mp)))
+    try:
+        return _ply_arrays(mp)
+    finally:
+        L.gzg_ply_free(mp)
+
+
+def write_ply(path, points, indices, normals=None, uvs=None, big_endian=False, list_type="uchar",
+              face_indices=None):
+    """Writes a binary PLY in one of the layouts read_ply accepts (test and
+    tooling helper)."""
+    points = np.asarray(points, np.float32).reshape(-1, 3)
+    indices = np.asarray(indices, np.int32).reshape(-1, 3)
+    end = ">" if big_endian else "<"
+    cols = [points]
+    props = ["x", "y", "z"]
+    if normals is not None:
+        cols.append(np.asarray(normals, np.float32).reshape(-1, 3))
+        props += ["nx", "ny", "nz"]
+    if uvs is not None:
+        cols.append(np.asarray(uvs, np.float32).reshape(-1, 2))
+        props += ["u", "v"]
+    head = ["ply", "format binary_%s_endian 1.0" % ("big" if big_endian else "little"),
+            "comment written by gonzales_b200", "element vertex %d" % len(points)]
+    head += ["property float %s" % p for p in props]
+    head += ["element face %d" % len(indices), "property list %s int vertex_indices" % list_type]
+    if face_indices is not None:
+        head.append("property int face_indices")
+    head.append("end_header")
+    vert = np.concatenate(cols, 1).astype(end + "f4")
+    ct = np.dtype(end + ("u1" if list_type == "uchar" else "u4"))
+    fields = [("n", ct), ("i", end + "i4", (3,))]
+    if face_indices is not None:
+        fields.append(("f", end + "i4"))
+    faces = np.zeros(len(indices), np.dtype(fields))
+    faces["n"] = 3
+    faces["i"] = indices
+    if face_indices is not None:
+        faces["f"] = face_indices
+    with open(path, "wb") as fh:
+        fh.write(("\n".join(head) + "\n").encode())
+        fh.write(vert.tobytes())
+        fh.write(faces.tobytes())

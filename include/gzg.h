@@ -371,6 +371,49 @@ GZG_API gzg_status gzg_scene_build_time(const gzg_scene *scene, float *device_ms
  * different builders over the same prims. */
 GZG_API gzg_status gzg_scene_tree_cost(const gzg_scene *scene, double *cost);
 
+/* ---- ingestion fast path ----------------------------------------------- */
+
+/* One mesh of gzg_gpu_build_mesh_scene: packed arrays as a PLY file holds
+ * them (12 B per vertex, 12 B per triangle, instead of the float4 points and
+ * int64 indices of TriangleMesh_C). */
+typedef struct gzg_mesh_arrays {
+        const float *points;      /* vertex_count x 3 */
+        int64_t vertex_count;
+        const int32_t *indices;   /* triangle_count x 3, into this mesh's points */
+        int64_t triangle_count;
+        int64_t material;         /* index into materials; an area-light material
+                                   * (type 2) makes every triangle an area light */
+} gzg_mesh_arrays;
+
+/* Builds a scene from packed HOST mesh arrays with no host-side per-triangle
+ * work: the arrays are copied to the device as they are, expanded there into
+ * the reference's records (prims: PrimId_C type 1, id2 = mesh << 32 | tri,
+ * or type 3 area lights numbered in mesh order; TriangleMesh_C copies with
+ * float4 points and int64 indices) and the tree is built on the device as
+ * gzg_gpu_build_scene does.  Indices out of range give GZG_ERR_BAD_SCENE. */
+GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64_t mesh_count,
+                                            const gzg_material *materials, int64_t material_count,
+                                            const gzg_build_options *options, gzg_scene **out_scene);
+
+/* A triangle mesh read from a PLY file (Shape/PlyMesh.swift): format
+ * binary_little_endian / binary_big_endian 1.0; vertex float properties
+ * x y z [u v | nx ny nz | nx ny nz u v (or s t) | u v nx ny nz]; faces as
+ * "list uchar|uint int vertex_indices" [+ "int face_indices"].  Faces must
+ * be triangles.  Arrays are library-owned until gzg_ply_free. */
+typedef struct gzg_ply_mesh {
+        int64_t vertex_count, face_count;
+        const float *points;        /* vertex_count x 3 */
+        const float *normals;       /* vertex_count x 3, or NULL */
+        const float *uvs;           /* vertex_count x 2, or NULL */
+        const int32_t *indices;     /* face_count x 3 */
+        const int32_t *face_indices;/* face_count, or NULL */
+        void *owner;
+} gzg_ply_mesh;
+
+GZG_API gzg_status gzg_ply_read(const char *path, gzg_ply_mesh **out);
+GZG_API gzg_status gzg_ply_parse(const void *data, int64_t size, gzg_ply_mesh **out);
+GZG_API gzg_status gzg_ply_free(gzg_ply_mesh *mesh);
+
 /* Parameters of the renderer's general materials, by Material_C.type:
  *   3 dielectric        (Material/Dielectric.swift): eta, roughness u/v;
  *   4 coated diffuse    (Material/CoatedDiffuse.swift, base = albedo): eta,

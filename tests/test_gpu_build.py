@@ -171,3 +171,77 @@ def test_full_size_device_build():
             {"build_ms": build_ms, "tree_cost_device": cost_dev, "tree_cost_host": cost_up,
              "prim_mismatch_equal_t": int((~same_prim).sum()), "info": info}))
     assert build_ms > 0
+
+
+# ---------------------------------------------------------------- ingestion fast path
+
+
+def _arrays_of(sb):
+    """(mesh arrays, materials) of a SceneBuilder: one entry per mesh with its
+    prims' material; area-light meshes get one emissive material each."""
+    hs = sb.build(host_bvh=False)
+    mats = list(hs.materials[: len(sb._materials)])
+    meshes = []
+    for mesh_idx, ntri, ptype, material, first in sb._prims:
+        m = sb.meshes[mesh_idx]
+        pts = m.points[:, :3]
+        idx = m.vertex_indices.reshape(-1, 3).astype(np.int32)
+        if ptype == 3:
+            le = sb._lights[first]
+            mats.append((2, (0, 0, 0), le))
+            mat = len(mats) - 1
+        else:
+            mat = material
+        meshes.append((pts, idx, mat))
+    arr = np.zeros(len(mats), F.MATERIAL_DTYPE)
+    for k, m in enumerate(mats):
+        arr[k] = tuple(m) if not isinstance(m, np.void) else m
+    return meshes, arr, hs
+
+
+def test_mesh_arrays_scene_matches_oracle(small, tmp_path):
+    from gonzales_b200 import scene as S
+
+    hs_sorted, o, d, t, isect, idx = small
+    sb = scenes.raycast_scene(subdiv=5)
+    m = sb.meshes[0]
+    # through a PLY file: write, read, build
+    path = tmp_path / "ico.ply"
+    S.write_ply(path, m.points[:, :3], m.vertex_indices.reshape(-1, 3))
+    ply = S.read_ply(path)
+    mats = np.zeros(1, F.MATERIAL_DTYPE)
+    mats[0] = (1, (0.5, 0.5, 0.5), (0, 0, 0))
+    with GpuAccelerator.from_mesh_arrays([(ply["points"], ply["indices"], 0)], mats) as acc:
+        info = acc.info()
+        assert info["triangles"] == len(ply["indices"]) and acc.build_time_ms() > 0
+        prim, tt, u, v = device_closest(acc, o, d, t)
+        assert acc.error_word() == 0
+    # prim k is triangle k of mesh 0 (id2 = 0 << 32 | k), the builder's convention
+    gpu_tri = np.where(prim >= 0, prim, -1)
+    ora_tri = _identity(hs_sorted, idx)
+    same_t = H.bits(tt) == H.bits(np.where(idx >= 0, isect["t_hit"], t))
+    culled = (~same_t) & (tt < np.where(idx >= 0, isect["t_hit"], np.inf)) & (prim >= 0)
+    assert np.all(same_t | culled)
+    assert (gpu_tri == ora_tri)[same_t].mean() > 0.999
+
+
+def test_mesh_arrays_render_equals_builder_render():
+    sb = scenes.box_scene()
+    meshes, mats, hs = _arrays_of(sb)
+    p = F.render_params(64, 64, 16, max_depth=5, rr_min_bounce=3)
+    with GpuAccelerator(sb.build()) as a, GpuAccelerator.from_mesh_arrays(meshes, mats) as b:
+        ra = a.render(p)
+        rb = b.render(p)
+    np.testing.assert_allclose(ra[0], rb[0], rtol=1e-5, atol=1e-6)
+    assert ra[3]["shadow_rays"] == rb[3]["shadow_rays"]
+
+
+def test_mesh_arrays_reject_out_of_range_index():
+    from gonzales_b200 import GzgError
+
+    mats = np.zeros(1, F.MATERIAL_DTYPE)
+    mats[0] = (1, (0.5, 0.5, 0.5), (0, 0, 0))
+    pts = np.zeros((3, 3), np.float32)
+    with pytest.raises(GzgError) as e:
+        GpuAccelerator.from_mesh_arrays([(pts, np.array([[0, 1, 3]], np.int32), 0)], mats)
+    assert "out of" in str(e.value)

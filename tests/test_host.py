@@ -245,3 +245,81 @@ def test_root_bounds_without_a_host_tree():
     lo_b, hi_b = b.root_bounds()
     np.testing.assert_allclose(lo_a, lo_b, atol=1e-6)
     np.testing.assert_allclose(hi_a, hi_b, atol=1e-6)
+
+
+# ---------------------------------------------------------------- PLY ingestion
+
+
+def _ply_mesh():
+    sb = scenes.raycast_scene(subdiv=2)
+    m = sb.meshes[0]
+    return m.points[:, :3].copy(), m.vertex_indices.reshape(-1, 3).astype(np.int32)
+
+
+@pytest.mark.parametrize("big_endian", [False, True])
+@pytest.mark.parametrize("list_type", ["uchar", "uint"])
+@pytest.mark.parametrize("layout", ["p", "pn", "puv", "pnuv"])
+def test_ply_round_trip(tmp_path, big_endian, list_type, layout):
+    from gonzales_b200 import scene as S
+
+    pts, idx = _ply_mesh()
+    nrm = (pts / np.linalg.norm(pts, axis=1, keepdims=True)).astype(np.float32) if "n" in layout else None
+    uv = pts[:, :2].copy() if "uv" in layout else None
+    fi = np.arange(len(idx), dtype=np.int32) * 3 if layout == "pnuv" else None
+    path = tmp_path / "m.ply"
+    S.write_ply(path, pts, idx, normals=nrm, uvs=uv, big_endian=big_endian, list_type=list_type, face_indices=fi)
+    r = S.read_ply(path)
+    assert np.array_equal(r["points"], pts) and np.array_equal(r["indices"], idx)
+    assert (r["normals"] is None) == (nrm is None) and (r["uvs"] is None) == (uv is None)
+    if nrm is not None:
+        assert np.array_equal(r["normals"], nrm)
+    if uv is not None:
+        assert np.array_equal(r["uvs"], uv)
+    if fi is not None:
+        assert np.array_equal(r["face_indices"], fi)
+    # the same bytes parsed from memory
+    r2 = S.read_ply(data=path.read_bytes())
+    assert np.array_equal(r2["indices"], idx)
+
+
+def _ply_error(data):
+    from gonzales_b200 import GzgError, scene as S
+
+    with pytest.raises(GzgError) as e:
+        S.read_ply(data=data)
+    return str(e.value)
+
+
+def test_ply_rejects_malformed_files(tmp_path):
+    from gonzales_b200 import scene as S
+
+    pts, idx = _ply_mesh()
+    path = tmp_path / "m.ply"
+    S.write_ply(path, pts, idx)
+    good = path.read_bytes()
+    assert "ply" in _ply_error(b"plx\n" + good[4:])
+    assert "format" in _ply_error(good.replace(b"binary_little_endian", b"ascii"))
+    assert "shorter" in _ply_error(good[:-5])
+    assert "vertex properties" in _ply_error(good.replace(b"property float z\n", b"property float w\n"))
+    # a quad face
+    head, body = good.split(b"end_header\n")
+    nv = len(pts)
+    quad = bytearray(body)
+    off = nv * 12
+    quad[off] = 4
+    assert "not 3" in _ply_error(head + b"end_header\n" + bytes(quad))
+    # an index out of range
+    bad = bytearray(body)
+    bad[off + 1:off + 5] = np.int32(nv).tobytes()
+    assert "out of range" in _ply_error(head + b"end_header\n" + bytes(bad))
+
+
+def test_mesh_arrays_build_rejects_bad_arguments_before_touching_a_device():
+    from gonzales_b200 import GpuAccelerator, GzgError
+
+    pts, idx = _ply_mesh()
+    mats = np.zeros(1, F.MATERIAL_DTYPE)
+    mats[0] = (1, (0.5, 0.5, 0.5), (0, 0, 0))
+    with pytest.raises(GzgError) as e:
+        GpuAccelerator.from_mesh_arrays([(pts, idx, 3)], mats)
+    assert "material index" in str(e.value)
