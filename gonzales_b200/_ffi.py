@@ -154,6 +154,8 @@ PROTOTYPES = {
     "gzg_ply_read": (ST, [C.c_char_p, C.POINTER(C.POINTER(PlyMesh))]),
     "gzg_ply_parse": (ST, [VP, I64, C.POINTER(C.POINTER(PlyMesh))]),
     "gzg_ply_free": (ST, [C.POINTER(PlyMesh)]),
+    "gzg_film_resolve_device": (ST, [VP, VP, I64, VP, VP, VP]),
+    "gzg_write_exr": (ST, [C.c_char_p, VP, C.c_int32, C.c_int32, C.c_int32]),
     "gzg_scene_tree_cost": (ST, [VP, C.POINTER(C.c_double)]),
     "gzg_host_instance_bounds": (ST, [VP, I64, VP, I64, VP]),
     "gzg_instanced_scene_create": (ST, [VP, I64, VP, I64, VP, I64, VP, I64, C.POINTER(VP)]),

@@ -251,10 +251,12 @@ class _ArraysHost:
     """What the Python side reads of a scene built from mesh arrays."""
 
     def __init__(self, meshes, materials):
-        pts = [np.asarray(p, np.float32).reshape(-1, 3)[np.asarray(i, np.int64).reshape(-1)] for p, i, _ in meshes]
-        pts = np.concatenate(pts) if pts else np.zeros((0, 3), np.float32)
-        self._lo = pts.min(0) if len(pts) else np.zeros(3, np.float32)
-        self._hi = pts.max(0) if len(pts) else np.zeros(3, np.float32)
+        # bounds of the vertices (a superset of the triangles' when some
+        # vertices are unreferenced: still a valid instance bound)
+        pts = [np.asarray(p, np.float32).reshape(-1, 3) for p, _, _ in meshes]
+        pts = [p for p in pts if len(p)]
+        self._lo = np.min([p.min(0) for p in pts], 0) if pts else np.zeros(3, np.float32)
+        self._hi = np.max([p.max(0) for p in pts], 0) if pts else np.zeros(3, np.float32)
         self.materials = materials
         self.nodes = None
         self.has_extended_materials = False

@@ -414,6 +414,25 @@ GZG_API gzg_status gzg_ply_read(const char *path, gzg_ply_mesh **out);
 GZG_API gzg_status gzg_ply_parse(const void *data, int64_t size, gzg_ply_mesh **out);
 GZG_API gzg_status gzg_ply_free(gzg_ply_mesh *mesh);
 
+/* ---- film output ---------------------------------------------------------- */
+
+/* Normalises device film sums into an image (Pixel.normalized,
+ * Core/Pixel.swift:12-16): image = film_rgb / film_w per pixel (3 floats per
+ * pixel), black stays black; non-black light with weight 0 (the reference
+ * throws) gives black and adds 1 to *zero_weight_count (a device counter;
+ * may be NULL).  The albedo and normal AOV sums resolve with the same film_w
+ * (Film.writeImages adds them with the sample weights).  Asynchronous on
+ * stream. */
+GZG_API gzg_status gzg_film_resolve_device(const float *film_rgb, const float *film_w, int64_t pixels, float *image,
+                                           unsigned long long *zero_weight_count, void *stream);
+
+/* Writes a HOST image (height x width x channels floats, channels 3 or 4,
+ * row 0 at the top) as an OpenEXR file with RGBA 32-bit float channels (alpha
+ * 1 when channels = 3), as Image/OpenImageIOWriter.swift writes the beauty,
+ * albedo and normal images: single-part scanlines, no compression. */
+GZG_API gzg_status gzg_write_exr(const char *path, const float *pixels, int32_t width, int32_t height,
+                                 int32_t channels);
+
 /* Parameters of the renderer's general materials, by Material_C.type:
  *   3 dielectric        (Material/Dielectric.swift): eta, roughness u/v;
  *   4 coated diffuse    (Material/CoatedDiffuse.swift, base = albedo): eta,

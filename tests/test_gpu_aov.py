@@ -68,3 +68,37 @@ def test_iso_scales_exactly_and_clamp_matches_oracle(box):
     within = (np.abs(gm - om) <= 3 * np.sqrt(gse ** 2 + ose ** 2) + 1e-4).mean()
     assert within >= 0.995, within
     np.testing.assert_allclose(g[0].sum(), o[0].sum(), rtol=1e-2)
+
+
+def test_film_resolve_and_exr_output(box, tmp_path):
+    """Film.writeImages: beauty, albedo and normal normalised by the film
+    weights on the device, written as RGBA float EXR files."""
+    from gonzales_b200 import film
+
+    torch = torch_mod()
+    hs, acc = box
+    p = dict(max_depth=4, rr_min_bounce=2)
+    rgb = torch.zeros((H, W, 3), device="cuda")
+    w = torch.zeros((H, W), device="cuda")
+    alb = torch.zeros((H, W, 3), device="cuda")
+    nrm = torch.zeros((H, W, 3), device="cuda")
+    with Renderer(acc, F.render_params(W, H, SPP, **p)) as r:
+        r.render(rgb, w, film_albedo=alb, film_normal=nrm)
+    torch.cuda.synchronize()
+    wn = w.cpu().numpy()
+    for name, sums in (("beauty", rgb), ("albedo", alb), ("normal", nrm)):
+        img, zero = film.resolve(sums, w)
+        assert zero == 0
+        s = sums.cpu().numpy()
+        black = np.all(s == 0, axis=-1, keepdims=True)
+        expect = np.where(black, 0.0, s / np.where(wn == 0, 1, wn)[..., None])
+        np.testing.assert_allclose(img.cpu().numpy(), expect, rtol=1e-6, atol=0)
+        path = tmp_path / (name + ".exr")
+        film.write_exr(path, img.cpu().numpy())
+        back, _ = film.read_exr(path)
+        assert np.array_equal(back[..., :3], img.cpu().numpy())
+    # non-black light with zero weight is counted (the reference throws)
+    rgb2 = torch.ones((2, 3), device="cuda")
+    w2 = torch.tensor([1.0, 0.0], device="cuda")
+    img, zero = film.resolve(rgb2, w2)
+    assert zero == 1 and float(img[1].abs().sum()) == 0.0

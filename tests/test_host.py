@@ -323,3 +323,26 @@ def test_mesh_arrays_build_rejects_bad_arguments_before_touching_a_device():
     with pytest.raises(GzgError) as e:
         GpuAccelerator.from_mesh_arrays([(pts, idx, 3)], mats)
     assert "material index" in str(e.value)
+
+
+def test_exr_round_trip(tmp_path):
+    from gonzales_b200 import film
+
+    rng = np.random.default_rng(5)
+    img = rng.random((7, 11, 3), dtype=np.float32) * 4
+    film.write_exr(tmp_path / "a.exr", img)
+    back, header = film.read_exr(tmp_path / "a.exr")
+    assert back.shape == (7, 11, 4)
+    assert np.array_equal(back[..., :3], img) and np.all(back[..., 3] == 1.0)
+    for k in ("channels", "compression", "dataWindow", "displayWindow", "lineOrder", "pixelAspectRatio",
+              "screenWindowCenter", "screenWindowWidth"):
+        assert k in header
+    raw = (tmp_path / "a.exr").read_bytes()
+    assert raw[:4] == bytes([0x76, 0x2F, 0x31, 0x01])
+    rgba = rng.random((3, 5, 4), dtype=np.float32)
+    film.write_exr(tmp_path / "b.exr", rgba)
+    assert np.array_equal(film.read_exr(tmp_path / "b.exr")[0], rgba)
+    from gonzales_b200 import GzgError
+
+    with pytest.raises(GzgError):
+        film.write_exr(tmp_path / "c.exr", np.zeros((2, 2, 2), np.float32))
