@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--small", action="store_true", help="small case for profiler captures")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-batch", action="store_true", help="omit the scene-batch and adjoint legs")
+    ap.add_argument("--case", default=None, choices=["instanced-small", "build"],
+                    help="run one small case alone (profiler captures) and print its own JSON line")
     return ap.parse_args()
 
 
@@ -687,10 +689,58 @@ def run_ours(args):
     return 0
 
 
+def run_case(args):
+    """Small single cases for profiler captures (one GPU):
+      instanced-small  one 640 x 360, 16-spp frame of the two-level scene with
+                       the general materials (after one warm-up frame)
+      build            the device tree build of the ray-cast mesh (three builds)"""
+    import torch
+
+    from gonzales_b200 import GpuAccelerator, InstancedAccelerator, Renderer, scenes
+    from gonzales_b200 import _ffi as F
+
+    torch.cuda.set_device(0)
+    if args.case == "instanced-small":
+        blas_hosts, inst = scenes.instanced_scene(mixed=True)
+        blas = [GpuAccelerator(h) for h in blas_hosts]
+        acc = InstancedAccelerator(blas, inst)
+        acc.set_environment(scenes.sky_map(), 1.0)
+        W, H, spp = 640, 360, 16
+        p = F.render_params(W, H, spp, max_depth=8, rr_min_bounce=2, eye=(0.0, 6.0, 48.0), target=(0.0, 0.0, 0.0),
+                            use_graph=1)
+        rgb = torch.zeros((H, W, 3), device="cuda")
+        w = torch.zeros((H, W), device="cuda")
+        with Renderer(acc, p) as r:
+            r.render(rgb, w)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r.render(rgb, w)
+            e1.record()
+            torch.cuda.synchronize()
+            stats = r.stats()
+        out = {"case": args.case, "ms_per_frame": e0.elapsed_time(e1), "stats": stats, "error_word": acc.error_word()}
+        acc.close()
+        for b in blas:
+            b.close()
+    else:
+        hs = scenes.raycast_scene(subdiv=8).build()
+        ms = []
+        for _ in range(3):
+            with GpuAccelerator(hs, device_build=True) as a:
+                ms.append(a.build_time_ms())
+        out = {"case": args.case, "device_build_ms": ms}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.case:
+        return run_case(args)
     return run_ours(args)
 
 

@@ -133,8 +133,10 @@ __device__ __forceinline__ int prefix(const uint64_t *__restrict__ k, int m, int
 
 // Binary radix tree: internal node i (0 .. m-2) gets children (>= 0:
 // internal node, < 0: ~leaf) and its sorted range [first, last].
-__global__ void k_radix_tree(const uint64_t *__restrict__ keys, int m, int2 *__restrict__ child,
-                             int2 *__restrict__ range, int *__restrict__ parent_int, int *__restrict__ parent_leaf) {
+__global__ void k_radix_tree(const uint64_t *__restrict__ keys, const unsigned long long *__restrict__ m_dev,
+                             int2 *__restrict__ child, int2 *__restrict__ range, int *__restrict__ parent_int,
+                             int *__restrict__ parent_leaf) {
+        const int m = (int)*m_dev;
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= m - 1) return;
         const int d = prefix(keys, m, i, i + 1) - prefix(keys, m, i, i - 1) >= 0 ? 1 : -1;
@@ -181,9 +183,11 @@ __device__ __forceinline__ void code_box(int code, const float4 *__restrict__ nb
 
 // Bottom-up node bounds: one thread per leaf climbs while it is the second
 // child to arrive.  Every climb ends (each node admits one second arrival).
-__global__ void k_refit(const uint64_t *__restrict__ keys, int m, const int2 *__restrict__ child,
-                        const int *__restrict__ parent_int, const int *__restrict__ parent_leaf,
-                        const float4 *__restrict__ pbox, float4 *__restrict__ nbox, int *__restrict__ arrivals) {
+__global__ void k_refit(const uint64_t *__restrict__ keys, const unsigned long long *__restrict__ m_dev,
+                        const int2 *__restrict__ child, const int *__restrict__ parent_int,
+                        const int *__restrict__ parent_leaf, const float4 *__restrict__ pbox, float4 *__restrict__ nbox,
+                        int *__restrict__ arrivals) {
+        const int m = (int)*m_dev;
         const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
         if (leaf >= m || m < 2) return;
         int node = parent_leaf[leaf];
@@ -202,7 +206,7 @@ __global__ void k_refit(const uint64_t *__restrict__ keys, int m, const int2 *__
 
 struct Tree {
         const uint64_t *keys;
-        int m;
+        const unsigned long long *m_dev;  // intersectable prims (sorted first)
         const int2 *child, *range;
         const float4 *nbox, *pbox;
         const float4 *pv0, *pv1, *pv2;
@@ -262,6 +266,8 @@ __device__ void quantise_axis_dev(const double *clo, const double *chi, int n, f
         }
 }
 
+constexpr int kRootItem = INT_MIN;  // the root's code, resolved on the device
+
 // One level of the collapse: item = (binary code, wide node index).
 __global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_t *__restrict__ n_items,
                            int2 *__restrict__ next, uint32_t *__restrict__ n_next, uint32_t *__restrict__ counters,
@@ -269,95 +275,102 @@ __global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_
                            float4 *__restrict__ tv2, uint32_t node_cap, uint32_t tri_cap, uint32_t *__restrict__ err) {
         const uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
         if (it >= *n_items) return;
-        const int2 item = items[it];
+        const int m = (int)*t.m_dev;
+        int2 item = items[it];
+        if (item.x == kRootItem) item.x = m >= 2 ? 0 : ~0;
         int kids[8];
+        double area[8];
         int n = 0;
-        if (t.m == 0) {
+        if (m == 0) {
                 n = 0;
         } else if (code_leaf(t, item.x)) {
                 kids[n++] = item.x;
         } else {
                 const int2 c = t.child[item.x];
-                kids[n++] = c.x;
-                kids[n++] = c.y;
+                kids[0] = c.x;
+                kids[1] = c.y;
+                area[0] = code_leaf(t, c.x) ? -1.0 : code_area(t, c.x);
+                area[1] = code_leaf(t, c.y) ? -1.0 : code_area(t, c.y);
+                n = 2;
                 while (n < 8) {
                         int best = -1;
                         double best_a = -1.0;
                         for (int i = 0; i < n; ++i)
-                                if (!code_leaf(t, kids[i])) {
-                                        const double a = code_area(t, kids[i]);
-                                        if (a > best_a) {
-                                                best_a = a;
-                                                best = i;
-                                        }
+                                if (area[i] > best_a) {
+                                        best_a = area[i];
+                                        best = i;
                                 }
                         if (best < 0) break;
                         const int2 c2 = t.child[kids[best]];
-                        for (int i = n; i > best + 1; --i) kids[i] = kids[i - 1];
+                        for (int i = n; i > best + 1; --i) {
+                                kids[i] = kids[i - 1];
+                                area[i] = area[i - 1];
+                        }
                         kids[best] = c2.x;
                         kids[best + 1] = c2.y;
+                        area[best] = code_leaf(t, c2.x) ? -1.0 : code_area(t, c2.x);
+                        area[best + 1] = code_leaf(t, c2.y) ? -1.0 : code_area(t, c2.y);
                         ++n;
                 }
         }
-        // child boxes and octant slots (assign_slots of wide_bvh.cpp)
-        double clo[8][3], chi[8][3], cc[8][3], pc[3] = {0, 0, 0};
+        // child boxes and octant slots: slot s takes the child farthest along
+        // (+-1, +-1, +-1) (bit a of s set = +), greedily by decreasing reach
+        double clo[8][3], chi[8][3], pc[3] = {0, 0, 0};
+        float cc[8][3];
         for (int k = 0; k < n; ++k) {
                 code_bounds(t, kids[k], clo[k], chi[k]);
-                for (int a = 0; a < 3; ++a) {
-                        cc[k][a] = 0.5 * (clo[k][a] + chi[k][a]);
-                        pc[a] += cc[k][a] / n;
-                }
+                for (int a = 0; a < 3; ++a) pc[a] += 0.5 * (clo[k][a] + chi[k][a]) / n;
         }
+        for (int k = 0; k < n; ++k)
+                for (int a = 0; a < 3; ++a) cc[k][a] = (float)(0.5 * (clo[k][a] + chi[k][a]) - pc[a]);
+        float cost[8][8];
+        for (int k = 0; k < n; ++k)
+                for (int s2 = 0; s2 < 8; ++s2)
+                        cost[k][s2] = -((s2 & 1 ? cc[k][0] : -cc[k][0]) + (s2 & 2 ? cc[k][1] : -cc[k][1]) +
+                                        (s2 & 4 ? cc[k][2] : -cc[k][2]));
         int kid_in_slot[8];
-        bool kdone[8], sdone[8];
-        for (int i = 0; i < 8; ++i) {
-                kid_in_slot[i] = -1;
-                kdone[i] = sdone[i] = false;
-        }
+        unsigned kfree = (1u << n) - 1u, sfree = 0xFFu;
+        for (int i = 0; i < 8; ++i) kid_in_slot[i] = -1;
         for (int round = 0; round < n; ++round) {
-                // the smallest cost -d over free pairs, ties to the lowest (k, s)
-                // index as the host's stable sort does
-                double best = CUDART_INF;
+                float best = CUDART_INF_F;
                 int bk = -1, bs = -1;
                 for (int k = 0; k < n; ++k) {
-                        if (kdone[k]) continue;
-                        for (int s = 0; s < 8; ++s) {
-                                if (sdone[s]) continue;
-                                double d = 0;
-                                for (int a = 0; a < 3; ++a) d += (cc[k][a] - pc[a]) * ((s >> a) & 1 ? 1.0 : -1.0);
-                                if (-d < best) {
-                                        best = -d;
+                        if (!((kfree >> k) & 1u)) continue;
+                        for (int s2 = 0; s2 < 8; ++s2)
+                                if (((sfree >> s2) & 1u) && cost[k][s2] < best) {
+                                        best = cost[k][s2];
                                         bk = k;
-                                        bs = s;
+                                        bs = s2;
                                 }
-                        }
                 }
-                kdone[bk] = sdone[bs] = true;
+                if (bk < 0) break;
+                kfree &= ~(1u << bk);
+                sfree &= ~(1u << bs);
                 kid_in_slot[bs] = bk;
         }
         WideNode w;
         memset(&w, 0, sizeof(w));
-        int m = 0, order[8];
+        int nq = 0, order[8];
         double ql[3][8], qh[3][8];
         for (int s = 0; s < 8; ++s)
                 if (kid_in_slot[s] >= 0) {
                         const int k = kid_in_slot[s];
                         for (int a = 0; a < 3; ++a) {
-                                ql[a][m] = clo[k][a];
-                                qh[a][m] = chi[k][a];
+                                ql[a][nq] = clo[k][a];
+                                qh[a][nq] = chi[k][a];
                         }
-                        order[m++] = s;
+                        order[nq++] = s;
                 }
         float pxyz[3] = {0, 0, 0};
         uint8_t ee[3] = {127, 127, 127};
         for (int a = 0; a < 3; ++a) {
                 uint8_t qlo8[8], qhi8[8];
-                if (m > 0) quantise_axis_dev(ql[a], qh[a], m, &pxyz[a], &ee[a], qlo8, qhi8);
+                if (nq > 0) quantise_axis_dev(ql[a], qh[a], nq, &pxyz[a], &ee[a], qlo8, qhi8);
                 for (int s = 0; s < 8; ++s) {
                         w.qlo[a][s] = 255;
                         w.qhi[a][s] = 0;
                 }
-                for (int i = 0; i < m; ++i) {
+                for (int i = 0; i < nq; ++i) {
                         w.qlo[a][order[i]] = qlo8[i];
                         w.qhi[a][order[i]] = qhi8[i];
                 }
@@ -440,106 +453,105 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
+        uint32_t *pinned = nullptr;  // level counts read back each level
+        GZG_CK(cudaMallocHost(reinterpret_cast<void **>(&pinned), 16), "build: host counters");
         struct Ev {
                 cudaEvent_t a, b;
+                uint32_t *h;
                 ~Ev() {
                         if (a) cudaEventDestroy(a);
                         if (b) cudaEventDestroy(b);
+                        if (h) cudaFreeHost(h);
                 }
-        } ev{e0, e1};
+        } ev{e0, e1, pinned};
         const float4 *d0 = reinterpret_cast<const float4 *>(pv0), *d1 = reinterpret_cast<const float4 *>(pv1),
                      *d2 = reinterpret_cast<const float4 *>(pv2);
-        float4 *pbox;
-        int *cb;
+        // every buffer up front (the intersectable count m <= n is known only
+        // on the device), so the timed build holds no allocation
+        const size_t N = (size_t)std::max<int64_t>(n, 1);
+        float4 *pbox, *nbox;
+        int *cb, *parent_int, *parent_leaf, *arrivals;
         unsigned long long *nvalid;
         uint64_t *keys, *sorted;
-        GZG_CK(dalloc(&pbox, 2 * (size_t)n, tmp), "build: prim bounds");
+        int2 *child, *range, *qa, *qb;
+        uint32_t *counts, *err;  // counts: [0] nodes used, [1] tris used, [2] items in, [3] items out
+        GZG_CK(dalloc(&pbox, 2 * N, tmp), "build: prim bounds");
+        GZG_CK(dalloc(&nbox, 2 * N, tmp), "build: node bounds");
         GZG_CK(dalloc(&cb, 6, tmp), "build: centroid bounds");
         GZG_CK(dalloc(&nvalid, 1, tmp), "build: prim count");
-        GZG_CK(dalloc(&keys, (size_t)n, tmp), "build: keys");
-        GZG_CK(dalloc(&sorted, (size_t)n, tmp), "build: keys");
+        GZG_CK(dalloc(&keys, N, tmp), "build: keys");
+        GZG_CK(dalloc(&sorted, N, tmp), "build: keys");
+        GZG_CK(dalloc(&child, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&range, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&parent_int, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&parent_leaf, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&arrivals, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&qa, N, tmp), "build: queue");
+        GZG_CK(dalloc(&qb, N, tmp), "build: queue");
+        GZG_CK(dalloc(&counts, 4, tmp), "build: counters");
+        GZG_CK(dalloc(&err, 1, tmp), "build: error word");
+        size_t temp_bytes = 0;
+        if (n > 0) cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys, sorted, (int)n, 0, 64, st);
+        uint8_t *temp;
+        GZG_CK(dalloc(&temp, temp_bytes, tmp), "build: sort scratch");
+        // outputs, at most one wide node per binary internal node (and the
+        // root), one record per prim
+        WideNode *nodes;
+        float4 *tv0, *tv1, *tv2;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&nodes), N * sizeof(WideNode)), "build: wide nodes");
+        out->nodes = nodes;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv0), N * sizeof(float4)), "build: triangles");
+        out->tv0 = tv0;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv1), N * sizeof(float4)), "build: triangles");
+        out->tv1 = tv1;
+        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv2), N * sizeof(float4)), "build: triangles");
+        out->tv2 = tv2;
+
         cudaEventRecord(e0, st);
         const int B = 256;
-        const unsigned grid = (unsigned)((n + B - 1) / B);
+        const unsigned grid = (unsigned)((N + B - 1) / B);
         GZG_CK(cudaMemsetAsync(cb, 0x7F, 6 * sizeof(int), st), "build: reset");
         GZG_CK(cudaMemsetAsync(nvalid, 0, sizeof(unsigned long long), st), "build: reset");
+        GZG_CK(cudaMemsetAsync(arrivals, 0, N * sizeof(int), st), "build: reset");
+        const uint32_t init[4] = {1u, 0u, 1u, 0u};  // the root is node 0
+        std::memcpy(pinned, init, sizeof(init));
+        GZG_CK(cudaMemcpyAsync(counts, pinned, sizeof(init), cudaMemcpyHostToDevice, st), "build: counters");
+        GZG_CK(cudaMemsetAsync(err, 0, 4, st), "build: error word");
+        const int2 root = make_int2(kRootItem, 0);
+        GZG_CK(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st), "build: queue");
         if (n > 0) {
                 k_prim_bounds<<<grid, B, 0, st>>>(d0, d1, d2, n, pbox, cb, nvalid);
                 k_keys<<<grid, B, 0, st>>>(d0, pbox, n, cb, keys);
-                size_t temp_bytes = 0;
-                cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys, sorted, (int)n, 0, 64, st);
-                void *temp;
-                GZG_CK(dalloc(reinterpret_cast<uint8_t **>(&temp), temp_bytes, tmp), "build: sort scratch");
                 GZG_CK(cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys, sorted, (int)n, 0, 64, st), "build: sort");
+                k_radix_tree<<<grid, B, 0, st>>>(sorted, nvalid, child, range, parent_int, parent_leaf);
+                k_refit<<<grid, B, 0, st>>>(sorted, nvalid, child, parent_int, parent_leaf, pbox, nbox, arrivals);
         }
-        unsigned long long hv = 0;
-        GZG_CK(cudaMemcpyAsync(&hv, nvalid, sizeof(hv), cudaMemcpyDeviceToHost, st), "build: prim count");
-        GZG_CK(cudaStreamSynchronize(st), "build: prim count");
-        const int m = (int)hv;
-        int2 *child, *range;
-        int *parent_int, *parent_leaf, *arrivals;
-        float4 *nbox;
-        const size_t ni = (size_t)std::max(m - 1, 1);
-        GZG_CK(dalloc(&child, ni, tmp), "build: radix tree");
-        GZG_CK(dalloc(&range, ni, tmp), "build: radix tree");
-        GZG_CK(dalloc(&parent_int, ni, tmp), "build: radix tree");
-        GZG_CK(dalloc(&parent_leaf, (size_t)std::max(m, 1), tmp), "build: radix tree");
-        GZG_CK(dalloc(&arrivals, ni, tmp), "build: radix tree");
-        GZG_CK(dalloc(&nbox, 2 * ni, tmp), "build: node bounds");
-        GZG_CK(cudaMemsetAsync(arrivals, 0, ni * sizeof(int), st), "build: reset");
-        if (m >= 2) {
-                k_radix_tree<<<(unsigned)((m - 1 + B - 1) / B), B, 0, st>>>(sorted, m, child, range, parent_int,
-                                                                            parent_leaf);
-                k_refit<<<(unsigned)((m + B - 1) / B), B, 0, st>>>(sorted, m, child, parent_int, parent_leaf, pbox,
-                                                                   nbox, arrivals);
-        }
-        // wide nodes: at most one per binary internal node (and one root)
-        const uint32_t node_cap = (uint32_t)std::max(m, 1), tri_cap = (uint32_t)std::max(m, 1);
-        WideNode *nodes;
-        float4 *tv0, *tv1, *tv2;
-        int2 *qa, *qb;
-        uint32_t *counts;  // [0] nodes used, [1] tris used, [2] items in, [3] items out
-        uint32_t *err;
-        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&nodes), (size_t)node_cap * sizeof(WideNode)), "build: wide nodes");
-        out->nodes = nodes;
-        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv0), (size_t)tri_cap * sizeof(float4)), "build: triangles");
-        out->tv0 = tv0;
-        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv1), (size_t)tri_cap * sizeof(float4)), "build: triangles");
-        out->tv1 = tv1;
-        GZG_CK(cudaMalloc(reinterpret_cast<void **>(&tv2), (size_t)tri_cap * sizeof(float4)), "build: triangles");
-        out->tv2 = tv2;
-        GZG_CK(dalloc(&qa, node_cap, tmp), "build: queue");
-        GZG_CK(dalloc(&qb, node_cap, tmp), "build: queue");
-        GZG_CK(dalloc(&counts, 4, tmp), "build: counters");
-        GZG_CK(dalloc(&err, 1, tmp), "build: error word");
-        const uint32_t init[4] = {1u, 0u, 1u, 0u};  // the root is node 0
-        GZG_CK(cudaMemcpyAsync(counts, init, sizeof(init), cudaMemcpyHostToDevice, st), "build: counters");
-        GZG_CK(cudaMemsetAsync(err, 0, 4, st), "build: error word");
-        const int2 root = make_int2(m >= 2 ? 0 : ~0, 0);
-        GZG_CK(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st), "build: queue");
-        Tree t{sorted, m, child, range, nbox, pbox, d0, d1, d2, leaf_size};
+        const uint32_t cap = (uint32_t)N;
+        Tree t{sorted, nvalid, child, range, nbox, pbox, d0, d1, d2, leaf_size};
         uint32_t level_items = 1;
         int depth = 0;
         while (level_items > 0) {
                 if (++depth > 64) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: tree deeper than 64 levels");
                 GZG_CK(cudaMemsetAsync(counts + 3, 0, 4, st), "build: counters");
                 k_collapse<<<(level_items + 127) / 128, 128, 0, st>>>(t, qa, counts + 2, qb, counts + 3, counts, nodes,
-                                                                     tv0, tv1, tv2, node_cap, tri_cap, err);
+                                                                     tv0, tv1, tv2, cap, cap, err);
                 GZG_CK(cudaMemcpyAsync(counts + 2, counts + 3, 4, cudaMemcpyDeviceToDevice, st), "build: counters");
-                GZG_CK(cudaMemcpyAsync(&level_items, counts + 3, 4, cudaMemcpyDeviceToHost, st), "build: counters");
+                GZG_CK(cudaMemcpyAsync(pinned, counts + 3, 4, cudaMemcpyDeviceToHost, st), "build: counters");
                 GZG_CK(cudaStreamSynchronize(st), "build: collapse");
+                level_items = pinned[0];
                 std::swap(qa, qb);
         }
         cudaEventRecord(e1, st);
-        uint32_t hc[2], herr = 0;
-        GZG_CK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, st), "build: counters");
-        GZG_CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st), "build: error word");
+        GZG_CK(cudaMemcpyAsync(pinned, counts, 8, cudaMemcpyDeviceToHost, st), "build: counters");
+        GZG_CK(cudaMemcpyAsync(pinned + 2, err, 4, cudaMemcpyDeviceToHost, st), "build: error word");
+        unsigned long long hv = 0;
+        GZG_CK(cudaMemcpyAsync(&hv, nvalid, sizeof(hv), cudaMemcpyDeviceToHost, st), "build: prim count");
         GZG_CK(cudaStreamSynchronize(st), "build");
-        if (herr) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: collapse ran out of node or triangle slots");
-        if (hc[1] != (uint32_t)m)
+        if (pinned[2]) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: collapse ran out of node or triangle slots");
+        if (pinned[1] != (uint32_t)hv)
                 return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: leaves do not cover every prim");
-        out->node_count = hc[0];
-        out->tri_count = hc[1];
+        out->node_count = pinned[0];
+        out->tri_count = pinned[1];
         out->depth = depth;
         cudaEventElapsedTime(device_ms, e0, e1);
         return clear_error();
