@@ -26,6 +26,11 @@
 namespace gzg {
 namespace {
 
+// Triangles per leaf child: a BVH2 leaf with more is split in order into a
+// balanced binary tree over groups of this size (each group gets its own
+// quantised box).
+constexpr int64_t kLeafTris = 4;
+
 struct BinNode {
         float lo[3], hi[3];
         int32_t l = -1, r = -1;        // children (interior)
@@ -148,7 +153,7 @@ class Converter {
 
         // Balanced binary tree over chunks [first, first+count) of tris_ with <= 4 each.
         int32_t split_leaf(int64_t first, int64_t count) {
-                if (count <= 4) {
+                if (count <= kLeafTris) {
                         float lo[3], hi[3];
                         for (int a = 0; a < 3; ++a) {
                                 lo[a] = std::numeric_limits<float>::infinity();
@@ -166,8 +171,8 @@ class Converter {
                         bin_[id].tri_count = (int32_t)count;
                         return id;
                 }
-                int64_t chunks = (count + 3) / 4;
-                int64_t left = (chunks / 2) * 4;
+                int64_t chunks = (count + kLeafTris - 1) / kLeafTris;
+                int64_t left = (chunks / 2) * kLeafTris;
                 int32_t l = split_leaf(first, left);
                 int32_t r = split_leaf(first + left, count - left);
                 float lo[3], hi[3];
@@ -213,11 +218,11 @@ class Converter {
                                         }
                                         const int64_t cnt = (int64_t)tris_.size() - first;
                                         int32_t id = -1;
-                                        if (cnt > 0 && cnt <= 4) {
+                                        if (cnt > 0 && cnt <= kLeafTris) {
                                                 id = new_bin(n.bounds_min, n.bounds_max);
                                                 bin_[id].tri_first = first;
                                                 bin_[id].tri_count = (int32_t)cnt;
-                                        } else if (cnt > 4) {
+                                        } else if (cnt > kLeafTris) {
                                                 id = split_leaf(first, cnt);
                                         }
                                         results.push_back(id);
