@@ -390,17 +390,21 @@ def build_leg(hs, rays_d, args, stream, barrier):
     upload_s = time.perf_counter() - t0
     host_rate, host_cost = timed(up), up.tree_cost()
     up.close()
-    ms = []
-    for _ in range(3):
-        t0 = time.perf_counter()
-        dev = GpuAccelerator(hs, device_build=True)
-        wall = time.perf_counter() - t0
-        ms.append(dev.build_time_ms())
-        if len(ms) < 3:
-            dev.close()
-    dev_rate, dev_cost, info = timed(dev), dev.tree_cost(), dev.info()
-    err = dev.error_word()
-    dev.close()
+    from gonzales_b200 import _ffi as F
+
+    res = {}
+    for builder, name in ((F.BUILD_PLOC, "ploc"), (F.BUILD_LBVH, "lbvh")):
+        ms = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            dev = GpuAccelerator(hs, device_build=True, builder=builder)
+            wall = time.perf_counter() - t0
+            ms.append(dev.build_time_ms())
+            if len(ms) < 3:
+                dev.close()
+        res[name] = {"build_ms": min(ms), "wall_s": wall, "tree_cost": dev.tree_cost(),
+                     "closest_mrays": timed(dev), "wide_nodes": dev.info()["wide_nodes"], "error_word": dev.error_word()}
+        dev.close()
     # ingestion fast path: packed float x3 points and int32 indices straight
     # to the device expansion and build (gzg_gpu_build_mesh_scene)
     packed = [(m.points[:, :3].copy(), m.vertex_indices.reshape(-1, 3).astype(np.int32), 0) for m in hs.meshes]
@@ -413,12 +417,10 @@ def build_leg(hs, rays_d, args, stream, barrier):
         fast_ms = acc_f.build_time_ms()
         acc_f.close()
     return {"config": "ray-cast mesh, %d triangles; closest hit on the %d bench rays" % (hs.triangle_count, n),
-            "device_build_ms": min(ms), "device_build_wall_s": wall, "host_sah_build_s": host_sah_s,
-            "packed_arrays_to_scene_wall_s": min(fast), "packed_arrays_build_ms": fast_ms,
-            "host_sah_threads": threads, "upload_with_host_tree_s": upload_s,
-            "tree_cost_device": dev_cost, "tree_cost_host_sah": host_cost,
-            "closest_mrays_device_tree": dev_rate, "closest_mrays_host_tree": host_rate,
-            "device_wide_nodes": info["wide_nodes"], "error_word": err}
+            "device_ploc": res["ploc"], "device_lbvh": res["lbvh"], "host_sah_build_s": host_sah_s,
+            "host_sah_threads": threads, "upload_with_host_tree_s": upload_s, "tree_cost_host_sah": host_cost,
+            "closest_mrays_host_tree": host_rate, "packed_arrays_to_scene_wall_s": min(fast),
+            "packed_arrays_build_ms": fast_ms}
 
 
 def adjoint_leg(args, stream, barrier):

@@ -70,8 +70,11 @@ class TraceOptions(C.Structure):
                 ("fetch_counters", C.c_void_p)]
 
 
+BUILD_DEFAULT, BUILD_LBVH, BUILD_PLOC = 0, 1, 2
+
+
 class BuildOptions(C.Structure):
-    _fields_ = [("leaf_size", C.c_int32), ("reserved", C.c_int32 * 3)]
+    _fields_ = [("leaf_size", C.c_int32), ("builder", C.c_int32), ("radius", C.c_int32), ("reserved", C.c_int32)]
 
 
 class MeshArrays(C.Structure):

@@ -39,7 +39,7 @@ def _stream_handle(stream):
 
 
 class GpuAccelerator:
-    def __init__(self, host_scene: HostScene, device_build=None, leaf_size=0):
+    def __init__(self, host_scene: HostScene, device_build=None, leaf_size=0, builder=0, radius=0):
         """Uploads the scene with the host's BVH2 (gzg_gpu_upload_scene), or
         builds its tree on the device (gzg_gpu_build_scene) when device_build
         is true or the scene has no BVH2 (SceneBuilder.build(host_bvh=False))."""
@@ -53,6 +53,8 @@ class GpuAccelerator:
         if self.device_built:
             opt = F.BuildOptions()
             opt.leaf_size = int(leaf_size)
+            opt.builder = int(builder)
+            opt.radius = int(radius)
             F.check(F.lib().gzg_gpu_build_scene(
                 F.ptr(host_scene.prims), len(host_scene.prims), C.addressof(meshes), len(host_scene.meshes),
                 F.ptr(pts), F.ptr(fi), F.ptr(vi), F.ptr(host_scene.materials), len(host_scene.materials),
@@ -71,7 +73,7 @@ class GpuAccelerator:
                 raise
 
     @classmethod
-    def from_mesh_arrays(cls, meshes, materials, leaf_size=0):
+    def from_mesh_arrays(cls, meshes, materials, leaf_size=0, builder=0, radius=0):
         """The ingestion fast path (gzg_gpu_build_mesh_scene): meshes is a list
         of (points (n, 3) float32, indices (m, 3) int32, material index);
         materials a MATERIAL_DTYPE array.  Prim k of the scene is triangle k
@@ -88,6 +90,8 @@ class GpuAccelerator:
         materials = np.ascontiguousarray(materials)
         opt = F.BuildOptions()
         opt.leaf_size = int(leaf_size)
+        opt.builder = int(builder)
+        opt.radius = int(radius)
         handle = C.c_void_p()
         F.check(F.lib().gzg_gpu_build_mesh_scene(C.addressof(arr), len(meshes), F.ptr(materials), len(materials),
                                                  C.byref(opt), C.byref(handle)))

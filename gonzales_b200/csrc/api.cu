@@ -401,7 +401,9 @@ gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count
             material_count < 0 || (material_count > 0 && !materials))
                 return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": bad arguments");
         if (build && (build->leaf_size < 0 || build->leaf_size > 4))
-                return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": leaf_size must be 0 (default 4) to 4");
+                return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": leaf_size must be 0 (default 1) to 4");
+        if (build && (build->builder < 0 || build->builder > GZG_BUILD_PLOC || build->radius < 0 || build->radius > 64))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, name + ": unknown builder or radius outside 0..64");
         if (prim_count > INT32_MAX - 1 || bvh2_node_count > INT32_MAX)
                 return set_error(GZG_ERR_LIMIT, name + ": more than 2^31 prims or nodes");
         // Host-side validation and conversion first: a malformed scene is
@@ -515,7 +517,8 @@ gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count
                 GpuWide gw;
                 float ms = 0.0f;
                 st = gpu_build_wide(reinterpret_cast<const float4_ *>(d.pv0), reinterpret_cast<const float4_ *>(d.pv1),
-                                    reinterpret_cast<const float4_ *>(d.pv2), prim_count, build->leaf_size, &gw, &ms);
+                                    reinterpret_cast<const float4_ *>(d.pv2), prim_count, build->leaf_size,
+                                    build->builder, build->radius, &gw, &ms);
                 for (void *p : {gw.nodes, gw.tv0, gw.tv1, gw.tv2})
                         if (p) scene->allocs.push_back(p);
                 if (st != GZG_OK) return st;
@@ -649,7 +652,9 @@ GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64
         const gzg_build_options defaults{};
         const gzg_build_options &opt = options ? *options : defaults;
         if (opt.leaf_size < 0 || opt.leaf_size > 4)
-                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": leaf_size must be 0 (default 4) to 4");
+                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": leaf_size must be 0 (default 1) to 4");
+        if (opt.builder < 0 || opt.builder > GZG_BUILD_PLOC || opt.radius < 0 || opt.radius > 64)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": unknown builder or radius outside 0..64");
         std::vector<MeshRange> ranges((size_t)mesh_count);
         int64_t nv = 0, nt = 0, lights = 0;
         for (int64_t k = 0; k < mesh_count; ++k) {
@@ -726,7 +731,7 @@ GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64
         d.err = const_cast<uint32_t *>(ew);
         GpuWide gw;
         float ms = 0.0f;
-        st = gpu_build_wide(pv[0], pv[1], pv[2], nt, opt.leaf_size, &gw, &ms);
+        st = gpu_build_wide(pv[0], pv[1], pv[2], nt, opt.leaf_size, opt.builder, opt.radius, &gw, &ms);
         for (void *p : {gw.nodes, gw.tv0, gw.tv1, gw.tv2})
                 if (p) scene->allocs.push_back(p);
         if (st != GZG_OK) return st;

@@ -9,11 +9,14 @@
 //      centroid in the upper half, the prim index in the lower half (unique
 //      keys, a deterministic order); other prims sort last;
 //   3. a radix sort of the keys (CUB);
-//   4. the binary radix tree over the sorted keys (Karras 2012: one thread
-//      per internal node finds its range and split from common-prefix
-//      lengths);
-//   5. node bounds bottom-up (one thread per leaf; the second of two
-//      children to arrive at a node computes it);
+//   4. the binary tree, by default the radix tree over the sorted keys
+//      (Karras 2012: one thread per internal node finds its range and split
+//      from common-prefix lengths) with node bounds computed bottom-up (one
+//      thread per leaf; the second of two children to arrive at a node
+//      computes it); or PLOC (Meister and Bittner 2018: clusters merge with
+//      their mutual nearest neighbour in Morton order, then compact), whose
+//      lower surface-area cost did not traverse faster on the ray-cast mesh;
+//   5. (bounds come with the tree)
 //   6. collapse into wide nodes level by level, as the host converter does
 //      (wide_bvh.cpp): a wide node opens the interior child of largest
 //      surface area until it has 8 children; a binary node covering at most
@@ -132,9 +135,9 @@ __device__ __forceinline__ int prefix(const uint64_t *__restrict__ k, int m, int
 }
 
 // Binary radix tree: internal node i (0 .. m-2) gets children (>= 0:
-// internal node, < 0: ~leaf) and its sorted range [first, last].
+// internal node, < 0: ~leaf) and the number of prims under it.
 __global__ void k_radix_tree(const uint64_t *__restrict__ keys, const unsigned long long *__restrict__ m_dev,
-                             int2 *__restrict__ child, int2 *__restrict__ range, int *__restrict__ parent_int,
+                             int2 *__restrict__ child, int *__restrict__ count, int *__restrict__ parent_int,
                              int *__restrict__ parent_leaf) {
         const int m = (int)*m_dev;
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,7 +161,7 @@ __global__ void k_radix_tree(const uint64_t *__restrict__ keys, const unsigned l
         const int left = first == gamma ? ~gamma : gamma;
         const int right = last == gamma + 1 ? ~(gamma + 1) : gamma + 1;
         child[i] = make_int2(left, right);
-        range[i] = make_int2(first, last);
+        count[i] = last - first + 1;
         if (left >= 0)
                 parent_int[left] = i;
         else
@@ -204,21 +207,133 @@ __global__ void k_refit(const uint64_t *__restrict__ keys, const unsigned long l
         }
 }
 
+// ---- PLOC (Meister & Bittner 2018): clusters in Morton order repeatedly
+// merge with their mutual nearest neighbour (surface area of the union box)
+// within a window of +-radius, then the survivors are compacted.
+struct alignas(16) Cluster {
+        float lo[3];
+        int code;  // >= 0 internal node, < 0 ~(sorted leaf position)
+        float hi[3];
+        int cnt;   // prims under the cluster
+};
+
+__device__ __forceinline__ float union_area(const Cluster &a, const Cluster &b) {
+        const float x = fmaxf(a.hi[0], b.hi[0]) - fminf(a.lo[0], b.lo[0]);
+        const float y = fmaxf(a.hi[1], b.hi[1]) - fminf(a.lo[1], b.lo[1]);
+        const float z = fmaxf(a.hi[2], b.hi[2]) - fminf(a.lo[2], b.lo[2]);
+        return x * y + x * z + y * z;
+}
+
+__global__ void k_ploc_init(const uint64_t *__restrict__ keys, const unsigned long long *__restrict__ m_dev,
+                            const float4 *__restrict__ pbox, Cluster *__restrict__ cl) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= (int)*m_dev) return;
+        const uint32_t p = (uint32_t)(keys[i] & 0xFFFFFFFFu);
+        const float4 lo = pbox[2 * (size_t)p], hi = pbox[2 * (size_t)p + 1];
+        Cluster c;
+        c.lo[0] = lo.x;
+        c.lo[1] = lo.y;
+        c.lo[2] = lo.z;
+        c.hi[0] = hi.x;
+        c.hi[1] = hi.y;
+        c.hi[2] = hi.z;
+        c.code = ~i;
+        c.cnt = 1;
+        cl[i] = c;
+}
+
+// nearest neighbour in the window (ties to the lower index); force: pair
+// 2k with 2k + 1 (used after an iteration without a merge)
+__global__ void k_ploc_nn(const Cluster *__restrict__ cl, int count, int radius, int force, int *__restrict__ nn) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count) return;
+        if (force) {
+                nn[i] = (i ^ 1) < count ? (i ^ 1) : i;
+                return;
+        }
+        const Cluster a = cl[i];
+        float best = CUDART_INF_F;
+        int bj = i;
+        const int j0 = max(0, i - radius), j1 = min(count - 1, i + radius);
+        for (int j = j0; j <= j1; ++j) {
+                if (j == i) continue;
+                const float d = union_area(a, cl[j]);
+                if (d < best) {
+                        best = d;
+                        bj = j;
+                }
+        }
+        nn[i] = bj;
+}
+
+__global__ void k_ploc_merge(Cluster *__restrict__ cl, const int *__restrict__ nn, int count,
+                             uint32_t *__restrict__ node_counter, uint32_t node_cap, int2 *__restrict__ child,
+                             int *__restrict__ ncount, float4 *__restrict__ nbox, int *__restrict__ keep,
+                             uint32_t *__restrict__ err) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count) return;
+        const int j = nn[i];
+        const bool mutual = j != i && nn[j] == i;
+        if (!mutual) {
+                keep[i] = 1;
+                return;
+        }
+        if (i > j) {
+                keep[i] = 0;
+                return;
+        }
+        const uint32_t node = atomicAdd(node_counter, 1u);
+        if (node >= node_cap) {
+                atomicOr(err, 1u);
+                keep[i] = 1;
+                return;
+        }
+        const Cluster a = cl[i], b = cl[j];
+        Cluster c;
+        for (int k = 0; k < 3; ++k) {
+                c.lo[k] = fminf(a.lo[k], b.lo[k]);
+                c.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+        }
+        c.code = (int)node;
+        c.cnt = a.cnt + b.cnt;
+        child[node] = make_int2(a.code, b.code);
+        ncount[node] = c.cnt;
+        nbox[2 * node] = make_float4(c.lo[0], c.lo[1], c.lo[2], 0.0f);
+        nbox[2 * node + 1] = make_float4(c.hi[0], c.hi[1], c.hi[2], 0.0f);
+        cl[i] = c;
+        keep[i] = 1;
+}
+
 struct Tree {
         const uint64_t *keys;
         const unsigned long long *m_dev;  // intersectable prims (sorted first)
-        const int2 *child, *range;
+        const int2 *child;
+        const int *count;                 // prims under each internal node
         const float4 *nbox, *pbox;
         const float4 *pv0, *pv1, *pv2;
         int leaf_size;
+        const int *root;                  // the root's code
 };
 
-__device__ __forceinline__ int code_count(const Tree &t, int code) {
-        if (code < 0) return 1;
-        const int2 r = t.range[code];
-        return r.y - r.x + 1;
+__device__ __forceinline__ int code_count(const Tree &t, int code) { return code < 0 ? 1 : t.count[code]; }
+
+// The sorted-key positions of the leaves under a code (at most 4), left to
+// right.
+__device__ int code_leaves(const Tree &t, int code, int out[4]) {
+        int stack[8], sp = 0, n = 0;
+        stack[sp++] = code;
+        while (sp > 0 && n < 4) {
+                const int c = stack[--sp];
+                if (c < 0) {
+                        out[n++] = ~c;
+                } else if (sp + 2 <= 8) {
+                        const int2 ch = t.child[c];
+                        stack[sp++] = ch.y;
+                        stack[sp++] = ch.x;
+                }
+        }
+        return n;
 }
-__device__ __forceinline__ int code_first(const Tree &t, int code) { return code < 0 ? ~code : t.range[code].x; }
 __device__ __forceinline__ bool code_leaf(const Tree &t, int code) { return code_count(t, code) <= t.leaf_size; }
 __device__ __forceinline__ void code_bounds(const Tree &t, int code, double lo[3], double hi[3]) {
         float4 l, h;
@@ -277,7 +392,7 @@ __global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_
         if (it >= *n_items) return;
         const int m = (int)*t.m_dev;
         int2 item = items[it];
-        if (item.x == kRootItem) item.x = m >= 2 ? 0 : ~0;
+        if (item.x == kRootItem) item.x = m >= 2 ? *t.root : ~0;
         int kids[8];
         double area[8];
         int n = 0;
@@ -407,10 +522,11 @@ __global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_
                         next[q] = make_int2(code, (int)(cbase + int_rank));
                         ++int_rank;
                 } else {
-                        const int cnt = code_count(t, code), first = code_first(t, code);
+                        int leaves[4];
+                        const int cnt = code_leaves(t, code, leaves);
                         w.meta[s] = (uint8_t)(0x80u | ((uint32_t)(cnt - 1) << 5) | tri_off);
                         for (int j = 0; j < cnt; ++j) {
-                                const uint32_t p = (uint32_t)(t.keys[first + j] & 0xFFFFFFFFu);
+                                const uint32_t p = (uint32_t)(t.keys[leaves[j]] & 0xFFFFFFFFu);
                                 float4 a = t.pv0[p];
                                 a.w = __int_as_float((int)p);
                                 float4 b = t.pv1[p], c = t.pv2[p];
@@ -438,7 +554,7 @@ cudaError_t dalloc(T **p, size_t count, std::vector<void *> &tmp) {
 }  // namespace
 
 gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ *pv2, int64_t n, int leaf_size,
-                          GpuWide *out, float *device_ms) {
+                          int builder, int radius, GpuWide *out, float *device_ms) {
         std::vector<void *> tmp;
         struct Free {
                 std::vector<void *> &v;
@@ -448,7 +564,9 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         } free_tmp{tmp};
         *out = GpuWide{};
         if (n < 0 || n >= INT32_MAX) return set_error(GZG_ERR_LIMIT, "gzg_gpu_build_scene: prim count out of range");
-        if (leaf_size < 1 || leaf_size > 4) leaf_size = 4;
+        if (leaf_size < 1 || leaf_size > 4) leaf_size = 1;
+        if (radius < 1 || radius > 64) radius = 16;
+        const bool ploc = builder == GZG_BUILD_PLOC;
         cudaStream_t st = nullptr;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         cudaEventCreate(&e0);
@@ -473,7 +591,9 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         int *cb, *parent_int, *parent_leaf, *arrivals;
         unsigned long long *nvalid;
         uint64_t *keys, *sorted;
-        int2 *child, *range, *qa, *qb;
+        int2 *child, *qa, *qb;
+        int *ncount, *nn, *keep, *root, *n_sel;
+        Cluster *ca, *cl_b;
         uint32_t *counts, *err;  // counts: [0] nodes used, [1] tris used, [2] items in, [3] items out
         GZG_CK(dalloc(&pbox, 2 * N, tmp), "build: prim bounds");
         GZG_CK(dalloc(&nbox, 2 * N, tmp), "build: node bounds");
@@ -482,7 +602,19 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         GZG_CK(dalloc(&keys, N, tmp), "build: keys");
         GZG_CK(dalloc(&sorted, N, tmp), "build: keys");
         GZG_CK(dalloc(&child, N, tmp), "build: radix tree");
-        GZG_CK(dalloc(&range, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&ncount, N, tmp), "build: radix tree");
+        GZG_CK(dalloc(&root, 1, tmp), "build: root");
+        GZG_CK(dalloc(&n_sel, 1, tmp), "build: cluster count");
+        size_t sel_bytes = 0;
+        if (ploc) {
+                GZG_CK(dalloc(&ca, N, tmp), "build: clusters");
+                GZG_CK(dalloc(&cl_b, N, tmp), "build: clusters");
+                GZG_CK(dalloc(&nn, N, tmp), "build: clusters");
+                GZG_CK(dalloc(&keep, N, tmp), "build: clusters");
+                cub::DeviceSelect::Flagged(nullptr, sel_bytes, ca, keep, cl_b, n_sel, (int)N, st);
+        }
+        uint8_t *sel_temp;
+        GZG_CK(dalloc(&sel_temp, sel_bytes, tmp), "build: cluster compaction scratch");
         GZG_CK(dalloc(&parent_int, N, tmp), "build: radix tree");
         GZG_CK(dalloc(&parent_leaf, N, tmp), "build: radix tree");
         GZG_CK(dalloc(&arrivals, N, tmp), "build: radix tree");
@@ -517,17 +649,48 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         std::memcpy(pinned, init, sizeof(init));
         GZG_CK(cudaMemcpyAsync(counts, pinned, sizeof(init), cudaMemcpyHostToDevice, st), "build: counters");
         GZG_CK(cudaMemsetAsync(err, 0, 4, st), "build: error word");
-        const int2 root = make_int2(kRootItem, 0);
-        GZG_CK(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st), "build: queue");
+        const int2 root_item = make_int2(kRootItem, 0);
+        GZG_CK(cudaMemcpyAsync(qa, &root_item, sizeof(root_item), cudaMemcpyHostToDevice, st), "build: queue");
         if (n > 0) {
                 k_prim_bounds<<<grid, B, 0, st>>>(d0, d1, d2, n, pbox, cb, nvalid);
                 k_keys<<<grid, B, 0, st>>>(d0, pbox, n, cb, keys);
                 GZG_CK(cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys, sorted, (int)n, 0, 64, st), "build: sort");
-                k_radix_tree<<<grid, B, 0, st>>>(sorted, nvalid, child, range, parent_int, parent_leaf);
+        }
+        GZG_CK(cudaMemsetAsync(root, 0, sizeof(int), st), "build: root");
+        if (n > 0 && !ploc) {
+                k_radix_tree<<<grid, B, 0, st>>>(sorted, nvalid, child, ncount, parent_int, parent_leaf);
                 k_refit<<<grid, B, 0, st>>>(sorted, nvalid, child, parent_int, parent_leaf, pbox, nbox, arrivals);
+        } else if (n > 0) {
+                unsigned long long hm = 0;
+                GZG_CK(cudaMemcpyAsync(&hm, nvalid, sizeof(hm), cudaMemcpyDeviceToHost, st), "build: prim count");
+                GZG_CK(cudaStreamSynchronize(st), "build: prim count");
+                int count = (int)hm;
+                k_ploc_init<<<grid, B, 0, st>>>(sorted, nvalid, pbox, ca);
+                uint32_t *node_counter = counts + 3;  // borrowed until the collapse
+                GZG_CK(cudaMemsetAsync(node_counter, 0, 4, st), "build: counters");
+                int force = 0, iters = 0;
+                while (count > 1) {
+                        if (++iters > 4 * (int)hm + 64)
+                                return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: clustering did not converge");
+                        const unsigned g = (unsigned)((count + B - 1) / B);
+                        k_ploc_nn<<<g, B, 0, st>>>(ca, count, radius, force, nn);
+                        k_ploc_merge<<<g, B, 0, st>>>(ca, nn, count, node_counter, (uint32_t)N, child, ncount, nbox, keep,
+                                                       err);
+                        GZG_CK(cub::DeviceSelect::Flagged(sel_temp, sel_bytes, ca, keep, cl_b, n_sel, count, st),
+                               "build: cluster compaction");
+                        GZG_CK(cudaMemcpyAsync(pinned + 3, n_sel, 4, cudaMemcpyDeviceToHost, st), "build: cluster count");
+                        GZG_CK(cudaStreamSynchronize(st), "build: clustering");
+                        const int next = (int)pinned[3];
+                        force = next == count;  // no mutual pair this time: pair neighbours next
+                        count = next;
+                        std::swap(ca, cl_b);
+                }
+                GZG_CK(cudaMemcpyAsync(root, &ca[0].code, sizeof(int), cudaMemcpyDeviceToDevice, st), "build: root");
+                // the collapse's counters start here
+                GZG_CK(cudaMemcpyAsync(counts, pinned, 16, cudaMemcpyHostToDevice, st), "build: counters");
         }
         const uint32_t cap = (uint32_t)N;
-        Tree t{sorted, nvalid, child, range, nbox, pbox, d0, d1, d2, leaf_size};
+        Tree t{sorted, nvalid, child, ncount, nbox, pbox, d0, d1, d2, leaf_size, root};
         uint32_t level_items = 1;
         int depth = 0;
         while (level_items > 0) {

@@ -83,10 +83,10 @@ struct GpuWide {
 
 // Builds the wide tree over device prim-order triangles pv0/pv1/pv2 (pv0.w =
 // int 1 for prims the traversal tests) with at most leaf_size (1..4) prims
-// per leaf; device_ms = the build's device time.  On an error the arrays
-// already allocated are in *out.
+// per leaf, by builder (GZG_BUILD_*) with the PLOC radius; device_ms = the
+// build's device time.  On an error the arrays already allocated are in *out.
 gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ *pv2, int64_t n, int leaf_size,
-                          GpuWide *out, float *device_ms);
+                          int builder, int radius, GpuWide *out, float *device_ms);
 
 // Device expansion of packed meshes (gpu_build.cu): per mesh its first
 // vertex and triangle in the concatenated arrays, counts, material and,

@@ -31,10 +31,11 @@ def small():
     return hs, o, d, t, isect, idx
 
 
+@pytest.mark.parametrize("builder", [F.BUILD_PLOC, F.BUILD_LBVH])
 @pytest.mark.parametrize("leaf_size", [1, 2, 4])
-def test_device_built_tree_matches_oracle(small, leaf_size):
+def test_device_built_tree_matches_oracle(small, leaf_size, builder):
     hs, o, d, t, isect, idx = small
-    with GpuAccelerator(hs, device_build=True, leaf_size=leaf_size) as acc:
+    with GpuAccelerator(hs, device_build=True, leaf_size=leaf_size, builder=builder) as acc:
         assert acc.device_built
         info = acc.info()
         assert info["bvh2_nodes"] == 0 and info["triangles"] == len(hs.prims)
@@ -90,12 +91,13 @@ def _tri_scene(tris):
     return _tri_builder(tris).build(host_bvh=False)
 
 
-def test_single_triangle_and_coincident_centroids():
+@pytest.mark.parametrize("builder", [F.BUILD_PLOC, F.BUILD_LBVH])
+def test_single_triangle_and_coincident_centroids(builder):
     hs = _tri_scene([[[-1, -1, 0], [1, -1, 0], [0, 1, 0]]])
     o = np.array([[0, 0, 2], [5, 5, 2]], np.float32)
     d = np.array([[0, 0, -1], [0, 0, -1]], np.float32)
     t = np.full(2, np.inf, np.float32)
-    with GpuAccelerator(hs) as acc:
+    with GpuAccelerator(hs, builder=builder) as acc:
         prim, tt, _, _ = device_closest(acc, o, d, t)
     assert prim.tolist() == [0, -1] and tt[0] == 2.0
     # 300 triangles tilted about the y axis by different amounts, all with
@@ -110,7 +112,7 @@ def test_single_triangle_and_coincident_centroids():
     d = np.tile(np.array([[0, 0, -1]], np.float32), (2000, 1))
     t = np.full(2000, np.inf, np.float32)
     isect, idx, _ = H.oracle_closest(sb.build(), o, d, t)
-    with GpuAccelerator(sb.build(host_bvh=False)) as acc:
+    with GpuAccelerator(sb.build(host_bvh=False), builder=builder) as acc:
         prim, tt, _, _ = device_closest(acc, o, d, t)
         assert acc.error_word() == 0
     hit = idx >= 0
@@ -155,22 +157,24 @@ def test_full_size_device_build():
     with GpuAccelerator(hs) as up:
         g_up = device_closest(up, o, d, t)
         cost_up = up.tree_cost()
-    with GpuAccelerator(hs, device_build=True) as dev:
-        g_dev = device_closest(dev, o, d, t)
-        build_ms = dev.build_time_ms()
-        cost_dev = dev.tree_cost()
-        info = dev.info()
-        assert dev.error_word() == 0
-    same_t = H.bits(g_up[1]) == H.bits(g_dev[1])
-    assert same_t.all(), int((~same_t).sum())
-    same_prim = g_up[0] == g_dev[0]
-    assert same_prim.mean() > 0.99999
+    record = {"tree_cost_host": cost_up}
+    for builder, name in ((F.BUILD_PLOC, "ploc"), (F.BUILD_LBVH, "lbvh")):
+        with GpuAccelerator(hs, device_build=True, builder=builder) as dev:
+            g_dev = device_closest(dev, o, d, t)
+            build_ms = dev.build_time_ms()
+            cost_dev = dev.tree_cost()
+            info = dev.info()
+            assert dev.error_word() == 0
+        same_t = H.bits(g_up[1]) == H.bits(g_dev[1])
+        assert same_t.all(), (name, int((~same_t).sum()))
+        same_prim = g_up[0] == g_dev[0]
+        assert same_prim.mean() > 0.99999
+        assert build_ms > 0
+        record[name] = {"build_ms": build_ms, "tree_cost": cost_dev, "prim_mismatch_equal_t": int((~same_prim).sum()),
+                        "info": info}
     out = Path(__file__).resolve().parent.parent / "gpurun_out"
     if out.is_dir():
-        (out / "device_build_full.json").write_text(json.dumps(
-            {"build_ms": build_ms, "tree_cost_device": cost_dev, "tree_cost_host": cost_up,
-             "prim_mismatch_equal_t": int((~same_prim).sum()), "info": info}))
-    assert build_ms > 0
+        (out / "device_build_full.json").write_text(json.dumps(record))
 
 
 # ---------------------------------------------------------------- ingestion fast path
