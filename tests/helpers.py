@@ -10,6 +10,10 @@ Parity rule (per ray, GPU vs oracle closest hit):
   fail             anything else (in particular the GPU missing a hit or
                    returning a farther one)
 """
+import json
+import os
+from pathlib import Path
+
 import numpy as np
 
 from gonzales_b200 import scenes
@@ -79,3 +83,10 @@ def small_raycast(subdiv=4, n_side=48, n_incoherent=4096, seed=0xC1):
     hs = sb.build()
     o, d, t = scenes.raycast_rays(hs, n_side, n_side, n_incoherent, seed=seed)
     return hs, o, d, t
+
+
+def record(name, data):
+    """Writes a measurement record (JSON) into $GZG_RECORD_DIR when it is set."""
+    d = os.environ.get("GZG_RECORD_DIR")
+    if d and Path(d).is_dir():
+        (Path(d) / name).write_text(json.dumps(data))

@@ -9,9 +9,6 @@ given (any order).  Edge cases: one triangle, no intersectable prim, many
 coincident centroids (equal Morton codes), leaves of 1 to 4 prims.  A
 render of a device-built scene equals the render of the uploaded one.
 """
-import json
-from pathlib import Path
-
 import numpy as np
 import pytest
 
@@ -172,9 +169,7 @@ def test_full_size_device_build():
         assert build_ms > 0
         record[name] = {"build_ms": build_ms, "tree_cost": cost_dev, "prim_mismatch_equal_t": int((~same_prim).sum()),
                         "info": info}
-    out = Path(__file__).resolve().parent.parent / "gpurun_out"
-    if out.is_dir():
-        (out / "device_build_full.json").write_text(json.dumps(record))
+    H.record("device_build_full.json", record)
 
 
 # ---------------------------------------------------------------- ingestion fast path

@@ -5,8 +5,6 @@ Per ray the (bottom-level prim, instance, t, u, v) is exact, a counted
 equal-t tie, or a counted reference-culled hit (a valid nearer hit the
 reference's slab test would cull); never a miss or a farther hit.
 """
-import json
-from pathlib import Path
 
 import numpy as np
 import pytest
@@ -17,7 +15,6 @@ from oracle import pyoracle as O
 from tests import helpers as H
 
 pytestmark = pytest.mark.gpu
-OUT = Path(__file__).resolve().parent.parent / "gpurun_out"
 
 
 def torch_mod():
@@ -128,7 +125,6 @@ def test_identity_instance_reproduces_single_level_scene():
 def test_instanced_full_size_parity():
     """16 meshes x 50,000 triangles, 4096 instances; 2M rays."""
     counts, fails, info, ora = run_case(16, 125, 200, 4096, 20.0, 1 << 21, 0xC2)
-    if OUT.is_dir():
-        (OUT / "parity_instanced.json").write_text(json.dumps({"wide": counts, "info": info}))
+    H.record("parity_instanced.json", {"wide": counts, "info": info})
     assert counts["fail"] == 0, (counts, fails[:10])
     assert info["triangles"] == 16 * 50000

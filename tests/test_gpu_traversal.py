@@ -6,7 +6,6 @@ restatement of kernel.mojo's traverse_bvh2_core) on identical rays.
       "reference-culled" hit (the reference's slab test culled a node the
       conservative wide boxes keep); never a missed or farther hit.
 """
-import json
 from pathlib import Path
 
 import numpy as np
@@ -257,9 +256,7 @@ def test_full_size_raycast_parity():
         assert info["triangles"] == 1310720
         gpu = device_closest(acc, o, d, t)
         counts, fails = _check(hs, o, d, t, gpu, isect, idx)
-        out = Path(__file__).resolve().parent.parent / "gpurun_out"
-        if out.is_dir():
-            (out / "parity_full_raycast.json").write_text(json.dumps({"wide": counts, "info": info}))
+        H.record("parity_full_raycast.json", {"wide": counts, "info": info})
         assert counts["fail"] == 0, (counts, fails[:10])
         gpu = device_closest(acc, o, d, t, options(traversal=F.TRAVERSAL_BVH2))
         assert np.array_equal(gpu[0], idx)
