@@ -244,3 +244,56 @@ def test_mesh_arrays_reject_out_of_range_index():
     with pytest.raises(GzgError) as e:
         GpuAccelerator.from_mesh_arrays([(pts, np.array([[0, 1, 3]], np.int32), 0)], mats)
     assert "out of" in str(e.value)
+
+
+# ---------------------------------------------------------------- device-built scenes elsewhere
+
+
+def test_device_built_blas_in_a_two_level_scene():
+    """Bottom-level scenes built on the device (their host tree copies feed
+    the two-level assembly) give the uploaded ones' closest hits."""
+    from gonzales_b200 import InstancedAccelerator
+    from tests.test_gpu_instanced import gpu_instanced
+
+    blas_hosts, inst = scenes.instanced_scene(n_meshes=4, n_u=30, n_v=20, n_instances=64, extent=5.0)
+    o, d, t = scenes.instanced_rays(200000, 5.0, 11)
+    res = []
+    for device in (False, True):
+        blas = [GpuAccelerator(h, device_build=device) for h in blas_hosts]
+        with InstancedAccelerator(blas, inst) as acc:
+            res.append(gpu_instanced(acc, o, d, t))
+            assert acc.error_word() == 0
+        for b in blas:
+            b.close()
+    (p0, i0, t0, _, _, a0), (p1, i1, t1, _, _, a1) = res
+    assert np.array_equal(H.bits(t0), H.bits(t1))
+    assert ((p0 == p1) & (i0 == i1)).mean() > 0.9999
+    assert np.array_equal(a0 >= 0, a1 >= 0)
+
+
+def test_batch_of_device_built_scenes_equals_solo_renders():
+    import torch
+
+    from gonzales_b200 import BatchRenderer
+
+    sb = scenes.box_scene()
+    meshes, mats, _ = _arrays_of(sb)
+    accs = [GpuAccelerator(sb.build(host_bvh=False)), GpuAccelerator.from_mesh_arrays(meshes, mats),
+            GpuAccelerator(scenes.batch_scene(11, 3_000).build(host_bvh=False))]
+    params = [F.render_params(48, 40, 8, max_depth=5, rr_min_bounce=3),
+              F.render_params(32, 32, 4, max_depth=4, rr_min_bounce=2, mis_corrected=1),
+              F.render_params(32, 32, 4, max_depth=6, rr_min_bounce=2)]
+    solo = [a.render(p) for a, p in zip(accs, params)]
+    with BatchRenderer(accs, params) as r:
+        rgb = torch.zeros((r.pixels, 3), device="cuda")
+        sq = torch.zeros((r.pixels, 3), device="cuda")
+        w = torch.zeros((r.pixels,), device="cuda")
+        r.render(rgb, w, sq)
+        torch.cuda.synchronize()
+        parts = list(zip(r.split(rgb.cpu().numpy()), r.split(w.cpu().numpy())))
+        assert r.error_word() == 0
+    for (b_rgb, b_w), (s_rgb, _, s_w, _) in zip(parts, solo):
+        np.testing.assert_allclose(b_rgb, s_rgb, rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(b_w, s_w, rtol=1e-6)
+    for a in accs:
+        a.close()
