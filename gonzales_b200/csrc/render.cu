@@ -84,9 +84,10 @@ __device__ __forceinline__ float power_heuristic(float f, float g) {
 }
 
 // concentricSampleDisk + cosineSampleHemisphere (Sampler/Sampling.swift:3-25).
-__device__ V3 cosine_hemisphere(float u0, float u1) {
+__device__ void concentric_disk(float u0, float u1, float &dx, float &dy) {
         const float ox = 2.0f * u0 - 1.0f, oy = 2.0f * u1 - 1.0f;
-        float dx = 0.0f, dy = 0.0f;
+        dx = 0.0f;
+        dy = 0.0f;
         if (!(ox == 0.0f && oy == 0.0f)) {
                 float theta, r;
                 if (fabsf(ox) > fabsf(oy)) {
@@ -99,6 +100,11 @@ __device__ V3 cosine_hemisphere(float u0, float u1) {
                 dx = r * cosf(theta);
                 dy = r * sinf(theta);
         }
+}
+
+__device__ V3 cosine_hemisphere(float u0, float u1) {
+        float dx, dy;
+        concentric_disk(u0, u1, dx, dy);
         return v3(dx, dy, sqrtf(fmaxf(0.0f, 1.0f - dx * dx - dy * dy)));
 }
 
@@ -231,6 +237,7 @@ struct SceneConst {
         V3 eye, right, up, fwd;
         float tan_half, sx0, sx1, sy0, sy1;
         float filter_radius, filter_sigma;
+        float lens_radius, focal_distance;  // thin lens (0: pinhole)
         int32_t width, height, spp, max_depth, rr_min, mis_corrected, first_sample;
         int32_t light_begin, light_count;  // light_count includes the environment light
         float light_total;
@@ -572,11 +579,25 @@ __global__ void k_generate(Wave w) {
         gaussian_sample_1d(u1, sc.filter_radius, sc.filter_sigma, dy, deny);
         const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
         float l0, l1;
-        zs_get2d(sc.zs, z, l0, l1);  // lens sample: drawn, unused by a pinhole
-        // raster -> screen -> camera -> world (pinhole)
+        zs_get2d(sc.zs, z, l0, l1);  // lens sample (drawn also by a pinhole)
+        // raster -> screen -> camera -> world
         const float scx = sc.sx0 + fx / (float)sc.width * (sc.sx1 - sc.sx0);
         const float scy = sc.sy1 - fy / (float)sc.height * (sc.sy1 - sc.sy0);
-        const V3 dcam = normalize(v3(scx * sc.tan_half, scy * sc.tan_half, 1.0f));
+        V3 dcam = normalize(v3(scx * sc.tan_half, scy * sc.tan_half, 1.0f));
+        V3 org = sc.eye;
+        if (sc.lens_radius > 0.0f) {
+                // PerspectiveCamera.depthOfField (Camera/PerspectiveCamera.swift:25-35):
+                // the origin moves to the lens point; as written the new
+                // direction is taken from the pinhole origin, so it keeps the
+                // pinhole direction (renormalised after scaling to the focal plane)
+                float lx, ly;
+                concentric_disk(l0, l1, lx, ly);
+                lx = sc.lens_radius * lx;
+                ly = sc.lens_radius * ly;
+                const float ft = sc.focal_distance / dcam.z;
+                dcam = normalize(dcam * ft);
+                org = sc.eye + sc.right * lx + sc.up * ly;
+        }
         const V3 dir = sc.right * dcam.x + sc.up * dcam.y + sc.fwd * dcam.z;
         // rayWeight = filter value / filter pdf (Tile.swift:36-40)
         const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
@@ -590,7 +611,7 @@ __global__ void k_generate(Wave w) {
         w.pixel[i] = sc.film_offset + pixel;
         w.scene[i] = (uint32_t)lo;
         w.weight[i] = fv / (denx * deny);
-        store_ray(w.q_ray[0], i, sc.eye, kInf, dir, sc.root);
+        store_ray(w.q_ray[0], i, org, kInf, dir, sc.root);
         w.q_id[0][i] = i;
 }
 
@@ -1362,12 +1383,17 @@ SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices
         sc.zs = make_zsobol(P.sampler_spp > 0 ? P.sampler_spp : P.spp, P.width, P.height, P.seed, matrices);
         sc.film_scale = 1.0f;  // iso 100
         sc.max_component = 0.0f;
+        sc.lens_radius = P.lens_radius;
+        sc.focal_distance = P.focal_distance;
         return sc;
 }
 
 bool params_ok(const gzg_render_params &P) {
+        const bool lens_ok = P.lens_radius == 0.0f ||
+                             (std::isfinite(P.lens_radius) && P.lens_radius > 0.0f && std::isfinite(P.focal_distance) &&
+                              P.focal_distance > 0.0f);
         return P.width > 0 && P.height > 0 && P.spp > 0 && P.max_depth >= 0 && P.fov_deg > 0.0f &&
-               P.filter_sigma > 0.0f && P.filter_radius > 0.0f && P.first_sample >= 0 && P.sampler_spp >= 0;
+               P.filter_sigma > 0.0f && P.filter_radius > 0.0f && P.first_sample >= 0 && P.sampler_spp >= 0 && lens_ok;
 }
 
 gzg_status cuda_err(cudaError_t e, const char *what) {

@@ -495,6 +495,8 @@ typedef struct gzg_render_params {
         int32_t sampler_spp;     /* ...of a Z-Sobol sampler with this many samples per pixel (0: spp) */
         int32_t wave_paths;      /* paths in flight per wave (0: library default) */
         int32_t use_graph;       /* capture one wave as a CUDA graph and replay it */
+        float lens_radius;       /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
+        float focal_distance;    /* distance of the plane in focus (reference default 1e6) */
 } gzg_render_params;
 
 typedef struct gzg_renderer gzg_renderer;

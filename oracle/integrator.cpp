@@ -73,7 +73,7 @@ inline float power_heuristic(float f, float g) {
 }
 
 // concentricSampleDisk / cosineSampleHemisphere (Sampler/Sampling.swift:3-25).
-V3 cosine_hemisphere(float u0, float u1) {
+void concentric_disk(float u0, float u1, float *dx_out, float *dy_out) {
         float ox = 2.0f * u0 - 1.0f, oy = 2.0f * u1 - 1.0f;
         float dx = 0.0f, dy = 0.0f;
         if (!(ox == 0.0f && oy == 0.0f)) {
@@ -88,6 +88,13 @@ V3 cosine_hemisphere(float u0, float u1) {
                 dx = r * std::cos(theta);
                 dy = r * std::sin(theta);
         }
+        *dx_out = dx;
+        *dy_out = dy;
+}
+
+V3 cosine_hemisphere(float u0, float u1) {
+        float dx, dy;
+        concentric_disk(u0, u1, &dx, &dy);
         float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
         return v3(dx, dy, z);
 }
@@ -864,13 +871,27 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                                 orc_zsobol_get2d(&smp, lens);
                                                 const float scx = sx0 + fx / (float)W * (sx1 - sx0);
                                                 const float scy = sy1 - fy / (float)H * (sy1 - sy0);
-                                                const V3 dcam = normalize(v3(scx * tan_half, scy * tan_half, 1.0f));
+                                                V3 dcam = normalize(v3(scx * tan_half, scy * tan_half, 1.0f));
+                                                V3 org = eye;
+                                                if (P.lens_radius > 0.0f) {
+                                                        // PerspectiveCamera.depthOfField
+                                                        // (Camera/PerspectiveCamera.swift:25-35): origin on
+                                                        // the lens, direction from the pinhole origin to the
+                                                        // focal point (the pinhole direction, renormalised)
+                                                        float lx, ly;
+                                                        concentric_disk(lens[0], lens[1], &lx, &ly);
+                                                        lx = P.lens_radius * lx;
+                                                        ly = P.lens_radius * ly;
+                                                        const float ft = P.focal_distance / dcam.z;
+                                                        dcam = normalize(mul(dcam, ft));
+                                                        org = add(add(eye, mul(right, lx)), mul(upv, ly));
+                                                }
                                                 const V3 dir = add(add(mul(right, dcam.x), mul(upv, dcam.y)), mul(fwd, dcam.z));
                                                 const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
                                                 const float fv = std::max(0.0f, gaussian(ddx, P.filter_sigma)) *
                                                                  std::max(0.0f, gaussian(ddy, P.filter_sigma));
                                                 const float w = fv / (denx * deny);
-                                                PathResult pr = trace_path(sc, &smp, eye, dir);
+                                                PathResult pr = trace_path(sc, &smp, org, dir);
                                                 cnt[4 * ti + 0] += 1;
                                                 cnt[4 * ti + 1] += pr.ext;
                                                 cnt[4 * ti + 2] += pr.shadow;

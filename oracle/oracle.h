@@ -101,6 +101,8 @@ typedef struct orc_render_params {
         int32_t sampler_spp;    /* of sampler_spp samples per pixel (0: spp) */
         float iso;              /* film sensitivity: light scaled by iso / 100 (0: 100) */
         float max_component;    /* clamp of a sample's largest component (0: none) */
+        float lens_radius;      /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
+        float focal_distance;
 } orc_render_params;
 
 /* Renders the scene; per pixel (row-major) accumulates the film sums of the

@@ -185,15 +185,17 @@ class RenderParams(C.Structure):
                 ("rr_min_bounce", C.c_int32), ("mis_corrected", C.c_int32), ("seed", C.c_int64),
                 ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
                 ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
-                ("sampler_spp", C.c_int32), ("iso", C.c_float), ("max_component", C.c_float)]
+                ("sampler_spp", C.c_int32), ("iso", C.c_float), ("max_component", C.c_float),
+                ("lens_radius", C.c_float), ("focal_distance", C.c_float)]
 
 
 def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
                   eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
-                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, iso=100.0, max_component=0.0):
+                  filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, iso=100.0, max_component=0.0,
+                  lens_radius=0.0, focal_distance=1e6):
     return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
                         (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
-                        first_sample, sampler_spp, iso, max_component)
+                        first_sample, sampler_spp, iso, max_component, lens_radius, focal_distance)
 
 
 class _Textures(C.Structure):

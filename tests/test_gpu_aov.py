@@ -102,3 +102,20 @@ def test_film_resolve_and_exr_output(box, tmp_path):
     w2 = torch.tensor([1.0, 0.0], device="cuda")
     img, zero = film.resolve(rgb2, w2)
     assert zero == 1 and float(img[1].abs().sum()) == 0.0
+
+
+def test_thin_lens_camera_matches_oracle():
+    """PerspectiveCamera.depthOfField: camera rays leave from a point of the
+    lens disk (concentric mapping of the lens sample); as written the
+    direction keeps the pinhole direction.  GPU and oracle agree per pixel."""
+    hs = scenes.box_scene().build()
+    p = dict(max_depth=4, rr_min_bounce=2, lens_radius=0.05, focal_distance=1.5)
+    with GpuAccelerator(hs) as acc:
+        g = acc.render(F.render_params(W, H, SPP, **p))
+        g0 = acc.render(F.render_params(W, H, SPP, max_depth=4, rr_min_bounce=2))
+    o = O.render(hs, O.render_params(W, H, SPP, **p))
+    gm, om = g[0] / SPP, o[0] / SPP
+    assert np.isclose(gm, om, rtol=1e-3, atol=1e-5).mean() > 0.9
+    np.testing.assert_allclose(g[0].sum((0, 1)) / g[2].sum(), o[0].sum((0, 1)) / o[2].sum(), rtol=1e-2)
+    # the lens moves the rays: the image differs from the pinhole one
+    assert not np.allclose(g[0], g0[0], rtol=1e-3)

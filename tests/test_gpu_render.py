@@ -18,7 +18,7 @@ import pytest
 from gonzales_b200 import GpuAccelerator, Renderer, scenes
 from gonzales_b200 import _ffi as F
 from oracle import pyoracle as O
-from tests import helpers as H
+from tests import helpers
 
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -167,7 +167,7 @@ def test_relmse_against_high_spp_oracle(box):
         result[spp] = relmse(g[0] / g[2][..., None], ref)
     o16 = O.render(hs, O.render_params(W, H, 16, max_depth=5, rr_min_bounce=3))
     result["oracle16"] = relmse(o16[0] / o16[2][..., None], ref)
-    H.record("relmse_box.json", {str(k): v for k, v in result.items()})
+    helpers.record("relmse_box.json", {str(k): v for k, v in result.items()})
     assert result[1024] < result[256] < result[16]
     assert abs(result[16] - result["oracle16"]) <= 0.25 * result["oracle16"]
     assert result[1024] < 1e-2
