@@ -154,6 +154,7 @@ PROTOTYPES = {
     "gzg_scene_set_launch": (ST, [VP, C.c_int32, C.POINTER(TraceOptions)]),
     "gzg_scene_set_environment": (ST, [VP, VP, C.c_int32, C.c_int32, C.c_float]),
     "gzg_scene_set_material_params": (ST, [VP, VP, I64]),
+    "gzg_scene_set_vertex_attributes": (ST, [VP, I64, VP, VP, I64]),
     "gzg_gpu_build_scene": (ST, [VP, I64, VP, I64, VP, VP, VP, VP, I64, VP, C.POINTER(VP)]),
     "gzg_scene_build_time": (ST, [VP, C.POINTER(C.c_float)]),
     "gzg_gpu_build_mesh_scene": (ST, [VP, I64, VP, I64, VP, C.POINTER(VP)]),

@@ -65,12 +65,15 @@ class GpuAccelerator:
                 C.addressof(meshes), len(host_scene.meshes), F.ptr(pts), F.ptr(fi), F.ptr(vi),
                 F.ptr(host_scene.materials), len(host_scene.materials), C.byref(handle)))
         self.handle = handle
-        if getattr(host_scene, "has_extended_materials", False) and host_scene.material_params is not None:
-            try:
+        try:
+            if getattr(host_scene, "has_extended_materials", False) and host_scene.material_params is not None:
                 self.set_material_params(host_scene.material_params)
-            except Exception:
-                self.close()
-                raise
+            for k, m in enumerate(host_scene.meshes):
+                if getattr(m, "normals", None) is not None or getattr(m, "uvs", None) is not None:
+                    self.set_vertex_attributes(k, m.normals, m.uvs)
+        except Exception:
+            self.close()
+            raise
 
     @classmethod
     def from_mesh_arrays(cls, meshes, materials, leaf_size=0, builder=0, radius=0):
@@ -235,6 +238,17 @@ class GpuAccelerator:
         F.check(F.lib().gzg_render_image(self.handle, C.byref(params), F.ptr(rgb), F.ptr(sq), F.ptr(w),
                                          C.byref(stats)))
         return rgb, sq, w, {name: getattr(stats, name) for name, _ in F.RenderStats._fields_}
+
+    def set_vertex_attributes(self, mesh, normals=None, uvs=None):
+        """Vertex normals (n, 3) and / or UVs (n, 2) of mesh `mesh`
+        (gzg_scene_set_vertex_attributes); a HostScene's meshes set theirs on
+        upload."""
+        nrm = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        uv = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
+        n = len(nrm) if nrm is not None else len(uv)
+        F.check(F.lib().gzg_scene_set_vertex_attributes(self.handle, int(mesh),
+                                                        F.ptr(nrm) if nrm is not None else None,
+                                                        F.ptr(uv) if uv is not None else None, n))
 
     def set_material_params(self, params):
         """Parameters of the dielectric, coated-diffuse, conductor and

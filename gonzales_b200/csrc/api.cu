@@ -113,6 +113,7 @@ struct gzg_scene {
         float root_bounds[6] = {0, 0, 0, 0, 0, 0};
         bool instanced = false;
         float build_ms = -1.0f;     // device time of gzg_gpu_build_scene's tree build
+        std::vector<int64_t> mesh_vertices;  // vertices per mesh (gzg_scene_set_vertex_attributes)
         // host copies of the shading arrays (batch assembly)
         HostShading host_shading;
         std::mutex pool_mu;
@@ -582,6 +583,8 @@ gzg_status upload_scene(const gzg_bvh2_node *bvh2_nodes, int64_t bvh2_node_count
         if (st != GZG_OK) return st;
         d.mesh_sizes = ms;
         d.mesh_count = mesh_count;
+        scene->mesh_vertices.resize((size_t)mesh_count);
+        for (int64_t k = 0; k < mesh_count; ++k) scene->mesh_vertices[k] = mesh_points_counts[k] / 4;
         if (!build) {
                 for (int a = 0; a < 3; ++a) {
                         scene->root_bounds[a] = bvh2_nodes[0].bounds_min[a];
@@ -774,6 +777,8 @@ GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64
         if ((st = scene->upload(sizes.data(), sizes.size(), &msz, "mesh sizes"))) return st;
         d.mesh_sizes = msz;
         d.mesh_count = mesh_count;
+        scene->mesh_vertices.resize((size_t)mesh_count);
+        for (int64_t k = 0; k < mesh_count; ++k) scene->mesh_vertices[k] = ranges[k].vcount;
         d.bvh2_count = 0;
         d.prim_count = nt;
         d.wide_count = (uint32_t)wide.nodes.size();
@@ -802,6 +807,59 @@ GZG_API gzg_status gzg_gpu_build_mesh_scene(const gzg_mesh_arrays *meshes, int64
                             materials, material_count);
         if (st != GZG_OK) return st;
         *out_scene = scene.release();
+        return clear_error();
+}
+
+// Vertex normals and UVs of one mesh of a flat scene (the data
+// Triangle.computeSurfaceInteraction reads from TriangleMesh, Shape/
+// Triangle.swift:386-452); gathered per prim on the device.
+GZG_API gzg_status gzg_scene_set_vertex_attributes(gzg_scene *scene, int64_t mesh, const float *normals,
+                                                   const float *uvs, int64_t vertex_count) {
+        const char *fn = "gzg_scene_set_vertex_attributes";
+        if (!scene || (!normals && !uvs)) return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": bad arguments");
+        if (scene->instanced)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": set them on the bottom-level scenes");
+        if (mesh < 0 || mesh >= (int64_t)scene->mesh_vertices.size() || vertex_count != scene->mesh_vertices[mesh])
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 std::string(fn) + ": mesh index out of range or vertex count differs from the mesh's");
+        for (int64_t i = 0; normals && i < 3 * vertex_count; ++i)
+                if (!std::isfinite(normals[i]))
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": normals must be finite");
+        for (int64_t i = 0; uvs && i < 2 * vertex_count; ++i)
+                if (!std::isfinite(uvs[i])) return set_error(GZG_ERR_INVALID_ARGUMENT, std::string(fn) + ": UVs must be finite");
+        DeviceGuard g(scene->device);
+        DevScene &d = scene->dev;
+        HostShading &hs = scene->host_shading;
+        const int64_t n = d.prim_count;
+        gzg_status st;
+        if (!d.attr) {
+                float4 *a;
+                if ((st = scene->alloc(&a, 5 * (size_t)std::max<int64_t>(n, 1), "vertex attributes"))) return st;
+                GZG_CK(cudaMemset(a, 0, 5 * sizeof(float4) * (size_t)std::max<int64_t>(n, 1)), "vertex attributes");
+                d.attr = a;
+        }
+        struct Tmp {
+                void *p = nullptr;
+                ~Tmp() {
+                        if (p) cudaFree(p);
+                }
+        } tn, tu;
+        if (normals) {
+                GZG_CK(cudaMalloc(&tn.p, 12 * (size_t)std::max<int64_t>(vertex_count, 1)), "vertex normals");
+                GZG_CK(cudaMemcpy(tn.p, normals, 12 * (size_t)vertex_count, cudaMemcpyHostToDevice), "vertex normals");
+        }
+        if (uvs) {
+                GZG_CK(cudaMalloc(&tu.p, 8 * (size_t)std::max<int64_t>(vertex_count, 1)), "vertex UVs");
+                GZG_CK(cudaMemcpy(tu.p, uvs, 8 * (size_t)vertex_count, cudaMemcpyHostToDevice), "vertex UVs");
+        }
+        if ((st = gpu_gather_attributes(d.prims, n, d.meshes, mesh, static_cast<const float *>(tn.p),
+                                        static_cast<const float *>(tu.p), vertex_count,
+                                        reinterpret_cast<float4_ *>(const_cast<float4 *>(d.attr)))))
+                return st;
+        hs.attr.resize(5 * (size_t)n);
+        if (n)
+                GZG_CK(cudaMemcpy(hs.attr.data(), d.attr, 5 * sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost),
+                       "vertex attributes");
         return clear_error();
 }
 
@@ -1094,6 +1152,17 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 }
                 hsd.materials.insert(hsd.materials.end(), bs.materials.begin(), bs.materials.end());
         }
+        bool any_attr = false;
+        for (int64_t b = 0; b < blas_count; ++b) any_attr = any_attr || !blas[b]->host_shading.attr.empty();
+        if (any_attr) {
+                for (int64_t b = 0; b < blas_count; ++b) {
+                        const HostShading &bs = blas[b]->host_shading;
+                        if (bs.attr.empty())
+                                hsd.attr.insert(hsd.attr.end(), 5 * bs.prims.size(), float4_{0, 0, 0, 0});
+                        else
+                                hsd.attr.insert(hsd.attr.end(), bs.attr.begin(), bs.attr.end());
+                }
+        }
         bool any_params = false;
         for (int64_t b = 0; b < blas_count; ++b) any_params = any_params || !blas[b]->host_shading.mat_params.empty();
         if (any_params) {
@@ -1164,6 +1233,12 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                                         &f, "material parameters")))
                         return st;
                 d.mat_params = f;
+        }
+        if (!hsd.attr.empty()) {
+                if ((st = scene->upload(reinterpret_cast<const float4 *>(hsd.attr.data()), hsd.attr.size(), &f,
+                                        "vertex attributes")))
+                        return st;
+                d.attr = f;
         }
         const int32_t *pb;
         if ((st = scene->upload(prim_base.data(), prim_base.size(), &pb, "prim bases"))) return st;

@@ -31,6 +31,9 @@ struct DevScene {
         // shading data (path integrator)
         const float4 *materials;       // 2 x float4 per material: albedo + type, emission
         const float4 *mat_params;      // per material 3 x float4 (gzg_material_params; null: none)
+        // per prim 5 x float4: vertex normals n0, n1, n2 (n0.w = int 1 when
+        // set), UVs (u0, v0, u1, v1), (u2, v2, int 1 when set, 0); null: none
+        const float4 *attr;
         const float4 *lights;          // 4 x float4 per area light: p0 + area, p1 + power, p2, emission
         const float *light_cdf;        // running sum of light powers
         int32_t material_count;

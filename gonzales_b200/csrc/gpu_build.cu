@@ -807,3 +807,50 @@ gzg_status gpu_expand_meshes(const float *points3, const int32_t *idx3, const Me
 }
 
 }  // namespace gzg
+
+namespace gzg {
+namespace {
+
+// Per prim of mesh `mesh`: its vertices' normals and UVs (5 float4 records,
+// DevScene::attr layout).  Prims of other meshes keep their records.
+__global__ void k_gather_attributes(const gzg_prim_id *__restrict__ prims, int64_t n,
+                                    const gzg_triangle_mesh *__restrict__ meshes, int64_t mesh,
+                                    const float *__restrict__ normals, const float *__restrict__ uvs, int64_t vcount,
+                                    float4 *__restrict__ attr) {
+        const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (k >= n) return;
+        int64_t m, base;
+        if (!prim_triangle(prims[k], &m, &base) || m != mesh) return;
+        const int64_t *vi = meshes[m].vertex_indices;
+        int64_t v[3];
+        for (int c = 0; c < 3; ++c) {
+                v[c] = vi[base + c];
+                if (v[c] < 0 || v[c] >= vcount) return;
+        }
+        float4 *a = attr + 5 * k;
+        if (normals) {
+                for (int c = 0; c < 3; ++c)
+                        a[c] = make_float4(normals[3 * v[c]], normals[3 * v[c] + 1], normals[3 * v[c] + 2],
+                                           c == 0 ? __int_as_float(1) : 0.0f);
+        }
+        if (uvs) {
+                a[3] = make_float4(uvs[2 * v[0]], uvs[2 * v[0] + 1], uvs[2 * v[1]], uvs[2 * v[1] + 1]);
+                a[4] = make_float4(uvs[2 * v[2]], uvs[2 * v[2] + 1], __int_as_float(1), 0.0f);
+        }
+}
+
+}  // namespace
+
+gzg_status gpu_gather_attributes(const gzg_prim_id *prims, int64_t n, const gzg_triangle_mesh *meshes_dev,
+                                 int64_t mesh, const float *normals, const float *uvs, int64_t vcount,
+                                 float4_ *attr) {
+        if (n <= 0) return clear_error();
+        const int B = 256;
+        k_gather_attributes<<<(unsigned)((n + B - 1) / B), B>>>(prims, n, meshes_dev, mesh, normals, uvs, vcount,
+                                                                reinterpret_cast<float4 *>(attr));
+        GZG_CK(cudaGetLastError(), "attributes: launch");
+        GZG_CK(cudaDeviceSynchronize(), "attributes");
+        return clear_error();
+}
+
+}  // namespace gzg

@@ -63,6 +63,9 @@ struct HostShading {
         // thickness; conductor eta, roughness u; conductor k, roughness v);
         // empty when none were set
         std::vector<float4_> mat_params;
+        // per prim 5 records of vertex normals and UVs (DevScene::attr); empty
+        // when none were set
+        std::vector<float4_> attr;
         std::vector<float4_> lights;         // 4 per light
         std::vector<float> light_cdf;
         float light_total = 0.0f;
@@ -101,6 +104,12 @@ struct MeshRange {
 gzg_status gpu_expand_meshes(const float *points3, const int32_t *idx3, const MeshRange *ranges_dev, int mesh_count,
                              int64_t total_verts, int64_t total_tris, float *points4, int64_t *vidx64,
                              gzg_prim_id *prims, float4_ *pv0, float4_ *pv1, float4_ *pv2, bool *bad);
+
+// Writes the attribute records (DevScene::attr) of the prims of one mesh from
+// device arrays of per-vertex normals (x3) and UVs (x2), either may be null.
+gzg_status gpu_gather_attributes(const gzg_prim_id *prims, int64_t n, const gzg_triangle_mesh *meshes_dev,
+                                 int64_t mesh, const float *normals, const float *uvs, int64_t vcount,
+                                 float4_ *attr);
 
 // Converts a validated reference BVH2 + prims + meshes into the wide layout.
 // Returns GZG_OK or an error (with set_error called).

@@ -162,6 +162,54 @@ __device__ bool make_frame(V3 p0, V3 p1, V3 p2, V3 ns, Frame &f) {
         return true;
 }
 
+// Triangle.computeSurfaceInteraction with vertex normals and / or UVs
+// (Shape/Triangle.swift:386-452): dpdu from the UV parametrisation unless it
+// is degenerate; the shading normal interpolated from the vertex normals
+// (normalised, or (6, 6, 6) when it vanishes); shading tangent from dpdu
+// made orthogonal to it.  a = the prim's 5 attribute records.  Returns the
+// shading tangent and the shading normal (normalised as the interaction
+// stores it), false when the triangle is degenerate.
+__device__ bool attr_shading(V3 p0, V3 p1, V3 p2, float b0, float b1, float b2, V3 ng, const float4 a[5],
+                             V3 &dpdu_out, V3 &ns_out) {
+        const bool has_n = __float_as_int(a[0].w) != 0, has_uv = __float_as_int(a[4].z) != 0;
+        const V3 dp02 = p0 - p2, dp12 = p1 - p2;
+        const float u0 = has_uv ? a[3].x : 0.0f, v0 = has_uv ? a[3].y : 0.0f;
+        const float u1 = has_uv ? a[3].z : 0.0f, v1 = has_uv ? a[3].w : 0.0f;
+        const float u2 = has_uv ? a[4].x : 0.0f, v2 = has_uv ? a[4].y : 0.0f;
+        const float du02 = u0 - u2, dv02 = v0 - v2, du12 = u1 - u2, dv12 = v1 - v2;
+        const float det = du02 * dv12 - dv02 * du12;
+        const bool degenerate = fabsf(det) < 1e-8f;
+        V3 dpdu = v3(0.0f, 1.0f, 0.0f), dpdv = v3(0.0f, 1.0f, 0.0f);
+        if (!degenerate) {
+                const float inv = 1.0f / det;
+                dpdu = (dp02 * dv12 - dp12 * dv02) * inv;
+                dpdv = (dp02 * (-du12) - dp12 * du02) * inv;
+        }
+        const V3 cuv = cross(dpdu, dpdv);
+        if (degenerate || dot(cuv, cuv) == 0.0f) {
+                const V3 gn = cross(p2 - p0, p1 - p0);
+                if (dot(gn, gn) == 0.0f) return false;
+                coordinate_system(normalize(gn), dpdu, dpdv);
+        }
+        V3 ns = ng;
+        if (has_n) {
+                const V3 n0 = v3(a[0]), n1 = v3(a[1]), n2 = v3(a[2]);
+                ns = n0 * b0 + n1 * b1 + n2 * b2;
+                ns = dot(ns, ns) > 0.0f ? normalize(ns) : v3(6.0f, 6.0f, 6.0f);
+        }
+        V3 sv = normalize(dpdu);
+        V3 t = cross(sv, ns);
+        if (dot(t, t) > 0.0f) {
+                t = normalize(t);
+                sv = cross(t, ns);
+        } else {
+                coordinate_system(ns, sv, t);
+        }
+        dpdu_out = sv;
+        ns_out = normalize(ns);
+        return true;
+}
+
 // Transform * Point / Vector / Normal (Geometry/Transform.swift:31-65) with a
 // 3x4 matrix given as three float4 rows; the normal uses the inverse's columns.
 __device__ __forceinline__ V3 xf_pt(float4 a, float4 b, float4 c, V3 p) {
@@ -373,6 +421,7 @@ __device__ __forceinline__ void prim_info(const DevScene &s, int prim, int &type
 // as vectors).  gprim is the prim's index in the scene's shading arrays.
 struct Surf {
         V3 pos, ng, wo;
+        V3 ns;  // shading normal (ng without vertex normals)
         Frame fr;
         bool frame_ok;
         int gprim;
@@ -386,8 +435,19 @@ __device__ void surface(const DevScene &s, int prim, int inst, float bu, float b
                 o.pos = p0 * b0 + p1 * bu + p2 * bv;
                 o.ng = normalize(cross(p0 - p2, p1 - p2));
                 o.wo = normalize(neg(d));
-                o.frame_ok = make_frame(p0, p1, p2, o.ng, o.fr);
                 o.gprim = prim;
+                o.ns = o.ng;
+                if (s.attr) {
+                        float4 a[5];
+                        for (int k = 0; k < 5; ++k) a[k] = __ldg(s.attr + 5 * (size_t)prim + k);
+                        if (__float_as_int(a[0].w) != 0 || __float_as_int(a[4].z) != 0) {
+                                V3 sv;
+                                o.frame_ok = attr_shading(p0, p1, p2, b0, bu, bv, o.ng, a, sv, o.ns);
+                                if (o.frame_ok) o.fr = frame_from(sv, o.ns);
+                                return;
+                        }
+                }
+                o.frame_ok = make_frame(p0, p1, p2, o.ng, o.fr);
                 return;
         }
         const float4 w0 = __ldg(s.instances + 4 * inst), w1 = __ldg(s.instances + 4 * inst + 1),
@@ -399,12 +459,20 @@ __device__ void surface(const DevScene &s, int prim, int inst, float bu, float b
         const V3 pos_o = p0 * b0 + p1 * bu + p2 * bv;
         const V3 n_o = normalize(cross(p0 - p2, p1 - p2));
         const V3 wo_o = normalize(neg(xf_vec(w0, w1, w2, d)));
-        V3 s_o = v3(0.0f, 0.0f, 0.0f);
-        o.frame_ok = shading_dpdu(p0, p1, p2, n_o, s_o);
+        V3 s_o = v3(0.0f, 0.0f, 0.0f), ns_o = n_o;
+        bool with_attr = false;
+        if (s.attr) {
+                float4 a[5];
+                for (int k = 0; k < 5; ++k) a[k] = __ldg(s.attr + 5 * (size_t)o.gprim + k);
+                with_attr = __float_as_int(a[0].w) != 0 || __float_as_int(a[4].z) != 0;
+                if (with_attr) o.frame_ok = attr_shading(p0, p1, p2, b0, bu, bv, n_o, a, s_o, ns_o);
+        }
+        if (!with_attr) o.frame_ok = shading_dpdu(p0, p1, p2, n_o, s_o);
         o.pos = xf_pt(o0, o1, o2, pos_o);
         o.ng = normalize(xf_nrm(w0, w1, w2, n_o));
+        o.ns = with_attr ? normalize(xf_nrm(w0, w1, w2, ns_o)) : o.ng;
         o.wo = normalize(xf_vec(o0, o1, o2, wo_o));
-        if (o.frame_ok) o.fr = frame_from(xf_vec(o0, o1, o2, s_o), o.ng);
+        if (o.frame_ok) o.fr = frame_from(xf_vec(o0, o1, o2, s_o), o.ns);
 }
 
 // Nearest texel of texture t at p (planar map), as a texel index.
@@ -712,7 +780,7 @@ __global__ void k_sort_scatter(Wave w, DevScene s, int cur) {
 template <int K>
 __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst &sc, uint32_t path, int bounce,
                               int cur, const BMat &bm, const Surf &sf, V3 thr, V3 L, ZSobol &z) {
-        const V3 pos = sf.pos, ng = sf.ng, wo = sf.wo;
+        const V3 pos = sf.pos, ng = sf.ng, ns = sf.ns, wo = sf.wo;
         const Frame &fr = sf.fr;
         bool alive = sf.frame_ok;
         bool specular = false;
@@ -759,7 +827,7 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                         const V3 wl = fr.to_local(light_dir);
                         const bool reflect = dot(light_dir, ng) * dot(wo, ng) > 0.0f;
                         const V3 f = reflect ? bmat_f<K>(bm, wo_l, wl) : v3(0, 0, 0);
-                        const V3 light_est = mulv(f * fabsf(dot(light_dir, ng)), rad);
+                        const V3 light_est = mulv(f * fabsf(dot(light_dir, ns)), rad);
                         if (!is_black(light_est)) {
                                 const float brdf_density = wo_l.z == 0.0f ? 0.0f : bmat_pdf<K>(bm, wo_l, wl);
                                 const float light_w = power_heuristic(light_pdf, brdf_density);
@@ -778,7 +846,7 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                         const BsdfS bs = bmat_sample<K>(bm, wo_l, v0, v1, v2);
                         const float pdf_b = bs.pdf;
                         const V3 wi = fr.to_world(bs.wi);
-                        const V3 est = bs.f * fabsf(dot(wi, ng));
+                        const V3 est = bs.f * fabsf(dot(wi, ns));
                         if (!is_black(est) && pdf_b > 0.0f) {
                                 const V3 po = offset_origin(pos, ng, wi);
                                 float light_density = 0.0f;
@@ -989,7 +1057,7 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                         if (!is_black(rad) && !isinf(pdf)) {
                                 const bool reflect = dot(dv, ng) * dot(wo, ng) > 0.0f;
                                 const V3 f = reflect ? f_val : v3(0, 0, 0);
-                                light_est = mulv(f * fabsf(dot(dv, ng)), rad);
+                                light_est = mulv(f * fabsf(dot(dv, sf.ns)), rad);
                                 light_dir = dv;
                                 light_pdf = pdf;
                         }
@@ -1011,7 +1079,7 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                         if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
                                 const bool reflect = dot(inc, ng) * dot(wo, ng) > 0.0f;
                                 const V3 f = reflect ? f_val : v3(0, 0, 0);
-                                light_est = mulv(f * fabsf(dot(inc, ng)), le);
+                                light_est = mulv(f * fabsf(dot(inc, sf.ns)), le);
                                 light_dir = inc;
                                 light_pdf = pdf;
                         }
@@ -1043,7 +1111,7 @@ __global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
                         if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
                         const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? fabsf(wi_l.z) / kPi : 0.0f;
                         const V3 wi = fr.to_world(wi_l);
-                        const V3 est = f_val * fabsf(dot(wi, ng));
+                        const V3 est = f_val * fabsf(dot(wi, sf.ns));
                         if (!is_black(est) && pdf_b > 0.0f) {
                                 const V3 po = offset_origin(pos, ng, wi);
                                 float light_density = 0.0f;
@@ -1682,7 +1750,9 @@ gzg_status build_batch(gzg_renderer *r) {
                 r->view.per_ray_root = 0;
         } else {
                 std::vector<WideNode> nodes;
-                std::vector<float4_> v0, v1, v2, pv0, pv1, pv2, mats, lights, mparams;
+                std::vector<float4_> v0, v1, v2, pv0, pv1, pv2, mats, lights, mparams, attr;
+                bool any_attr = false;
+                for (size_t k = 0; k < n; ++k) any_attr = any_attr || !scene_host_shading(r->scenes[k]).attr.empty();
                 bool any_params = false;
                 for (size_t k = 0; k < n; ++k) any_params = any_params || !scene_host_shading(r->scenes[k]).mat_params.empty();
                 std::vector<gzg_prim_id> prims;
@@ -1716,6 +1786,12 @@ gzg_status build_batch(gzg_renderer *r) {
                                 prims.push_back(p);
                         }
                         mats.insert(mats.end(), hs.materials.begin(), hs.materials.end());
+                        if (any_attr) {
+                                if (hs.attr.empty())
+                                        attr.insert(attr.end(), 5 * hs.prims.size(), float4_{0, 0, 0, 0});
+                                else
+                                        attr.insert(attr.end(), hs.attr.begin(), hs.attr.end());
+                        }
                         if (any_params) {
                                 if (hs.mat_params.empty())
                                         mparams.insert(mparams.end(), 3 * (hs.materials.size() / 2), float4_{1, 0, 0, 0});
@@ -1746,6 +1822,7 @@ gzg_status build_batch(gzg_renderer *r) {
                     (st = r->upload(&d.light_cdf, cdf)))
                         return st;
                 if (any_params && (st = r->upload(&d.mat_params, mparams))) return st;
+                if (any_attr && (st = r->upload(&d.attr, attr))) return st;
                 uint32_t *err = nullptr;
                 if ((st = r->alloc(&err, 1))) return st;
                 if ((st = cuda_err(cudaMemset(err, 0, 4), "batch error word"))) return st;

@@ -47,18 +47,22 @@ class Mesh:
     points: np.ndarray          # (n, 4) float32, w unused
     vertex_indices: np.ndarray  # (3 * ntri,) int64
     face_indices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    normals: np.ndarray = None  # (n, 3) float32 vertex normals (renderer shading), or None
+    uvs: np.ndarray = None      # (n, 2) float32 vertex UVs (renderer shading), or None
 
     @property
     def triangle_count(self):
         return len(self.vertex_indices) // 3
 
 
-def make_mesh(points, triangles):
+def make_mesh(points, triangles, normals=None, uvs=None):
     pts = np.asarray(points, dtype=np.float32).reshape(-1, 3)
     p4 = np.ones((len(pts), 4), np.float32)
     p4[:, :3] = pts
     vi = np.ascontiguousarray(np.asarray(triangles, dtype=np.int64).reshape(-1))
-    return Mesh(points=np.ascontiguousarray(p4), vertex_indices=vi)
+    nrm = None if normals is None else np.ascontiguousarray(np.asarray(normals, np.float32).reshape(len(pts), 3))
+    uv = None if uvs is None else np.ascontiguousarray(np.asarray(uvs, np.float32).reshape(len(pts), 2))
+    return Mesh(points=np.ascontiguousarray(p4), vertex_indices=vi, normals=nrm, uvs=uv)
 
 
 def triangle_bounds(mesh):
@@ -166,8 +170,10 @@ class SceneBuilder:
                                      (conductor_roughness,))
         return len(self._materials) - 1
 
-    def add_mesh(self, points, triangles, material=0):
-        mesh = make_mesh(points, triangles)
+    def add_mesh(self, points, triangles, material=0, normals=None, uvs=None):
+        """A mesh of diffuse (or `material`) triangles; optional vertex normals
+        and UVs shade it as Triangle.computeSurfaceInteraction does."""
+        mesh = make_mesh(points, triangles, normals, uvs)
         self.meshes.append(mesh)
         idx = len(self.meshes) - 1
         self._prims.append((idx, mesh.triangle_count, PRIM_GEOMETRIC, material, self._geometric))

@@ -373,6 +373,26 @@ def materials_box_scene(seed=0xB1):
     return sb
 
 
+def smooth_box_scene(seed=0xB2):
+    """The box scene with two shaded-smooth meshes: an icosphere with vertex
+    normals and spherical UVs (coated diffuse, roughness 0.3) and a coarse
+    displaced sphere with vertex normals only (diffuse)."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    _room(sb, rng)
+    sp, st = icosphere(2)
+    nrm = sp / np.linalg.norm(sp, axis=1, keepdims=True)
+    uv = np.stack([0.5 + np.arctan2(nrm[:, 2], nrm[:, 0]) / (2 * np.pi), np.arccos(np.clip(nrm[:, 1], -1, 1)) / np.pi], 1)
+    sb.add_mesh(sp * 0.18 + np.array([0.35, 0.18, 0.45]), st,
+                sb.add_material(rng.uniform(0.2, 0.8, 3), kind="coateddiffuse", roughness=0.3), normals=nrm, uvs=uv)
+    pts, tris = displaced_icosphere(2, amplitude=0.1, seed=7)
+    n2 = pts / np.linalg.norm(pts, axis=1, keepdims=True)
+    sb.add_mesh(pts * 0.15 + np.array([0.7, 0.16, 0.55]), tris, sb.add_material(rng.uniform(0.2, 0.8, 3)), normals=n2)
+    lp, lt = _quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
+    sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
+    return sb
+
+
 # ---------------------------------------------------------------- scene batches
 
 BATCH_SIDES = (64, 128, 256, 512)

@@ -424,6 +424,17 @@ GZG_API gzg_status gzg_ply_read(const char *path, gzg_ply_mesh **out);
 GZG_API gzg_status gzg_ply_parse(const void *data, int64_t size, gzg_ply_mesh **out);
 GZG_API gzg_status gzg_ply_free(gzg_ply_mesh *mesh);
 
+/* Vertex normals (vertex_count x 3) and / or UVs (vertex_count x 2) of mesh
+ * `mesh` of an uploaded flat scene (HOST arrays; either may be NULL;
+ * vertex_count = the mesh's points count / 4).  The renderer then shades as
+ * Triangle.computeSurfaceInteraction does with them (Shape/Triangle.swift:
+ * 386-452): dpdu from the UVs unless degenerate, the shading normal
+ * interpolated from the vertex normals; the shading normal weighs light
+ * samples and BSDF samples, the geometric normal the path throughput.  Call
+ * before the scene enters a renderer, batch or two-level scene. */
+GZG_API gzg_status gzg_scene_set_vertex_attributes(gzg_scene *scene, int64_t mesh, const float *normals,
+                                                   const float *uvs, int64_t vertex_count);
+
 /* ---- film output ---------------------------------------------------------- */
 
 /* Normalises device film sums into an image (Pixel.normalized,

@@ -279,6 +279,75 @@ bool prim_tri(const Scene &sc, int64_t k, V3 *p0, V3 *p1, V3 *p2) {
         return prim_tri_of(sc.prims, sc.meshes, k, p0, p1, p2);
 }
 
+// The mesh and the vertex indices of prim k's triangle.
+bool prim_vertices(const orc_prim_id *prims, const orc_mesh *meshes, int64_t k, const orc_mesh **m, int64_t v[3]) {
+        const orc_prim_id &pr = prims[k];
+        int64_t mesh, base;
+        if (pr.type == 0) {
+                mesh = pr.id1;
+                base = pr.id2;
+        } else if (pr.type >= 1 && pr.type <= 3 && pr.id2 != -1) {
+                mesh = pr.id2 >> 32;
+                base = (pr.id2 & 0xFFFFFFFFll) * 3;
+        } else {
+                return false;
+        }
+        *m = &meshes[mesh];
+        for (int c = 0; c < 3; ++c) v[c] = (*m)->vertex_indices[base + c];
+        return true;
+}
+
+// Triangle.computeSurfaceInteraction with vertex normals and / or UVs
+// (Shape/Triangle.swift:386-452): dpdu from the UVs unless degenerate (then
+// a coordinate system around the geometric normal), the shading normal
+// interpolated from the vertex normals (normalised, (6, 6, 6) when it
+// vanishes), the shading tangent made orthogonal to it.  Returns false for
+// a degenerate triangle; ns = the interaction's (normalised) shading normal.
+bool attr_shading(const orc_mesh &m, const int64_t v[3], V3 p0, V3 p1, V3 p2, float b0, float b1, float b2, V3 ng,
+                  V3 *dpdu_out, V3 *ns_out) {
+        const bool has_uv = m.uvs != nullptr, has_n = m.normals != nullptr;
+        float uv[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        if (has_uv)
+                for (int c = 0; c < 3; ++c) {
+                        uv[c][0] = m.uvs[2 * v[c]];
+                        uv[c][1] = m.uvs[2 * v[c] + 1];
+                }
+        const V3 dp02 = sub(p0, p2), dp12 = sub(p1, p2);
+        const float du02 = uv[0][0] - uv[2][0], dv02 = uv[0][1] - uv[2][1];
+        const float du12 = uv[1][0] - uv[2][0], dv12 = uv[1][1] - uv[2][1];
+        const float det = du02 * dv12 - dv02 * du12;
+        const bool degenerate = std::fabs(det) < 1e-8f;
+        V3 dpdu = v3(0, 1, 0), dpdv = v3(0, 1, 0);
+        if (!degenerate) {
+                const float inv = 1.0f / det;
+                dpdu = mul(sub(mul(dp02, dv12), mul(dp12, dv02)), inv);
+                dpdv = mul(sub(mul(dp02, -du12), mul(dp12, du02)), inv);
+        }
+        if (degenerate || length_sq(cross(dpdu, dpdv)) == 0.0f) {
+                const V3 gn = cross(sub(p2, p0), sub(p1, p0));
+                if (length_sq(gn) == 0.0f) return false;
+                coordinate_system(normalize(gn), &dpdu, &dpdv);
+        }
+        V3 ns = ng;
+        if (has_n) {
+                V3 n[3];
+                for (int c = 0; c < 3; ++c) n[c] = v3(m.normals[3 * v[c]], m.normals[3 * v[c] + 1], m.normals[3 * v[c] + 2]);
+                ns = add(add(mul(n[0], b0), mul(n[1], b1)), mul(n[2], b2));
+                ns = length_sq(ns) > 0.0f ? normalize(ns) : v3(6.0f, 6.0f, 6.0f);
+        }
+        V3 s = normalize(dpdu);
+        V3 t = cross(s, ns);
+        if (length_sq(t) > 0.0f) {
+                t = normalize(t);
+                s = cross(t, ns);
+        } else {
+                coordinate_system(ns, &s, &t);
+        }
+        *dpdu_out = s;
+        *ns_out = normalize(ns);
+        return true;
+}
+
 struct Hit {
         bool hit;
         int32_t prim, inst;
@@ -320,6 +389,7 @@ V3 xf_normal(const float *inv, V3 n) {
 // Transform * SurfaceInteraction, Core/Transform+SurfaceInteraction.swift:3-14).
 struct Isect {
         V3 pos, ng, wo;
+        V3 ns;  // shading normal (ng without vertex normals)
         Frame fr;
         bool frame_ok;
         const orc_prim_id *pr;
@@ -335,7 +405,16 @@ bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
                 is->pos = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
                 is->ng = normalize(cross(sub(p0, p2), sub(p1, p2)));
                 is->wo = normalize(neg(d));
-                is->frame_ok = make_frame(p0, p1, p2, is->ng, &is->fr);
+                is->ns = is->ng;
+                const orc_mesh *m;
+                int64_t vv[3];
+                if (prim_vertices(sc.prims, sc.meshes, h.prim, &m, vv) && (m->normals || m->uvs)) {
+                        V3 s;
+                        is->frame_ok = attr_shading(*m, vv, p0, p1, p2, b0, h.u, h.v, is->ng, &s, &is->ns);
+                        if (is->frame_ok) is->fr = frame_from(s, is->ns);
+                } else {
+                        is->frame_ok = make_frame(p0, p1, p2, is->ng, &is->fr);
+                }
                 is->pr = &sc.prims[h.prim];
                 is->mats = sc.materials;
                 is->blas = -1;
@@ -349,12 +428,19 @@ bool interaction(const Scene &sc, const Hit &h, V3 d, Isect *is) {
         const V3 pos_o = add(add(mul(p0, b0), mul(p1, h.u)), mul(p2, h.v));
         const V3 n_o = normalize(cross(sub(p0, p2), sub(p1, p2)));
         const V3 wo_o = normalize(neg(xf_vector(w2o, d)));
-        V3 s_o = v3(0, 0, 0);
-        is->frame_ok = shading_dpdu(p0, p1, p2, n_o, &s_o);
+        V3 s_o = v3(0, 0, 0), ns_o = n_o;
+        const orc_mesh *m;
+        int64_t vv[3];
+        const bool with_attr = prim_vertices(B.prims, B.meshes, h.prim, &m, vv) && (m->normals || m->uvs);
+        if (with_attr)
+                is->frame_ok = attr_shading(*m, vv, p0, p1, p2, b0, h.u, h.v, n_o, &s_o, &ns_o);
+        else
+                is->frame_ok = shading_dpdu(p0, p1, p2, n_o, &s_o);
         is->pos = xf_point(o2w, pos_o);
         is->ng = normalize(xf_normal(w2o, n_o));
+        is->ns = with_attr ? normalize(xf_normal(w2o, ns_o)) : is->ng;
         is->wo = normalize(xf_vector(o2w, wo_o));
-        if (is->frame_ok) is->fr = frame_from(xf_vector(o2w, s_o), is->ng);
+        if (is->frame_ok) is->fr = frame_from(xf_vector(o2w, s_o), is->ns);
         is->pr = &B.prims[h.prim];
         is->mats = I.blas_materials[b];
         is->blas = b;
@@ -466,7 +552,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         Hit sh = trace(sc, so, sub(target, so), 1.0f - 0.00001f);
                         ++res.shadow;
                         if (!sh.hit) {
-                                light_est = mulv(mul(f_world(dv), std::fabs(dot(dv, ng))), rad);
+                                light_est = mulv(mul(f_world(dv), std::fabs(dot(dv, is.ns))), rad);
                                 light_dir = dv;
                                 light_pdf = pdf;
                         }
@@ -484,7 +570,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         Hit sh = trace(sc, so, sub(lp, so), 1.0f - 0.00001f);
                         ++res.shadow;
                         if (!sh.hit) {
-                                light_est = mulv(mul(f_world(inc), std::fabs(dot(inc, ng))), emitted(sc, lt.le));
+                                light_est = mulv(mul(f_world(inc), std::fabs(dot(inc, is.ns))), emitted(sc, lt.le));
                                 light_dir = inc;
                                 light_pdf = pdf;
                         }
@@ -501,7 +587,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                 float pdf_b;
                 sample_local(u3, fs, wi_l, pdf_b);
                 const V3 wi = fr.to_world(wi_l);
-                V3 est = mul(fs, std::fabs(dot(wi, ng)));
+                V3 est = mul(fs, std::fabs(dot(wi, is.ns)));
                 if ((P.mis_corrected || lt.is_env) && !is_black(est) && pdf_b > 0.0f) {
                         const V3 po = offset_origin(pos, ng, wi);
                         Hit ph = trace(sc, po, wi, kInfF);
@@ -664,7 +750,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                 if (!sh.hit) {
                                         const bool reflect = dot(dv, ng) * dot(wo, ng) > 0.0f;
                                         const V3 f = reflect ? f_val : v3(0, 0, 0);
-                                        light_est = mulv(mul(f, std::fabs(dot(dv, ng))), rad);
+                                        light_est = mulv(mul(f, std::fabs(dot(dv, is.ns))), rad);
                                         light_dir = dv;
                                         light_pdf = pdf;
                                 }
@@ -691,7 +777,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                 if (!sh.hit) {
                                         const bool reflect = dot(dir, ng) * dot(wo, ng) > 0.0f;
                                         const V3 f = reflect ? f_val : v3(0, 0, 0);
-                                        const V3 scatter = mul(f, std::fabs(dot(dir, ng)));
+                                        const V3 scatter = mul(f, std::fabs(dot(dir, is.ns)));
                                         light_est = mulv(scatter, emitted(sc, lt.le));
                                         light_dir = dir;
                                         light_pdf = pdf;
@@ -718,7 +804,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                         if (wo_l.z < 0.0f) wi_l.z = -wi_l.z;
                         const float pdf_b = (wo_l.z * wi_l.z > 0.0f) ? std::fabs(wi_l.z) / kPi : 0.0f;
                         const V3 wi = fr.to_world(wi_l);
-                        V3 est = mul(f_val, std::fabs(dot(wi, ng)));
+                        V3 est = mul(f_val, std::fabs(dot(wi, is.ns)));
                         if ((P.mis_corrected || lt.is_env) && !is_black(est) && pdf_b > 0.0f) {
                                 const V3 po = offset_origin(pos, ng, wi);
                                 Hit ph = trace(sc, po, wi, kInfF);

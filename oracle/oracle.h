@@ -41,6 +41,8 @@ typedef struct orc_mesh {
         const float *points;
         const int64_t *face_indices;
         const int64_t *vertex_indices;
+        const float *normals; /* per vertex x3, or NULL (renderer only) */
+        const float *uvs;     /* per vertex x2, or NULL (renderer only) */
 } orc_mesh;
 typedef struct orc_ray {
         float ox, oy, oz, dx, dy, dz;

@@ -24,7 +24,24 @@ ISECT_DTYPE = np.dtype({"names": ["prim_id", "t_hit", "u", "v", "hit"],
 
 
 class _Mesh(C.Structure):
-    _fields_ = [("points", C.c_void_p), ("face_indices", C.c_void_p), ("vertex_indices", C.c_void_p)]
+    _fields_ = [("points", C.c_void_p), ("face_indices", C.c_void_p), ("vertex_indices", C.c_void_p),
+                ("normals", C.c_void_p), ("uvs", C.c_void_p)]
+
+
+def _render_mesh(m, keep):
+    """An orc_mesh for the renderer, with the mesh's vertex normals / UVs when it has them."""
+    p4 = np.ascontiguousarray(m.points, np.float32)
+    vi = np.ascontiguousarray(m.vertex_indices, np.int64)
+    keep += [p4, vi]
+    nrm = uvs = None
+    if getattr(m, "normals", None) is not None:
+        nrm = np.ascontiguousarray(m.normals, np.float32)
+        keep.append(nrm)
+    if getattr(m, "uvs", None) is not None:
+        uvs = np.ascontiguousarray(m.uvs, np.float32)
+        keep.append(uvs)
+    return _Mesh(p4.ctypes.data, None, vi.ctypes.data, nrm.ctypes.data if nrm is not None else None,
+                 uvs.ctypes.data if uvs is not None else None)
 
 
 class ZSobolState(C.Structure):
@@ -298,10 +315,7 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
         for i, b in enumerate(blas_scenes):
             marr = (_Mesh * max(len(b.meshes), 1))()
             for k, m in enumerate(b.meshes):
-                p4 = np.ascontiguousarray(m.points, np.float32)
-                vi = np.ascontiguousarray(m.vertex_indices, np.int64)
-                keep += [p4, vi]
-                marr[k] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+                marr[k] = _render_mesh(m, keep)
             nodes_b = np.ascontiguousarray(b.nodes)
             prims_b = np.ascontiguousarray(b.prims)
             mats_b = np.ascontiguousarray(b.materials)
@@ -325,10 +339,7 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
         hs = blas_scenes[0]  # flat arrays unused
     arr = (_Mesh * max(len(hs.meshes), 1))()
     for i, m in enumerate(hs.meshes):
-        p4 = np.ascontiguousarray(m.points, np.float32)
-        vi = np.ascontiguousarray(m.vertex_indices, np.int64)
-        keep += [p4, vi]
-        arr[i] = _Mesh(p4.ctypes.data, None, vi.ctypes.data)
+        arr[i] = _render_mesh(m, keep)
     mats = np.ascontiguousarray(hs.materials)
     mparams = None
     if instances is None and getattr(hs, "material_params", None) is not None:
