@@ -78,13 +78,15 @@ class GpuAccelerator:
     @classmethod
     def from_mesh_arrays(cls, meshes, materials, leaf_size=0, builder=0, radius=0):
         """The ingestion fast path (gzg_gpu_build_mesh_scene): meshes is a list
-        of (points (n, 3) float32, indices (m, 3) int32, material index);
-        materials a MATERIAL_DTYPE array.  Prim k of the scene is triangle k
-        in mesh order (id2 = mesh << 32 | triangle)."""
+        of (points (n, 3) float32, indices (m, 3) int32, material index[,
+        normals (n, 3) or None[, uvs (n, 2) or None]]); materials a
+        MATERIAL_DTYPE array.  Prim k of the scene is triangle k in mesh order
+        (id2 = mesh << 32 | triangle)."""
         self = cls.__new__(cls)
         keep = []
         arr = (F.MeshArrays * max(len(meshes), 1))()
-        for k, (pts, idx, mat) in enumerate(meshes):
+        for k, entry in enumerate(meshes):
+            pts, idx, mat = entry[:3]
             pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
             idx = np.ascontiguousarray(idx, np.int32).reshape(-1, 3)
             keep += [pts, idx]
@@ -101,6 +103,15 @@ class GpuAccelerator:
         self.handle = handle
         self.device_built = True
         self.host = _ArraysHost(meshes, materials)
+        try:
+            for k, entry in enumerate(meshes):
+                nrm = entry[3] if len(entry) > 3 else None
+                uv = entry[4] if len(entry) > 4 else None
+                if nrm is not None or uv is not None:
+                    self.set_vertex_attributes(k, nrm, uv)
+        except Exception:
+            self.close()
+            raise
         return self
 
     # ------------------------------------------------------------ lifetime
@@ -271,7 +282,7 @@ class _ArraysHost:
     def __init__(self, meshes, materials):
         # bounds of the vertices (a superset of the triangles' when some
         # vertices are unreferenced: still a valid instance bound)
-        pts = [np.asarray(p, np.float32).reshape(-1, 3) for p, _, _ in meshes]
+        pts = [np.asarray(e[0], np.float32).reshape(-1, 3) for e in meshes]
         pts = [p for p in pts if len(p)]
         self._lo = np.min([p.min(0) for p in pts], 0) if pts else np.zeros(3, np.float32)
         self._hi = np.max([p.max(0) for p in pts], 0) if pts else np.zeros(3, np.float32)

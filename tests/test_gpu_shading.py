@@ -90,3 +90,38 @@ def test_vertex_attributes_are_validated():
             acc.set_vertex_attributes(0, normals=np.zeros((3, 3), np.float32))  # wrong vertex count
         with pytest.raises(GzgError):
             acc.set_vertex_attributes(99, normals=np.zeros((3, 3), np.float32))  # no such mesh
+
+
+def test_ply_normals_through_the_fast_path(tmp_path):
+    """A PLY mesh with vertex normals and UVs (x y z nx ny nz u v) read and
+    built on the device shades like the same mesh through the builder."""
+    from gonzales_b200 import scene as S
+
+    pts, tris = scenes.icosphere(2)
+    pts = pts * 0.2 + np.array([0.5, 0.2, 0.5])
+    nrm = (pts - np.array([0.5, 0.2, 0.5])) / 0.2
+    uv = pts[:, :2].copy()
+    path = tmp_path / "s.ply"
+    S.write_ply(path, pts, tris, normals=nrm, uvs=uv)
+    ply = S.read_ply(path)
+    sb = SceneBuilder()
+    rng = np.random.default_rng(4)
+    scenes._room(sb, rng)
+    m = sb.add_material((0.6, 0.5, 0.4))
+    sb.add_mesh(ply["points"], ply["indices"], m, normals=ply["normals"], uvs=ply["uvs"])
+    lp, lt = scenes._quad((0.35, 0.999, 0.35), (0.65, 0.999, 0.35), (0.65, 0.999, 0.65), (0.35, 0.999, 0.65))
+    sb.add_area_light(lp, lt, (15.0, 11.0, 4.0))
+    hs = sb.build()
+    room = hs.meshes[0]
+    mats = np.zeros(3, F.MATERIAL_DTYPE)
+    mats[0] = hs.materials[0]
+    mats[1] = hs.materials[1]
+    mats[2] = (2, (0, 0, 0), (15.0, 11.0, 4.0))
+    light = hs.meshes[2]
+    arrays = [(room.points[:, :3], room.vertex_indices.reshape(-1, 3), 0),
+              (ply["points"], ply["indices"], 1, ply["normals"], ply["uvs"]),
+              (light.points[:, :3], light.vertex_indices.reshape(-1, 3), 2)]
+    p = F.render_params(48, 48, 8, max_depth=4, rr_min_bounce=3)
+    with GpuAccelerator(hs) as a, GpuAccelerator.from_mesh_arrays(arrays, mats) as b:
+        ra, rb = a.render(p), b.render(p)
+    np.testing.assert_allclose(ra[0], rb[0], rtol=1e-5, atol=1e-6)
