@@ -119,3 +119,17 @@ def test_thin_lens_camera_matches_oracle():
     np.testing.assert_allclose(g[0].sum((0, 1)) / g[2].sum(), o[0].sum((0, 1)) / o[2].sum(), rtol=1e-2)
     # the lens moves the rays: the image differs from the pinhole one
     assert not np.allclose(g[0], g0[0], rtol=1e-3)
+
+
+def test_film_resolve_reference_pixel_cases():
+    """Tests/libgonzalesTests/PixelTests.swift: light / weight; black with
+    weight 0 stays black; non-black with weight 0 is the reference's error
+    (counted here)."""
+    from gonzales_b200 import film
+
+    torch = torch_mod()
+    rgb = torch.tensor([[4.0, 6.0, 8.0], [0.0, 0.0, 0.0], [1.0, 1.0, 1.0]], device="cuda")
+    w = torch.tensor([2.0, 0.0, 0.0], device="cuda")
+    img, zero = film.resolve(rgb, w)
+    np.testing.assert_allclose(img.cpu().numpy(), [[2.0, 3.0, 4.0], [0, 0, 0], [0, 0, 0]], atol=1e-6)
+    assert zero == 1
