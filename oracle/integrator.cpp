@@ -1032,3 +1032,45 @@ extern "C" void orc_render_textured(const orc_node *nodes, const orc_prim_id *pr
         orc_render_ex(nodes, prims, meshes, materials, n_materials, n_prims, nullptr, nullptr, nullptr, params,
                       textures, sum_rgb, sum_sq, sum_w, nullptr, nullptr, counters, threads);
 }
+
+// Sampling and interaction helpers, exported one by one so that tests can pin
+// them on the reference's own unit tests (Tests/libgonzalesTests/
+// SamplingTests.swift, InteractionTests.swift, FilterTests.swift).
+extern "C" float orc_power_heuristic(float f, float g) { return power_heuristic(f, g); }
+
+extern "C" void orc_concentric_disk(float u0, float u1, float *xy) { concentric_disk(u0, u1, &xy[0], &xy[1]); }
+
+extern "C" void orc_cosine_hemisphere(float u0, float u1, float *d) {
+        const V3 v = cosine_hemisphere(u0, u1);
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+}
+
+extern "C" void orc_offset_origin(const float *p, const float *n, const float *dir, float *out) {
+        const V3 o = offset_origin(v3(p[0], p[1], p[2]), v3(n[0], n[1], n[2]), v3(dir[0], dir[1], dir[2]));
+        out[0] = o.x;
+        out[1] = o.y;
+        out[2] = o.z;
+}
+
+// spawnRay(from:target:) as the shadow test uses it: origin nudged toward the
+// target, direction to the target, tHit just below 1.
+extern "C" float orc_spawn_to(const float *from, const float *target, float *origin, float *dir) {
+        const V3 pf = v3(from[0], from[1], from[2]), pt = v3(target[0], target[1], target[2]);
+        const V3 so = add(pf, mul(sub(pt, pf), 0.0001f));
+        const V3 sd = sub(pt, so);
+        origin[0] = so.x;
+        origin[1] = so.y;
+        origin[2] = so.z;
+        dir[0] = sd.x;
+        dir[1] = sd.y;
+        dir[2] = sd.z;
+        return 1.0f - 0.00001f;
+}
+
+extern "C" float orc_gaussian(float x, float sigma) { return gaussian(x, sigma); }
+
+extern "C" void orc_gaussian_sample_1d(float u, float radius, float sigma, float *x, float *density) {
+        gaussian_sample_1d(u, radius, sigma, x, density);
+}

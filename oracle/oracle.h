@@ -249,6 +249,18 @@ void orc_bsdf_eval(const orc_bsdf_params *p, const float *wo, const float *wi, f
 int orc_bsdf_sample(const orc_bsdf_params *p, const float *wo, const float *u, float *f, float *wi, float *pdf);
 int orc_bsdf_is_specular(const orc_bsdf_params *p);
 
+/* --- sampling and interaction helpers (Sampler/Sampling.swift,
+ * Core/Interaction.swift, Filter/GaussianFilter.swift) ------------------- */
+
+float orc_power_heuristic(float f, float g);
+void orc_concentric_disk(float u0, float u1, float *xy);
+void orc_cosine_hemisphere(float u0, float u1, float *dir);
+void orc_offset_origin(const float *p, const float *n, const float *dir, float *out);
+/* Shadow-ray spawn toward a target: writes origin and direction, returns tHit. */
+float orc_spawn_to(const float *from, const float *target, float *origin, float *dir);
+float orc_gaussian(float x, float sigma);
+void orc_gaussian_sample_1d(float u, float radius, float sigma, float *x, float *density);
+
 /* --- environment light (Light/InfiniteLight.swift) ----------------------- */
 
 /* Map rgb[h][w][3] (row v, column u); scale enters the light's power only. */

@@ -90,6 +90,13 @@ def lib():
             "orc_zsobol_get2d": (None, [vp, vp]),
             "orc_zsobol_get3d": (None, [vp, vp]),
             "orc_zsobol_batch": (None, [i64, i32, i32, i64, vp, vp, vp, i64, vp, i32, vp]),
+            "orc_power_heuristic": (f32, [f32, f32]),
+            "orc_concentric_disk": (None, [f32, f32, vp]),
+            "orc_cosine_hemisphere": (None, [f32, f32, vp]),
+            "orc_offset_origin": (None, [vp, vp, vp, vp]),
+            "orc_spawn_to": (f32, [vp, vp, vp, vp]),
+            "orc_gaussian": (f32, [f32, f32]),
+            "orc_gaussian_sample_1d": (None, [f32, f32, f32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -506,3 +513,52 @@ def bsdf_sample(p, wo, u):
 
 def bsdf_is_specular(p):
     return bool(_bsdf_lib().orc_bsdf_is_specular(C.byref(p)))
+
+
+def power_heuristic(f, g):
+    return float(lib().orc_power_heuristic(f, g))
+
+
+def concentric_disk(u0, u1):
+    out = np.zeros(2, np.float32)
+    lib().orc_concentric_disk(u0, u1, out.ctypes.data)
+    return out
+
+
+def cosine_hemisphere(u0, u1):
+    out = np.zeros(3, np.float32)
+    lib().orc_cosine_hemisphere(u0, u1, out.ctypes.data)
+    return out
+
+
+def offset_origin(p, n, d):
+    p, n, d = (np.ascontiguousarray(x, np.float32) for x in (p, n, d))
+    out = np.zeros(3, np.float32)
+    lib().orc_offset_origin(p.ctypes.data, n.ctypes.data, d.ctypes.data, out.ctypes.data)
+    return out
+
+
+def spawn_to(frm, target):
+    """Shadow-ray spawn: (origin, direction, tHit)."""
+    frm, target = (np.ascontiguousarray(x, np.float32) for x in (frm, target))
+    o, d = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    t = lib().orc_spawn_to(frm.ctypes.data, target.ctypes.data, o.ctypes.data, d.ctypes.data)
+    return o, d, float(t)
+
+
+def gaussian_filter_evaluate(x, y, sigma):
+    """GaussianFilter.evaluate: the separable product, each factor clamped at 0."""
+    L = lib()
+    return max(0.0, L.orc_gaussian(x, sigma)) * max(0.0, L.orc_gaussian(y, sigma))
+
+
+def gaussian_filter_sample(u0, u1, radius, sigma):
+    """GaussianFilter.sample: ((x, y), density)."""
+    L = lib()
+    xs, ds = [], []
+    for u in (u0, u1):
+        x, dn = C.c_float(), C.c_float()
+        L.orc_gaussian_sample_1d(u, radius, sigma, C.byref(x), C.byref(dn))
+        xs.append(x.value)
+        ds.append(dn.value)
+    return (xs[0], xs[1]), ds[0] * ds[1]

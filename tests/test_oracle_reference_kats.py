@@ -15,7 +15,20 @@ text; values and bounds as those tests state them):
       0.5 is not; getAlpha(0.25) = 0.5 (the remapping the materials apply).
 
 The Fresnel term is read through the smooth dielectric's sample: its
-reflection probability is F(cos theta)."""
+reflection probability is F(cos theta).
+
+The sampling, interaction and filter helpers the integrator uses are pinned
+the same way:
+
+  Tests/libgonzalesTests/SamplingTests.swift    power heuristic values,
+      concentric disk centre and unit circle, cosine hemisphere length and
+      upper half;
+  Tests/libgonzalesTests/InteractionTests.swift offset origin on the
+      direction's side of the normal; shadow spawn toward the target with
+      tHit in (0.99, 1);
+  Tests/libgonzalesTests/FilterTests.swift      Gaussian filter (support 2,
+      sigma 1): centre above edge, non-negative, symmetric, samples inside
+      the support with positive density."""
 import math
 
 import numpy as np
@@ -103,3 +116,67 @@ def test_roughness_remapping():
     assert not O.bsdf_is_specular(O.bsdf_params(3, eta=1.5, roughness=0.25))
     # roughness 0.0005^2 gives alpha 0.0005 < 0.001: smooth
     assert O.bsdf_is_specular(O.bsdf_params(3, eta=1.5, roughness=0.0005 ** 2))
+
+
+# --- Tests/libgonzalesTests/SamplingTests.swift -----------------------------
+
+
+@pytest.mark.parametrize("f,g,want", [(1.0, 1.0, 0.5), (0.0, 1.0, 0.0), (1.0, 0.0, 0.0), (0.0, 0.0, 0.0),
+                                      (2.0, 3.0, 4.0 / 13.0)])
+def test_power_heuristic_known_values(f, g, want):
+    assert abs(O.power_heuristic(f, g) - want) <= 1e-6
+
+
+def test_power_heuristic_dominating_and_dominated():
+    assert O.power_heuristic(100.0, 1.0) > 0.99
+    assert O.power_heuristic(1.0, 100.0) < 0.01
+
+
+def test_concentric_disk_center_and_unit_circle():
+    c = O.concentric_disk(0.5, 0.5)
+    assert abs(c[0]) <= 1e-6 and abs(c[1]) <= 1e-6
+    for u in [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0), (1.0, 1.0), (0.25, 0.75), (0.8, 0.2)]:
+        d = O.concentric_disk(*u)
+        assert d[0] * d[0] + d[1] * d[1] <= 1.0 + 1e-6, u
+
+
+def test_cosine_hemisphere_unit_length_and_upper():
+    v = O.cosine_hemisphere(0.3, 0.7)
+    assert abs(np.linalg.norm(v.astype(np.float64)) - 1.0) <= 1e-5
+    for u in [(0.1, 0.1), (0.5, 0.5), (0.9, 0.9), (0.0, 0.0)]:
+        assert O.cosine_hemisphere(*u)[2] >= 0, u
+
+
+# --- Tests/libgonzalesTests/InteractionTests.swift --------------------------
+
+
+def test_offset_origin_follows_direction_side():
+    p, n = [0, 0, 0], [0, 0, 1]
+    assert O.offset_origin(p, n, [0, 0, 1])[2] > 0
+    assert O.offset_origin(p, n, [0, 0, -1])[2] < 0
+
+
+def test_spawn_to_target():
+    o, d, t = O.spawn_to([0, 0, 0], [10, 0, 0])
+    assert d[0] > 0
+    assert 0.99 < t < 1.0
+    # the ray ends on the target at t = 1
+    np.testing.assert_allclose(o + d, [10, 0, 0], atol=1e-5)
+
+
+# --- Tests/libgonzalesTests/FilterTests.swift (GaussianFilter) ------------
+
+
+def test_gaussian_filter_shape():
+    ev = lambda x, y: O.gaussian_filter_evaluate(x, y, 1.0)
+    assert ev(0, 0) > ev(1.5, 1.5)
+    for x, y in [(0, 0), (1, 0), (0, 1), (1.9, 1.9)]:
+        assert ev(x, y) >= 0
+    assert abs(ev(0.5, 0.7) - ev(-0.5, -0.7)) <= 1e-6
+
+
+def test_gaussian_filter_sample_within_support():
+    for u in [(0.1, 0.1), (0.5, 0.5), (0.9, 0.9)]:
+        (x, y), dens = O.gaussian_filter_sample(u[0], u[1], 2.0, 1.0)
+        assert abs(x) <= 2.0 + 1e-6 and abs(y) <= 2.0 + 1e-6
+        assert dens > 0
