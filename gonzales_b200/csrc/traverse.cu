@@ -445,7 +445,9 @@ __global__ void __launch_bounds__(128, 6) k_wide_instanced(DevScene s, const voi
 
                 bool finished = false, fault = false;
                 if (pend_mask == 0) {
-                        if ((group.y >> 24) == 0 && sp > 0) {
+                        // pop until there is work: a world-ray marker restores the
+                        // world ray and pops again in the same step
+                        while ((group.y >> 24) == 0 && sp > 0) {
                                 --sp;
                                 const uint2 e = stack[sp * stride];
                                 if (e.x == 0xFFFFFFFFu) {
@@ -460,6 +462,7 @@ __global__ void __launch_bounds__(128, 6) k_wide_instanced(DevScene s, const voi
                                 } else if (e.x & 0x80000000u) {
                                         pend_base = e.x & 0x7FFFFFFFu;
                                         pend_mask = e.y;
+                                        break;
                                 } else {
                                         group = e;
                                 }
