@@ -58,8 +58,8 @@ class DeviceGuard {
         int prev_ = 0, dev_ = 0;
 };
 
-constexpr int kSlots = 3;
-constexpr int64_t kChunk = 1 << 20;  // rays per pipelined chunk
+constexpr int kSlots = 4;
+constexpr int64_t kChunk = 1 << 19;  // rays per pipelined chunk (512K x 4 streams: 2 % faster end to end than 1M x 3)
 
 // Per-call staging: device buffers and pinned host buffers for kSlots chunks
 // in flight, each slot with its own stream.
