@@ -219,8 +219,12 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
 // iteration, so lanes are not left idle while the slowest ray of a fixed
 // 32-ray batch finishes.  Each iteration opens one node and tests its
 // triangles.  No atomics or per-launch state: the assignment is static.
+// Capped at 72 registers (7 blocks of 128 per SM): closest hit, 80 registers
+// uncapped, goes 4,011 -> 4,123 Mrays/s on the ray-cast workload; any hit
+// (71-72 uncapped) 5,238 -> 5,205.  Looser minimums are not the uncapped
+// build: at 6 blocks any hit takes 80 registers and drops to 4,779.
 template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
-__global__ void __launch_bounds__(128) k_wide_persistent(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const void *__restrict__ rays,
                                                          const float *__restrict__ tmaxs, int64_t n,
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
