@@ -390,11 +390,12 @@ __device__ __forceinline__ float xf_vector(const float4 &row, float x, float y, 
 // ray to object space and descends into the bottom-level root.  Popping the
 // marker restores the world ray.  Bottom-level trees are ordinary wide trees
 // stored after the top-level nodes in the same arrays.
-// Bounded to 128-thread blocks, 6 resident per SM (at most 80 registers):
-// 1.6x the closest-hit rate of camera rays over the unbounded build, whose 99
-// registers left 4 blocks per SM.
+// Bounded to 128-thread blocks, 7 resident per SM (at most 72 registers, a
+// few dozen bytes of spills): the unbounded build's 99 registers left 4 blocks
+// per SM; 6 blocks (80 registers) gave 1.6x its camera-ray rate and 7 another
+// 2 % on the two-level frame (1,187 -> 1,162 ms); 5 and 8 were slower.
 template <int OUTFMT, bool ANY, int STACK>
-__global__ void __launch_bounds__(128, 6) k_wide_instanced(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const void *__restrict__ rays,
                                                         const float *__restrict__ tmaxs, int64_t n,
                                                         void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
