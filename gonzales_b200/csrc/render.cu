@@ -1192,13 +1192,17 @@ __global__ void k_shadow_resolve(Wave w) {
 
 // Adds the radiance a BSDF probe reaches: the emission of an area light whose
 // normal faces back along the probe, or, on a miss, the environment light.
-__global__ void k_probe_resolve(Wave w, DevScene s) {
+// any_only: the view has no area light and the probes were traced as any-hit
+// queries (pr_hits holds one int32 prim or -1 per probe); a blocked probe
+// reaches nothing, exactly as a closest hit on a non-emitting surface.
+__global__ void k_probe_resolve(Wave w, DevScene s, int any_only) {
         const uint32_t n = w.counts[kCountProbe];
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= n) return;
-        const float4 h = w.pr_hits[i];
-        const int prim = __float_as_int(h.w);
         const V3 wi = v3(w.pr_ray[2 * i + 1]);
+        if (any_only && reinterpret_cast<const int32_t *>(w.pr_hits)[i] >= 0) return;
+        const float4 h = any_only ? make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1)) : w.pr_hits[i];
+        const int prim = __float_as_int(h.w);
         V3 le;
         if (prim < 0) {
                 if (!s.env_rgb) return;
@@ -1492,6 +1496,9 @@ struct gzg_renderer {
         uint32_t max_capacity = 0;
         DevScene view{};
         int wide_depth = 0;
+        // no prim of the view is an area light: a BSDF probe can only reach
+        // the environment, so it is traced as an any-hit query
+        bool probe_any = false;
         std::vector<void *> allocs;
         cudaGraphExec_t graph = nullptr;
         cudaGraph_t graph_def = nullptr;
@@ -1601,12 +1608,18 @@ struct gzg_renderer {
                         if (e != cudaSuccess) return e;
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
                         if (corrected) {
-                                lp.n_dev = w.counts + kCountProbe;
-                                lp.inst_out = w.pr_inst;
-                                e = launch_trace(view, lp, kRayDevice, kOutHit, w.pr_ray, nullptr, w.capacity, w.pr_hits,
-                                                 st);
+                                if (probe_any) {
+                                        lpa.n_dev = w.counts + kCountProbe;
+                                        e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.pr_ray, nullptr, w.capacity,
+                                                         w.pr_hits, st);
+                                } else {
+                                        lp.n_dev = w.counts + kCountProbe;
+                                        lp.inst_out = w.pr_inst;
+                                        e = launch_trace(view, lp, kRayDevice, kOutHit, w.pr_ray, nullptr, w.capacity,
+                                                         w.pr_hits, st);
+                                }
                                 if (e != cudaSuccess) return e;
-                                k_probe_resolve<<<grid, block, 0, st>>>(w, view);
+                                k_probe_resolve<<<grid, block, 0, st>>>(w, view, probe_any ? 1 : 0);
                         }
                         k_bounce_tally<<<1, 1, 0, st>>>(w, cur);
                         cur ^= 1;
@@ -1838,6 +1851,10 @@ gzg_status build_batch(gzg_renderer *r) {
                 d.per_ray_root = 1;
         }
         r->wide_depth = wide_depth;
+        r->probe_any = true;
+        for (gzg_scene *sc : r->scenes)
+                for (const gzg_prim_id &p : scene_host_shading(sc).prims)
+                        if (p.type == 3) r->probe_any = false;
         return GZG_OK;
 }
 
