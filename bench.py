@@ -660,7 +660,7 @@ def run_ours(args):
             "any_hit_mrays_s": world * n / any_ms * 1000.0 / 1e6,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_wide (closest hit)",
+                         "kernel": "k_wide_persistent (closest hit)",
                          "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_per_launch / n,
                          "tris_per_ray": tris_per_launch / n},
             "e2e": {"value": world * n / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": n * 28,
