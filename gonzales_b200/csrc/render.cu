@@ -925,8 +925,15 @@ __device__ __forceinline__ uint32_t gen_pos(const Wave &w, int kind, uint32_t sl
 // hits and misses and queues hits on the general materials on their kind's
 // shade queue, which the kShadeDielectric .. kShadeCoatedConductor launches
 // then shade (one material kind per kernel: coherent warps, one BSDF's code).
+// Register bounds per kind: the split kernel at 6 blocks of 128 per SM (80
+// registers instead of 98), diffuse, dielectric and conductor at 5, the
+// layered kinds at 3 (their natural occupancy): 1,099 -> 1,091 ms on the
+// two-level frame.  Capping the layered kinds at 4 blocks spilled and lost.
 template <int kKind>
-__global__ void k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
+__global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 6
+                                      : (kKind == kShadeCoated || kKind == kShadeCoatedConductor) ? 3
+                                                                                                  : 5)
+    k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
         uint32_t i;
         if (kKind >= kShadeDielectric) {
