@@ -87,8 +87,9 @@ GZG_API gzg_status gzg_film_resolve_device(const float *film_rgb, const float *f
 
 GZG_API gzg_status gzg_write_exr(const char *path, const float *pixels, int32_t width, int32_t height,
                                  int32_t channels) {
+        // a scanline's byte count is a 32-bit field: width x 4 channels x 4 bytes
         if (!path || !pixels || width <= 0 || height <= 0 || (channels != 3 && channels != 4) ||
-            (int64_t)width * height > ((int64_t)1 << 31))
+            (int64_t)width * height > ((int64_t)1 << 31) || (int64_t)width * 16 > (int64_t)UINT32_MAX)
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_write_exr: bad arguments");
         std::vector<uint8_t> h;
         put_u32(h, 20000630u);  // magic 0x762f3101
@@ -147,7 +148,7 @@ GZG_API gzg_status gzg_write_exr(const char *path, const float *pixels, int32_t 
         for (int32_t y = 0; ok && y < height; ++y) {
                 line.clear();
                 put_u32(line, (uint32_t)y);
-                put_u32(line, (uint32_t)(width * 16));
+                put_u32(line, (uint32_t)((int64_t)width * 16));
                 const float *row = pixels + (size_t)y * width * channels;
                 for (int c : {3, 2, 1, 0})  // A, B, G, R
                         for (int32_t x = 0; x < width; ++x)
