@@ -504,7 +504,8 @@ typedef struct gzg_render_params {
         float filter_radius, filter_sigma; /* Gaussian pixel filter (reference default 2, 0.5) */
         int32_t first_sample;    /* render sample indices [first_sample, first_sample + spp) */
         int32_t sampler_spp;     /* ...of a Z-Sobol sampler with this many samples per pixel (0: spp) */
-        int32_t wave_paths;      /* paths in flight per wave (0: library default) */
+        int32_t wave_paths;      /* paths in flight per wave (0: library default, 2^24 paths or the
+                                    frame's path count if smaller; about 350 device bytes per path) */
         int32_t use_graph;       /* capture one wave as a CUDA graph and replay it */
         float lens_radius;       /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
         float focal_distance;    /* distance of the plane in focus (reference default 1e6) */
@@ -556,7 +557,8 @@ typedef enum gzg_sort_key {
 /* Options of a batch renderer (the per-scene wave_paths / use_graph of
  * gzg_render_params are not used by a batch). */
 typedef struct gzg_batch_options {
-        int32_t wave_paths;  /* paths in flight per wave (0: library default) */
+        int32_t wave_paths;  /* paths in flight per wave (0: library default, 2^24 paths; about 350
+                                device bytes per path) */
         int32_t use_graph;   /* capture one wave as a CUDA graph and replay it */
         int32_t sort_key;    /* gzg_sort_key */
         int32_t reserved;
