@@ -16,16 +16,18 @@ outputs (256 MiB of hits) are larger than the 126 MB L2, so no flush is done.
   roofline  algorithmic bytes of the traversal kernel (48 B ray I/O + 80 B per
             wide node + 48 B per triangle, counts from an instrumented replay)
             over the average launch time, against the measured HBM copy
-            bandwidth
-  cpu_baseline  the oracle (CPU restatement of the reference traversal) on the
-            host cores
+            bandwidth; `coherent` and `incoherent` give the same for each half
+            of the rays launched alone
+  cpu_baseline  the oracle (CPU restatement of the reference traversal, over
+            a tree built by the oracle's own SAH builder) on the host cores
   render, batch, adjoint, instanced, device_build
             the renderer legs (box scene, 64-scene batch, adjoint step,
             two-level scene with the general materials) and the device tree
             build against the host's SAH build, each described in its entry
 
---impl reference times that CPU implementation alone (the reference's own
-Swift/Mojo build cannot run here).  Multi-GPU (torchrun): every rank traces
+--impl reference times that CPU implementation alone over all rays per step
+(the reference's own Swift/Mojo build cannot run here); it builds its tree
+with the oracle, so libgzg.so is never loaded in that process.  Multi-GPU (torchrun): every rank traces
 its own full ray set against a replica of the scene (weak scaling, no
 collective on the data path).
 """
@@ -70,6 +72,40 @@ def workload(small, rank):
     o, d, t = scenes.raycast_rays(hs, cfg["width"], cfg["height"], cfg["incoherent"], seed=0xC1 + 7 * rank)
     name = "raycast_icosphere_%dtri_%dM_rays" % (hs.triangle_count, round(len(t) / 2 ** 20))
     return cfg, hs, o, d, t, name
+
+
+def oracle_workload(small):
+    """The same mesh, rays and SAH BVH2 built by the oracle alone (its own
+    triangle bounds and builder), for the CPU legs: libgzg.so is never loaded
+    for them.  The oracle's node array and prim order are byte-identical to
+    the library builder's (tests/test_host.py)."""
+    from types import SimpleNamespace
+
+    from gonzales_b200 import scenes
+    from gonzales_b200.scene import make_mesh
+    from oracle import pyoracle as O
+
+    cfg = SMALL if small else FULL
+    pts, tris = scenes.displaced_icosphere(cfg["subdiv"], seed=0xC1)
+    mesh = make_mesh(pts, tris)
+    nodes, order = O.build_bvh2(O.triangle_bounds(mesh.points, mesh.vertex_indices))
+    prims = np.zeros(len(order), O.PRIM_DTYPE)
+    prims["id1"] = order
+    prims["id2"] = order  # mesh 0 << 32 | triangle
+    prims["type"] = 1     # geometric primitive
+    hs = SimpleNamespace(meshes=[mesh], nodes=nodes, prims=prims, triangle_count=mesh.triangle_count)
+    o, d, t = scenes.raycast_rays(hs, cfg["width"], cfg["height"], cfg["incoherent"], seed=0xC1)
+    name = "raycast_icosphere_%dtri_%dM_rays" % (hs.triangle_count, round(len(t) / 2 ** 20))
+    return cfg, hs, o, d, t, name
+
+
+def workload_config(cfg, hs, name, world):
+    """The `config` object both arms print (the workload, not the method)."""
+    return {"workload": name, "triangles": int(hs.triangle_count), "rays": cfg["width"] * cfg["height"] +
+            cfg["incoherent"], "coherent_rays": cfg["width"] * cfg["height"], "incoherent_rays": cfg["incoherent"],
+            "query": "closest hit", "leaf_test": "moller_trumbore",
+            "l2": "inputs 512 MiB + outputs 256 MiB > L2, no flush",
+            "parallelism": "replica per GPU" if world > 1 else "single GPU"}
 
 
 def measured_hbm():
@@ -143,11 +179,14 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def cpu_baseline(hs, o, d, t, budget_s=20.0):
-    """The oracle traversal on all host threads; a strided sample of the
-    workload sized to roughly budget_s seconds of wall time."""
+def cpu_baseline(small, budget_s=20.0):
+    """The oracle traversal on all host threads over the oracle-built tree; a
+    strided sample of the workload sized to roughly budget_s seconds of wall
+    time."""
     from gonzales_b200 import scenes
     from oracle import pyoracle as O
+
+    _, hs, o, d, t, _ = oracle_workload(small)
 
     cores = os.cpu_count() or 1
     meshes = [(m.points, m.vertex_indices) for m in hs.meshes]
@@ -493,40 +532,39 @@ def dist_setup(args):
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path (the oracle: the
+    restated Mojo traversal, BVH2 + Moller-Trumbore) on all host threads,
+    over the full ray set each step.  Only rank 0 runs; the tree is built by
+    the oracle, so libgzg.so is not loaded."""
     world, rank, local = dist_setup(args)
     if rank != 0:
         return 0
     from gonzales_b200 import scenes
     from oracle import pyoracle as O
 
-    cfg, hs, o, d, t, name = workload(args.small, 0)
+    cfg, hs, o, d, t, name = oracle_workload(args.small)
     cores = os.cpu_count() or 1
     meshes = [(m.points, m.vertex_indices) for m in hs.meshes]
-    # A step traces a strided sample of 1/8 of the rays (coherent and
-    # incoherent in proportion) so K + W steps stay within minutes.
-    stride = 8
-    sel = np.arange(0, len(t), stride)
-    r6 = scenes.pack_reference_rays(o[sel], d[sel])
-    ts = t[sel]
+    r6 = scenes.pack_reference_rays(o, d)
     for _ in range(args.warmup):
-        O.traverse(hs.nodes, hs.prims, meshes, r6, ts, threads=cores)
+        O.traverse(hs.nodes, hs.prims, meshes, r6, t, threads=cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.traverse(hs.nodes, hs.prims, meshes, r6, ts, threads=cores)
+        O.traverse(hs.nodes, hs.prims, meshes, r6, t, threads=cores)
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    value = len(sel) * args.steps / total / 1e6
+    value = len(t) * args.steps / total / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": name, "rays": int(len(t)), "sample_rays_per_step": int(len(sel)),
-                   "triangles": hs.triangle_count},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural mesh and rays)",
+        "config": workload_config(cfg, hs, name, 1),
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
-                         "sample": "every 8th ray (%d rays) per step, closest hit, oracle BVH2 + Moller-Trumbore "
+                         "sample": "all %d rays per step, closest hit, oracle SAH BVH2 + Moller-Trumbore "
                                    "(CPU restatement of the reference traversal; the Swift/Mojo reference has no "
-                                   "toolchain here)" % len(sel)},
+                                   "toolchain here)" % len(t)},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -611,6 +649,29 @@ def run_ours(args):
     barrier()
     any_ms = a0.elapsed_time(a1) / args.steps
 
+    # each half alone (coherent camera rays, incoherent rays): its own
+    # instrumented replay, timed launches and roofline
+    nc = cfg["width"] * cfg["height"]
+    halves = {}
+    for label, sl in (("coherent", slice(0, nc)), ("incoherent", slice(nc, n))):
+        rh, hh = rays_d[sl], hits_d[sl]
+        cnt.zero_()
+        acc.trace_closest(rh, hh, options(fetch_counters=cnt.data_ptr()))
+        torch.cuda.synchronize()
+        h_nodes, h_tris, h_rays = [int(x) for x in cnt.cpu()]
+        for _ in range(args.warmup):
+            acc.trace_closest(rh, hh)
+        barrier()
+        hs_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                 for _ in range(args.steps)]
+        for e_start, e_end in hs_ev:
+            e_start.record(stream)
+            acc.trace_closest(rh, hh)
+            e_end.record(stream)
+        barrier()
+        halves[label] = dict(rays=h_rays, nodes=h_nodes, tris=h_tris,
+                             launch_s=statistics.mean(a.elapsed_time(b) for a, b in hs_ev) / 1000.0)
+
     # end to end through the drop-in C-ABI call, pinned host buffers
     rays_h = torch.from_numpy(scenes.pack_reference_rays(o, d)).pin_memory()
     tmax_h = torch.from_numpy(t).pin_memory()
@@ -646,27 +707,35 @@ def run_ours(args):
         prof = ROOT / "profiles" / "k_wide_closest_raycast.json"
         if prof.exists() and not args.small:
             traffic = json.loads(prof.read_text()).get("dram_bytes_per_full_launch")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                    "kernel": "k_wide_persistent (closest hit)",
+                    "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_per_launch / n,
+                    "tris_per_ray": tris_per_launch / n}
+        for label, hv in halves.items():
+            hb = hv["rays"] * 48 + hv["nodes"] * 80 + hv["tris"] * 48
+            ach = hb / hv["launch_s"] / 1e9
+            h_traffic = None
+            if prof.exists() and not args.small:
+                h_traffic = json.loads(prof.read_text()).get("dram_bytes_per_full_launch_" + label)
+            roofline[label] = {"rays": hv["rays"], "mrays_per_s": hv["rays"] / hv["launch_s"] / 1e6,
+                               "ms_per_launch": hv["launch_s"] * 1000.0, "achieved": ach, "frac": ach / peak,
+                               "traffic": h_traffic, "bytes_per_ray": hb / hv["rays"],
+                               "nodes_per_ray": hv["nodes"] / hv["rays"], "tris_per_ray": hv["tris"] / hv["rays"]}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
-            "config": {"workload": name, "triangles": hs.triangle_count, "rays": n, "coherent_rays":
-                       cfg["width"] * cfg["height"], "incoherent_rays": cfg["incoherent"], "traversal": "wide8",
-                       "leaf_test": "moller_trumbore", "l2": "inputs 512 MiB + outputs 256 MiB > L2, no flush",
-                       "parallelism": "replica per GPU" if world > 1 else "single GPU",
-                       "wide_nodes": info["wide_nodes"], "wide_depth": info["wide_depth"],
+            "config": workload_config(cfg, hs, name, world),
+            "method": {"traversal": "wide8", "wide_nodes": info["wide_nodes"], "wide_depth": info["wide_depth"],
                        "bvh2_nodes": info["bvh2_nodes"], "launch_closest": tuned_closest,
                        "launch_any": tuned_any},
             "any_hit_mrays_s": world * n / any_ms * 1000.0 / 1e6,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_wide_persistent (closest hit)",
-                         "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_per_launch / n,
-                         "tris_per_ray": tris_per_launch / n},
+            "roofline": roofline,
             "e2e": {"value": world * n / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": n * 28,
                     "d2h_bytes_per_step": n * 48, "call": "gzg_gpu_traverse_batch (pinned host Ray_C + tMax -> "
                                                          "Intersection_C)"},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps,  # closest-hit launches in the timed region of `value`
             "clocks": sampler.summary(),
         }
         if render is not None:
@@ -680,7 +749,7 @@ def run_ours(args):
         if build is not None:
             line["device_build"] = build
         if world == 1 and not args.skip_cpu:
-            line["cpu_baseline"] = cpu_baseline(hs, o, d, t)
+            line["cpu_baseline"] = cpu_baseline(args.small)
             if render is not None:
                 line["cpu_baseline"]["render_spp_per_s"] = cpu_render_baseline()
         print(json.dumps(line), flush=True)

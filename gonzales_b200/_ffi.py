@@ -182,6 +182,7 @@ PROTOTYPES = {
     "gzg_renderer_render_f64": (ST, [VP, VP, VP, VP, VP]),
     "gzg_renderer_adjoint": (ST, [VP, VP, VP, VP, VP, VP]),
     "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),
+    "gzg_camera_rays": (ST, [C.POINTER(RenderParams), I64, I64, VP, VP, VP]),
     "gzg_zsobol_fill_device": (ST, [I64, C.c_int32, C.c_int32, I64, VP, VP, VP, I64, VP, C.c_int32, VP, VP]),
     "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),
     "gzg_host_triangle_bounds": (ST, [VP, VP, I64, VP]),

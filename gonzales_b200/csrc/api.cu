@@ -178,6 +178,14 @@ struct gzg_scene {
         }
 };
 
+gzg_status gzg::kernel_fault(uint32_t w) {
+        std::string m = "kernel error word " + std::to_string(w) + ":";
+        if (w & kErrStackOverflow) m += " traversal stack overflow";
+        if (w & kErrStepCap) m += " step cap exceeded (cyclic or corrupt tree)";
+        if (w & kErrBadIndex) m += " index out of range";
+        return set_error(GZG_ERR_KERNEL_FAULT, m);
+}
+
 namespace {
 
 // Options fields left at 0 take the scene's tuned values (gzg_scene_autotune),
@@ -214,13 +222,6 @@ gzg_status read_error_word(gzg_scene *s, uint32_t *word, bool clear) {
         return GZG_OK;
 }
 
-gzg_status kernel_fault(uint32_t w) {
-        std::string m = "kernel error word 0x" + std::to_string(w) + ":";
-        if (w & kErrStackOverflow) m += " traversal stack overflow";
-        if (w & kErrStepCap) m += " step cap exceeded (cyclic or corrupt tree)";
-        if (w & kErrBadIndex) m += " index out of range";
-        return set_error(GZG_ERR_KERNEL_FAULT, m);
-}
 
 // Host batch: chunks of Ray_C + tMax through kSlots streams; results are
 // `out_bytes` per ray in format `out_fmt`.

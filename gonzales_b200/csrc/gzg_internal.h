@@ -15,6 +15,10 @@ namespace gzg {
 gzg_status set_error(gzg_status code, const std::string &msg);
 gzg_status clear_error();
 
+// GZG_ERR_KERNEL_FAULT with the bits of a nonzero device error word decoded
+// (stack overflow, step cap, index out of range) into the message.
+gzg_status kernel_fault(uint32_t word);
+
 // ------------------------------------------------------------------ layouts
 
 // Wide node: 8 children, 80 bytes, fetched as five 16-byte loads.

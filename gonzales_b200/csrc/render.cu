@@ -611,6 +611,45 @@ __device__ V3 env_radiance(const DevScene &s, V3 d) {
 
 // ------------------------------------------------------------ kernels
 
+// Camera sample and ray of one path: Tile.render phase 1 (Core/Tile.swift:
+// 27-59) with getCameraSample (Sampler/Sampler.swift:69-82), the Gaussian
+// filter sample and PerspectiveCamera.generateRay.  Leaves z after the camera
+// and lens dimensions; weight = filter value / filter pdf (Tile.swift:36-40).
+__device__ void camera_ray(const SceneConst &sc, uint32_t px, uint32_t py, uint32_t sample, ZSobol &z, V3 &org,
+                           V3 &dir, float &weight) {
+        zs_start(sc.zs, z, px, py, sample);
+        float u0, u1;
+        zs_get2d(sc.zs, z, u0, u1);
+        float dx, dy, denx, deny;
+        gaussian_sample_1d(u0, sc.filter_radius, sc.filter_sigma, dx, denx);
+        gaussian_sample_1d(u1, sc.filter_radius, sc.filter_sigma, dy, deny);
+        const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
+        float l0, l1;
+        zs_get2d(sc.zs, z, l0, l1);  // lens sample (drawn also by a pinhole)
+        // raster -> screen -> camera -> world
+        const float scx = sc.sx0 + fx / (float)sc.width * (sc.sx1 - sc.sx0);
+        const float scy = sc.sy1 - fy / (float)sc.height * (sc.sy1 - sc.sy0);
+        V3 dcam = normalize(v3(scx * sc.tan_half, scy * sc.tan_half, 1.0f));
+        org = sc.eye;
+        if (sc.lens_radius > 0.0f) {
+                // PerspectiveCamera.depthOfField (Camera/PerspectiveCamera.swift:25-35):
+                // the origin moves to the lens point; as written the new
+                // direction is taken from the pinhole origin, so it keeps the
+                // pinhole direction (renormalised after scaling to the focal plane)
+                float lx, ly;
+                concentric_disk(l0, l1, lx, ly);
+                lx = sc.lens_radius * lx;
+                ly = sc.lens_radius * ly;
+                const float ft = sc.focal_distance / dcam.z;
+                dcam = normalize(dcam * ft);
+                org = sc.eye + sc.right * lx + sc.up * ly;
+        }
+        dir = sc.right * dcam.x + sc.up * dcam.y + sc.fwd * dcam.z;
+        const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
+        const float fv = fmaxf(0.0f, gaussian(ddx, sc.filter_sigma)) * fmaxf(0.0f, gaussian(ddy, sc.filter_sigma));
+        weight = fv / (denx * deny);
+}
+
 // generate: Tile.render phase 1 (Core/Tile.swift:27-59).  Batch path p belongs
 // to the scene whose [path_begin, next path_begin) holds it; within the scene
 // path q is sample q % spp of pixel q / spp.
@@ -638,38 +677,9 @@ __global__ void k_generate(Wave w) {
         const uint32_t sample = (uint32_t)(q % (uint64_t)sc.spp) + (uint32_t)sc.first_sample;
         const uint32_t px = pixel % (uint32_t)sc.width, py = pixel / (uint32_t)sc.width;
         ZSobol z;
-        zs_start(sc.zs, z, px, py, sample);
-        // getCameraSample (Sampler/Sampler.swift:69-82)
-        float u0, u1;
-        zs_get2d(sc.zs, z, u0, u1);
-        float dx, dy, denx, deny;
-        gaussian_sample_1d(u0, sc.filter_radius, sc.filter_sigma, dx, denx);
-        gaussian_sample_1d(u1, sc.filter_radius, sc.filter_sigma, dy, deny);
-        const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
-        float l0, l1;
-        zs_get2d(sc.zs, z, l0, l1);  // lens sample (drawn also by a pinhole)
-        // raster -> screen -> camera -> world
-        const float scx = sc.sx0 + fx / (float)sc.width * (sc.sx1 - sc.sx0);
-        const float scy = sc.sy1 - fy / (float)sc.height * (sc.sy1 - sc.sy0);
-        V3 dcam = normalize(v3(scx * sc.tan_half, scy * sc.tan_half, 1.0f));
-        V3 org = sc.eye;
-        if (sc.lens_radius > 0.0f) {
-                // PerspectiveCamera.depthOfField (Camera/PerspectiveCamera.swift:25-35):
-                // the origin moves to the lens point; as written the new
-                // direction is taken from the pinhole origin, so it keeps the
-                // pinhole direction (renormalised after scaling to the focal plane)
-                float lx, ly;
-                concentric_disk(l0, l1, lx, ly);
-                lx = sc.lens_radius * lx;
-                ly = sc.lens_radius * ly;
-                const float ft = sc.focal_distance / dcam.z;
-                dcam = normalize(dcam * ft);
-                org = sc.eye + sc.right * lx + sc.up * ly;
-        }
-        const V3 dir = sc.right * dcam.x + sc.up * dcam.y + sc.fwd * dcam.z;
-        // rayWeight = filter value / filter pdf (Tile.swift:36-40)
-        const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
-        const float fv = fmaxf(0.0f, gaussian(ddx, sc.filter_sigma)) * fmaxf(0.0f, gaussian(ddy, sc.filter_sigma));
+        V3 org, dir;
+        float weight;
+        camera_ray(sc, px, py, sample, z, org, dir, weight);
         w.zs_morton[i] = z.morton;
         w.zs_dim[i] = z.dim;
         w.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -678,9 +688,34 @@ __global__ void k_generate(Wave w) {
         w.nrm[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         w.pixel[i] = sc.film_offset + pixel;
         w.scene[i] = (uint32_t)lo;
-        w.weight[i] = fv / (denx * deny);
+        w.weight[i] = weight;
         store_ray(w.q_ray[0], i, org, kInf, dir, sc.root);
         w.q_id[0][i] = i;
+}
+
+// Camera rays of paths [first, first + n) of one frame for host-driven bounce
+// loops: Ray_C records (origin, direction), ray weights and pixel indices.
+__global__ void k_camera_rays(SceneConst sc, uint64_t first, uint64_t n, float *rays6, float *weight,
+                              int32_t *pixel_out) {
+        const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n) return;
+        const uint64_t q = first + i;
+        const uint32_t pixel = (uint32_t)(q / (uint64_t)sc.spp);
+        const uint32_t sample = (uint32_t)(q % (uint64_t)sc.spp) + (uint32_t)sc.first_sample;
+        const uint32_t px = pixel % (uint32_t)sc.width, py = pixel / (uint32_t)sc.width;
+        ZSobol z;
+        V3 org, dir;
+        float w;
+        camera_ray(sc, px, py, sample, z, org, dir, w);
+        float *r = rays6 + 6 * i;
+        r[0] = org.x;
+        r[1] = org.y;
+        r[2] = org.z;
+        r[3] = dir.x;
+        r[4] = dir.y;
+        r[5] = dir.z;
+        weight[i] = w;
+        pixel_out[i] = (int32_t)pixel;
 }
 
 // Power light sampler over the scene's lights (area lights, then the
@@ -2200,6 +2235,45 @@ GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         k_zsobol_fill<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(c, px, py, index, n, kl, nkinds, per, out);
         st = cuda_err(cudaGetLastError(), "zsobol launch");
+        if (!st) clear_error();
+        return st;
+}
+
+GZG_API gzg_status gzg_camera_rays(const gzg_render_params *params, int64_t first_path, int64_t count, gzg_ray *rays,
+                                   float *weights, int32_t *pixels) {
+        if (!params || first_path < 0 || count < 0 || (count > 0 && (!rays || !weights || !pixels)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: null argument or negative range");
+        if (!params_ok(*params)) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: bad render parameters");
+        const int64_t total = (int64_t)params->width * params->height * params->spp;
+        if (first_path > total || count > total - first_path)
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: paths beyond width x height x spp");
+        if (count == 0) return clear_error();
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const uint32_t *matrices = nullptr;
+        gzg_status st = device_sobol(dev, &matrices);
+        if (st) return st;
+        const SceneConst sc = make_scene_const(*params, matrices);
+        const size_t bytes = (size_t)count * (6 * sizeof(float) + sizeof(float) + sizeof(int32_t));
+        char *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(GZG_ERR_OUT_OF_MEMORY, "gzg_camera_rays: device buffer");
+        }
+        float *d_rays = reinterpret_cast<float *>(d);
+        float *d_w = d_rays + 6 * count;
+        int32_t *d_px = reinterpret_cast<int32_t *>(d_w + count);
+        do {
+                k_camera_rays<<<(unsigned)((count + 127) / 128), 128>>>(sc, (uint64_t)first_path, (uint64_t)count,
+                                                                        d_rays, d_w, d_px);
+                if ((st = cuda_err(cudaGetLastError(), "camera ray launch"))) break;
+                if ((st = cuda_err(cudaMemcpy(rays, d_rays, (size_t)count * 24, cudaMemcpyDeviceToHost), "ray copy")))
+                        break;
+                if ((st = cuda_err(cudaMemcpy(weights, d_w, (size_t)count * 4, cudaMemcpyDeviceToHost), "weight copy")))
+                        break;
+                st = cuda_err(cudaMemcpy(pixels, d_px, (size_t)count * 4, cudaMemcpyDeviceToHost), "pixel copy");
+        } while (false);
+        cudaFree(d);
         if (!st) clear_error();
         return st;
 }

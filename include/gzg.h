@@ -237,9 +237,14 @@ GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays,
  * pinned-host allocation, and stages rays, tMax values and results through a
  * fixed array in the library's device image (a file-scope __device__ array of
  * 4,980,736 bytes, held on every GPU that loads the library until exit).
- * At most 65,536 rays per call (more: GZG_ERR_LIMIT).  The first call on a
- * device looks up that array's device address, so make it before any stream
- * capture.  Calls share the array and are serialised by a process-wide lock.
+ * At most 65,536 rays per call (more: GZG_ERR_LIMIT); two-level scenes are
+ * rejected (GZG_ERR_INVALID_ARGUMENT).  Every call looks up the array's device
+ * address afresh, launches with the scene's tuned closest-hit parameters on
+ * the calling thread's per-thread default stream (cudaStreamPerThread), waits
+ * for that stream, then reads and clears the scene's device error word (as
+ * gzg_gpu_traverse_batch does).  All calls share the one array, which keeps
+ * the last call's contents; calls are serialised by a process-wide lock, and
+ * nothing else may use the array (overlapping uses would race on it).
  * No counterpart in the reference: Gonzales' GPU batch call allocates device
  * buffers on every call. */
 GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, const gzg_ray *rays,
@@ -637,6 +642,18 @@ GZG_API gzg_status gzg_renderer_adjoint(gzg_renderer *renderer, const float *adj
 GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res_x, int32_t res_y, int64_t seed,
                                           const int32_t *px, const int32_t *py, const int64_t *index, int64_t n,
                                           const int32_t *kinds, int32_t nkinds, float *out, void *stream);
+
+/* Camera rays of Tile.render's first phase (Core/Tile.swift:27-59) for host
+ * callers that drive the bounce loop through gzg_gpu_traverse_batch and
+ * gzg_gpu_shade_batch themselves: for paths [first_path, first_path + count)
+ * of the frame described by params (path = pixel * spp + sample, pixel =
+ * y * width + x; samples first_sample + sample of the Z-Sobol sampler) writes
+ * the Ray_C record (camera-space sample through the Gaussian filter and the
+ * perspective camera, Sampler.getCameraSample + PerspectiveCamera.generateRay),
+ * the ray weight (filter value / filter pdf, Tile.swift:36-40) and the pixel
+ * index into HOST arrays.  Computed on the current device; synchronous. */
+GZG_API gzg_status gzg_camera_rays(const gzg_render_params *params, int64_t first_path, int64_t count,
+                                   gzg_ray *rays, float *weights, int32_t *pixels);
 
 /* Convenience: renders into HOST films (overwritten); synchronous. */
 GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *params, float *film_rgb,
