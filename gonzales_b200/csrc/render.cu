@@ -293,6 +293,7 @@ struct SceneConst {
         float env_power;
         float film_scale;                  // Film.add: iso / 100
         float max_component;               // clamp of a sample's largest component (0: none)
+        int32_t two_sided;                 // area lights emit on both sides (the live shade step's rule)
         int32_t material_begin;  // the scene's material 0 (area-light hits scatter with it)
         int32_t material_count;
         uint32_t root;            // wide-node root of the scene's tree
@@ -852,7 +853,7 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                         const V3 inc = normalize(target - pos);
                         const V3 dl = pos - target;
                         const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
-                        if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
+                        if ((sc.two_sided || dot(ln, neg(inc)) > 0.0f) && !isinf(pdf)) {
                                 rad = v3(le4) * w.emission_scale;
                                 light_dir = inc;
                                 light_pdf = pdf;
@@ -1016,7 +1017,7 @@ __global__ void __launch_bounds__(128, kKind == kShadeSplit                     
         V3 L = v3(w.L[path]);
         if ((bounce == 0 || after_specular) && is_light && mat_index >= 0 && mat_index < s.material_count) {
                 const V3 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
-                if (dot(ng, wo) > 0.0f) L = L + mulv(thr, le);
+                if (sc.two_sided || dot(ng, wo) > 0.0f) L = L + mulv(thr, le);
         }
         // Area-light hits scatter with the scene's material 0 (their interaction
         // keeps materialIndex 0, Core/SurfaceInteraction.swift:20).
@@ -1118,7 +1119,7 @@ __global__ void __launch_bounds__(128, kKind == kShadeSplit                     
                         const V3 inc = normalize(target - pos);
                         const V3 dl = pos - target;
                         const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
-                        if (dot(ln, neg(inc)) > 0.0f && !isinf(pdf)) {
+                        if ((sc.two_sided || dot(ln, neg(inc)) > 0.0f) && !isinf(pdf)) {
                                 const bool reflect = dot(inc, ng) * dot(wo, ng) > 0.0f;
                                 const V3 f = reflect ? f_val : v3(0, 0, 0);
                                 light_est = mulv(f * fabsf(dot(inc, sf.ns)), le);
@@ -1256,7 +1257,7 @@ __global__ void k_probe_resolve(Wave w, DevScene s, int any_only) {
                 int64_t mat_index;
                 prim_info(s, sf.gprim, type, mat_index);
                 if (type != 3 || mat_index < 0 || mat_index >= s.material_count) return;
-                if (!(dot(sf.ng, neg(wi)) > 0.0f)) return;
+                if (!w.scenes[w.scene[w.pr_id[i]]].two_sided && !(dot(sf.ng, neg(wi)) > 0.0f)) return;
                 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
         }
         const uint32_t path = w.pr_id[i];
@@ -1499,6 +1500,7 @@ SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices
         sc.max_component = 0.0f;
         sc.lens_radius = P.lens_radius;
         sc.focal_distance = P.focal_distance;
+        sc.two_sided = P.two_sided_emission != 0;
         return sc;
 }
 

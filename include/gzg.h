@@ -514,6 +514,10 @@ typedef struct gzg_render_params {
         int32_t use_graph;       /* capture one wave as a CUDA graph and replay it */
         float lens_radius;       /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
         float focal_distance;    /* distance of the plane in focus (reference default 1e6) */
+        int32_t two_sided_emission; /* 0: area lights emit on the side their geometric normal faces
+                                       (AreaLight.emittedRadiance, Light/AreaLight.swift:13-19);
+                                       1: on both sides, as the live shading step counts any hit
+                                       on an emitter (shade_core, kernel.mojo:696-701) */
 } gzg_render_params;
 
 typedef struct gzg_renderer gzg_renderer;

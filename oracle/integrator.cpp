@@ -565,7 +565,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                 const V3 inc = normalize(sub(lp, pos));
                 const V3 dl = sub(pos, lp);
                 const float pdf = (1.0f / lt.area) * (dot(dl, dl) / std::fabs(dot(ln, neg(inc))));
-                if (dot(ln, neg(inc)) > 0.0f && !std::isinf(pdf)) {
+                if ((P.two_sided_emission || dot(ln, neg(inc)) > 0.0f) && !std::isinf(pdf)) {
                         const V3 so = add(pos, mul(sub(lp, pos), 0.0001f));
                         Hit sh = trace(sc, so, sub(lp, so), 1.0f - 0.00001f);
                         ++res.shadow;
@@ -597,7 +597,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         if (ph.hit) {
                                 if (interaction(sc, ph, wi, &pi) && pi.pr->type == 3) {
                                         const orc_material &lm = pi.mats[pi.pr->material_index];
-                                        if (dot(pi.ng, neg(wi)) > 0.0f)
+                                        if (P.two_sided_emission || dot(pi.ng, neg(wi)) > 0.0f)
                                                 radiance = emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]));
                                 }
                         } else if (sc.env) {
@@ -669,7 +669,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                 const bool is_light = pr.type == 3;
                 if ((bounce == 0 || specular) && is_light) {
                         const orc_material &lm = is.mats[pr.material_index];
-                        if (dot(ng, wo) > 0.0f)
+                        if (P.two_sided_emission || dot(ng, wo) > 0.0f)
                                 L = add(L, mulv(thr, emitted(sc, v3(lm.emission[0], lm.emission[1], lm.emission[2]))));
                 }
                 // Area lights have materialIndex 0 in their interaction
@@ -767,7 +767,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                         const float angle = std::fabs(dot(ln, neg(inc)));
                         pdf = pdf * (d2 / angle);
                         const V3 dir = inc;
-                        const bool lit = dot(ln, neg(dir)) > 0.0f;
+                        const bool lit = P.two_sided_emission || dot(ln, neg(dir)) > 0.0f;
                         if (lit && !std::isinf(pdf)) {
                                 // Visibility.occluded: spawnRay(from:target:) (Interaction.swift:15-24)
                                 const V3 so = add(pos, mul(sub(lp, pos), 0.0001f));
@@ -814,7 +814,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                 if (ph.hit) {
                                         if (interaction(sc, ph, wi, &pi) && pi.pr->type == 3) {
                                                 const orc_material &lm = pi.mats[pi.pr->material_index];
-                                                if (dot(pi.ng, neg(wi)) > 0.0f)
+                                                if (P.two_sided_emission || dot(pi.ng, neg(wi)) > 0.0f)
                                                         radiance = emitted(sc, v3(lm.emission[0], lm.emission[1],
                                                                                   lm.emission[2]));
                                         }
@@ -865,6 +865,68 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
         res.L = L;
         return res;
 }
+
+// The camera of a frame and one path's camera ray: Tile.render phase 1
+// (Core/Tile.swift:27-59) with Sampler.getCameraSample (Sampler/Sampler.swift:
+// 69-82), GaussianFilter.sample and PerspectiveCamera.generateRay; the basis
+// is right-handed (+x right, +y up in the image).
+struct Camera {
+        const orc_render_params &P;
+        V3 eye, fwd, right, upv;
+        float tan_half, sx0, sx1, sy0, sy1;
+        int sampler_spp;
+        explicit Camera(const orc_render_params &p) : P(p) {
+                eye = v3(P.eye[0], P.eye[1], P.eye[2]);
+                fwd = normalize(sub(v3(P.target[0], P.target[1], P.target[2]), eye));
+                right = normalize(cross(fwd, v3(P.up[0], P.up[1], P.up[2])));
+                upv = cross(right, fwd);
+                tan_half = std::tan(P.fov_deg * kPi / 180.0f / 2.0f);
+                const float aspect = (float)P.width / (float)P.height;
+                sx0 = aspect > 1.0f ? -aspect : -1.0f;
+                sx1 = -sx0;
+                sy0 = aspect > 1.0f ? -1.0f : -1.0f / aspect;
+                sy1 = -sy0;
+                sampler_spp = P.sampler_spp > 0 ? P.sampler_spp : P.spp;
+        }
+        // Starts *smp at sample `sample` of pixel (px, py) and draws the
+        // camera and lens dimensions; w = filter value / filter pdf
+        // (Tile.swift:36-40).
+        void ray(int px, int py, int sample, orc_zsobol *smp, V3 *org_out, V3 *dir_out, float *w_out) const {
+                const int W = P.width, H = P.height;
+                orc_zsobol_init(smp, sampler_spp, W, H, P.seed);
+                orc_zsobol_start_pixel_sample(smp, px, py, sample, 0);
+                float u2[2];
+                orc_zsobol_get2d(smp, u2);
+                float dx, dy, denx, deny;
+                gaussian_sample_1d(u2[0], P.filter_radius, P.filter_sigma, &dx, &denx);
+                gaussian_sample_1d(u2[1], P.filter_radius, P.filter_sigma, &dy, &deny);
+                const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
+                float lens[2];
+                orc_zsobol_get2d(smp, lens);
+                const float scx = sx0 + fx / (float)W * (sx1 - sx0);
+                const float scy = sy1 - fy / (float)H * (sy1 - sy0);
+                V3 dcam = normalize(v3(scx * tan_half, scy * tan_half, 1.0f));
+                V3 org = eye;
+                if (P.lens_radius > 0.0f) {
+                        // PerspectiveCamera.depthOfField (Camera/PerspectiveCamera.swift:25-35):
+                        // origin on the lens, direction from the pinhole origin to the
+                        // focal point (the pinhole direction, renormalised)
+                        float lx, ly;
+                        concentric_disk(lens[0], lens[1], &lx, &ly);
+                        lx = P.lens_radius * lx;
+                        ly = P.lens_radius * ly;
+                        const float ft = P.focal_distance / dcam.z;
+                        dcam = normalize(mul(dcam, ft));
+                        org = add(add(eye, mul(right, lx)), mul(upv, ly));
+                }
+                *dir_out = add(add(mul(right, dcam.x), mul(upv, dcam.y)), mul(fwd, dcam.z));
+                *org_out = org;
+                const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
+                const float fv = std::max(0.0f, gaussian(ddx, P.filter_sigma)) *
+                                 std::max(0.0f, gaussian(ddy, P.filter_sigma));
+                *w_out = fv / (denx * deny);
+        }
+};
 
 }  // namespace
 
@@ -921,16 +983,7 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
         const orc_render_params &P = *params;
         const float film_scale = (P.iso > 0.0f ? P.iso : 100.0f) / 100.0f;
         const int W = P.width, H = P.height;
-        const int sampler_spp = P.sampler_spp > 0 ? P.sampler_spp : P.spp;
-        // camera basis (right-handed: +x right, +y up in the image)
-        const V3 eye = v3(P.eye[0], P.eye[1], P.eye[2]);
-        const V3 fwd = normalize(sub(v3(P.target[0], P.target[1], P.target[2]), eye));
-        const V3 right = normalize(cross(fwd, v3(P.up[0], P.up[1], P.up[2])));
-        const V3 upv = cross(right, fwd);
-        const float tan_half = std::tan(P.fov_deg * kPi / 180.0f / 2.0f);
-        const float aspect = (float)W / (float)H;
-        const float sx0 = aspect > 1.0f ? -aspect : -1.0f, sx1 = -sx0;
-        const float sy0 = aspect > 1.0f ? -1.0f : -1.0f / aspect, sy1 = -sy0;
+        const Camera cam(P);
         if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
         std::atomic<int> next_row{0};
         std::vector<uint64_t> cnt(4 * threads, 0);
@@ -945,38 +998,9 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                         float acca[3] = {0, 0, 0}, accn[3] = {0, 0, 0};
                                         for (int si = 0; si < P.spp; ++si) {
                                                 orc_zsobol smp;
-                                                orc_zsobol_init(&smp, sampler_spp, W, H, P.seed);
-                                                orc_zsobol_start_pixel_sample(&smp, px, py, P.first_sample + si, 0);
-                                                float u2[2];
-                                                orc_zsobol_get2d(&smp, u2);
-                                                float dx, dy, denx, deny;
-                                                gaussian_sample_1d(u2[0], P.filter_radius, P.filter_sigma, &dx, &denx);
-                                                gaussian_sample_1d(u2[1], P.filter_radius, P.filter_sigma, &dy, &deny);
-                                                const float fx = (float)px + 0.5f + dx, fy = (float)py + 0.5f + dy;
-                                                float lens[2];
-                                                orc_zsobol_get2d(&smp, lens);
-                                                const float scx = sx0 + fx / (float)W * (sx1 - sx0);
-                                                const float scy = sy1 - fy / (float)H * (sy1 - sy0);
-                                                V3 dcam = normalize(v3(scx * tan_half, scy * tan_half, 1.0f));
-                                                V3 org = eye;
-                                                if (P.lens_radius > 0.0f) {
-                                                        // PerspectiveCamera.depthOfField
-                                                        // (Camera/PerspectiveCamera.swift:25-35): origin on
-                                                        // the lens, direction from the pinhole origin to the
-                                                        // focal point (the pinhole direction, renormalised)
-                                                        float lx, ly;
-                                                        concentric_disk(lens[0], lens[1], &lx, &ly);
-                                                        lx = P.lens_radius * lx;
-                                                        ly = P.lens_radius * ly;
-                                                        const float ft = P.focal_distance / dcam.z;
-                                                        dcam = normalize(mul(dcam, ft));
-                                                        org = add(add(eye, mul(right, lx)), mul(upv, ly));
-                                                }
-                                                const V3 dir = add(add(mul(right, dcam.x), mul(upv, dcam.y)), mul(fwd, dcam.z));
-                                                const float ddx = fx - ((float)px + 0.5f), ddy = fy - ((float)py + 0.5f);
-                                                const float fv = std::max(0.0f, gaussian(ddx, P.filter_sigma)) *
-                                                                 std::max(0.0f, gaussian(ddy, P.filter_sigma));
-                                                const float w = fv / (denx * deny);
+                                                V3 org, dir;
+                                                float w;
+                                                cam.ray(px, py, P.first_sample + si, &smp, &org, &dir, &w);
                                                 PathResult pr = trace_path(sc, &smp, org, dir);
                                                 cnt[4 * ti + 0] += 1;
                                                 cnt[4 * ti + 1] += pr.ext;
@@ -1073,4 +1097,29 @@ extern "C" float orc_gaussian(float x, float sigma) { return gaussian(x, sigma);
 
 extern "C" void orc_gaussian_sample_1d(float u, float radius, float sigma, float *x, float *density) {
         gaussian_sample_1d(u, radius, sigma, x, density);
+}
+
+// Camera rays of paths [first, first + count) of a frame (path = pixel * spp
+// + sample, pixel = y * width + x): Ray_C records, ray weights and pixels.
+extern "C" void orc_camera_rays(const orc_render_params *params, int64_t first, int64_t count, float *rays6,
+                                float *weights, int32_t *pixels) {
+        const Camera cam(*params);
+        for (int64_t i = 0; i < count; ++i) {
+                const int64_t q = first + i;
+                const int64_t pixel = q / params->spp;
+                const int sample = (int)(q % params->spp) + params->first_sample;
+                orc_zsobol smp;
+                V3 org, dir;
+                float w;
+                cam.ray((int)(pixel % params->width), (int)(pixel / params->width), sample, &smp, &org, &dir, &w);
+                float *r = rays6 + 6 * i;
+                r[0] = org.x;
+                r[1] = org.y;
+                r[2] = org.z;
+                r[3] = dir.x;
+                r[4] = dir.y;
+                r[5] = dir.z;
+                weights[i] = w;
+                pixels[i] = (int32_t)pixel;
+        }
 }

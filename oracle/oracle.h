@@ -105,6 +105,7 @@ typedef struct orc_render_params {
         float max_component;    /* clamp of a sample's largest component (0: none) */
         float lens_radius;      /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
         float focal_distance;
+        int32_t two_sided_emission; /* 1: area lights emit on both sides (the live shade_core's rule) */
 } orc_render_params;
 
 /* Renders the scene; per pixel (row-major) accumulates the film sums of the
@@ -115,6 +116,13 @@ void orc_render(const orc_node *nodes, const orc_prim_id *prims, const orc_mesh 
                 const orc_material *materials, int64_t n_materials, int64_t n_prims,
                 const orc_render_params *params, float *sum_rgb, float *sum_sq, float *sum_w,
                 uint64_t *counters, int threads);
+
+/* Camera rays of paths [first, first + count) of the frame in params (path =
+ * pixel * spp + sample, pixel = y * width + x): Ray_C records (6 floats),
+ * ray weights (filter value / filter pdf) and pixel indices.  Tile.render
+ * phase 1 (Core/Tile.swift:27-59). */
+void orc_camera_rays(const orc_render_params *params, int64_t first, int64_t count, float *rays6, float *weights,
+                     int32_t *pixels);
 
 /* Albedo textures and an emission scale for the differentiable renderer's
  * scene: material m with material_texture[m] = t >= 0 takes its albedo from

@@ -210,16 +210,17 @@ class RenderParams(C.Structure):
                 ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
                 ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
                 ("sampler_spp", C.c_int32), ("iso", C.c_float), ("max_component", C.c_float),
-                ("lens_radius", C.c_float), ("focal_distance", C.c_float)]
+                ("lens_radius", C.c_float), ("focal_distance", C.c_float), ("two_sided_emission", C.c_int32)]
 
 
 def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
                   eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
                   filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, iso=100.0, max_component=0.0,
-                  lens_radius=0.0, focal_distance=1e6):
+                  lens_radius=0.0, focal_distance=1e6, two_sided_emission=0):
     return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
                         (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
-                        first_sample, sampler_spp, iso, max_component, lens_radius, focal_distance)
+                        first_sample, sampler_spp, iso, max_component, lens_radius, focal_distance,
+                        two_sided_emission)
 
 
 class _Textures(C.Structure):
@@ -387,6 +388,21 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
 PATH_DTYPE = np.dtype({"names": ["ray", "throughput", "estimate", "albedo", "pcg_state", "pcg_inc", "active"],
                        "formats": [("<f4", 6), ("<f4", 3), ("<f4", 3), ("<f4", 3), "<u8", "<u8", "i1"],
                        "offsets": [0, 24, 36, 48, 64, 72, 80], "itemsize": 88})
+
+
+def camera_rays(params, first, count):
+    """Camera rays of paths [first, first + count): (rays6 (n, 6) float32,
+    weights (n,) float32, pixels (n,) int32)."""
+    L = lib()
+    if not getattr(L, "_camera_bound", False):
+        L.orc_camera_rays.restype = None
+        L.orc_camera_rays.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L._camera_bound = True
+    rays = np.zeros((count, 6), np.float32)
+    w = np.zeros(count, np.float32)
+    px = np.zeros(count, np.int32)
+    L.orc_camera_rays(C.addressof(params), first, count, _p(rays), _p(w), _p(px))
+    return rays, w, px
 
 
 def shade_batch(hs, paths, isects):

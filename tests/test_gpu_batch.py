@@ -119,3 +119,52 @@ def test_batch_rejects_bad_arguments(batch):
     bad = F.render_params(width=0, height=8, spp=1)
     with pytest.raises(GzgError):
         BatchRenderer(accs[:1], [bad])
+
+
+def test_batch_configuration_subset_matches_oracle():
+    """Four scenes of the scene-batch configuration itself (the first of each
+    image side in the seeded 64-scene workload: 64^2, 128^2, 256^2 and 512^2,
+    972 to 50,398 triangles) at its parameters (32 spp, depth 6, roulette from
+    bounce 2), rendered in one batch and compared per pixel with the oracle's
+    renders of the same scenes at equal Z-Sobol samples."""
+    from oracle import pyoracle as O
+    from tests import helpers
+
+    torch = torch_mod()
+    work = scenes.batch_workload(64, 0xC3)
+    picks = {}
+    for k, (_, side) in enumerate(work):
+        picks.setdefault(side, k)
+    chosen = [picks[s] for s in sorted(picks)]
+    hosts = [work[k][0].build() for k in chosen]
+    accs = [GpuAccelerator(h) for h in hosts]
+    kw = [dict(width=work[k][1], height=work[k][1], spp=32, max_depth=6, rr_min_bounce=2) for k in chosen]
+    params = [F.render_params(**p) for p in kw]
+    record = []
+    try:
+        with BatchRenderer(accs, params, use_graph=1) as r:
+            rgb = torch.zeros((r.pixels, 3), device="cuda")
+            sq = torch.zeros((r.pixels, 3), device="cuda")
+            w = torch.zeros((r.pixels,), device="cuda")
+            r.render(rgb, w, sq)
+            torch.cuda.synchronize()
+            assert r.error_word() == 0
+            parts = list(zip(r.split(rgb.cpu().numpy()), r.split(sq.cpu().numpy()), r.split(w.cpu().numpy())))
+        for hs, p, (g_rgb, g_sq, g_w) in zip(hosts, kw, parts):
+            o_rgb, o_sq, o_w, _ = O.render(hs, O.render_params(**p))
+            n = p["spp"]
+            side = p["width"]
+            g_rgb, g_sq, g_w = (a.reshape(o.shape) for a, o in ((g_rgb, o_rgb), (g_sq, o_sq), (g_w, o_w)))
+            gm, om = g_rgb / n, o_rgb / n
+            gse = np.sqrt(np.maximum(g_sq / n - gm * gm, 0.0) / n)
+            ose = np.sqrt(np.maximum(o_sq / n - om * om, 0.0) / n)
+            within = float((np.abs(gm - om) <= 3.0 * np.sqrt(gse ** 2 + ose ** 2) + 1e-4).mean())
+            record.append({"side": side, "triangles": hs.triangle_count, "within_3se": within})
+            np.testing.assert_allclose(g_w, o_w, rtol=1e-4)
+            assert within >= 0.997, record[-1]
+            np.testing.assert_allclose(g_rgb.sum(axis=(0, 1)) / g_w.sum(), o_rgb.sum(axis=(0, 1)) / o_w.sum(),
+                                       rtol=1e-2)
+    finally:
+        helpers.record("batch_subset_vs_oracle.json", record)
+        for a in accs:
+            a.close()

@@ -1,0 +1,119 @@
+"""The GPU path against the reference's own golden render.
+
+The scene and image are the reference's render regression test
+(Tests/reference/regression-test.pbrt / .exr, committed as
+tests/golden/regression_test.npz; the reference accepts a normalised RMSE
+below 0.1, Tests/libgonzalesTests/RenderRegressionTests.swift:40-62).  The
+golden image was denoised by Open Image Denoise (Film.writeImages always runs
+it, Core/Film.swift:40-58), so a raw render meets the bound once its own noise
+is small; the RMSE at the scene's own 64 samples per pixel is recorded beside
+the asserted one.
+
+Two loops are checked:
+  - the loop that actually runs in the reference (Core/Tile.swift:19-223):
+    gzg_camera_rays, then up to maxDepth + 1 rounds of gzg_gpu_traverse_batch
+    and gzg_gpu_shade_batch through the C ABI (gonzales_b200.tile);
+  - the wavefront MIS renderer (gzg_render_image) with corrected MIS, no
+    roulette and two-sided emission, an estimator of the same image with
+    next-event estimation.
+"""
+import numpy as np
+import pytest
+
+from gonzales_b200 import GpuAccelerator, tile
+from gonzales_b200 import _ffi as F
+from oracle import pyoracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def regression():
+    z = H.regression_fixture()
+    sb, kw = H.regression_scene(z)
+    hs = sb.build()
+    acc = GpuAccelerator(hs)
+    yield z, hs, kw, acc
+    acc.close()
+
+
+def test_camera_rays_match_oracle(regression):
+    z, hs, kw, acc = regression
+    n = kw["width"] * kw["height"] * kw["spp"]
+    rays, w, px = tile.camera_rays(F.render_params(**kw), 0, n)
+    ro, wo, pxo = O.camera_rays(O.render_params(**kw), 0, n)
+    assert np.array_equal(px, pxo)
+    # origins are the pinhole itself; directions are unit vectors, equal to
+    # about an ulp (the Gaussian filter sample and weight call expf / erff /
+    # sqrtf, library functions on each side)
+    assert np.array_equal(rays[:, :3], ro[:, :3])
+    assert np.abs(rays[:, 3:] - ro[:, 3:]).max() < 1e-6
+    assert np.abs(w / wo - 1.0).max() < 1e-5
+    H.record("camera_rays_vs_oracle.json", {"rays": int(n), "bit_identical": float((rays == ro).all(axis=1).mean()),
+                                            "max_dir_abs_diff": float(np.abs(rays[:, 3:] - ro[:, 3:]).max())})
+    # a window in the middle of the frame
+    first = 1000 * kw["spp"] + 17
+    r2, w2, p2 = tile.camera_rays(F.render_params(**kw), first, 333)
+    assert np.array_equal(r2, rays[first:first + 333]) and np.array_equal(p2, px[first:first + 333])
+
+
+def test_live_tile_loop_matches_reference_golden_render(regression):
+    z, hs, kw, acc = regression
+    golden = z["golden"][..., :3]
+    out = {}
+    for spp in (64, 1024):
+        light, weight, traced = tile.render_tile_loop(acc, F.render_params(**dict(kw, spp=spp)), seed=spp)
+        img = tile.normalized(light, weight)
+        out[spp] = {"normalised_rmse": H.normalised_rmse(img, golden), "mean": img.mean((0, 1)).tolist(),
+                    "rays_per_bounce": traced.tolist()}
+    out["golden_mean"] = golden.mean((0, 1)).tolist()
+    H.record("regression_live_loop.json", out)
+    assert acc.error_word() == 0
+    assert out[1024]["normalised_rmse"] < 0.1, out
+    assert out[1024]["normalised_rmse"] < out[64]["normalised_rmse"], out
+    mean, gmean = np.array(out[1024]["mean"]), np.array(out["golden_mean"])
+    assert np.all(np.abs(mean / gmean - 1.0) < 0.02), (mean, gmean)
+    # every camera ray is traced; paths end at the light or a miss
+    assert out[64]["rays_per_bounce"][0] == kw["width"] * kw["height"] * 64
+
+
+def test_mis_renderer_matches_reference_golden_render(regression):
+    """The MIS renderer with two-sided emission: the live shading step adds an
+    emitter's radiance on any hit (kernel.mojo:696-701) while the MIS
+    integrator's AreaLight emits on one side only (Light/AreaLight.swift:
+    13-19).  This scene's light hangs 0.02 below the ceiling, and its back
+    face lights the ceiling in the reference's render, so only the two-sided
+    rule renders the same scene.  (One-sided, the image is 16 % darker; the
+    remaining difference is the MIS loop letting area-light hits scatter with
+    material 0, Core/SurfaceInteraction.swift:20, where the live loop stops.)
+    The device render is checked against the oracle's in the same mode."""
+    z, hs, kw, acc = regression
+    golden = z["golden"][..., :3]
+    out = {}
+    for two_sided, spp in ((1, 64), (1, 1024), (0, 1024)):
+        p = F.render_params(**dict(kw, spp=spp), mis_corrected=1, rr_min_bounce=kw["max_depth"] + 1,
+                            two_sided_emission=two_sided)
+        rgb, sq, w, stats = acc.render(p)
+        img = tile.normalized(rgb.astype(np.float64), w.astype(np.float64))
+        out["%s_%d" % ("two_sided" if two_sided else "one_sided", spp)] = {
+            "normalised_rmse": H.normalised_rmse(img, golden), "mean": img.mean((0, 1)).tolist()}
+        if spp == 64:
+            po = O.render_params(**dict(kw, spp=spp), mis_corrected=1, rr_min_bounce=kw["max_depth"] + 1,
+                                 two_sided_emission=two_sided)
+            o_rgb, o_sq, o_w, _ = O.render(hs, po)
+            # per pixel, the sample means agree within 3 combined standard
+            # errors (the two draw the same Z-Sobol samples; paths part only
+            # after an ulp difference in a library function)
+            gm, om = rgb / spp, o_rgb / spp
+            gse = np.sqrt(np.maximum(sq / spp - gm * gm, 0.0) / spp)
+            ose = np.sqrt(np.maximum(o_sq / spp - om * om, 0.0) / spp)
+            within = np.abs(gm - om) <= 3.0 * np.sqrt(gse ** 2 + ose ** 2) + 1e-4
+            out["device_vs_oracle_within_3se"] = float(within.mean())
+            np.testing.assert_allclose(w, o_w, rtol=1e-4)
+            assert within.mean() >= 0.997, out
+    out["golden_mean"] = golden.mean((0, 1)).tolist()
+    H.record("regression_mis_renderer.json", out)
+    assert acc.error_word() == 0
+    assert out["two_sided_1024"]["normalised_rmse"] < 0.1, out
+    assert out["one_sided_1024"]["normalised_rmse"] > out["two_sided_1024"]["normalised_rmse"], out
