@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--small", action="store_true", help="small case for profiler captures")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-batch", action="store_true", help="omit the scene-batch and adjoint legs")
-    ap.add_argument("--case", default=None, choices=["instanced-small", "build"],
+    ap.add_argument("--case", default=None, choices=["instanced-small", "build", "incoherent", "coherent"],
                     help="run one small case alone (profiler captures) and print its own JSON line")
     return ap.parse_args()
 
@@ -377,13 +377,19 @@ def batch_leg(args, stream, barrier):
             "error_word": err}
 
 
+INSTANCED_MEDIUM = dict(box_min=(-10.0, -6.0, -10.0), box_max=(10.0, 6.0, 10.0), sigma_a=(0.05, 0.05, 0.05),
+                        sigma_s=(0.2, 0.2, 0.2), g=0.0)
+
+
 def instanced_leg(args, stream, barrier):
     """The two-level scene lit by an environment map: 16 displaced tubes and
     spheres of 50,000 triangles each, 4096 instances under seeded affine
     transforms, a 1024 x 512 sky map with a sun lobe, materials mixed per
     mesh (diffuse, coated diffuse, dielectric, conductor, coated conductor;
-    roughness uniform in [0.05, 0.5]), 1920 x 1080, 64 spp, depth 8 (MIS as
-    written; roulette from bounce 2).  One frame per step through a graph-captured renderer."""
+    roughness uniform in [0.05, 0.5]), one homogeneous medium box (sigma_a
+    0.05, sigma_s 0.2, isotropic) around the middle of the instance field,
+    1920 x 1080, 64 spp, depth 8 (MIS as written; roulette from bounce 2).
+    One frame per step through a graph-captured renderer."""
     import torch
 
     from gonzales_b200 import GpuAccelerator, InstancedAccelerator, Renderer, scenes
@@ -394,6 +400,7 @@ def instanced_leg(args, stream, barrier):
     blas = [GpuAccelerator(h) for h in blas_hosts]
     acc = InstancedAccelerator(blas, inst)
     acc.set_environment(scenes.sky_map(), 1.0)
+    acc.set_medium(INSTANCED_MEDIUM)
     setup_s = time.perf_counter() - t0
     W, H, spp = 1920, 1080, 64
     p = F.render_params(W, H, spp, max_depth=8, rr_min_bounce=2, eye=(0.0, 6.0, 48.0), target=(0.0, 0.0, 0.0),
@@ -421,11 +428,10 @@ def instanced_leg(args, stream, barrier):
     rays = sum(s1[k] - s0[k] for k in ("camera_rays", "extension_rays", "shadow_rays", "probe_rays")) / steps
     return {"config": "16 x 50k-triangle meshes, 4096 instances, sky map 1024x512 + sun lobe, diffuse / "
                       "coated diffuse / dielectric / conductor / coated conductor meshes (roughness "
-                      "U[0.05,0.5]), %dx%d, %d spp, depth 8, roulette from bounce 2" % (W, H, spp),
+                      "U[0.05,0.5]), homogeneous medium box [-10,10]x[-6,6]x[-10,10] sigma_a 0.05 sigma_s 0.2, "
+                      "%dx%d, %d spp, depth 8, roulette from bounce 2" % (W, H, spp),
             "spp_per_s": W * H * spp / ms * 1000.0, "ms_per_frame": ms, "mrays_per_s": rays / ms / 1000.0,
-            "rays_per_frame": rays, "steps": steps, "setup_s": setup_s, "error_word": err,
-            "not_built": "the homogeneous medium box (never sampled by the reference's integrator, whose "
-                         "interface material throws)"}
+            "rays_per_frame": rays, "steps": steps, "setup_s": setup_s, "error_word": err}
 
 
 def build_leg(hs, rays_d, args, stream, barrier):
@@ -800,7 +806,11 @@ def run_case(args):
     """Small single cases for profiler captures (one GPU):
       instanced-small  one 640 x 360, 16-spp frame of the two-level scene with
                        the general materials (after one warm-up frame)
-      build            the device tree build of the ray-cast mesh (three builds)"""
+      build            the device tree build of the ray-cast mesh (three builds)
+      incoherent       the ray-cast mesh's 8,388,608 incoherent rays alone:
+      coherent         or its 8,388,608 coherent rays alone; tuned launch,
+                       two warm-up closest-hit launches, then three timed ones
+                       (384 MiB of rays and hits on the device)"""
     import torch
 
     from gonzales_b200 import GpuAccelerator, InstancedAccelerator, Renderer, scenes
@@ -812,6 +822,7 @@ def run_case(args):
         blas = [GpuAccelerator(h) for h in blas_hosts]
         acc = InstancedAccelerator(blas, inst)
         acc.set_environment(scenes.sky_map(), 1.0)
+        acc.set_medium(INSTANCED_MEDIUM)
         W, H, spp = 640, 360, 16
         p = F.render_params(W, H, spp, max_depth=8, rr_min_bounce=2, eye=(0.0, 6.0, 48.0), target=(0.0, 0.0, 0.0),
                             use_graph=1)
@@ -831,6 +842,31 @@ def run_case(args):
         acc.close()
         for b in blas:
             b.close()
+    elif args.case in ("incoherent", "coherent"):
+        cfg, hs, o, d, t, name = workload(False, 0)
+        nc = cfg["width"] * cfg["height"]
+        sl = slice(nc, len(t)) if args.case == "incoherent" else slice(0, nc)
+        rays = torch.from_numpy(scenes.pack_device_rays(o[sl], d[sl], t[sl])).cuda()
+        hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        with GpuAccelerator(hs) as acc:
+            tuned, _ = acc.autotune(rays)
+            for _ in range(2):
+                acc.trace_closest(rays, hits)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            # the profiler range (cudaProfilerStart / Stop) holds only these
+            # launches, for captures with --profile-from-start off
+            torch.cuda.profiler.start()
+            e0.record()
+            for _ in range(3):
+                acc.trace_closest(rays, hits)
+            e1.record()
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+            ms = e0.elapsed_time(e1) / 3
+            out = {"case": args.case, "rays": int(rays.shape[0]), "ms_per_launch": ms,
+                   "mrays_per_s": rays.shape[0] / ms / 1e3, "launch": tuned, "error_word": acc.error_word()}
     else:
         hs = scenes.raycast_scene(subdiv=8).build()
         ms = []

@@ -134,6 +134,11 @@ class BatchOptions(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class Medium(C.Structure):
+    _fields_ = [("box_min", C.c_float * 3), ("box_max", C.c_float * 3), ("sigma_a", C.c_float * 3),
+                ("sigma_s", C.c_float * 3), ("g", C.c_float), ("reserved", C.c_int32)]
+
+
 VP = C.c_void_p
 I64 = C.c_int64
 ST = C.c_int32
@@ -184,6 +189,7 @@ PROTOTYPES = {
     "gzg_renderer_adjoint": (ST, [VP, VP, VP, VP, VP, VP]),
     "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),
     "gzg_camera_rays": (ST, [C.POINTER(RenderParams), I64, I64, VP, VP, VP]),
+    "gzg_scene_set_medium": (ST, [VP, C.POINTER(Medium)]),
     "gzg_zsobol_fill_device": (ST, [I64, C.c_int32, C.c_int32, I64, VP, VP, VP, I64, VP, C.c_int32, VP, VP]),
     "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),
     "gzg_host_triangle_bounds": (ST, [VP, VP, I64, VP]),

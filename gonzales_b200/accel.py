@@ -30,6 +30,18 @@ def _host_rays(rays):
     return rays
 
 
+def _set_medium(handle, medium):
+    """gzg_scene_set_medium from a dict(box_min, box_max, sigma_a, sigma_s,
+    g) or None (removes the medium)."""
+    if medium is None:
+        F.check(F.lib().gzg_scene_set_medium(handle, None))
+        return
+    m = F.Medium((C.c_float * 3)(*medium["box_min"]), (C.c_float * 3)(*medium["box_max"]),
+                 (C.c_float * 3)(*medium["sigma_a"]), (C.c_float * 3)(*medium["sigma_s"]),
+                 float(medium.get("g", 0.0)), 0)
+    F.check(F.lib().gzg_scene_set_medium(handle, C.byref(m)))
+
+
 def _stream_handle(stream):
     if stream is None:
         import torch
@@ -275,6 +287,11 @@ class GpuAccelerator:
         rgb = np.ascontiguousarray(rgb, np.float32)
         F.check(F.lib().gzg_scene_set_environment(self.handle, F.ptr(rgb), rgb.shape[1], rgb.shape[0], float(scale)))
 
+    def set_medium(self, medium):
+        """Sets the homogeneous medium box (gzg_scene_set_medium):
+        dict(box_min, box_max, sigma_a, sigma_s, g), or None to remove it."""
+        _set_medium(self.handle, medium)
+
 
 class _ArraysHost:
     """What the Python side reads of a scene built from mesh arrays."""
@@ -355,6 +372,7 @@ class InstancedAccelerator:
 
     render = GpuAccelerator.render
     set_environment = GpuAccelerator.set_environment
+    set_medium = GpuAccelerator.set_medium
 
     def trace_closest(self, rays_d, hits_d, inst_d, options=None, stream=None):
         opt = C.byref(options) if options is not None else None

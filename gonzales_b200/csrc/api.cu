@@ -1317,6 +1317,27 @@ GZG_API gzg_status gzg_scene_set_material_params(gzg_scene *scene, const gzg_mat
 // running power sum gains one entry (Light/PowerLightSampler.swift) and the
 // total the light's power pi * 50^2 * average(scale)
 // (Light/InfiniteLight.swift:141-144).
+GZG_API gzg_status gzg_scene_set_medium(gzg_scene *scene, const gzg_medium *medium) {
+        if (!scene) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_scene_set_medium: null scene");
+        if (!medium) {
+                scene->host_shading.has_medium = false;
+                return clear_error();
+        }
+        bool ok = std::isfinite(medium->g) && std::fabs(medium->g) < 1.0f && medium->reserved == 0;
+        for (int a = 0; a < 3; ++a) {
+                ok = ok && std::isfinite(medium->box_min[a]) && std::isfinite(medium->box_max[a]) &&
+                     medium->box_min[a] < medium->box_max[a];
+                ok = ok && std::isfinite(medium->sigma_a[a]) && medium->sigma_a[a] >= 0.0f &&
+                     std::isfinite(medium->sigma_s[a]) && medium->sigma_s[a] >= 0.0f;
+        }
+        if (!ok)
+                return set_error(GZG_ERR_INVALID_ARGUMENT,
+                                 "gzg_scene_set_medium: empty box, negative or non-finite coefficient, or |g| >= 1");
+        scene->host_shading.medium = *medium;
+        scene->host_shading.has_medium = true;
+        return clear_error();
+}
+
 GZG_API gzg_status gzg_scene_set_environment(gzg_scene *scene, const float *rgb, int32_t width, int32_t height,
                                              float scale) {
         if (!scene || !rgb || width <= 0 || height <= 0 || (int64_t)width * height > ((int64_t)1 << 28) ||

@@ -73,6 +73,9 @@ struct HostShading {
         std::vector<float4_> lights;         // 4 per light
         std::vector<float> light_cdf;
         float light_total = 0.0f;
+        // homogeneous medium box (gzg_medium), when set
+        bool has_medium = false;
+        gzg_medium medium{};
         // environment light, after the area lights in the light list
         bool has_env = false;
         float env_power = 0.0f;

@@ -294,6 +294,9 @@ struct SceneConst {
         float film_scale;                  // Film.add: iso / 100
         float max_component;               // clamp of a sample's largest component (0: none)
         int32_t two_sided;                 // area lights emit on both sides (the live shade step's rule)
+        int32_t has_medium;                // homogeneous medium box (gzg_medium)
+        V3 med_min, med_max, sigma_a, sigma_s;
+        float med_g;
         int32_t material_begin;  // the scene's material 0 (area-light hits scatter with it)
         int32_t material_count;
         uint32_t root;            // wide-node root of the scene's tree
@@ -301,6 +304,103 @@ struct SceneConst {
         uint64_t path_begin;      // first batch-wide path index of the scene
         ZSobolConfig zs;
 };
+
+// ------------------------------------------------------------ medium
+// A homogeneous medium filling an axis-aligned box (gzg_scene_set_medium;
+// Medium/Homogeneous.swift:5-23, phase function Medium/HenyeyGreenstein.swift:
+// 13-39).  The reference's integrator never samples it (VolumePathIntegrator.
+// swift:394 hard-codes (white, nil)); these run the branch as meant: each
+// segment's part inside the box is sampled for a scattering event before the
+// segment is shaded, and shadow rays and MIS probes through the box carry its
+// transmittance.  The box boundary scatters nothing (an interface).
+
+// Parametric overlap [t0, t1] of o + t d (t in [0, tmax]) with the box.
+__device__ bool medium_overlap(const SceneConst &sc, V3 o, V3 d, float tmax, float &t0, float &t1) {
+        float lo = 0.0f, hi = tmax;
+        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        const float mn[3] = {sc.med_min.x, sc.med_min.y, sc.med_min.z};
+        const float mx[3] = {sc.med_max.x, sc.med_max.y, sc.med_max.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+                if (dd[a] == 0.0f) {
+                        if (oo[a] < mn[a] || oo[a] > mx[a]) return false;
+                        continue;
+                }
+                const float inv = 1.0f / dd[a];
+                float tn = (mn[a] - oo[a]) * inv, tf = (mx[a] - oo[a]) * inv;
+                if (tn > tf) {
+                        const float t = tn;
+                        tn = tf;
+                        tf = t;
+                }
+                lo = fmaxf(lo, tn);
+                hi = fminf(hi, tf);
+        }
+        t0 = lo;
+        t1 = hi;
+        return lo < hi;
+}
+
+// Transmittance along the part of [0, tmax] inside the box.
+__device__ V3 medium_tr(const SceneConst &sc, V3 o, V3 d, float tmax) {
+        float t0, t1;
+        if (!sc.has_medium || !medium_overlap(sc, o, d, tmax, t0, t1)) return v3(1.0f, 1.0f, 1.0f);
+        const V3 st = sc.sigma_a + sc.sigma_s;
+        const float len = (t1 - t0) * sqrtf(dot(d, d));
+        return v3(expf(-st.x * len), expf(-st.y * len), expf(-st.z * len));
+}
+
+// Homogeneous.sample on the in-box part of [0, tmax]: channel number uc,
+// distance number ud.  True with the scattering parameter t when the medium
+// is sampled; weight = transmittance x sigma_s / density there, else
+// transmittance / density (Homogeneous.swift:19 writes sigma_t where the PBRT
+// sampler it restates has sigma_s, which would scatter in a purely absorbing
+// medium).
+__device__ bool medium_sample(const SceneConst &sc, V3 o, V3 d, float tmax, float uc, float ud, float &t,
+                              V3 &weight) {
+        float t0, t1;
+        weight = v3(1.0f, 1.0f, 1.0f);
+        if (!medium_overlap(sc, o, d, tmax, t0, t1)) return false;
+        const V3 st = sc.sigma_a + sc.sigma_s;
+        const int channel = min((int)(uc * 3.0f), 2);
+        const float stc = channel == 0 ? st.x : (channel == 1 ? st.y : st.z);
+        const float distance = -logf(1.0f - ud) / stc;
+        const float len = sqrtf(dot(d, d));
+        const float seg = t1 - t0;
+        const float param = fminf(distance / len, seg);
+        const bool sampled = param < seg;
+        const V3 tr = v3(expf(-st.x * param * len), expf(-st.y * param * len), expf(-st.z * param * len));
+        const V3 density = sampled ? mulv(st, tr) : tr;
+        const float pdf = (density.x + density.y + density.z) / 3.0f;
+        weight = sampled ? mulv(tr, sc.sigma_s) * (1.0f / pdf) : tr * (1.0f / pdf);
+        t = t0 + param;
+        return sampled;
+}
+
+// HenyeyGreenstein.phase (HenyeyGreenstein.swift:13-16).
+__device__ float hg_phase(float cos_theta, float g) {
+        const float denom = 1.0f + g * g + 2.0f * g * cos_theta;
+        return (1.0f / (4.0f * kPi)) * (1.0f - g * g) / (denom * sqrtf(denom));
+}
+
+// HenyeyGreenstein.samplePhase (HenyeyGreenstein.swift:18-36): incident
+// direction in the frame (makeCoordinateSystem(outgoing), outgoing); value =
+// density.
+__device__ V3 hg_sample(V3 wo, float g, float u0, float u1, float &value) {
+        float cos_theta;
+        if (fabsf(g) < 1e-3f) {
+                cos_theta = 1.0f - 2.0f * u0;
+        } else {
+                const float sqr = (1.0f - g * g) / (1.0f + g - 2.0f * g * u0);
+                cos_theta = -(1.0f + g * g - sqr * sqr) / (2.0f * g);
+        }
+        const float sin_theta = sqrtf(fmaxf(0.0f, 1.0f - cos_theta * cos_theta));
+        const float phi = 2.0f * kPi * u1;
+        V3 v1, v2;
+        coordinate_system(wo, v1, v2);
+        value = hg_phase(cos_theta, g);
+        return v1 * (sin_theta * cosf(phi)) + v2 * (sin_theta * sinf(phi)) + wo * cos_theta;
+}
 
 enum {
         kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4,
@@ -869,7 +969,8 @@ __device__ void shade_generic(const Wave &w, const DevScene &s, const SceneConst
                                 const float light_w = power_heuristic(light_pdf, brdf_density);
                                 const V3 so = pos + (target - pos) * 0.0001f;
                                 const V3 sd = target - so;
-                                const V3 c = mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf));
+                                const V3 c = mulv(mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf)),
+                                                  medium_tr(sc, so, sd, 1.0f - 0.00001f));
                                 const uint32_t q = queue_slot(w.counts + kCountShadow);
                                 store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
                                 w.sh_id[q] = path;
@@ -956,6 +1057,122 @@ __device__ __forceinline__ uint32_t gen_pos(const Wave &w, int kind, uint32_t sl
         return (kind == 3 || kind == 5) ? half + slot : half + w.capacity - 1u - slot;
 }
 
+// A scattering event in the medium at p (the oracle's shade_medium): light
+// sample with MIS against the phase function (light choice 1D, light point
+// 2D, phase sample 2D), then the phase sample (2D) that continues the path
+// from p with its throughput unchanged (value / density = 1), then roulette.
+__device__ void shade_medium(const Wave &w, const DevScene &s, const SceneConst &sc, uint32_t path, int bounce,
+                             int cur, V3 p, V3 wo, V3 thr, V3 L, ZSobol &z) {
+        const float g = sc.med_g;
+        bool alive = true;
+        if (sc.light_count > 0) {
+                float choose_pdf;
+                const int lo = choose_light(s, sc, zs_get1d(sc.zs, z), choose_pdf);
+                const bool chose_env = lo == sc.env_index;
+                const int li = sc.light_begin + lo;
+                float u0, u1;
+                zs_get2d(sc.zs, z, u0, u1);
+                float light_pdf = 0.0f, area = 0.0f;
+                V3 light_est = v3(0, 0, 0), light_dir = v3(0, 0, 0), lp0, lp1, lp2, target;
+                if (chose_env) {
+                        V3 dv, rad;
+                        const float pdf = env_sample(s, u0, u1, dv, rad);
+                        target = p + dv * 100.0f;
+                        if (!is_black(rad) && !isinf(pdf)) {
+                                light_est = rad * hg_phase(dot(wo, dv), g);
+                                light_dir = dv;
+                                light_pdf = pdf;
+                        }
+                } else {
+                        const float4 l0 = __ldg(s.lights + 4 * li), l1 = __ldg(s.lights + 4 * li + 1),
+                                     l2 = __ldg(s.lights + 4 * li + 2), le4 = __ldg(s.lights + 4 * li + 3);
+                        lp0 = v3(l0);
+                        lp1 = v3(l1);
+                        lp2 = v3(l2);
+                        area = l0.w;
+                        const float su0 = sqrtf(u0);
+                        const float lb0 = 1.0f - su0, lb1 = u1 * su0;
+                        target = lp0 * lb0 + lp1 * lb1 + lp2 * ((1.0f - lb0) - lb1);
+                        const V3 ln = normalize(cross(lp1 - lp0, lp2 - lp0));
+                        const V3 inc = normalize(target - p);
+                        const V3 dl = p - target;
+                        const float pdf = (1.0f / area) * (dot(dl, dl) / fabsf(dot(ln, neg(inc))));
+                        if ((sc.two_sided || dot(ln, neg(inc)) > 0.0f) && !isinf(pdf)) {
+                                light_est = v3(le4) * w.emission_scale * hg_phase(dot(wo, inc), g);
+                                light_dir = inc;
+                                light_pdf = pdf;
+                        }
+                }
+                const float phase_density = light_pdf == 0.0f ? 0.0f : hg_phase(dot(wo, light_dir), g);
+                const float light_w = power_heuristic(light_pdf, phase_density);
+                if (light_pdf != 0.0f && !is_black(light_est)) {
+                        const V3 so = p + (target - p) * 0.0001f;
+                        const V3 sd = target - so;
+                        const V3 c = mulv(mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf)),
+                                          medium_tr(sc, so, sd, 1.0f - 0.00001f));
+                        const uint32_t q = queue_slot(w.counts + kCountShadow);
+                        store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
+                        w.sh_id[q] = path;
+                        w.sh_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
+                }
+                float v0, v1;
+                zs_get2d(sc.zs, z, v0, v1);
+                if (sc.mis_corrected || chose_env) {
+                        float value;
+                        const V3 wi = hg_sample(wo, g, v0, v1, value);
+                        if (value > 0.0f) {
+                                float light_density = 0.0f;
+                                if (chose_env) {
+                                        light_density = env_pdf(s, wi);
+                                } else {
+                                        float tl, lu, lv;
+                                        const float4 a4 = make_float4(lp0.x, lp0.y, lp0.z, 0.0f),
+                                                     b4 = make_float4(lp1.x, lp1.y, lp1.z, 0.0f),
+                                                     c4 = make_float4(lp2.x, lp2.y, lp2.z, 0.0f);
+                                        if (watertight_test(p.x, p.y, p.z, wi.x, wi.y, wi.z, a4, b4, c4, kInf, tl, lu, lv)) {
+                                                const V3 hp = p + wi * tl;
+                                                const V3 dq = p - hp;
+                                                const V3 lnn = normalize(cross(lp0 - lp2, lp1 - lp2));
+                                                const float dens = dot(dq, dq) / (fabsf(dot(lnn, neg(wi))) * area);
+                                                light_density = isinf(dens) ? 0.0f : dens;
+                                        }
+                                }
+                                const float bw = power_heuristic(value, light_density);
+                                if (bw > 0.0f) {
+                                        // value / density = 1; the probe's resolve applies the
+                                        // medium's transmittance up to what it reaches
+                                        const V3 c = thr * (bw / choose_pdf);
+                                        const uint32_t q = queue_slot(w.counts + kCountProbe);
+                                        store_ray(w.pr_ray, q, p, kInf, wi, sc.root);
+                                        w.pr_id[q] = path;
+                                        w.pr_contrib[q] = make_float4(c.x, c.y, c.z, 0.0f);
+                                }
+                        }
+                }
+        }
+        float v0, v1;
+        zs_get2d(sc.zs, z, v0, v1);
+        float value;
+        const V3 wi = hg_sample(wo, g, v0, v1, value);
+        const float mv = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+        if (mv < 1.0f && bounce >= sc.rr_min) {
+                const float qq = fmaxf(0.0f, 1.0f - mv);
+                if (zs_get1d(sc.zs, z) < qq)
+                        alive = false;
+                else
+                        thr = thr * (1.0f / (1.0f - qq));
+        }
+        if (alive && bounce + 1 < sc.max_depth) {
+                const int nxt = cur ^ 1;
+                const uint32_t q = queue_slot(w.counts + nxt);
+                store_ray(w.q_ray[nxt], q, p, kInf, wi, sc.root);
+                w.q_id[nxt][q] = path;
+        }
+        w.thr[path] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+        w.L[path] = make_float4(L.x, L.y, L.z, 0.0f);
+        w.zs_dim[path] = z.dim;
+}
+
 // shade: VolumePathIntegrator.shadeBounce + surfaceEstimate (:325-430).
 // kShadeDiffuse: a scene without general BSDFs.  kShadeSplit: shades diffuse
 // hits and misses and queues hits on the general materials on their kind's
@@ -986,6 +1203,36 @@ __global__ void __launch_bounds__(128, kKind == kShadeSplit                     
         const int prim = __float_as_int(hit.w);
         const float4 rd = w.q_ray[cur][2 * i + 1];
         const V3 d = v3(rd);
+        if (kKind < kShadeDielectric) {
+                const SceneConst &scm = w.scenes[w.scene[path]];
+                if (scm.has_medium) {
+                        // Homogeneous.sample on the segment before it is shaded (the
+                        // branch of shadeBounce :394-408 as meant to run); its two
+                        // numbers are drawn at every segment of a scene with a medium
+                        ZSobol z;
+                        z.morton = w.zs_morton[path];
+                        z.dim = w.zs_dim[path];
+                        const float uc = zs_get1d(scm.zs, z);
+                        const float ud = zs_get1d(scm.zs, z);
+                        const V3 o = v3(w.q_ray[cur][2 * i]);
+                        float tm;
+                        V3 wgt;
+                        const bool scattered = medium_sample(scm, o, d, prim < 0 ? kInf : hit.x, uc, ud, tm, wgt);
+                        const float4 t4 = w.thr[path];
+                        const V3 thr = mulv(v3(t4), wgt);
+                        if (scattered) {
+                                if (is_black(thr) || bounce >= scm.max_depth) {
+                                        w.thr[path] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                                        w.zs_dim[path] = z.dim;
+                                } else {
+                                        shade_medium(w, s, scm, path, bounce, cur, o + d * tm, neg(d), thr, v3(w.L[path]), z);
+                                }
+                                return;
+                        }
+                        w.thr[path] = make_float4(thr.x, thr.y, thr.z, t4.w);
+                        w.zs_dim[path] = z.dim;
+                }
+        }
         if (prim < 0) {
                 // shadeBounce on a miss (:375-387): the environment light on
                 // camera rays and after specular bounces
@@ -1137,7 +1384,8 @@ __global__ void __launch_bounds__(128, kKind == kShadeSplit                     
                         // Visibility.occluded via spawnRay(from:target:) (Interaction.swift:15-24)
                         const V3 so = pos + (target - pos) * 0.0001f;
                         const V3 sd = target - so;
-                        const V3 c = mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf));
+                        const V3 c = mulv(mulv(thr, light_est * (light_w / light_pdf) * (1.0f / choose_pdf)),
+                                          medium_tr(sc, so, sd, 1.0f - 0.00001f));
                         const uint32_t q = queue_slot(w.counts + kCountShadow);
                         store_ray(w.sh_ray, q, so, 1.0f - 0.00001f, sd, sc.root);
                         w.sh_id[q] = path;
@@ -1261,7 +1509,15 @@ __global__ void k_probe_resolve(Wave w, DevScene s, int any_only) {
                 le = v3(__ldg(s.materials + 2 * mat_index + 1)) * w.emission_scale;
         }
         const uint32_t path = w.pr_id[i];
-        const float4 c = w.pr_contrib[i];
+        float4 c = w.pr_contrib[i];
+        const SceneConst &sc = w.scenes[w.scene[path]];
+        if (sc.has_medium) {
+                // the medium's transmittance up to what the probe reaches
+                const V3 tr = medium_tr(sc, v3(w.pr_ray[2 * i]), wi, prim < 0 ? kInf : h.x);
+                c.x *= tr.x;
+                c.y *= tr.y;
+                c.z *= tr.z;
+        }
         float4 L = w.L[path];
         L.x += c.x * le.x;
         L.y += c.y * le.y;
@@ -1795,6 +2051,17 @@ gzg_status build_batch(gzg_renderer *r) {
         if (r->film_offsets[n] >= (int64_t)0xFFFFFFFFll)
                 return set_error(GZG_ERR_LIMIT, "renderer: more than 2^32 film pixels in a batch");
         r->w.total_paths = paths;
+        for (size_t k = 0; k < n; ++k) {
+                const HostShading &hs = scene_host_shading(r->scenes[k]);
+                SceneConst &sc = r->consts[k];
+                sc.has_medium = hs.has_medium ? 1 : 0;
+                const gzg_medium &m = hs.medium;
+                sc.med_min = V3{m.box_min[0], m.box_min[1], m.box_min[2]};
+                sc.med_max = V3{m.box_max[0], m.box_max[1], m.box_max[2]};
+                sc.sigma_a = V3{m.sigma_a[0], m.sigma_a[1], m.sigma_a[2]};
+                sc.sigma_s = V3{m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]};
+                sc.med_g = m.g;
+        }
         int wide_depth = 0;
         if (n == 1) {
                 scene_view(r->scenes[0], &r->view, &r->device, &wide_depth);

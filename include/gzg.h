@@ -332,6 +332,29 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
  * default for closest-hit (any_hit = 0) or any-hit queries. */
 GZG_API gzg_status gzg_scene_set_launch(gzg_scene *scene, int32_t any_hit, const gzg_trace_options *config);
 
+/* A homogeneous participating medium (Medium/Homogeneous.swift) filling an
+ * axis-aligned box whose boundary scatters nothing (an interface,
+ * Material/Interface.swift), with a Henyey-Greenstein phase function
+ * (Medium/HenyeyGreenstein.swift).  The reference's integrator never samples
+ * its media (VolumePathIntegrator.swift:394 hard-codes the transmittance to
+ * white); renderers run the branch as meant: each path segment samples a
+ * scattering distance in the box (a random color channel, as
+ * Homogeneous.sample), a scattering event shades with the phase function
+ * (light sample with MIS, phase sample), and shadow rays and MIS probes carry
+ * the box's transmittance. */
+typedef struct gzg_medium {
+        float box_min[3], box_max[3];
+        float sigma_a[3];  /* absorption per unit length, per RGB channel */
+        float sigma_s[3];  /* scattering per unit length, per RGB channel */
+        float g;           /* Henyey-Greenstein asymmetry in (-1, 1) */
+        int32_t reserved;  /* 0 */
+} gzg_medium;
+
+/* Sets (or, with medium NULL, removes) the scene's medium; flat or two-level
+ * scenes.  Renderers created afterwards use it.  Rejects an empty box,
+ * negative or non-finite coefficients and |g| >= 1. */
+GZG_API gzg_status gzg_scene_set_medium(gzg_scene *scene, const gzg_medium *medium);
+
 /* Adds an environment light (Light/InfiniteLight.swift) to an uploaded scene
  * (flat or two-level), after its area lights in the light list: the HOST map
  * rgb[height][width][3] (row v, column u) in the equal-area square layout the

@@ -460,6 +460,103 @@ V3 offset_origin(V3 p, V3 n, V3 dir) {
         return dot(dir, n) > 0.0f ? add(p, off) : add(p, neg(off));
 }
 
+// ---- homogeneous medium in a box (Medium/Homogeneous.swift:5-23, phase
+// function Medium/HenyeyGreenstein.swift:13-39).  The reference's integrator
+// never samples it (VolumePathIntegrator.swift:394 hard-codes (white, nil));
+// this is the branch as it evidently was meant to run: before a segment is
+// shaded, the part of it inside the box is sampled for a scattering event;
+// shadow rays and MIS probes through the box carry its transmittance.  The
+// box boundary scatters nothing (an interface: Material/Interface.swift).
+
+// Parametric overlap [t0, t1] of o + t d (t in [0, tmax]) with the medium
+// box (slab test); false when empty.
+bool medium_overlap(const orc_render_params &P, V3 o, V3 d, float tmax, float *t0, float *t1) {
+        float lo = 0.0f, hi = tmax;
+        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        for (int a = 0; a < 3; ++a) {
+                if (dd[a] == 0.0f) {
+                        if (oo[a] < P.medium_min[a] || oo[a] > P.medium_max[a]) return false;
+                        continue;
+                }
+                const float inv = 1.0f / dd[a];
+                float tn = (P.medium_min[a] - oo[a]) * inv, tf = (P.medium_max[a] - oo[a]) * inv;
+                if (tn > tf) std::swap(tn, tf);
+                lo = std::max(lo, tn);
+                hi = std::min(hi, tf);
+        }
+        *t0 = lo;
+        *t1 = hi;
+        return lo < hi;
+}
+
+V3 sigma_t_of(const orc_render_params &P) {
+        return v3(P.sigma_a[0] + P.sigma_s[0], P.sigma_a[1] + P.sigma_s[1], P.sigma_a[2] + P.sigma_s[2]);
+}
+
+// Transmittance exp(-sigma_t * length) along the part of [0, tmax] inside
+// the box.
+V3 medium_tr(const orc_render_params &P, V3 o, V3 d, float tmax) {
+        float t0, t1;
+        if (!P.has_medium || !medium_overlap(P, o, d, tmax, &t0, &t1)) return v3(1, 1, 1);
+        const V3 st = sigma_t_of(P);
+        const float len = (t1 - t0) * std::sqrt(dot(d, d));
+        return v3(std::exp(-st.x * len), std::exp(-st.y * len), std::exp(-st.z * len));
+}
+
+// Homogeneous.sample on the segment [0, tmax] of the ray, restricted to its
+// part inside the box, with the two uniform numbers uc (channel) and ud
+// (distance).  Returns true with the scattering parameter t when the medium
+// is sampled; `weight` is the throughput factor: transmittance x sigma_s /
+// density at a scattering event and transmittance / density otherwise.
+// Homogeneous.swift:19 writes sigma_t (`transmission`) where the PBRT
+// sampler it restates has sigma_s; with sigma_t a purely absorbing medium
+// would still scatter, so the scattering coefficient is used here.
+bool medium_sample(const orc_render_params &P, V3 o, V3 d, float tmax, float uc, float ud, float *t, V3 *weight) {
+        float t0, t1;
+        *weight = v3(1, 1, 1);
+        if (!medium_overlap(P, o, d, tmax, &t0, &t1)) return false;
+        const V3 st = sigma_t_of(P);
+        const float stc[3] = {st.x, st.y, st.z};
+        const int channel = std::min((int)(uc * 3.0f), 2);
+        const float distance = -std::log(1.0f - ud) / stc[channel];
+        const float len = std::sqrt(dot(d, d));
+        const float seg = t1 - t0;
+        const float param = std::min(distance / len, seg);
+        const bool sampled = param < seg;
+        const V3 tr = v3(std::exp(-st.x * param * len), std::exp(-st.y * param * len), std::exp(-st.z * param * len));
+        const V3 density = sampled ? mulv(st, tr) : tr;
+        const float pdf = (density.x + density.y + density.z) / 3.0f;
+        const V3 ss = v3(P.sigma_s[0], P.sigma_s[1], P.sigma_s[2]);
+        *weight = sampled ? mul(mulv(tr, ss), 1.0f / pdf) : mul(tr, 1.0f / pdf);
+        *t = t0 + param;
+        return sampled;
+}
+
+// HenyeyGreenstein.phase (HenyeyGreenstein.swift:13-16).
+float hg_phase(float cos_theta, float g) {
+        const float denom = 1.0f + g * g + 2.0f * g * cos_theta;
+        return (1.0f / (4.0f * kPi)) * (1.0f - g * g) / (denom * std::sqrt(denom));
+}
+
+// HenyeyGreenstein.samplePhase (HenyeyGreenstein.swift:18-36): the incident
+// direction in the frame (makeCoordinateSystem(outgoing), outgoing) and the
+// phase value, which is also its density.
+V3 hg_sample(V3 wo, float g, float u0, float u1, float *value) {
+        float cos_theta;
+        if (std::fabs(g) < 1e-3f) {
+                cos_theta = 1.0f - 2.0f * u0;
+        } else {
+                const float sqr = (1.0f - g * g) / (1.0f + g - 2.0f * g * u0);
+                cos_theta = -(1.0f + g * g - sqr * sqr) / (2.0f * g);
+        }
+        const float sin_theta = std::sqrt(std::max(0.0f, 1.0f - cos_theta * cos_theta));
+        const float phi = 2.0f * kPi * u1;
+        V3 v1, v2;
+        coordinate_system(wo, &v1, &v2);
+        *value = hg_phase(cos_theta, g);
+        return add(add(mul(v1, sin_theta * std::cos(phi)), mul(v2, sin_theta * std::sin(phi))), mul(wo, cos_theta));
+}
+
 // PowerLightSampler.chooseLight with the lowerBound search of
 // PowerLightSampler.swift:4-18.
 int choose_light(const Scene &sc, float u, float *pdf) {
@@ -552,7 +649,8 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         Hit sh = trace(sc, so, sub(target, so), 1.0f - 0.00001f);
                         ++res.shadow;
                         if (!sh.hit) {
-                                light_est = mulv(mul(f_world(dv), std::fabs(dot(dv, is.ns))), rad);
+                                light_est = mulv(mulv(mul(f_world(dv), std::fabs(dot(dv, is.ns))), rad),
+                                                 medium_tr(P, so, sub(target, so), 1.0f - 0.00001f));
                                 light_dir = dv;
                                 light_pdf = pdf;
                         }
@@ -570,7 +668,8 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         Hit sh = trace(sc, so, sub(lp, so), 1.0f - 0.00001f);
                         ++res.shadow;
                         if (!sh.hit) {
-                                light_est = mulv(mul(f_world(inc), std::fabs(dot(inc, is.ns))), emitted(sc, lt.le));
+                                light_est = mulv(mulv(mul(f_world(inc), std::fabs(dot(inc, is.ns))), emitted(sc, lt.le)),
+                                                 medium_tr(P, so, sub(lp, so), 1.0f - 0.00001f));
                                 light_dir = inc;
                                 light_pdf = pdf;
                         }
@@ -603,7 +702,7 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
                         } else if (sc.env) {
                                 radiance = env_radiance(sc, wi);
                         }
-                        est = mulv(est, radiance);
+                        est = mulv(mulv(est, radiance), medium_tr(P, po, wi, ph.hit ? ph.t : kInfF));
                         float light_density = 0.0f;
                         if (lt.is_env) {
                                 const float dd[3] = {wi.x, wi.y, wi.z};
@@ -644,6 +743,122 @@ bool shade_generic(const Scene &sc, orc_zsobol *smp, const orc_bsdf_params &bp, 
         return true;
 }
 
+// A scattering event in the medium at p: mediumEstimate / sampleMedium
+// (VolumePathIntegrator.swift:286-323) with the Henyey-Greenstein phase
+// function as the distribution model (PhaseFunction.swift: value without a
+// cosine, density = value): sampleOneLight with MIS (light choice 1D, light
+// point 2D, phase sample 2D), then the phase sample (2D) that continues the
+// path with its throughput unchanged (value / density = 1), then roulette.
+// The new ray starts at p itself (a medium interaction has no normal to
+// offset along).  false ends the path.
+bool shade_medium(const Scene &sc, orc_zsobol *smp, V3 p, V3 wo, int bounce, V3 &L, V3 &thr, V3 &o, V3 &d,
+                  PathResult &res) {
+        const orc_render_params &P = *sc.p;
+        const float g = P.medium_g;
+        if (!sc.lights.empty()) {
+                float choose_pdf;
+                const int li = choose_light(sc, orc_zsobol_get1d(smp), &choose_pdf);
+                const Light &lt = sc.lights[li];
+                float u2[2];
+                orc_zsobol_get2d(smp, u2);
+                V3 light_est = v3(0, 0, 0), light_dir = v3(0, 0, 0);
+                float light_pdf = 0.0f;
+                if (lt.is_env) {
+                        float dir[3], rgb[3];
+                        const float pdf = orc_env_sample(sc.env, u2[0], u2[1], dir, rgb);
+                        const V3 dv = v3(dir[0], dir[1], dir[2]), rad = v3(rgb[0], rgb[1], rgb[2]);
+                        if (!is_black(rad) && !std::isinf(pdf)) {
+                                const V3 target = add(p, mul(dv, 100.0f));
+                                const V3 so = add(p, mul(sub(target, p), 0.0001f));
+                                const V3 sd = sub(target, so);
+                                Hit sh = trace(sc, so, sd, 1.0f - 0.00001f);
+                                ++res.shadow;
+                                if (!sh.hit) {
+                                        light_est = mulv(mul(rad, hg_phase(dot(wo, dv), g)),
+                                                         medium_tr(P, so, sd, 1.0f - 0.00001f));
+                                        light_dir = dv;
+                                        light_pdf = pdf;
+                                }
+                        }
+                } else {
+                        const float su0 = std::sqrt(u2[0]);
+                        const float lb0 = 1.0f - su0, lb1 = u2[1] * su0;
+                        const V3 lp = add(add(mul(lt.p0, lb0), mul(lt.p1, lb1)), mul(lt.p2, (1.0f - lb0) - lb1));
+                        const V3 ln = normalize(cross(sub(lt.p1, lt.p0), sub(lt.p2, lt.p0)));
+                        const V3 inc = normalize(sub(lp, p));
+                        const V3 dl = sub(p, lp);
+                        const float pdf = (1.0f / lt.area) * (dot(dl, dl) / std::fabs(dot(ln, neg(inc))));
+                        if ((P.two_sided_emission || dot(ln, neg(inc)) > 0.0f) && !std::isinf(pdf)) {
+                                const V3 so = add(p, mul(sub(lp, p), 0.0001f));
+                                const V3 sd = sub(lp, so);
+                                Hit sh = trace(sc, so, sd, 1.0f - 0.00001f);
+                                ++res.shadow;
+                                if (!sh.hit) {
+                                        light_est = mulv(mul(emitted(sc, lt.le), hg_phase(dot(wo, inc), g)),
+                                                         medium_tr(P, so, sd, 1.0f - 0.00001f));
+                                        light_dir = inc;
+                                        light_pdf = pdf;
+                                }
+                        }
+                }
+                const float phase_density = light_pdf == 0.0f ? 0.0f : hg_phase(dot(wo, light_dir), g);
+                const float light_w = power_heuristic(light_pdf, phase_density);
+                V3 contrib = light_pdf == 0.0f ? v3(0, 0, 0) : mul(light_est, light_w / light_pdf);
+                float u[2];
+                orc_zsobol_get2d(smp, u);
+                if (P.mis_corrected || lt.is_env) {
+                        float value;
+                        const V3 wi = hg_sample(wo, g, u[0], u[1], &value);
+                        if (value > 0.0f) {
+                                Hit ph = trace(sc, p, wi, kInfF);
+                                ++res.probe;
+                                V3 radiance = v3(0, 0, 0);
+                                Isect pi;
+                                if (ph.hit) {
+                                        if (interaction(sc, ph, wi, &pi) && pi.pr->type == 3) {
+                                                const orc_material &lm = pi.mats[pi.pr->material_index];
+                                                if (P.two_sided_emission || dot(pi.ng, neg(wi)) > 0.0f)
+                                                        radiance = emitted(sc, v3(lm.emission[0], lm.emission[1],
+                                                                                  lm.emission[2]));
+                                        }
+                                } else if (sc.env) {
+                                        radiance = env_radiance(sc, wi);
+                                }
+                                radiance = mulv(radiance, medium_tr(P, p, wi, ph.hit ? ph.t : kInfF));
+                                float light_density = 0.0f;
+                                if (lt.is_env) {
+                                        const float dd[3] = {wi.x, wi.y, wi.z};
+                                        light_density = orc_env_pdf(sc.env, dd);
+                                } else {
+                                        float tl;
+                                        if (hit_light(lt, p, wi, &tl)) {
+                                                const V3 hp = add(p, mul(wi, tl));
+                                                const V3 dq = sub(p, hp);
+                                                const V3 lnn = normalize(cross(sub(lt.p0, lt.p2), sub(lt.p1, lt.p2)));
+                                                const float dens = dot(dq, dq) / (std::fabs(dot(lnn, neg(wi))) * lt.area);
+                                                light_density = std::isinf(dens) ? 0.0f : dens;
+                                        }
+                                }
+                                const float bw = power_heuristic(value, light_density);
+                                contrib = add(contrib, mul(radiance, bw));  // value / density = 1
+                        }
+                }
+                L = add(L, mulv(thr, mul(contrib, 1.0f / choose_pdf)));
+        }
+        float u[2];
+        orc_zsobol_get2d(smp, u);
+        float value;
+        d = hg_sample(wo, g, u[0], u[1], &value);
+        o = p;
+        const float mv = max_value(thr);
+        if (mv < 1.0f && bounce >= P.rr_min_bounce) {
+                const float q = std::max(0.0f, 1.0f - mv);
+                if (orc_zsobol_get1d(smp) < q) return false;
+                thr = mul(thr, 1.0f / (1.0f - q));
+        }
+        return true;
+}
+
 // One path: VolumePathIntegrator.bounces (:448-463) with shadeBounce (:373-430)
 // and surfaceEstimate (:325-371).
 PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
@@ -654,6 +869,23 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
         for (int bounce = 0; bounce <= P.max_depth; ++bounce) {
                 Hit h = trace(sc, o, d, kInfF);
                 ++res.ext;
+                if (P.has_medium) {
+                        // Homogeneous.sample on the segment before it is shaded (the
+                        // branch of shadeBounce :394-408 as meant to run); its two
+                        // numbers are drawn at every segment of a scene with a medium
+                        const float uc = orc_zsobol_get1d(smp);
+                        const float ud = orc_zsobol_get1d(smp);
+                        float tm;
+                        V3 wgt;
+                        const bool scattered = medium_sample(P, o, d, h.hit ? h.t : kInfF, uc, ud, &tm, &wgt);
+                        thr = mulv(thr, wgt);
+                        if (scattered) {
+                                if (is_black(thr) || bounce >= P.max_depth) break;
+                                if (!shade_medium(sc, smp, add(o, mul(d, tm)), neg(d), bounce, L, thr, o, d, res)) break;
+                                specular = false;
+                                continue;
+                        }
+                }
                 if (!h.hit) {
                         // shadeBounce on a miss (:375-387): environment light on
                         // camera rays (no specular bounces in these scenes)
@@ -750,7 +982,8 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                 if (!sh.hit) {
                                         const bool reflect = dot(dv, ng) * dot(wo, ng) > 0.0f;
                                         const V3 f = reflect ? f_val : v3(0, 0, 0);
-                                        light_est = mulv(mul(f, std::fabs(dot(dv, is.ns))), rad);
+                                        light_est = mulv(mulv(mul(f, std::fabs(dot(dv, is.ns))), rad),
+                                                         medium_tr(P, so, sd, 1.0f - 0.00001f));
                                         light_dir = dv;
                                         light_pdf = pdf;
                                 }
@@ -778,7 +1011,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                         const bool reflect = dot(dir, ng) * dot(wo, ng) > 0.0f;
                                         const V3 f = reflect ? f_val : v3(0, 0, 0);
                                         const V3 scatter = mul(f, std::fabs(dot(dir, is.ns)));
-                                        light_est = mulv(scatter, emitted(sc, lt.le));
+                                        light_est = mulv(mulv(scatter, emitted(sc, lt.le)), medium_tr(P, so, sd, 1.0f - 0.00001f));
                                         light_dir = dir;
                                         light_pdf = pdf;
                                 }
@@ -821,7 +1054,7 @@ PathResult trace_path(const Scene &sc, orc_zsobol *smp, V3 o, V3 d) {
                                 } else if (sc.env) {
                                         radiance = env_radiance(sc, wi);
                                 }
-                                est = mulv(est, radiance);
+                                est = mulv(mulv(est, radiance), medium_tr(P, po, wi, ph.hit ? ph.t : kInfF));
                                 float light_density = 0.0f;
                                 if (lt.is_env) {
                                         const float dd[3] = {wi.x, wi.y, wi.z};

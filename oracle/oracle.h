@@ -106,6 +106,13 @@ typedef struct orc_render_params {
         float lens_radius;      /* thin lens (PerspectiveCamera.depthOfField); 0: pinhole */
         float focal_distance;
         int32_t two_sided_emission; /* 1: area lights emit on both sides (the live shade_core's rule) */
+        /* a homogeneous medium (Medium/Homogeneous.swift) filling the box
+         * medium_min..medium_max, whose boundary does not scatter (an
+         * interface); phase function Henyey-Greenstein with asymmetry medium_g */
+        int32_t has_medium;
+        float medium_min[3], medium_max[3];
+        float sigma_a[3], sigma_s[3];
+        float medium_g;
 } orc_render_params;
 
 /* Renders the scene; per pixel (row-major) accumulates the film sums of the

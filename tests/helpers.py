@@ -89,7 +89,7 @@ def record(name, data):
     """Writes a measurement record (JSON) into $GZG_RECORD_DIR when it is set."""
     d = os.environ.get("GZG_RECORD_DIR")
     if d and Path(d).is_dir():
-        (Path(d) / name).write_text(json.dumps(data))
+        (Path(d) / name).write_text(json.dumps(data, default=lambda o: o.item() if hasattr(o, "item") else str(o)))
 
 
 # ---------------------------------------------------------------- the reference's regression scene

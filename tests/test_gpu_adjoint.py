@@ -239,11 +239,11 @@ def test_adjoint_matches_oracle_differences_uniform_texels_full_textures(setup):
             assert d_tex[idx] == 0.0, (idx, d_tex[idx])
             continue
         nonzero += 1
-        err = abs(d_tex[idx] - fd) / abs(fd)
+        err = float(abs(float(d_tex[idx]) - fd) / abs(fd))
         worst = max(worst, err)
         assert err <= 0.02, (idx, d_tex[idx], fd)
     fd_em = (oracle_loss(tex, scale + H) - oracle_loss(tex, scale - H)) / (2 * H)
-    em_err = abs(d_em - fd_em) / abs(fd_em)
+    em_err = float(abs(d_em - fd_em) / abs(fd_em))
     helpers.record("adjoint_uniform_texels.json", {"texels": checked, "nonzero": nonzero, "worst_rel_err": worst,
                                                    "emission_rel_err": em_err, "render": [W, Hh, spp, depth]})
     assert em_err <= 0.02, (d_em, fd_em)
