@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <chrono>
+#include <cstdlib>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -178,6 +181,44 @@ struct gzg_scene {
         }
 };
 
+gzg_status gzg::wait_stream(void *stream, const char *what) {
+        int64_t limit_us = 300000000;
+        if (const char *env = std::getenv("GZG_WAIT_LIMIT_US")) limit_us = std::atoll(env);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        cudaEvent_t ev = nullptr;
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, st);
+        if (e != cudaSuccess) {
+                if (ev) cudaEventDestroy(ev);
+                return set_error(GZG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        gzg_status status = GZG_OK;
+        for (;;) {
+                e = cudaEventQuery(ev);
+                if (e == cudaSuccess) break;
+                if (e != cudaErrorNotReady) {
+                        status = set_error(GZG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+                        break;
+                }
+                const int64_t us =
+                    std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+                if (limit_us > 0 && us >= limit_us) {
+                        status = set_error(GZG_ERR_TIMEOUT, std::string(what) + ": no completion within " +
+                                                                std::to_string(limit_us) + " us (GZG_WAIT_LIMIT_US)");
+                        break;
+                }
+                // spin with yields for the first 2 ms (batch chunks finish in
+                // well under that), then poll every 50 us
+                if (us < 2000)
+                        std::this_thread::yield();
+                else
+                        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+        cudaEventDestroy(ev);
+        return status;
+}
+
 gzg_status gzg::kernel_fault(uint32_t w) {
         std::string m = "kernel error word " + std::to_string(w) + ":";
         if (w & kErrStackOverflow) m += " traversal stack overflow";
@@ -243,9 +284,16 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
         const bool direct = is_pinned(rays) && is_pinned(tmax) && is_pinned(results);
         const int64_t nchunks = (count + kChunk - 1) / kChunk;
         char *res = reinterpret_cast<char *>(results);
+        // A wait that ran out leaves chunks in flight on the staging streams:
+        // their buffers are left to them (never freed nor pooled again).
+        auto abandon = [&](gzg_status s) -> gzg_status {
+                if (s == GZG_ERR_TIMEOUT) stg.release();
+                return s;
+        };
         auto drain = [&](int64_t c) -> gzg_status {
                 const int k = (int)(c % kSlots);
-                GZG_CK(cudaStreamSynchronize(stg->st[k]), "batch chunk");
+                const gzg_status ws = wait_stream(stg->st[k], "batch chunk");
+                if (ws != GZG_OK) return ws;
                 const int64_t off = c * kChunk, n = std::min(kChunk, count - off);
                 std::memcpy(res + off * out_bytes, stg->h_out[k], (size_t)n * out_bytes);
                 return GZG_OK;
@@ -259,7 +307,7 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
                 if (!direct) {
                         if (c >= kSlots) {
                                 st = drain(c - kSlots);
-                                if (st != GZG_OK) return st;
+                                if (st != GZG_OK) return abandon(st);
                         }
                         std::memcpy(stg->h_in[k], rays + off, (size_t)n * sizeof(gzg_ray));
                         std::memcpy(stg->h_tmax[k], tmax + off, (size_t)n * sizeof(float));
@@ -280,10 +328,13 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
         if (!direct) {
                 for (int64_t c = std::max<int64_t>(0, nchunks - kSlots); c < nchunks; ++c) {
                         st = drain(c);
-                        if (st != GZG_OK) return st;
+                        if (st != GZG_OK) return abandon(st);
                 }
         }
-        for (int k = 0; k < kSlots; ++k) GZG_CK(cudaStreamSynchronize(stg->st[k]), "batch sync");
+        for (int k = 0; k < kSlots; ++k) {
+                st = wait_stream(stg->st[k], "batch sync");
+                if (st != GZG_OK) return abandon(st);
+        }
         s->release(std::move(stg));
         uint32_t w = 0;
         st = read_error_word(s, &w, true);

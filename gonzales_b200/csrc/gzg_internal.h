@@ -19,6 +19,14 @@ gzg_status clear_error();
 // (stack overflow, step cap, index out of range) into the message.
 gzg_status kernel_fault(uint32_t word);
 
+// Host wait for the work queued so far on `stream` (a cudaStream_t; NULL =
+// the legacy default stream): polls an event with cudaEventQuery, yielding
+// between polls, for at most the wait limit, GZG_WAIT_LIMIT_US in the
+// environment (microseconds; default 300 s; 0 = no limit).  GZG_ERR_TIMEOUT
+// when the limit runs out: the queued work keeps running, so the caller must
+// leave its buffers to it.
+gzg_status wait_stream(void *stream, const char *what);
+
 // ------------------------------------------------------------------ layouts
 
 // Wide node: 8 children, 80 bytes, fetched as five 16-byte loads.

@@ -33,6 +33,7 @@
 // (primal pass, then replay with the same samples) and accumulates
 // dLoss/dtexel and dLoss/dscale.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -45,6 +46,22 @@
 #include "gzg_internal.h"
 #include "kernels.h"
 #include "sobol.cuh"
+
+namespace gzg {
+
+// An NVTX range (push on construction, pop on end() or destruction), marking
+// one wavefront stage's launches for a profiler; a no-op without one.
+struct NvtxRange {
+        bool open = true;
+        explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+        void end() {
+                if (open) nvtxRangePop();
+                open = false;
+        }
+        ~NvtxRange() { end(); }
+};
+
+}  // namespace gzg
 
 namespace gzg {
 
@@ -1878,16 +1895,23 @@ struct gzg_renderer {
                         if (lp_closest.traversal == GZG_TRAVERSAL_BVH2) lp_closest.traversal = GZG_TRAVERSAL_WIDE;
                         if (lp_any.traversal == GZG_TRAVERSAL_BVH2) lp_any.traversal = GZG_TRAVERSAL_WIDE;
                 }
-                k_generate<<<grid, block, 0, st>>>(w);
+                NvtxRange wave_range("gzg wave");
+                {
+                        NvtxRange r("gzg generate");
+                        k_generate<<<grid, block, 0, st>>>(w);
+                }
                 int cur = 0;
                 for (int b = 0; b < max_depth; ++b) {
                         k_clear_counts<<<1, 1, 0, st>>>(w, cur ^ 1);
                         LaunchParams lp = lp_closest, lpa = lp_any;
                         lp.n_dev = w.counts + cur;
                         lp.inst_out = w.hit_inst;
+                        NvtxRange extend_range("gzg extend");
                         cudaError_t e = launch_trace(view, lp, kRayDevice, kOutHit, w.q_ray[cur], nullptr, w.capacity,
                                                      w.hits, st);
                         if (e != cudaSuccess) return e;
+                        extend_range.end();
+                        NvtxRange shade_range("gzg shade");
                         const int sorted = w.sort_key != kSortNone;
                         if (sorted) {
                                 k_sort_count<<<grid, block, 0, st>>>(w, view, cur);
@@ -1903,10 +1927,14 @@ struct gzg_renderer {
                         } else {
                                 k_shade<kShadeDiffuse><<<grid, block, 0, st>>>(w, view, b, cur, sorted);
                         }
+                        shade_range.end();
+                        NvtxRange shadow_range("gzg shadow");
                         lpa.n_dev = w.counts + kCountShadow;
                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
+                        shadow_range.end();
+                        NvtxRange probe_range("gzg probe");
                         if (corrected) {
                                 if (probe_any) {
                                         lpa.n_dev = w.counts + kCountProbe;
@@ -1924,6 +1952,7 @@ struct gzg_renderer {
                         k_bounce_tally<<<1, 1, 0, st>>>(w, cur);
                         cur ^= 1;
                 }
+                NvtxRange accumulate_range("gzg accumulate");
                 if (w.mode == kPrimal) {
                         k_store_total<<<grid, block, 0, st>>>(w);  // the replay runs the same paths
                         return cudaGetLastError();
@@ -2567,7 +2596,7 @@ GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *p
                 if ((st = cuda_err(cudaMemset(d_w, 0, pix * 4), "film clear"))) break;
                 if (d_sq && (st = cuda_err(cudaMemset(d_sq, 0, 3 * pix * 4), "film clear"))) break;
                 if ((st = r->render(d_rgb, d_sq, d_w, nullptr))) break;
-                if ((st = cuda_err(cudaDeviceSynchronize(), "render"))) break;
+                if ((st = wait_stream(nullptr, "gzg_render_image"))) break;
                 if ((st = cuda_err(cudaMemcpy(film_rgb, d_rgb, 3 * pix * 4, cudaMemcpyDeviceToHost), "film copy"))) break;
                 if ((st = cuda_err(cudaMemcpy(film_w, d_w, pix * 4, cudaMemcpyDeviceToHost), "film copy"))) break;
                 if (d_sq && (st = cuda_err(cudaMemcpy(film_sq, d_sq, 3 * pix * 4, cudaMemcpyDeviceToHost), "film copy")))
@@ -2578,6 +2607,9 @@ GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *p
                 if (word) st = set_error(GZG_ERR_KERNEL_FAULT, "render: kernel error word " + std::to_string(word));
         } while (false);
         if (prev != r->device) cudaSetDevice(prev);
+        // after a wait that ran out the frame is still rendering into the
+        // renderer's buffers and the films: they are left to it
+        if (st == GZG_ERR_TIMEOUT) hold.release();
         if (!st) clear_error();
         return st;
 }

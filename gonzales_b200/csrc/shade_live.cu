@@ -189,16 +189,18 @@ extern "C" GZG_API gzg_status gzg_gpu_shade_batch(gzg_scene *scene, gzg_path_sta
                 k_shade_live<<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
                     view, static_cast<gzg_path_state *>(d_paths), static_cast<const gzg_intersection *>(d_isects), count);
                 if ((e = cudaGetLastError()) != cudaSuccess ||
-                    (e = cudaMemcpyAsync(paths, d_paths, pb, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-                    (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+                    (e = cudaMemcpyAsync(paths, d_paths, pb, cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
                         status = cuda_fail2(e, "shade");
                         break;
                 }
+                status = wait_stream(st, "gzg_gpu_shade_batch");
         } while (false);
+        // stream-ordered frees: after a wait that ran out (the copy back may
+        // still be writing `paths`) they run when the stream's work is done
         if (d_paths) cudaFreeAsync(d_paths, st);
         if (d_isects) cudaFreeAsync(d_isects, st);
         if (st) {
-                cudaStreamSynchronize(st);
+                if (status != GZG_ERR_TIMEOUT) cudaStreamSynchronize(st);
                 cudaStreamDestroy(st);
         }
         if (!status) {

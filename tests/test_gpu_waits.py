@@ -1,0 +1,37 @@
+"""Bounded host waits.  Every host wait of the batch calls polls an event for
+at most GZG_WAIT_LIMIT_US microseconds (default 300 s) and then returns
+GZG_ERR_TIMEOUT instead of blocking; the call's queued work keeps running and
+its staging buffers are left to it.  The limit is made to run out on the host
+(1 us, far below the time a chunk of rays needs): nothing faults or hangs on
+the GPU.  Afterwards the same scene handle serves new calls unchanged.
+"""
+import numpy as np
+import pytest
+
+from gonzales_b200 import GpuAccelerator, GzgError, scenes
+
+pytestmark = pytest.mark.gpu
+
+GZG_ERR_TIMEOUT = 8
+
+
+def test_wait_limit_returns_timeout_and_scene_stays_usable(monkeypatch):
+    import torch
+
+    hs = scenes.raycast_scene(subdiv=6).build()
+    o, d, t = scenes.raycast_rays(hs, 2048, 1024, 4_000_000, seed=0x77)
+    rays6 = scenes.pack_reference_rays(o, d)
+    with GpuAccelerator(hs) as acc:
+        ref = acc.intersect_batch(rays6[:5000], t[:5000])
+        monkeypatch.setenv("GZG_WAIT_LIMIT_US", "1")
+        with pytest.raises(GzgError) as e:
+            acc.intersect_batch(rays6, t)
+        assert e.value.status == GZG_ERR_TIMEOUT
+        assert "GZG_WAIT_LIMIT_US" in str(e.value)
+        monkeypatch.delenv("GZG_WAIT_LIMIT_US")
+        torch.cuda.synchronize()  # the abandoned chunks run to the end
+        again = acc.intersect_batch(rays6[:5000], t[:5000])
+        assert again.tobytes() == ref.tobytes()
+        full = acc.intersect_batch(rays6, t)
+        assert full[:5000].tobytes() == ref.tobytes()
+        assert acc.error_word() == 0
