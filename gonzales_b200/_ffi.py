@@ -100,7 +100,17 @@ class RenderParams(C.Structure):
                 ("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
                 ("filter_radius", C.c_float), ("filter_sigma", C.c_float), ("first_sample", C.c_int32),
                 ("sampler_spp", C.c_int32), ("wave_paths", C.c_int32), ("use_graph", C.c_int32),
-                ("lens_radius", C.c_float), ("focal_distance", C.c_float), ("two_sided_emission", C.c_int32)]
+                ("lens_radius", C.c_float), ("focal_distance", C.c_float), ("two_sided_emission", C.c_int32),
+                ("crop", C.c_int32 * 4)]
+
+    @property
+    def film_width(self):
+        """Width of the film: the crop window's, or the frame's."""
+        return self.crop[2] - self.crop[0] if any(self.crop) else self.width
+
+    @property
+    def film_height(self):
+        return self.crop[3] - self.crop[1] if any(self.crop) else self.height
 
 
 class RenderStats(C.Structure):
@@ -111,14 +121,14 @@ class RenderStats(C.Structure):
 def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
                   eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
                   filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, wave_paths=0, use_graph=0,
-                  lens_radius=0.0, focal_distance=1e6, two_sided_emission=0):
+                  lens_radius=0.0, focal_distance=1e6, two_sided_emission=0, crop=None):
     """gzg_render_params with the reference's defaults (Gaussian filter radius 2,
     sigma 0.5; Z-Sobol seed 1234; roulette from bounce 2; pinhole camera,
     focal distance 1e6)."""
     return RenderParams(width, height, spp, max_depth, rr_min_bounce, mis_corrected, seed, (C.c_float * 3)(*eye),
                         (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
                         first_sample, sampler_spp, wave_paths, use_graph, lens_radius, focal_distance,
-                        two_sided_emission)
+                        two_sided_emission, (C.c_int32 * 4)(*(crop or (0, 0, 0, 0))))
 
 
 SORT_NONE, SORT_MATERIAL, SORT_SCENE = 0, 1, 2

@@ -253,7 +253,7 @@ class GpuAccelerator:
     def render(self, params):
         """Renders on the device (gzg_render_image); returns host film sums
         (rgb (H, W, 3), squares (H, W, 3), weights (H, W)) and statistics."""
-        W, H = params.width, params.height
+        W, H = params.film_width, params.film_height
         rgb = np.zeros((H, W, 3), np.float32)
         sq = np.zeros((H, W, 3), np.float32)
         w = np.zeros((H, W), np.float32)
@@ -476,7 +476,7 @@ class BatchRenderer(Renderer):
         out = []
         for k, p in enumerate(self.params):
             part = film[self.offsets[k]:self.offsets[k + 1]]
-            out.append(part.reshape((p.height, p.width) + tuple(part.shape[1:])))
+            out.append(part.reshape((p.film_height, p.film_width) + tuple(part.shape[1:])))
         return out
 
     def autotune(self, stream=None):

@@ -126,7 +126,7 @@ class DifferentiableRenderer:
         import torch
 
         self.bind(texels, emission_scale)
-        H, W = self.params.height, self.params.width
+        H, W = self.params.film_height, self.params.film_width
         dt = torch.float64 if f64 else torch.float32
         rgb = torch.zeros((H, W, 3), dtype=dt, device=texels.device)
         w = torch.zeros((H, W), dtype=dt, device=texels.device)

@@ -304,6 +304,7 @@ struct SceneConst {
         float filter_radius, filter_sigma;
         float lens_radius, focal_distance;  // thin lens (0: pinhole)
         int32_t width, height, spp, max_depth, rr_min, mis_corrected, first_sample;
+        int32_t crop_x0, crop_y0, crop_w, crop_h;  // film window (the whole frame without a crop)
         int32_t light_begin, light_count;  // light_count includes the environment light
         float light_total;
         int32_t env_index;                 // scene-local index of the environment light or -1
@@ -793,7 +794,8 @@ __global__ void k_generate(Wave w) {
         const uint64_t q = path - sc.path_begin;
         const uint32_t pixel = (uint32_t)(q / (uint64_t)sc.spp);
         const uint32_t sample = (uint32_t)(q % (uint64_t)sc.spp) + (uint32_t)sc.first_sample;
-        const uint32_t px = pixel % (uint32_t)sc.width, py = pixel / (uint32_t)sc.width;
+        const uint32_t px = (uint32_t)sc.crop_x0 + pixel % (uint32_t)sc.crop_w,
+                       py = (uint32_t)sc.crop_y0 + pixel / (uint32_t)sc.crop_w;
         ZSobol z;
         V3 org, dir;
         float weight;
@@ -820,7 +822,8 @@ __global__ void k_camera_rays(SceneConst sc, uint64_t first, uint64_t n, float *
         const uint64_t q = first + i;
         const uint32_t pixel = (uint32_t)(q / (uint64_t)sc.spp);
         const uint32_t sample = (uint32_t)(q % (uint64_t)sc.spp) + (uint32_t)sc.first_sample;
-        const uint32_t px = pixel % (uint32_t)sc.width, py = pixel / (uint32_t)sc.width;
+        const uint32_t px = (uint32_t)sc.crop_x0 + pixel % (uint32_t)sc.crop_w,
+                       py = (uint32_t)sc.crop_y0 + pixel / (uint32_t)sc.crop_w;
         ZSobol z;
         V3 org, dir;
         float w;
@@ -1763,6 +1766,11 @@ SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices
         sc.filter_sigma = P.filter_sigma;
         sc.width = P.width;
         sc.height = P.height;
+        const bool cropped = P.crop[0] || P.crop[1] || P.crop[2] || P.crop[3];
+        sc.crop_x0 = cropped ? P.crop[0] : 0;
+        sc.crop_y0 = cropped ? P.crop[1] : 0;
+        sc.crop_w = cropped ? P.crop[2] - P.crop[0] : P.width;
+        sc.crop_h = cropped ? P.crop[3] - P.crop[1] : P.height;
         sc.spp = P.spp;
         sc.max_depth = P.max_depth;
         sc.rr_min = P.rr_min_bounce;
@@ -1777,11 +1785,21 @@ SceneConst make_scene_const(const gzg_render_params &P, const uint32_t *matrices
         return sc;
 }
 
+// Pixels of a frame's film: its crop window's, or the whole frame's.
+int64_t film_pixels(const gzg_render_params &P) {
+        if (P.crop[0] || P.crop[1] || P.crop[2] || P.crop[3])
+                return (int64_t)(P.crop[2] - P.crop[0]) * (P.crop[3] - P.crop[1]);
+        return (int64_t)P.width * P.height;
+}
+
 bool params_ok(const gzg_render_params &P) {
         const bool lens_ok = P.lens_radius == 0.0f ||
                              (std::isfinite(P.lens_radius) && P.lens_radius > 0.0f && std::isfinite(P.focal_distance) &&
                               P.focal_distance > 0.0f);
-        return P.width > 0 && P.height > 0 && P.spp > 0 && P.max_depth >= 0 && P.fov_deg > 0.0f &&
+        const bool cropped = P.crop[0] || P.crop[1] || P.crop[2] || P.crop[3];
+        const bool crop_ok = !cropped || (P.crop[0] >= 0 && P.crop[1] >= 0 && P.crop[0] < P.crop[2] &&
+                                          P.crop[1] < P.crop[3] && P.crop[2] <= P.width && P.crop[3] <= P.height);
+        return crop_ok && P.width > 0 && P.height > 0 && P.spp > 0 && P.max_depth >= 0 && P.fov_deg > 0.0f &&
                P.filter_sigma > 0.0f && P.filter_radius > 0.0f && P.first_sample >= 0 && P.sampler_spp >= 0 && lens_ok;
 }
 
@@ -2074,8 +2092,8 @@ gzg_status build_batch(gzg_renderer *r) {
                 r->consts[k] = make_scene_const(r->params[k], matrices);
                 r->consts[k].path_begin = paths;
                 r->consts[k].film_offset = (uint32_t)r->film_offsets[k];
-                r->film_offsets[k + 1] = r->film_offsets[k] + (int64_t)r->params[k].width * r->params[k].height;
-                paths += (uint64_t)r->params[k].width * r->params[k].height * r->params[k].spp;
+                r->film_offsets[k + 1] = r->film_offsets[k] + film_pixels(r->params[k]);
+                paths += (uint64_t)film_pixels(r->params[k]) * r->params[k].spp;
         }
         if (r->film_offsets[n] >= (int64_t)0xFFFFFFFFll)
                 return set_error(GZG_ERR_LIMIT, "renderer: more than 2^32 film pixels in a batch");
@@ -2542,9 +2560,9 @@ GZG_API gzg_status gzg_camera_rays(const gzg_render_params *params, int64_t firs
         if (!params || first_path < 0 || count < 0 || (count > 0 && (!rays || !weights || !pixels)))
                 return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: null argument or negative range");
         if (!params_ok(*params)) return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: bad render parameters");
-        const int64_t total = (int64_t)params->width * params->height * params->spp;
+        const int64_t total = film_pixels(*params) * params->spp;
         if (first_path > total || count > total - first_path)
-                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: paths beyond width x height x spp");
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_camera_rays: paths beyond the film's pixels x spp");
         if (count == 0) return clear_error();
         int dev = 0;
         cudaGetDevice(&dev);
@@ -2584,7 +2602,7 @@ GZG_API gzg_status gzg_render_image(gzg_scene *scene, const gzg_render_params *p
         gzg_status st = gzg_renderer_create(scene, params, &r);
         if (st) return st;
         std::unique_ptr<gzg_renderer> hold(r);
-        const size_t pix = (size_t)params->width * params->height;
+        const size_t pix = (size_t)film_pixels(*params);
         float *d_rgb = nullptr, *d_sq = nullptr, *d_w = nullptr;
         if ((st = r->alloc(&d_rgb, 3 * pix)) || (st = r->alloc(&d_w, pix))) return st;
         if (film_sq && (st = r->alloc(&d_sq, 3 * pix))) return st;

@@ -27,7 +27,8 @@ from . import _ffi as F
 def camera_rays(params, first, count):
     """Camera rays of paths [first, first + count) of the frame in params
     (gzg_camera_rays): (rays (n, 6) float32 Ray_C, weights (n,) float32,
-    pixels (n,) int32; pixel = y * width + x)."""
+    pixels (n,) int32: the film pixel, (y - y0) * film width + (x - x0) within
+    the crop window, y * width + x without one)."""
     rays = np.zeros((count, 6), np.float32)
     w = np.zeros(count, np.float32)
     px = np.zeros(count, np.int32)
@@ -44,7 +45,7 @@ def render_tile_loop(accel, params, seed=0, batch_paths=1 << 20, iso=100.0, max_
     Api/RenderConfiguration.swift:208-211).  Returns the film sums
     (light (H, W, 3) float64, weight (H, W) float64) and per-bounce counts of
     the rays traced."""
-    W, H, spp = params.width, params.height, params.spp
+    W, H, spp = params.film_width, params.film_height, params.spp
     total = W * H * spp
     rng = np.random.Generator(np.random.PCG64(seed))
     light = np.zeros((H * W, 3), np.float64)

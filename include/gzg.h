@@ -541,6 +541,11 @@ typedef struct gzg_render_params {
                                        (AreaLight.emittedRadiance, Light/AreaLight.swift:13-19);
                                        1: on both sides, as the live shading step counts any hit
                                        on an emitter (shade_core, kernel.mojo:696-701) */
+        int32_t crop[4];         /* crop window in pixels [x0, x1) x [y0, y1) as {x0, y0, x1, y1}
+                                    (Film's crop, the pixels Film.getSampleBounds covers,
+                                    Core/Film.swift:7-27); all 0: the whole frame.  The camera and
+                                    the sampler keep the whole frame; films hold the window's
+                                    pixels only, row-major, (x1 - x0) x (y1 - y0) */
 } gzg_render_params;
 
 typedef struct gzg_renderer gzg_renderer;
@@ -673,8 +678,9 @@ GZG_API gzg_status gzg_zsobol_fill_device(int64_t samples_per_pixel, int32_t res
 /* Camera rays of Tile.render's first phase (Core/Tile.swift:27-59) for host
  * callers that drive the bounce loop through gzg_gpu_traverse_batch and
  * gzg_gpu_shade_batch themselves: for paths [first_path, first_path + count)
- * of the frame described by params (path = pixel * spp + sample, pixel =
- * y * width + x; samples first_sample + sample of the Z-Sobol sampler) writes
+ * of the frame described by params (path = pixel * spp + sample, pixel = the
+ * film pixel, row-major over the crop window or the whole frame; samples
+ * first_sample + sample of the Z-Sobol sampler) writes
  * the Ray_C record (camera-space sample through the Gaussian filter and the
  * perspective camera, Sampler.getCameraSample + PerspectiveCamera.generateRay),
  * the ray weight (filter value / filter pdf, Tile.swift:36-40) and the pixel

@@ -1215,18 +1215,22 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
 
         const orc_render_params &P = *params;
         const float film_scale = (P.iso > 0.0f ? P.iso : 100.0f) / 100.0f;
-        const int W = P.width, H = P.height;
+        // the film window: the crop (Film.getSampleBounds) or the whole frame
+        const bool cropped = P.crop[0] || P.crop[1] || P.crop[2] || P.crop[3];
+        const int x0 = cropped ? P.crop[0] : 0, y0 = cropped ? P.crop[1] : 0;
+        const int x1 = cropped ? P.crop[2] : P.width, y1 = cropped ? P.crop[3] : P.height;
+        const int FW = x1 - x0;
         const Camera cam(P);
         if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-        std::atomic<int> next_row{0};
+        std::atomic<int> next_row{y0};
         std::vector<uint64_t> cnt(4 * threads, 0);
         std::vector<std::thread> pool;
         for (int ti = 0; ti < threads; ++ti)
                 pool.emplace_back([&, ti]() {
                         for (;;) {
                                 const int py = next_row.fetch_add(1);
-                                if (py >= H) break;
-                                for (int px = 0; px < W; ++px) {
+                                if (py >= y1) break;
+                                for (int px = x0; px < x1; ++px) {
                                         float acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0}, accw = 0.0f;
                                         float acca[3] = {0, 0, 0}, accn[3] = {0, 0, 0};
                                         for (int si = 0; si < P.spp; ++si) {
@@ -1257,7 +1261,7 @@ extern "C" void orc_render_ex(const orc_node *nodes, const orc_prim_id *prims, c
                                                 }
                                                 accw += w;
                                         }
-                                        const size_t pix = (size_t)py * W + px;
+                                        const size_t pix = (size_t)(py - y0) * FW + (px - x0);
                                         for (int c = 0; c < 3; ++c) {
                                                 sum_rgb[3 * pix + c] += acc[c];
                                                 if (sum_sq) sum_sq[3 * pix + c] += acc2[c];
@@ -1337,6 +1341,10 @@ extern "C" void orc_gaussian_sample_1d(float u, float radius, float sigma, float
 extern "C" void orc_camera_rays(const orc_render_params *params, int64_t first, int64_t count, float *rays6,
                                 float *weights, int32_t *pixels) {
         const Camera cam(*params);
+        const int32_t *cr = params->crop;
+        const bool cropped = cr[0] || cr[1] || cr[2] || cr[3];
+        const int x0 = cropped ? cr[0] : 0, y0 = cropped ? cr[1] : 0;
+        const int fw = cropped ? cr[2] - cr[0] : params->width;
         for (int64_t i = 0; i < count; ++i) {
                 const int64_t q = first + i;
                 const int64_t pixel = q / params->spp;
@@ -1344,7 +1352,7 @@ extern "C" void orc_camera_rays(const orc_render_params *params, int64_t first, 
                 orc_zsobol smp;
                 V3 org, dir;
                 float w;
-                cam.ray((int)(pixel % params->width), (int)(pixel / params->width), sample, &smp, &org, &dir, &w);
+                cam.ray(x0 + (int)(pixel % fw), y0 + (int)(pixel / fw), sample, &smp, &org, &dir, &w);
                 float *r = rays6 + 6 * i;
                 r[0] = org.x;
                 r[1] = org.y;

@@ -113,6 +113,7 @@ typedef struct orc_render_params {
         float medium_min[3], medium_max[3];
         float sigma_a[3], sigma_s[3];
         float medium_g;
+        int32_t crop[4];  /* film window {x0, y0, x1, y1} in pixels; all 0: the whole frame */
 } orc_render_params;
 
 /* Renders the scene; per pixel (row-major) accumulates the film sums of the

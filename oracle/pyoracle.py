@@ -212,13 +212,14 @@ class RenderParams(C.Structure):
                 ("sampler_spp", C.c_int32), ("iso", C.c_float), ("max_component", C.c_float),
                 ("lens_radius", C.c_float), ("focal_distance", C.c_float), ("two_sided_emission", C.c_int32),
                 ("has_medium", C.c_int32), ("medium_min", C.c_float * 3), ("medium_max", C.c_float * 3),
-                ("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("medium_g", C.c_float)]
+                ("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("medium_g", C.c_float),
+                ("crop", C.c_int32 * 4)]
 
 
 def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_corrected=0, seed=1234,
                   eye=(0.5, 0.5, 2.2), target=(0.5, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0,
                   filter_radius=2.0, filter_sigma=0.5, first_sample=0, sampler_spp=0, iso=100.0, max_component=0.0,
-                  lens_radius=0.0, focal_distance=1e6, two_sided_emission=0, medium=None):
+                  lens_radius=0.0, focal_distance=1e6, two_sided_emission=0, medium=None, crop=None):
     """medium: None or dict(box_min, box_max, sigma_a, sigma_s, g)."""
     m = medium or {}
     f3 = lambda k: (C.c_float * 3)(*m.get(k, (0.0, 0.0, 0.0)))  # noqa: E731
@@ -226,7 +227,7 @@ def render_params(width, height, spp, max_depth=5, rr_min_bounce=2, mis_correcte
                         (C.c_float * 3)(*target), (C.c_float * 3)(*up), fov_deg, filter_radius, filter_sigma,
                         first_sample, sampler_spp, iso, max_component, lens_radius, focal_distance,
                         two_sided_emission, 1 if medium else 0, f3("box_min"), f3("box_max"), f3("sigma_a"),
-                        f3("sigma_s"), float(m.get("g", 0.0)))
+                        f3("sigma_s"), float(m.get("g", 0.0)), (C.c_int32 * 4)(*(crop or (0, 0, 0, 0))))
 
 
 class _Textures(C.Structure):
@@ -360,6 +361,8 @@ def render(hs, params, threads=0, textures=None, env=None, instances=None, aovs=
         mparams = np.ascontiguousarray(hs.material_params, np.float32)
         keep.append(mparams)
     W, H = params.width, params.height
+    if any(params.crop):  # the film holds the crop window only
+        W, H = params.crop[2] - params.crop[0], params.crop[3] - params.crop[1]
     s = np.zeros((H, W, 3), np.float32)
     s2 = np.zeros((H, W, 3), np.float32)
     sw = np.zeros((H, W), np.float32)
