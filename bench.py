@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--small", action="store_true", help="small case for profiler captures")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-batch", action="store_true", help="omit the scene-batch and adjoint legs")
-    ap.add_argument("--case", default=None, choices=["instanced-small", "build", "incoherent", "coherent"],
+    ap.add_argument("--case", default=None, choices=["instanced-small", "build", "incoherent", "coherent", "mixed"],
                     help="run one small case alone (profiler captures) and print its own JSON line")
     return ap.parse_args()
 
@@ -731,6 +731,19 @@ def run_ours(args):
         tt = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
+    # the same through the compact-result call (16-byte hits back)
+    hits_h = torch.zeros((n, 4), dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        acc.intersect_batch_hits(rays_h.numpy(), tmax_h.numpy(), out=hits_h.numpy())
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        acc.intersect_batch_hits(rays_h.numpy(), tmax_h.numpy(), out=hits_h.numpy())
+    e2e_compact_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        tt = torch.tensor([e2e_compact_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_compact_s = float(tt.item())
 
     render = render_leg(acc_box=None, args=args, stream=stream, barrier=barrier) if not args.small else None
     build = build_leg(hs, rays_d, args, stream, barrier) if not (args.small or args.skip_batch) else None
@@ -777,6 +790,9 @@ def run_ours(args):
             "e2e": {"value": world * n / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": n * 28,
                     "d2h_bytes_per_step": n * 48, "call": "gzg_gpu_traverse_batch (pinned host Ray_C + tMax -> "
                                                          "Intersection_C)"},
+            "e2e_compact": {"value": world * n / e2e_compact_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": n * 28,
+                            "d2h_bytes_per_step": n * 16,
+                            "call": "gzg_gpu_traverse_batch_hits (pinned host Ray_C + tMax -> 16-byte hits)"},
             "gpu_launches": args.steps,  # closest-hit launches in the timed region of `value`
             "clocks": sampler.summary(),
         }
@@ -808,9 +824,11 @@ def run_case(args):
                        the general materials (after one warm-up frame)
       build            the device tree build of the ray-cast mesh (three builds)
       incoherent       the ray-cast mesh's 8,388,608 incoherent rays alone:
-      coherent         or its 8,388,608 coherent rays alone; tuned launch,
-                       two warm-up closest-hit launches, then three timed ones
-                       (384 MiB of rays and hits on the device)"""
+      coherent         or its 8,388,608 coherent rays alone,
+      mixed            or all 16,777,216 rays (the bench's launch); tuned
+                       launch, two warm-up closest-hit launches, then three
+                       timed ones inside a profiler range (384 MiB or 768 MiB
+                       of rays and hits on the device)"""
     import torch
 
     from gonzales_b200 import GpuAccelerator, InstancedAccelerator, Renderer, scenes
@@ -842,10 +860,10 @@ def run_case(args):
         acc.close()
         for b in blas:
             b.close()
-    elif args.case in ("incoherent", "coherent"):
+    elif args.case in ("incoherent", "coherent", "mixed"):
         cfg, hs, o, d, t, name = workload(False, 0)
         nc = cfg["width"] * cfg["height"]
-        sl = slice(nc, len(t)) if args.case == "incoherent" else slice(0, nc)
+        sl = {"incoherent": slice(nc, len(t)), "coherent": slice(0, nc), "mixed": slice(0, len(t))}[args.case]
         rays = torch.from_numpy(scenes.pack_device_rays(o[sl], d[sl], t[sl])).cuda()
         hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
         with GpuAccelerator(hs) as acc:

@@ -160,6 +160,7 @@ PROTOTYPES = {
     "gzg_gpu_upload_scene": (ST, [VP, I64, VP, I64, VP, I64, VP, VP, VP, VP, I64, C.POINTER(VP)]),
     "gzg_gpu_free_scene": (ST, [VP]),
     "gzg_gpu_traverse_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
+    "gzg_gpu_traverse_batch_hits": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
     "gzg_gpu_occluded_batch": (ST, [VP, VP, VP, I64, VP, C.POINTER(TraceOptions)]),
     "gzg_gpu_traverse_batch_static": (ST, [VP, VP, VP, I64, VP]),
     "gzg_gpu_shade_batch": (ST, [VP, VP, I64, VP]),

@@ -178,6 +178,19 @@ class GpuAccelerator:
         F.check(F.lib().gzg_gpu_traverse_batch(self.handle, F.ptr(rays), F.ptr(tmax), n, F.ptr(out), opt))
         return out
 
+    def intersect_batch_hits(self, rays, tmax, options=None, out=None):
+        """Closest hit for host rays with compact results
+        (gzg_gpu_traverse_batch_hits): (n, 4) float32 rows t, u, v, prim
+        (prim as int32 bits: index into the prim-id array, -1 on a miss)."""
+        rays = _host_rays(rays)
+        tmax = np.ascontiguousarray(tmax, dtype=np.float32)
+        n = len(tmax)
+        if out is None:
+            out = np.zeros((n, 4), np.float32)
+        opt = C.byref(options) if options is not None else None
+        F.check(F.lib().gzg_gpu_traverse_batch_hits(self.handle, F.ptr(rays), F.ptr(tmax), n, F.ptr(out), opt))
+        return out
+
     def occluded_batch(self, rays, tmax, options=None, out=None):
         rays = _host_rays(rays)
         tmax = np.ascontiguousarray(tmax, dtype=np.float32)

@@ -966,6 +966,11 @@ GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays,
         return host_batch(scene, rays, t_max_values, count, results, sizeof(gzg_intersection), kOutIntersection, options);
 }
 
+GZG_API gzg_status gzg_gpu_traverse_batch_hits(gzg_scene *scene, const gzg_ray *rays, const float *t_max_values,
+                                               int64_t count, gzg_hit_d *hits, const gzg_trace_options *options) {
+        return host_batch(scene, rays, t_max_values, count, hits, sizeof(gzg_hit_d), kOutHit, options);
+}
+
 GZG_API gzg_status gzg_gpu_occluded_batch(gzg_scene *scene, const gzg_ray *rays, const float *t_max_values,
                                           int64_t count, uint8_t *occluded, const gzg_trace_options *options) {
         return host_batch(scene, rays, t_max_values, count, occluded, 1, kOutOccluded, options);

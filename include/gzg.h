@@ -260,6 +260,17 @@ GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, const gzg_ray
 GZG_API gzg_status gzg_gpu_shade_batch(gzg_scene *scene, gzg_path_state *paths, int64_t count,
                                        const gzg_intersection *intersections);
 
+/* gzg_gpu_traverse_batch with compact results: one 16-byte gzg_hit_d per ray
+ * (t, u, v, prim = index into the uploaded prim-id array, -1 on a miss with
+ * t = tMax) instead of the 48-byte Intersection_C.  The host transfer is 28 +
+ * 16 bytes per ray instead of 28 + 48; a caller that keeps its prim array
+ * (as the Swift BoundingHierarchy does) reads the PrimId_C record from it by
+ * index.  No counterpart in the reference (its batch call returns
+ * Intersection_C records only). */
+GZG_API gzg_status gzg_gpu_traverse_batch_hits(gzg_scene *scene, const gzg_ray *rays,
+                                               const float *t_max_values, int64_t count,
+                                               gzg_hit_d *hits, const gzg_trace_options *options);
+
 /* Shadow / any-hit batch (new; Visibility.occluded, Core/Visibility.swift:5-24,
  * answers it with a closest-hit query, BoundingHierarchy.swift:348-384).
  * occluded[i] = 1 iff some triangle is hit with 0 < t <= tMax[i]. */

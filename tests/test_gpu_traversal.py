@@ -264,3 +264,20 @@ def test_full_size_raycast_parity():
         anyp = device_any(acc, o, d, t)
         assert np.all(anyp[idx >= 0] >= 0)
         assert acc.error_word() == 0
+
+
+def test_compact_host_batch_matches_drop_in_records():
+    """gzg_gpu_traverse_batch_hits: the 16-byte records carry the same hits
+    as the drop-in Intersection_C records (prim record = prims[index])."""
+    hs, o, d, t = H.small_raycast(subdiv=5, n_side=96, n_incoherent=30000)
+    r6 = scenes.pack_reference_rays(o, d)
+    with GpuAccelerator(hs) as acc:
+        full = acc.intersect_batch(r6, t)
+        hits = acc.intersect_batch_hits(r6, t)
+        assert acc.error_word() == 0
+    prim = hits[:, 3].view(np.int32)
+    assert np.array_equal(prim >= 0, full["hit"] != 0)
+    assert np.array_equal(H.bits(hits[:, 0]), H.bits(full["t_hit"]))
+    assert np.array_equal(H.bits(hits[:, 1]), H.bits(full["u"])) and np.array_equal(H.bits(hits[:, 2]), H.bits(full["v"]))
+    hit = prim >= 0
+    assert full["prim_id"][hit].tobytes() == hs.prims[prim[hit]].tobytes()
