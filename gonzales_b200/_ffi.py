@@ -200,6 +200,7 @@ PROTOTYPES = {
     "gzg_renderer_adjoint": (ST, [VP, VP, VP, VP, VP, VP]),
     "gzg_render_image": (ST, [VP, C.POINTER(RenderParams), VP, VP, VP, C.POINTER(RenderStats)]),
     "gzg_camera_rays": (ST, [C.POINTER(RenderParams), I64, I64, VP, VP, VP]),
+    "gzg_host_instance_bounds_from_scenes": (ST, [VP, I64, VP, I64, VP]),
     "gzg_scene_set_medium": (ST, [VP, C.POINTER(Medium)]),
     "gzg_zsobol_fill_device": (ST, [I64, C.c_int32, C.c_int32, I64, VP, VP, VP, I64, VP, C.c_int32, VP, VP]),
     "gzg_scene_error_word": (ST, [VP, C.POINTER(C.c_uint32), C.c_int]),

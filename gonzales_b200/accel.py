@@ -346,9 +346,13 @@ class InstancedAccelerator:
 
         self.blas = list(blas_accels)
         self.instances = np.ascontiguousarray(instances, F.INSTANCE_DTYPE)
-        self.bounds = instance_bounds([a.host for a in self.blas], self.instances)
-        self.tlas_nodes, self.leaf_instance = build_bvh2(self.bounds)
         handles = (C.c_void_p * len(self.blas))(*[a.handle.value for a in self.blas])
+        # the top-level tree over the instances' bounds from their bottom-level
+        # trees (gzg_host_instance_bounds_from_scenes), as the scene uses them
+        self.bounds = np.zeros((len(self.instances), 6), np.float32)
+        F.check(F.lib().gzg_host_instance_bounds_from_scenes(handles, len(self.blas), F.ptr(self.instances),
+                                                             len(self.instances), F.ptr(self.bounds)))
+        self.tlas_nodes, self.leaf_instance = build_bvh2(self.bounds)
         h = C.c_void_p()
         F.check(F.lib().gzg_instanced_scene_create(handles, len(self.blas), F.ptr(self.instances),
                                                    len(self.instances), F.ptr(self.tlas_nodes),

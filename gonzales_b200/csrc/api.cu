@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -1114,6 +1115,90 @@ static void instance_world_bounds(const float *lo_hi, const float *m, float *out
         std::memcpy(out6 + 3, hi, 12);
 }
 
+// World bounds of an instance from its bottom-level wide tree: the boxes of
+// the root's children and, for interior children, of their children (up to
+// 64 boxes, decoded in double precision and rounded outward), each carried to
+// world space by its 8 corners, then united.  They contain the instance's
+// geometry as the root box's transformed corners do (the reference's
+// TransformedPrimitive.worldBound), but hug rotated shapes far more closely,
+// so rays enter fewer instances.
+static void instance_world_bounds_tree(const WideBvh &w, const float *root6, const float *m, float *out6) {
+        std::vector<std::array<double, 6>> boxes;
+        auto child_box = [](const WideNode &n, int s) {
+                std::array<double, 6> b;
+                const double p[3] = {n.px, n.py, n.pz};
+                const int e[3] = {n.ex, n.ey, n.ez};
+                for (int a = 0; a < 3; ++a) {
+                        const double step = std::ldexp(1.0, e[a] - 127);
+                        b[a] = p[a] + n.qlo[a][s] * step;
+                        b[3 + a] = p[a] + n.qhi[a][s] * step;
+                }
+                return b;
+        };
+        auto used = [](const WideNode &n, int s) { return ((n.imask >> s) & 1u) || (n.meta[s] & 0x80u); };
+        if (!w.nodes.empty()) {
+                const WideNode &root = w.nodes[0];
+                for (int s = 0; s < 8; ++s) {
+                        if (!used(root, s)) continue;
+                        if ((root.imask >> s) & 1u) {
+                                const uint32_t ci = root.child_base + (uint32_t)__builtin_popcount(root.imask & ((1u << s) - 1u));
+                                if (ci < w.nodes.size()) {
+                                        const WideNode &c = w.nodes[ci];
+                                        bool any = false;
+                                        for (int t = 0; t < 8; ++t)
+                                                if (used(c, t)) {
+                                                        boxes.push_back(child_box(c, t));
+                                                        any = true;
+                                                }
+                                        if (any) continue;
+                                }
+                        }
+                        boxes.push_back(child_box(root, s));
+                }
+        }
+        if (boxes.empty()) {
+                instance_world_bounds(root6, m, out6);
+                return;
+        }
+        double lo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, hi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+        for (const auto &b : boxes)
+                for (int i = 0; i < 8; ++i) {
+                        const double x = (i & 4) ? b[3] : b[0], y = (i & 2) ? b[4] : b[1], z = (i & 1) ? b[5] : b[2];
+                        for (int r = 0; r < 3; ++r) {
+                                const float *row = m + 4 * r;
+                                const double v = (double)row[0] * x + (double)row[1] * y + (double)row[2] * z + (double)row[3];
+                                lo[r] = std::min(lo[r], v);
+                                hi[r] = std::max(hi[r], v);
+                        }
+                }
+        for (int a = 0; a < 3; ++a) {
+                // outward to float, with a relative margin for the float
+                // transform the traversal applies to rays
+                const double mg = std::ldexp(std::max(std::fabs(lo[a]), std::fabs(hi[a])), -20);
+                out6[a] = std::nextafter((float)(lo[a] - mg), -HUGE_VALF);
+                out6[3 + a] = std::nextafter((float)(hi[a] + mg), HUGE_VALF);
+        }
+}
+
+GZG_API gzg_status gzg_host_instance_bounds_from_scenes(gzg_scene *const *blas, int64_t blas_count,
+                                                        const gzg_instance *inst, int64_t instance_count,
+                                                        float *bounds6) {
+        if (blas_count <= 0 || !blas || instance_count < 0 || (instance_count > 0 && (!inst || !bounds6)))
+                return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_host_instance_bounds_from_scenes: bad arguments");
+        for (int64_t b = 0; b < blas_count; ++b)
+                if (!blas[b] || blas[b]->instanced)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_host_instance_bounds_from_scenes: bottom-level scene " +
+                                                                       std::to_string(b) + " is NULL or two-level");
+        for (int64_t k = 0; k < instance_count; ++k) {
+                if (inst[k].blas < 0 || inst[k].blas >= blas_count)
+                        return set_error(GZG_ERR_INVALID_ARGUMENT, "gzg_host_instance_bounds_from_scenes: instance " +
+                                                                       std::to_string(k) + " references a missing bottom-level scene");
+                const gzg_scene *s = blas[inst[k].blas];
+                instance_world_bounds_tree(s->host_wide, s->root_bounds, inst[k].object_to_world, bounds6 + 6 * k);
+        }
+        return clear_error();
+}
+
 GZG_API gzg_status gzg_host_instance_bounds(const float *blas_bounds6, int64_t blas_count, const gzg_instance *inst,
                                             int64_t instance_count, float *bounds6) {
         if (blas_count < 0 || instance_count < 0 || (instance_count > 0 && (!blas_bounds6 || !inst || !bounds6)))
@@ -1148,7 +1233,7 @@ GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t bl
                 std::memcpy(&blas_bounds[6 * b], blas[b]->root_bounds, 24);
         }
         std::vector<float> ib((size_t)instance_count * 6);
-        gzg_status st = gzg_host_instance_bounds(blas_bounds.data(), blas_count, inst, instance_count, ib.data());
+        gzg_status st = gzg_host_instance_bounds_from_scenes(blas, blas_count, inst, instance_count, ib.data());
         if (st) return st;
         WideBvh tlas;
         int32_t tlas_bvh2_depth = 0;

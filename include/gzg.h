@@ -312,10 +312,21 @@ GZG_API gzg_status gzg_host_instance_bounds(const float *blas_bounds6, int64_t b
                                             const gzg_instance *instances, int64_t instance_count,
                                             float *bounds6);
 
+/* Tighter world bounds of each instance from its uploaded bottom-level scene:
+ * the boxes of the top two levels of its wide tree (up to 64, rounded
+ * outward) through object_to_world, united.  They contain the geometry like
+ * the root box's corners do but hug rotated shapes, so fewer rays enter an
+ * instance they miss; gzg_instanced_scene_create uses them for the top-level
+ * tree's leaf boxes, and a host building the top-level BVH2 should too. */
+GZG_API gzg_status gzg_host_instance_bounds_from_scenes(gzg_scene *const *blas, int64_t blas_count,
+                                                        const gzg_instance *instances, int64_t instance_count,
+                                                        float *bounds6);
+
 /* Creates a two-level scene from uploaded bottom-level scenes (each from
  * gzg_gpu_upload_scene; they stay owned by the caller and must outlive the
  * new scene), the instances, and a top-level BVH2 the host built over the
- * instance bounds (leaf prim k is instance tlas_leaf_instance[k]).  Only the
+ * instance bounds of gzg_host_instance_bounds_from_scenes (leaf prim k is
+ * instance tlas_leaf_instance[k]).  Only the
  * wide traversal runs on a two-level scene; hits report the bottom-level prim
  * index and, through gzg_trace_closest_instanced_device, the instance. */
 GZG_API gzg_status gzg_instanced_scene_create(gzg_scene *const *blas, int64_t blas_count,

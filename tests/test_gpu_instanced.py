@@ -128,3 +128,31 @@ def test_instanced_full_size_parity():
     H.record("parity_instanced.json", {"wide": counts, "info": info})
     assert counts["fail"] == 0, (counts, fails[:10])
     assert info["triangles"] == 16 * 50000
+
+
+def test_instance_bounds_from_trees_contain_geometry_and_are_tighter():
+    """gzg_host_instance_bounds_from_scenes: every vertex of every instance,
+    carried to world space, lies inside its box, and the boxes are no larger
+    than those from the bottom-level root box's corners (the reference's
+    TransformedPrimitive.worldBound)."""
+    from gonzales_b200.accel import instance_bounds
+
+    blas_hosts, inst = scenes.instanced_scene(n_meshes=4, n_u=30, n_v=40, n_instances=256, extent=5.0, seed=0xB5)
+    accs = [GpuAccelerator(b) for b in blas_hosts]
+    try:
+        iacc = InstancedAccelerator(accs, inst)
+        tight = iacc.bounds
+        loose = instance_bounds(blas_hosts, inst)
+        for k in range(len(inst)):
+            m = inst["object_to_world"][k].reshape(3, 4).astype(np.float64)
+            pts = blas_hosts[inst["blas"][k]].meshes[0].points[:, :3].astype(np.float64)
+            world = pts @ m[:, :3].T + m[:, 3]
+            assert np.all(world >= tight[k, :3] - 1e-6) and np.all(world <= tight[k, 3:] + 1e-6), k
+        vol_t = np.prod(tight[:, 3:] - tight[:, :3], axis=1)
+        vol_l = np.prod(loose[:, 3:] - loose[:, :3], axis=1)
+        assert np.all(vol_t <= vol_l * (1 + 1e-4))
+        assert vol_t.sum() < 0.9 * vol_l.sum()
+        iacc.close()
+    finally:
+        for a in accs:
+            a.close()
