@@ -821,7 +821,8 @@ def run_ours(args):
 def run_case(args):
     """Small single cases for profiler captures (one GPU):
       instanced-small  one 640 x 360, 16-spp frame of the two-level scene with
-                       the general materials (after one warm-up frame)
+                       the general materials and the medium, in 2^20-path
+                       waves (after one warm-up frame)
       build            the device tree build of the ray-cast mesh (three builds)
       incoherent       the ray-cast mesh's 8,388,608 incoherent rays alone:
       coherent         or its 8,388,608 coherent rays alone,
@@ -842,8 +843,9 @@ def run_case(args):
         acc.set_environment(scenes.sky_map(), 1.0)
         acc.set_medium(INSTANCED_MEDIUM)
         W, H, spp = 640, 360, 16
+        # a 2^20-path wave (about 0.37 GB) keeps profiler captures small
         p = F.render_params(W, H, spp, max_depth=8, rr_min_bounce=2, eye=(0.0, 6.0, 48.0), target=(0.0, 0.0, 0.0),
-                            use_graph=1)
+                            use_graph=1, wave_paths=1 << 20)
         rgb = torch.zeros((H, W, 3), device="cuda")
         w = torch.zeros((H, W), device="cuda")
         with Renderer(acc, p) as r:
