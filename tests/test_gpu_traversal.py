@@ -284,3 +284,48 @@ def test_compact_host_batch_matches_drop_in_records():
     # leaves its padding bytes unset, so fields are compared, not bytes)
     for f in ("id1", "id2", "material_index", "type"):
         assert np.array_equal(full["prim_id"][f][hit], hs.prims[f][prim[hit]])
+
+
+@pytest.fixture(scope="module")
+def full():
+    hs = scenes.raycast_scene(subdiv=8).build()
+    o, d, t = scenes.raycast_rays(hs, 4096, 2048, 8388608)
+    acc = GpuAccelerator(hs)
+    yield hs, acc, o, d, t
+    acc.close()
+
+
+def test_full_size_any_hit_exact(full):
+    """Any hit (a10, the shadow query) on the full ray-cast workload: every
+    reported prim is a valid Moller-Trumbore hit with 0 < t <= tMax, every ray
+    the oracle's closest hit hits is reported occluded, and a ray the oracle
+    misses is reported clear unless its reported prim is such a valid hit
+    (the reference's slab test culls a few)."""
+    hs, acc, o, d, t = full
+    isect, idx, _ = H.oracle_closest(hs, o, d, t)
+    anyp = device_any(acc, o, d, t)
+    assert np.all(anyp[idx >= 0] >= 0)
+    extra = np.nonzero((idx < 0) & (anyp >= 0))[0]
+    sample = np.concatenate([extra, np.nonzero(anyp >= 0)[0][::50000]])
+    for i in sample:
+        p0, p1, p2 = H.prim_triangle(hs, int(anyp[i]))
+        ok, tt, _, _ = O.mt(o[i], d[i], p0, p1, p2, float(t[i]))
+        assert ok and 0.0 < tt <= t[i], (i, anyp[i])
+    H.record("any_hit_full.json", {"rays": int(len(t)), "occluded": int((anyp >= 0).sum()),
+                                   "oracle_hits": int((idx >= 0).sum()), "occluded_where_oracle_misses": int(len(extra))})
+    assert len(extra) <= 1e-5 * len(t)
+    assert acc.error_word() == 0
+
+
+def test_full_size_watertight_parity(full):
+    """The watertight leaf test (Shape/Triangle.swift:269-352) in the wide
+    traversal on the full workload against the oracle's watertight traversal:
+    exact, a counted tie or a counted reference-culled hit on every ray."""
+    hs, acc, o, d, t = full
+    isect, idx, _ = H.oracle_closest(hs, o, d, t, watertight=True)
+    gpu = device_closest(acc, o, d, t, options(leaf_test=F.LEAF_WATERTIGHT))
+    counts, fails = _check(hs, o, d, t, gpu, isect, idx, watertight=True)
+    H.record("parity_full_watertight.json", counts)
+    assert counts["fail"] == 0, (counts, fails[:10])
+    assert counts["exact"] >= 0.9999 * counts["rays"], counts
+    assert acc.error_word() == 0
