@@ -66,12 +66,15 @@ constexpr int kSlots = 4;
 constexpr int64_t kChunk = 1 << 19;  // rays per pipelined chunk (512K x 4 streams: 2 % faster end to end than 1M x 3)
 
 // Per-call staging: device buffers and pinned host buffers for kSlots chunks
-// in flight, each slot with its own stream.
+// in flight, each slot with its own stream and its pull counter for the
+// persistent kernel (cleared on the slot's stream before each launch).
 struct Staging {
         cudaStream_t st[kSlots] = {};
         void *d_in[kSlots] = {}, *d_tmax[kSlots] = {}, *d_out[kSlots] = {};
         void *h_in[kSlots] = {}, *h_tmax[kSlots] = {}, *h_out[kSlots] = {};
+        uint32_t *d_sched = nullptr;  // one word per slot
         ~Staging() {
+                cudaFree(d_sched);
                 for (int k = 0; k < kSlots; ++k) {
                         if (st[k]) cudaStreamDestroy(st[k]);
                         cudaFree(d_in[k]);
@@ -163,6 +166,7 @@ struct gzg_scene {
                         }
                 }
                 auto s = std::make_unique<Staging>();
+                GZG_CK(cudaMalloc(&s->d_sched, kSlots * sizeof(uint32_t)), "staging schedule words");
                 for (int k = 0; k < kSlots; ++k) {
                         GZG_CK(cudaStreamCreateWithFlags(&s->st[k], cudaStreamNonBlocking), "staging stream");
                         GZG_CK(cudaMalloc(&s->d_in[k], kChunk * sizeof(gzg_ray_d)), "staging device buffer");
@@ -245,6 +249,7 @@ LaunchParams params_for(const gzg_scene *s, const gzg_trace_options *o, bool any
         p.counters = o ? reinterpret_cast<unsigned long long *>(o->fetch_counters) : nullptr;
         p.n_dev = nullptr;
         p.inst_out = nullptr;
+        p.sched = nullptr;
         return p;
 }
 
@@ -281,7 +286,7 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
         std::unique_ptr<Staging> stg;
         st = s->acquire(&stg);
         if (st != GZG_OK) return st;
-        const LaunchParams p = params_for(s, opt, out_fmt == kOutAnyPrim || out_fmt == kOutOccluded);
+        LaunchParams p = params_for(s, opt, out_fmt == kOutAnyPrim || out_fmt == kOutOccluded);
         const bool direct = is_pinned(rays) && is_pinned(tmax) && is_pinned(results);
         const int64_t nchunks = (count + kChunk - 1) / kChunk;
         char *res = reinterpret_cast<char *>(results);
@@ -319,6 +324,8 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
                        "ray upload");
                 GZG_CK(cudaMemcpyAsync(stg->d_tmax[k], src_tmax, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, stream),
                        "tMax upload");
+                p.sched = stg->d_sched + k;  // this slot's stream orders its launches
+                GZG_CK(cudaMemsetAsync(p.sched, 0, sizeof(uint32_t), stream), "schedule word");
                 GZG_CK(launch_trace(s->dev, p, kRayReference, out_fmt, stg->d_in[k],
                                     reinterpret_cast<const float *>(stg->d_tmax[k]), n, stg->d_out[k], stream),
                        "trace launch");

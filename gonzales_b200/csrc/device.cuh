@@ -27,6 +27,7 @@ struct DevScene {
         uint32_t wide_count;
         uint32_t *err;
         unsigned long long *counters;  // optional fetch counters (nodes, triangles, rays)
+        uint32_t *sched;               // persistent kernels: per-launch pull counter (zero at launch) or null
         const uint32_t *n_dev;         // optional device-side ray count (overrides the launch's n)
         // shading data (path integrator)
         const float4 *materials;       // 2 x float4 per material: albedo + type, emission

@@ -19,7 +19,16 @@ struct LaunchParams {
         unsigned long long *counters;  // optional fetch counters (device)
         const uint32_t *n_dev;         // optional device-side ray count; n is then the capacity
         int32_t *inst_out;             // two-level scenes: hit instance per ray (optional)
+        // Persistent launches: the pull counter of the chunk schedule, a
+        // device word that is zero when the launch starts (its owner clears it
+        // before every launch) and that no concurrent launch uses.  Null:
+        // launch_trace takes a zeroed word of a stream-ordered pool.
+        uint32_t *sched;
 };
+
+// Rays per kernel launch; launch_trace splits larger calls (32-bit chunk
+// indices in the persistent kernels).
+constexpr int64_t kMaxLaunchRays = int64_t(1) << 30;
 
 // ray_fmt: RayFormat; out_fmt: OutFormat.  Asynchronous on `st`.
 cudaError_t launch_trace(const DevScene &s, const LaunchParams &p, int ray_fmt, int out_fmt, const void *rays,

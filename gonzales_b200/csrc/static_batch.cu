@@ -12,7 +12,8 @@
 //
 // The scratch: g_static_scratch, a file-scope __device__ array holding the
 // rays (Ray_C, 24 B), their tMax (4 B) and the results (Intersection_C, 48 B)
-// of at most kStaticMaxRays = 65,536 rays: 4,980,736 bytes.  Every GPU on which
+// of at most kStaticMaxRays = 65,536 rays, then the traversal kernel's pull
+// counter in a 256-byte tail: 4,980,992 bytes.  Every GPU on which
 // the library's device code is loaded keeps this array until the process exits.
 // In host code `g_static_scratch` is only a host-side stand-in for the symbol,
 // never a device address.  Every call looks the device address up again with
@@ -23,7 +24,7 @@
 //
 // Sharing: every call uses the same array, which keeps the last call's
 // contents.  Nothing in it has to start at zero (each call overwrites the rays,
-// tMax values and results it uses).  Calls that overlapped on the GPU would
+// tMax values and results it uses and zeroes the pull counter).  Calls that overlapped on the GPU would
 // race on the array; calls through this entry point are serialised by a
 // process-wide lock, so the array must not be touched by anything else.
 //
@@ -48,9 +49,12 @@ constexpr size_t kTmaxBytes = (size_t)kStaticMaxRays * sizeof(float);
 constexpr size_t kOutBytes = (size_t)kStaticMaxRays * sizeof(gzg_intersection);
 constexpr size_t kTmaxOffset = kRayBytes;
 constexpr size_t kOutOffset = kRayBytes + kTmaxBytes;
-static_assert(kTmaxOffset % 256 == 0 && kOutOffset % 256 == 0, "scratch sections must stay 256-byte aligned");
+constexpr size_t kSchedOffset = kOutOffset + kOutBytes;
+constexpr size_t kSchedBytes = 256;
+static_assert(kTmaxOffset % 256 == 0 && kOutOffset % 256 == 0 && kSchedOffset % 256 == 0,
+              "scratch sections must stay 256-byte aligned");
 
-static __device__ __align__(256) unsigned char g_static_scratch[kRayBytes + kTmaxBytes + kOutBytes];
+static __device__ __align__(256) unsigned char g_static_scratch[kSchedOffset + kSchedBytes];
 
 std::mutex g_static_mu;
 
@@ -119,8 +123,11 @@ extern "C" GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, co
                                "tMax copy");
                 if (st != GZG_OK) break;
                 // the scene's tuned closest-hit launch, as gzg_gpu_traverse_batch
-                // uses with default options
-                const LaunchParams p = scene_launch(scene, false);
+                // uses with default options, with the scratch's pull counter
+                LaunchParams p = scene_launch(scene, false);
+                p.sched = reinterpret_cast<uint32_t *>(base + kSchedOffset);
+                st = cuda_step(cudaMemsetAsync(p.sched, 0, sizeof(uint32_t), stream), "pull counter");
+                if (st != GZG_OK) break;
                 launched = true;
                 st = cuda_step(launch_trace(view, p, kRayReference, kOutIntersection, base,
                                             reinterpret_cast<const float *>(base + kTmaxOffset), count,

@@ -26,6 +26,57 @@ namespace gzg {
 // at 8, 3,664 at 16).
 constexpr int kRefillMin = 4;
 
+// Fetch statistics of the persistent kernels (instrumented launches only,
+// s.counters set): adds the lanes that reach the call to counter `which`
+// (0 nodes opened, 1 triangles tested, 2 rays finished), one atomic per
+// converged group.  Uninstrumented launches pay one uniform branch and keep no
+// per-thread tallies (three registers under the 72-register cap).
+__device__ __forceinline__ void count_lanes(const DevScene &s, int which) {
+        if (s.counters == nullptr) return;
+        const unsigned m = __activemask();
+        if ((threadIdx.x & 31u) == (unsigned)(__ffs(m) - 1)) atomicAdd(s.counters + which, (unsigned long long)__popc(m));
+}
+
+// Chunk schedule of the persistent kernels.  Rays go out in 32-ray chunks;
+// warp w of W starts with chunk w.  A warp that has used up its chunk pulls
+// the next from the launch's pull counter (s.sched, zero when the launch
+// starts; one atomicAdd per 32 rays gives chunk W + the old value; the owner of
+// the word clears it before each launch), or, without a counter, takes w + W,
+// w + 2W, ...  Chunks differ in cost by the depth of their rays' traversals;
+// the static sequence left the warps that drew costly chunks running alone at
+// the launch's tail (ray-cast workload, closest hit: incoherent half 2,884 ->
+// 3,148 Mrays/s, coherent half 7,097 -> 8,401 with the pull counter).
+// 32-bit indices: launch_trace splits launches above kMaxLaunchRays.  (A
+// kernel-side reset of the word by the launch's last warp kept one more value
+// live and spilled at the 72-register cap.)
+struct ChunkCursor {
+        uint32_t chunk, cursor, end;
+};
+
+__device__ __forceinline__ uint32_t grid_warps() { return (gridDim.x * blockDim.x) >> 5; }
+
+__device__ __forceinline__ void chunk_first(ChunkCursor &c, uint32_t n) {
+        c.chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        c.cursor = c.chunk * 32u;
+        c.end = c.cursor + 32u < n ? c.cursor + 32u : n;
+}
+
+// Warp-uniform: moves the warp to its next chunk; false when none is left.
+// A warp stops pulling once a pull lands past n, so the counter ends below
+// n / 32 + 2W and every index stays below 2^32.
+__device__ __forceinline__ bool chunk_next(ChunkCursor &c, uint32_t *sched, uint32_t n) {
+        if (sched) {
+                uint32_t k = 0u;
+                if ((threadIdx.x & 31u) == 0u) k = atomicAdd(sched, 1u);
+                c.chunk = grid_warps() + __shfl_sync(0xFFFFFFFFu, k, 0);
+        } else {
+                c.chunk += grid_warps();
+        }
+        c.cursor = c.chunk * 32u;
+        c.end = c.cursor + 32u < n ? c.cursor + 32u : n;
+        return c.cursor < n;
+}
+
 // 8-bit quantised plane -> float: 0x4B0000qq is 2^23 + q exactly.
 __device__ __forceinline__ float qbyte(uint32_t word, uint32_t sel) {
         return __uint_as_float(__byte_perm(word, 0x4B000000u, sel)) - 8388608.0f;
@@ -269,38 +320,31 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
         const unsigned FULL = 0xFFFFFFFFu;
-        n = ray_count(s, n);
+        const uint32_t nr = (uint32_t)ray_count(s, n);
         const unsigned lane = threadIdx.x & 31u;
         const unsigned lt_mask = (1u << lane) - 1u;
-        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-        int64_t chunk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        int64_t cursor = chunk * 32;
-        int64_t chunk_end = cursor + 32 < n ? cursor + 32 : n;
+        ChunkCursor cc;
+        chunk_first(cc, nr);
 
         uint2 *stack = smem_stack + threadIdx.x;
         const int stride = blockDim.x;
-        int64_t ray_i = -1;
+        int ray_i = -1;
         WideRay r;
-        float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
+        float thit = 0.0f, bu = 0.0f, bv = 0.0f;
         int prim = -1, sp = 0;
         uint2 group = make_uint2(0u, 0u);
-        uint32_t steps = 0, n_nodes = 0, n_tris = 0, n_rays = 0;
+        uint32_t steps = 0;
 
         for (;;) {
                 // ---- refill idle lanes from this warp's chunk sequence (warp-uniform cursor)
                 unsigned need = __ballot_sync(FULL, ray_i < 0);
                 if (__popc(need) < kRefillMin && need != FULL) need = 0u;
-                while (need != 0u && cursor < n) {
-                        if (cursor >= chunk_end) {
-                                chunk += nwarps;
-                                cursor = chunk * 32;
-                                chunk_end = cursor + 32 < n ? cursor + 32 : n;
-                                if (cursor >= n) break;
-                        }
-                        const int avail = (int)(chunk_end - cursor);
+                while (need != 0u && cc.cursor < nr) {
+                        if (cc.cursor >= cc.end && !chunk_next(cc, s.sched, nr)) break;
+                        const int avail = (int)(cc.end - cc.cursor);
                         const int rank = __popc(need & lt_mask);
                         if (ray_i < 0 && rank < avail) {
-                                ray_i = cursor + rank;
+                                ray_i = (int)(cc.cursor + (uint32_t)rank);
                                 const RayIn in = load_ray<RAYFMT>(rays, tmaxs, ray_i);
                                 r.ox = in.ox;
                                 r.oy = in.oy;
@@ -313,7 +357,6 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                                 r.rdz = wide_rcp(in.dz);
                                 r.oct = (__float_as_uint(r.rdx) >> 31) | ((__float_as_uint(r.rdy) >> 31) << 1) |
                                         ((__float_as_uint(r.rdz) >> 31) << 2);
-                                tmax = in.tmax;
                                 thit = in.tmax;
                                 bu = bv = 0.0f;
                                 prim = -1;
@@ -322,7 +365,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                                 group = make_uint2(s.per_ray_root ? in.root : 0u, (1u << 24) | (1u << r.oct));
                         }
                         const int npop = __popc(need);
-                        cursor += npop < avail ? npop : avail;
+                        cc.cursor += (uint32_t)(npop < avail ? npop : avail);
                         need = __ballot_sync(FULL, ray_i < 0);
                 }
                 if (__all_sync(FULL, ray_i < 0)) break;
@@ -358,7 +401,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                         } else {
                                 uint32_t nh, nim, cb;
                                 open_node(s.wide + 5 * (size_t)node, r, thit, nh, nim, cb, tri_hits, tri_base);
-                                ++n_nodes;
+                                count_lanes(s, 0);
                                 group = make_uint2(cb, (nh << 24) | nim);
                         }
                 }
@@ -366,7 +409,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                         const uint32_t b = __ffs(tri_hits) - 1;
                         tri_hits &= tri_hits - 1;
                         const uint32_t ti = tri_base + b;
-                        ++n_tris;
+                        count_lanes(s, 1);
                         const float4 a = __ldg(s.tv0 + ti);
                         const float4 bb = __ldg(s.tv1 + ti);
                         const float4 c = __ldg(s.tv2 + ti);
@@ -392,16 +435,17 @@ __global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const vo
                 }
                 if (finished) {
                         if (prim < 0) {
-                                thit = tmax;
+                                // a miss reports the ray's tMax, read again
+                                // rather than kept in a register
+                                thit = load_ray<RAYFMT>(rays, tmaxs, ray_i).tmax;
                                 bu = 0.0f;
                                 bv = 0.0f;
                         }
                         store_hit<OUTFMT>(s, out, ray_i, prim, thit, bu, bv);
                         ray_i = -1;
-                        ++n_rays;
+                        count_lanes(s, 2);
                 }
         }
-        add_counters(s, n_nodes, n_tris, n_rays);
 }
 
 __device__ __forceinline__ void set_ray_dirs(WideRay &r) {
@@ -440,39 +484,32 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                                         void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
         const unsigned FULL = 0xFFFFFFFFu;
-        n = ray_count(s, n);
+        const uint32_t nr = (uint32_t)ray_count(s, n);
         const unsigned lane = threadIdx.x & 31u;
         const unsigned lt_mask = (1u << lane) - 1u;
-        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-        int64_t chunk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        int64_t cursor = chunk * 32;
-        int64_t chunk_end = cursor + 32 < n ? cursor + 32 : n;
+        ChunkCursor cc;
+        chunk_first(cc, nr);
 
         uint2 *stack = smem_stack + threadIdx.x;
         const int stride = blockDim.x;
-        int64_t ray_i = -1;
+        int ray_i = -1;
         WideRay r;
         float wox = 0, woy = 0, woz = 0, wdx = 0, wdy = 0, wdz = 0;  // world ray
         float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
         int prim = -1, hit_inst = -1, cur_inst = -1, sp = 0;
         uint2 group = make_uint2(0u, 0u);
         uint32_t pend_base = 0, pend_mask = 0;
-        uint32_t steps = 0, n_nodes = 0, n_tris = 0, n_rays = 0;
+        uint32_t steps = 0;
 
         for (;;) {
                 unsigned need = __ballot_sync(FULL, ray_i < 0);
                 if (__popc(need) < kRefillMin && need != FULL) need = 0u;
-                while (need != 0u && cursor < n) {
-                        if (cursor >= chunk_end) {
-                                chunk += nwarps;
-                                cursor = chunk * 32;
-                                chunk_end = cursor + 32 < n ? cursor + 32 : n;
-                                if (cursor >= n) break;
-                        }
-                        const int avail = (int)(chunk_end - cursor);
+                while (need != 0u && cc.cursor < nr) {
+                        if (cc.cursor >= cc.end && !chunk_next(cc, s.sched, nr)) break;
+                        const int avail = (int)(cc.end - cc.cursor);
                         const int rank = __popc(need & lt_mask);
                         if (ray_i < 0 && rank < avail) {
-                                ray_i = cursor + rank;
+                                ray_i = (int)(cc.cursor + (uint32_t)rank);
                                 const RayIn in = load_ray<kRayDevice>(rays, tmaxs, ray_i);
                                 wox = r.ox = in.ox;
                                 woy = r.oy = in.oy;
@@ -490,7 +527,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                 group = make_uint2(0u, (1u << 24) | (1u << r.oct));
                         }
                         const int npop = __popc(need);
-                        cursor += npop < avail ? npop : avail;
+                        cc.cursor += (uint32_t)(npop < avail ? npop : avail);
                         need = __ballot_sync(FULL, ray_i < 0);
                 }
                 if (__all_sync(FULL, ray_i < 0)) break;
@@ -543,7 +580,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                 if (!fault) {
                                         uint32_t nh, nim, cb;
                                         open_node(s.wide + 5 * (size_t)node, r, thit, nh, nim, cb, pend_mask, pend_base);
-                                        ++n_nodes;
+                                        count_lanes(s, 0);
                                         group = make_uint2(cb, (nh << 24) | nim);
                                 }
                         }
@@ -588,7 +625,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                 group = make_uint2((uint32_t)__float_as_int(m3.x), (1u << 24) | (1u << r.oct));
                                 break;
                         }
-                        ++n_tris;
+                        count_lanes(s, 1);
                         const float4 bb = __ldg(s.tv1 + ti);
                         const float4 c = __ldg(s.tv2 + ti);
                         float t, u, v;
@@ -615,10 +652,9 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                         store_hit<OUTFMT>(s, out, ray_i, prim, thit, bu, bv);
                         if (s.inst_out) s.inst_out[ray_i] = hit_inst;
                         ray_i = -1;
-                        ++n_rays;
+                        count_lanes(s, 2);
                 }
         }
-        add_counters(s, n_nodes, n_tris, n_rays);
 }
 
 // The reference's slab test (kernel.mojo:171-206), separately rounded.
@@ -755,6 +791,27 @@ using TraceKernel = void (*)(DevScene, const void *, const float *, int64_t, voi
 // SM, from the occupancy calculator unless blocks_per_sm is given), capped at
 // the blocks the ray count needs; the one-ray-per-thread kernel one thread per
 // ray.
+// A zeroed pull counter for one launch on `st` whose caller owns none: a word
+// of the current device's stream-ordered pool, taken and given back on `st`
+// around the launch, so no launch on another stream can use it meanwhile.
+// When the pool has no memory the launch runs the static schedule.
+struct PooledSchedule {
+        uint32_t *word = nullptr;
+        cudaStream_t st = nullptr;
+        cudaError_t take(cudaStream_t s) {
+                st = s;
+                if (cudaMallocAsync(reinterpret_cast<void **>(&word), sizeof(uint32_t), s) != cudaSuccess) {
+                        word = nullptr;
+                        cudaGetLastError();
+                        return cudaSuccess;
+                }
+                return cudaMemsetAsync(word, 0, sizeof(uint32_t), s);
+        }
+        ~PooledSchedule() {
+                if (word) cudaFreeAsync(word, st);
+        }
+};
+
 cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const LaunchParams &p, const DevScene &s,
                                const void *rays, const float *tmax, int64_t n, void *out, cudaStream_t st) {
         // The persistent kernel is compiled for blocks of at most 128 threads
@@ -784,6 +841,16 @@ cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const 
                 }
                 const int64_t wave = (int64_t)sms * per_sm;
                 if (wave < grid) grid = wave;
+                // Pull counter: needed once some warp has a second chunk.
+                if (s.sched == nullptr && s.n_dev == nullptr && n > grid * block) {
+                        PooledSchedule pull;
+                        cudaError_t e = pull.take(st);
+                        if (e != cudaSuccess) return e;
+                        DevScene ws = s;
+                        ws.sched = pull.word;
+                        k<<<(unsigned)grid, block, smem, st>>>(ws, rays, tmax, n, out);
+                        return cudaGetLastError();
+                }
         }
         k<<<(unsigned)grid, block, smem, st>>>(s, rays, tmax, n, out);
         return cudaGetLastError();
@@ -836,10 +903,28 @@ cudaError_t launch_fmt(const DevScene &s, const LaunchParams &p, const void *ray
 cudaError_t launch_trace(const DevScene &scene, const LaunchParams &p, int ray_fmt, int out_fmt, const void *rays,
                          const float *tmax, int64_t n, void *out, cudaStream_t st) {
         if (n <= 0) return cudaSuccess;
+        if (n > kMaxLaunchRays) {
+                // consecutive launches over slices of the arrays
+                if (p.n_dev) return cudaErrorInvalidValue;
+                const size_t ray_bytes = ray_fmt == kRayDevice ? 32 : 24;
+                const size_t out_bytes = out_fmt == kOutHit ? 16 : out_fmt == kOutIntersection ? 48 : out_fmt == kOutAnyPrim ? 4 : 1;
+                LaunchParams q = p;
+                for (int64_t off = 0; off < n; off += kMaxLaunchRays) {
+                        const int64_t m = n - off < kMaxLaunchRays ? n - off : kMaxLaunchRays;
+                        q.inst_out = p.inst_out ? p.inst_out + off : nullptr;
+                        const cudaError_t e = launch_trace(scene, q, ray_fmt, out_fmt,
+                                                           reinterpret_cast<const char *>(rays) + off * ray_bytes,
+                                                           tmax ? tmax + off : nullptr, m,
+                                                           reinterpret_cast<char *>(out) + off * out_bytes, st);
+                        if (e != cudaSuccess) return e;
+                }
+                return cudaSuccess;
+        }
         DevScene s = scene;
         s.counters = p.counters;
         s.n_dev = p.n_dev;
         s.inst_out = p.inst_out;
+        s.sched = p.sched;
         if (s.instances) {
                 // two-level scenes: persistent wide traversal only
                 if (ray_fmt != kRayDevice || (out_fmt != kOutHit && out_fmt != kOutAnyPrim)) return cudaErrorNotSupported;

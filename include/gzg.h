@@ -236,7 +236,7 @@ GZG_API gzg_status gzg_gpu_traverse_batch(gzg_scene *scene, const gzg_ray *rays,
  * for callers that must not allocate: it makes no cudaMalloc, cudaFree or
  * pinned-host allocation, and stages rays, tMax values and results through a
  * fixed array in the library's device image (a file-scope __device__ array of
- * 4,980,736 bytes, held on every GPU that loads the library until exit).
+ * 4,980,992 bytes, held on every GPU that loads the library until exit).
  * At most 65,536 rays per call (more: GZG_ERR_LIMIT); two-level scenes are
  * rejected (GZG_ERR_INVALID_ARGUMENT).  Every call looks up the array's device
  * address afresh, launches with the scene's tuned closest-hit parameters on
