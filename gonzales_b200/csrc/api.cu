@@ -67,7 +67,7 @@ constexpr int64_t kChunk = 1 << 19;  // rays per pipelined chunk (512K x 4 strea
 
 // Per-call staging: device buffers and pinned host buffers for kSlots chunks
 // in flight, each slot with its own stream and its pull counter for the
-// persistent kernel (cleared on the slot's stream before each launch).
+// persistent kernel.
 struct Staging {
         cudaStream_t st[kSlots] = {};
         void *d_in[kSlots] = {}, *d_tmax[kSlots] = {}, *d_out[kSlots] = {};
@@ -98,6 +98,38 @@ bool is_pinned(const void *p) {
 
 }  // namespace
 
+// Pull counters of the persistent kernels for the device calls, which run on
+// the callers' streams: kWords device words (one allocation, made by the first
+// call that needs one), each with an event recorded after the last launch that
+// used it.  A launch takes the next word, makes its stream wait for that
+// word's previous launch, and records the word's event after itself, so
+// launches that share a word run one after another whatever their streams,
+// while up to kWords launches on different streams can run at once.
+struct PullRing {
+        static constexpr int kWords = 32;
+        uint32_t *words = nullptr;
+        cudaEvent_t ev[kWords] = {};
+        bool recorded[kWords] = {};
+        int next = 0;
+        std::mutex mu;
+
+        cudaError_t create() {
+                cudaError_t e = cudaMalloc(&words, kWords * sizeof(uint32_t));
+                for (int k = 0; e == cudaSuccess && k < kWords; ++k)
+                        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+                if (e != cudaSuccess) release();
+                return e;
+        }
+        void release() {
+                for (cudaEvent_t &e : ev) {
+                        if (e) cudaEventDestroy(e);
+                        e = nullptr;
+                }
+                cudaFree(words);
+                words = nullptr;
+        }
+};
+
 // Launch configuration chosen by gzg_scene_autotune (or the defaults).
 struct TunedLaunch {
         int block_size = 128;
@@ -125,10 +157,12 @@ struct gzg_scene {
         HostShading host_shading;
         std::mutex pool_mu;
         std::vector<std::unique_ptr<Staging>> pool;
+        PullRing pull;
 
         ~gzg_scene() {
                 DeviceGuard g(device);
                 pool.clear();
+                pull.release();
                 for (void *p : allocs) cudaFree(p);
         }
 
@@ -270,6 +304,38 @@ gzg_status read_error_word(gzg_scene *s, uint32_t *word, bool clear) {
 }
 
 
+// launch_trace for the device calls, on the caller's stream, with one of the
+// scene's pull counters.  A stream being captured into a graph gets the static
+// schedule (no word, no event waits across the capture's boundary).
+cudaError_t device_trace(gzg_scene *scene, LaunchParams p, int out_fmt, const void *rays, int64_t n, void *out,
+                         cudaStream_t st) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+                cudaGetLastError();
+                cs = cudaStreamCaptureStatusActive;
+        }
+        p.sched = nullptr;
+        if (cs != cudaStreamCaptureStatusNone || n <= 0)
+                return launch_trace(scene->dev, p, kRayDevice, out_fmt, rays, nullptr, n, out, st);
+        PullRing &r = scene->pull;
+        std::lock_guard<std::mutex> lk(r.mu);
+        if (!r.words) {
+                const cudaError_t e = r.create();
+                if (e != cudaSuccess) return e;
+        }
+        const int k = r.next;
+        r.next = (k + 1) % PullRing::kWords;
+        if (r.recorded[k]) {
+                const cudaError_t e = cudaStreamWaitEvent(st, r.ev[k], 0);
+                if (e != cudaSuccess) return e;
+        }
+        p.sched = r.words + k;
+        const cudaError_t e = launch_trace(scene->dev, p, kRayDevice, out_fmt, rays, nullptr, n, out, st);
+        if (e != cudaSuccess) return e;
+        r.recorded[k] = true;
+        return cudaEventRecord(r.ev[k], st);
+}
+
 // Host batch: chunks of Ray_C + tMax through kSlots streams; results are
 // `out_bytes` per ray in format `out_fmt`.
 gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int64_t count, void *results,
@@ -325,7 +391,6 @@ gzg_status host_batch(gzg_scene *s, const gzg_ray *rays, const float *tmax, int6
                 GZG_CK(cudaMemcpyAsync(stg->d_tmax[k], src_tmax, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, stream),
                        "tMax upload");
                 p.sched = stg->d_sched + k;  // this slot's stream orders its launches
-                GZG_CK(cudaMemsetAsync(p.sched, 0, sizeof(uint32_t), stream), "schedule word");
                 GZG_CK(launch_trace(s->dev, p, kRayReference, out_fmt, stg->d_in[k],
                                     reinterpret_cast<const float *>(stg->d_tmax[k]), n, stg->d_out[k], stream),
                        "trace launch");
@@ -991,8 +1056,8 @@ GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *r
         gzg_status st = check_options(options);
         if (st != GZG_OK) return st;
         DeviceGuard g(scene->device);
-        GZG_CK(launch_trace(scene->dev, params_for(scene, options, false), kRayDevice, kOutHit, rays, nullptr, count,
-                            hits, reinterpret_cast<cudaStream_t>(stream)),
+        GZG_CK(device_trace(scene, params_for(scene, options, false), kOutHit, rays, count, hits,
+                            reinterpret_cast<cudaStream_t>(stream)),
                "gzg_trace_closest_device launch");
         return clear_error();
 }
@@ -1021,14 +1086,14 @@ GZG_API gzg_status gzg_scene_autotune(gzg_scene *scene, const gzg_ray_d *rays, i
                 p.stack_depth = t.stack_depth;
                 p.l1_carveout = t.l1_carveout;
                 const int fmt = any_hit ? kOutAnyPrim : kOutHit;
-                GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st), "autotune launch");
+                GZG_CK(device_trace(scene, p, fmt, rays, count, out, st), "autotune launch");
                 // the faster of two timed batches of three launches (a single
                 // batch let one noisy sample pick a slow configuration)
                 float best_el = 0.0f;
                 for (int rep = 0; rep < 2; ++rep) {
                         GZG_CK(cudaEventRecord(e0, st), "autotune event");
                         for (int k = 0; k < 3; ++k)
-                                GZG_CK(launch_trace(scene->dev, p, kRayDevice, fmt, rays, nullptr, count, out, st),
+                                GZG_CK(device_trace(scene, p, fmt, rays, count, out, st),
                                        "autotune launch");
                         GZG_CK(cudaEventRecord(e1, st), "autotune event");
                         GZG_CK(cudaEventSynchronize(e1), "autotune sync");
@@ -1542,8 +1607,7 @@ GZG_API gzg_status gzg_trace_closest_instanced_device(gzg_scene *scene, const gz
         DeviceGuard g(scene->device);
         LaunchParams p = params_for(scene, options, false);
         p.inst_out = instance;
-        GZG_CK(launch_trace(scene->dev, p, kRayDevice, kOutHit, rays, nullptr, count, hits,
-                            reinterpret_cast<cudaStream_t>(stream)),
+        GZG_CK(device_trace(scene, p, kOutHit, rays, count, hits, reinterpret_cast<cudaStream_t>(stream)),
                "gzg_trace_closest_instanced_device launch");
         return clear_error();
 }
@@ -1568,8 +1632,8 @@ GZG_API gzg_status gzg_trace_any_device(gzg_scene *scene, const gzg_ray_d *rays,
         gzg_status st = check_options(options);
         if (st != GZG_OK) return st;
         DeviceGuard g(scene->device);
-        GZG_CK(launch_trace(scene->dev, params_for(scene, options, true), kRayDevice, kOutAnyPrim, rays, nullptr, count,
-                            hit_prim, reinterpret_cast<cudaStream_t>(stream)),
+        GZG_CK(device_trace(scene, params_for(scene, options, true), kOutAnyPrim, rays, count, hit_prim,
+                            reinterpret_cast<cudaStream_t>(stream)),
                "gzg_trace_any_device launch");
         return clear_error();
 }

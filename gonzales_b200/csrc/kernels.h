@@ -20,9 +20,9 @@ struct LaunchParams {
         const uint32_t *n_dev;         // optional device-side ray count; n is then the capacity
         int32_t *inst_out;             // two-level scenes: hit instance per ray (optional)
         // Persistent launches: the pull counter of the chunk schedule, a
-        // device word that is zero when the launch starts (its owner clears it
-        // before every launch) and that no concurrent launch uses.  Null:
-        // launch_trace takes a zeroed word of a stream-ordered pool.
+        // device word that no launch running at the same time uses;
+        // launch_trace clears it on the launch's stream first.  Null: the
+        // static schedule.
         uint32_t *sched;
 };
 

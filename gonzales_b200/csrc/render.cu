@@ -423,8 +423,8 @@ __device__ V3 hg_sample(V3 wo, float g, float u0, float u1, float &value) {
 enum {
         kCountExt0 = 0, kCountExt1 = 1, kCountShadow = 2, kCountProbe = 3, kCountWaveBase = 4,
         kCountDielectric = 6, kCountCoated = 7, kCountConductor = 8, kCountCoatedConductor = 9,
-        kCountSched = 10,  // 3 words: pull counters of a bounce's extend, shadow and probe launches
-        kCountWords = 16
+        kCountSched = 10,  // pull counter of the wave's trace launches (one after another on its stream)
+        kCountWords = 12
 };
 enum { kStatCamera = 0, kStatExt = 1, kStatShadow = 2, kStatProbe = 3, kStatWaves = 4, kStatWords = 8 };
 enum SortKey { kSortNone = 0, kSortMaterial = 1, kSortScene = 2 };
@@ -1563,9 +1563,6 @@ __global__ void k_clear_counts(Wave w, int next) {
         w.counts[kCountCoated] = 0;
         w.counts[kCountConductor] = 0;
         w.counts[kCountCoatedConductor] = 0;
-        w.counts[kCountSched] = 0;
-        w.counts[kCountSched + 1] = 0;
-        w.counts[kCountSched + 2] = 0;
 }
 
 // Film.add (Core/Film.swift:107-119): the sample's light scaled by iso / 100
@@ -1927,7 +1924,7 @@ struct gzg_renderer {
                 for (int b = 0; b < max_depth; ++b) {
                         k_clear_counts<<<1, 1, 0, st>>>(w, cur ^ 1);
                         LaunchParams lp = lp_closest, lpa = lp_any;
-                        lp.sched = w.counts + kCountSched;  // cleared by k_clear_counts
+                        lp.sched = lpa.sched = w.counts + kCountSched;
                         lp.n_dev = w.counts + cur;
                         lp.inst_out = w.hit_inst;
                         NvtxRange extend_range("gzg extend");
@@ -1954,7 +1951,6 @@ struct gzg_renderer {
                         shade_range.end();
                         NvtxRange shadow_range("gzg shadow");
                         lpa.n_dev = w.counts + kCountShadow;
-                        lpa.sched = w.counts + kCountSched + 1;
                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.sh_ray, nullptr, w.capacity, w.sh_occ, st);
                         if (e != cudaSuccess) return e;
                         k_shadow_resolve<<<grid, block, 0, st>>>(w);
@@ -1963,12 +1959,10 @@ struct gzg_renderer {
                         if (corrected) {
                                 if (probe_any) {
                                         lpa.n_dev = w.counts + kCountProbe;
-                                        lpa.sched = w.counts + kCountSched + 2;
                                         e = launch_trace(view, lpa, kRayDevice, kOutAnyPrim, w.pr_ray, nullptr, w.capacity,
                                                          w.pr_hits, st);
                                 } else {
                                         lp.n_dev = w.counts + kCountProbe;
-                                        lp.sched = w.counts + kCountSched + 2;
                                         lp.inst_out = w.pr_inst;
                                         e = launch_trace(view, lp, kRayDevice, kOutHit, w.pr_ray, nullptr, w.capacity,
                                                          w.pr_hits, st);

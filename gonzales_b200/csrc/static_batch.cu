@@ -24,7 +24,8 @@
 //
 // Sharing: every call uses the same array, which keeps the last call's
 // contents.  Nothing in it has to start at zero (each call overwrites the rays,
-// tMax values and results it uses and zeroes the pull counter).  Calls that overlapped on the GPU would
+// tMax values and results it uses; the traversal launch clears its pull
+// counter).  Calls that overlapped on the GPU would
 // race on the array; calls through this entry point are serialised by a
 // process-wide lock, so the array must not be touched by anything else.
 //
@@ -126,8 +127,6 @@ extern "C" GZG_API gzg_status gzg_gpu_traverse_batch_static(gzg_scene *scene, co
                 // uses with default options, with the scratch's pull counter
                 LaunchParams p = scene_launch(scene, false);
                 p.sched = reinterpret_cast<uint32_t *>(base + kSchedOffset);
-                st = cuda_step(cudaMemsetAsync(p.sched, 0, sizeof(uint32_t), stream), "pull counter");
-                if (st != GZG_OK) break;
                 launched = true;
                 st = cuda_step(launch_trace(view, p, kRayReference, kOutIntersection, base,
                                             reinterpret_cast<const float *>(base + kTmaxOffset), count,

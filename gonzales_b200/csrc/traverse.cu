@@ -39,16 +39,16 @@ __device__ __forceinline__ void count_lanes(const DevScene &s, int which) {
 
 // Chunk schedule of the persistent kernels.  Rays go out in 32-ray chunks;
 // warp w of W starts with chunk w.  A warp that has used up its chunk pulls
-// the next from the launch's pull counter (s.sched, zero when the launch
-// starts; one atomicAdd per 32 rays gives chunk W + the old value; the owner of
-// the word clears it before each launch), or, without a counter, takes w + W,
+// the next from the launch's pull counter (s.sched, cleared by launch_trace
+// before the launch; one atomicAdd per 32 rays gives chunk W + the old value),
+// or, without a counter, takes w + W,
 // w + 2W, ...  Chunks differ in cost by the depth of their rays' traversals;
 // the static sequence left the warps that drew costly chunks running alone at
 // the launch's tail (ray-cast workload, closest hit: incoherent half 2,884 ->
 // 3,148 Mrays/s, coherent half 7,097 -> 8,401 with the pull counter).
 // 32-bit indices: launch_trace splits launches above kMaxLaunchRays.  (A
-// kernel-side reset of the word by the launch's last warp kept one more value
-// live and spilled at the 72-register cap.)
+// reset of the word by the launch's last warp, instead of a clear before the
+// launch, kept one more value live and spilled at the 72-register cap.)
 struct ChunkCursor {
         uint32_t chunk, cursor, end;
 };
@@ -304,12 +304,13 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
 }
 
 // Persistent variant of k_wide.  The grid is sized to the resident capacity
-// (SM count x blocks per SM); warp w owns the 32-ray chunks w, w + W, w + 2W,
-// ... (W = warps in the grid) and hands out the rays of its current chunk in
-// order.  A lane whose ray finishes takes the next ray at the top of the next
-// iteration, so lanes are not left idle while the slowest ray of a fixed
-// 32-ray batch finishes.  Each iteration opens one node and tests its
-// triangles.  No atomics or per-launch state: the assignment is static.
+// (SM count x blocks per SM); each warp takes 32-ray chunks by the chunk
+// schedule above (the pull counter when the launch has one) and hands out the
+// rays of its current chunk in order.  A lane whose ray finishes takes the
+// next ray at the top of the next iteration, so lanes are not left idle while
+// the slowest ray of a fixed 32-ray batch finishes.  Each iteration opens one
+// node and tests its triangles.  A miss reads its tMax again at the end
+// instead of keeping it in a register.
 // Capped at 72 registers (7 blocks of 128 per SM): closest hit, 80 registers
 // uncapped, goes 4,011 -> 4,123 Mrays/s on the ray-cast workload; any hit
 // (71-72 uncapped) 5,238 -> 5,205.  Looser minimums are not the uncapped
@@ -791,27 +792,6 @@ using TraceKernel = void (*)(DevScene, const void *, const float *, int64_t, voi
 // SM, from the occupancy calculator unless blocks_per_sm is given), capped at
 // the blocks the ray count needs; the one-ray-per-thread kernel one thread per
 // ray.
-// A zeroed pull counter for one launch on `st` whose caller owns none: a word
-// of the current device's stream-ordered pool, taken and given back on `st`
-// around the launch, so no launch on another stream can use it meanwhile.
-// When the pool has no memory the launch runs the static schedule.
-struct PooledSchedule {
-        uint32_t *word = nullptr;
-        cudaStream_t st = nullptr;
-        cudaError_t take(cudaStream_t s) {
-                st = s;
-                if (cudaMallocAsync(reinterpret_cast<void **>(&word), sizeof(uint32_t), s) != cudaSuccess) {
-                        word = nullptr;
-                        cudaGetLastError();
-                        return cudaSuccess;
-                }
-                return cudaMemsetAsync(word, 0, sizeof(uint32_t), s);
-        }
-        ~PooledSchedule() {
-                if (word) cudaFreeAsync(word, st);
-        }
-};
-
 cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const LaunchParams &p, const DevScene &s,
                                const void *rays, const float *tmax, int64_t n, void *out, cudaStream_t st) {
         // The persistent kernel is compiled for blocks of at most 128 threads
@@ -841,15 +821,18 @@ cudaError_t launch_wide_kernel(TraceKernel k, int stack, bool persistent, const 
                 }
                 const int64_t wave = (int64_t)sms * per_sm;
                 if (wave < grid) grid = wave;
-                // Pull counter: needed once some warp has a second chunk.
-                if (s.sched == nullptr && s.n_dev == nullptr && n > grid * block) {
-                        PooledSchedule pull;
-                        cudaError_t e = pull.take(st);
+                // The pull counter pays off once some warp has a second chunk
+                // (with one chunk per warp both schedules are the same); it
+                // starts every launch at zero.
+                if (s.sched != nullptr) {
+                        if (s.n_dev == nullptr && n <= grid * block) {
+                                DevScene ws = s;
+                                ws.sched = nullptr;
+                                k<<<(unsigned)grid, block, smem, st>>>(ws, rays, tmax, n, out);
+                                return cudaGetLastError();
+                        }
+                        const cudaError_t e = cudaMemsetAsync(s.sched, 0, sizeof(uint32_t), st);
                         if (e != cudaSuccess) return e;
-                        DevScene ws = s;
-                        ws.sched = pull.word;
-                        k<<<(unsigned)grid, block, smem, st>>>(ws, rays, tmax, n, out);
-                        return cudaGetLastError();
                 }
         }
         k<<<(unsigned)grid, block, smem, st>>>(s, rays, tmax, n, out);
