@@ -352,14 +352,11 @@ __device__ __forceinline__ double code_area(const Tree &t, int code) {
         return 2.0 * (x * y + x * z + y * z);
 }
 
-// quantise_axis of wide_bvh.cpp on the device (same arithmetic in double).
-__device__ void quantise_axis_dev(const double *clo, const double *chi, int n, float *p_out, uint8_t *e_out,
-                                  uint8_t *qlo, uint8_t *qhi) {
-        double lo = CUDART_INF, hi = -CUDART_INF;
-        for (int i = 0; i < n; ++i) {
-                lo = fmin(lo, clo[i]);
-                hi = fmax(hi, chi[i]);
-        }
+// quantise_axis of wide_bvh.cpp on the device (same arithmetic in double),
+// in two parts: the axis's grid from the extent [lo, hi] of the node's
+// children (origin p rounded down to a float, exponent e, margin, step), and
+// one child plane quantised outward on that grid.
+__device__ void axis_grid(double lo, double hi, float *p_out, int *e_out, double *margin_out, double *step_out) {
         const double mag = fmax(fabs(lo), fabs(hi));
         double margin = ldexp(fmax(mag, hi - lo), -18);
         if (!(margin > 0)) margin = 1e-30;
@@ -370,176 +367,291 @@ __device__ void quantise_axis_dev(const double *clo, const double *chi, int n, f
         k = max(k, -126);
         while (ldexp(255.0, k) < span) ++k;
         k = min(k, 127);
-        const double s = ldexp(1.0, k);
         *p_out = p;
-        *e_out = (uint8_t)(k + 127);
-        for (int i = 0; i < n; ++i) {
-                const double a = floor((clo[i] - margin - (double)p) / s);
-                const double b = ceil((chi[i] + margin - (double)p) / s);
-                qlo[i] = (uint8_t)fmin(255.0, fmax(0.0, a));
-                qhi[i] = (uint8_t)fmin(255.0, fmax(0.0, b));
-        }
+        *e_out = k + 127;
+        *margin_out = margin;
+        *step_out = ldexp(1.0, k);
+}
+
+__device__ __forceinline__ uint8_t quantise_lo(double v, double margin, float p, double step) {
+        return (uint8_t)fmin(255.0, fmax(0.0, floor((v - margin - (double)p) / step)));
+}
+__device__ __forceinline__ uint8_t quantise_hi(double v, double margin, float p, double step) {
+        return (uint8_t)fmin(255.0, fmax(0.0, ceil((v + margin - (double)p) / step)));
 }
 
 constexpr int kRootItem = INT_MIN;  // the root's code, resolved on the device
 
-// One level of the collapse: item = (binary code, wide node index).
-__global__ void k_collapse(Tree t, const int2 *__restrict__ items, const uint32_t *__restrict__ n_items,
-                           int2 *__restrict__ next, uint32_t *__restrict__ n_next, uint32_t *__restrict__ counters,
-                           WideNode *__restrict__ nodes, float4 *__restrict__ tv0, float4 *__restrict__ tv1,
-                           float4 *__restrict__ tv2, uint32_t node_cap, uint32_t tri_cap, uint32_t *__restrict__ err) {
-        const uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
-        if (it >= *n_items) return;
+// Reductions within an aligned group of 8 lanes (one wide node per group);
+// every lane of the group gets the result.  argmax / argmin keep the lowest
+// lane on ties.
+__device__ __forceinline__ int g8_argmax(double v, int idx, double *best) {
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xFFFFFFFFu, v, off);
+                const int oi = __shfl_xor_sync(0xFFFFFFFFu, idx, off);
+                if (ov > v || (ov == v && oi < idx)) {
+                        v = ov;
+                        idx = oi;
+                }
+        }
+        *best = v;
+        return idx;
+}
+__device__ __forceinline__ int g8_argmin(float v, int idx, float *best) {
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) {
+                const float ov = __shfl_xor_sync(0xFFFFFFFFu, v, off);
+                const int oi = __shfl_xor_sync(0xFFFFFFFFu, idx, off);
+                if (ov < v || (ov == v && oi < idx)) {
+                        v = ov;
+                        idx = oi;
+                }
+        }
+        *best = v;
+        return idx;
+}
+__device__ __forceinline__ uint32_t g8_or(uint32_t v) {
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) v |= __shfl_xor_sync(0xFFFFFFFFu, v, off);
+        return v;
+}
+__device__ __forceinline__ uint32_t g8_sum(uint32_t v) {
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
+        return v;
+}
+
+// One level of the collapse, one group of 8 lanes per item (binary code, wide
+// node index), four items per warp.  The steps are the host converter's, with
+// the serial loops spread over the group's lanes (lane j of a group = child j
+// or slot j):
+//   - lane j < n holds child j while the node opens the interior child of
+//     largest surface area (lowest index on ties) until it has 8 children;
+//   - lane j loads child j's box and its 8 slot costs; each of n rounds gives
+//     the lowest remaining cost (lowest child, then lowest slot, on ties) its
+//     slot;
+//   - lane s quantises the three axes of the child in slot s;
+//   - lane j writes child j's slot fields and copies its triangles.
+// The node is assembled in shared memory and stored as five 16-byte words.
+// Every loop runs a fixed 8 steps (or until no group of the warp is still
+// opening children) so that all 32 lanes take every shuffle.  One thread per
+// node took about 85 us per node at the top of the tree (a chain of dependent
+// loads and local-memory loops), so every level cost at least that however few
+// nodes it held; a whole warp per node left most lanes idle on the wide levels.
+__global__ void __launch_bounds__(128) k_collapse(Tree t, const int2 *__restrict__ items,
+                                                  const uint32_t *__restrict__ n_items, int2 *__restrict__ next,
+                                                  uint32_t *__restrict__ n_next, uint32_t *__restrict__ counters,
+                                                  WideNode *__restrict__ nodes, float4 *__restrict__ tv0,
+                                                  float4 *__restrict__ tv1, float4 *__restrict__ tv2, uint32_t node_cap,
+                                                  uint32_t tri_cap, uint32_t *__restrict__ err) {
+        const unsigned FULL = 0xFFFFFFFFu;
+        __shared__ __align__(16) unsigned char s_node[16][80];
+        const int lane = (int)(threadIdx.x & 31u);
+        const int j = lane & 7;             // child / slot index within the group
+        const int base = lane & ~7;         // the group's first lane
+        unsigned char *wn = s_node[threadIdx.x >> 3];
+        const uint32_t first = (blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) >> 3;  // the warp's first item
+        const uint32_t count = *n_items;
+        if (first >= count) return;  // whole warps
+        const uint32_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+        const bool valid = it < count;
         const int m = (int)*t.m_dev;
-        int2 item = items[it];
-        if (item.x == kRootItem) item.x = m >= 2 ? *t.root : ~0;
-        int kids[8];
-        double area[8];
+        int2 item = valid ? items[it] : make_int2(0, 0);
+        if (valid && item.x == kRootItem) item.x = m >= 2 ? *t.root : ~0;
+
+        // ---- children: open the largest interior child until there are 8
+        int kid = 0;
+        double area = -1.0;  // -1: a leaf (never opened)
         int n = 0;
-        if (m == 0) {
+        bool opening = false;
+        if (!valid || m == 0) {
                 n = 0;
         } else if (code_leaf(t, item.x)) {
-                kids[n++] = item.x;
+                kid = item.x;
+                n = 1;
         } else {
                 const int2 c = t.child[item.x];
-                kids[0] = c.x;
-                kids[1] = c.y;
-                area[0] = code_leaf(t, c.x) ? -1.0 : code_area(t, c.x);
-                area[1] = code_leaf(t, c.y) ? -1.0 : code_area(t, c.y);
+                kid = j == 0 ? c.x : c.y;
+                if (j < 2) area = code_leaf(t, kid) ? -1.0 : code_area(t, kid);
                 n = 2;
-                while (n < 8) {
-                        int best = -1;
-                        double best_a = -1.0;
-                        for (int i = 0; i < n; ++i)
-                                if (area[i] > best_a) {
-                                        best_a = area[i];
-                                        best = i;
-                                }
-                        if (best < 0) break;
-                        const int2 c2 = t.child[kids[best]];
-                        for (int i = n; i > best + 1; --i) {
-                                kids[i] = kids[i - 1];
-                                area[i] = area[i - 1];
+                opening = true;
+        }
+        while (__any_sync(FULL, opening)) {
+                double best_a;
+                const int best = g8_argmax(opening && j < n ? area : -1.0, j, &best_a);
+                if (!(best_a > -1.0)) opening = false;
+                const int best_kid = __shfl_sync(FULL, kid, base + best);
+                const int up_kid = __shfl_up_sync(FULL, kid, 1, 8);
+                const double up_area = __shfl_up_sync(FULL, area, 1, 8);
+                if (opening) {
+                        const int2 c2 = t.child[best_kid];
+                        if (j == best || j == best + 1) {
+                                kid = j == best ? c2.x : c2.y;
+                                area = code_leaf(t, kid) ? -1.0 : code_area(t, kid);
+                        } else if (j > best + 1) {
+                                kid = up_kid;
+                                area = up_area;
                         }
-                        kids[best] = c2.x;
-                        kids[best + 1] = c2.y;
-                        area[best] = code_leaf(t, c2.x) ? -1.0 : code_area(t, c2.x);
-                        area[best + 1] = code_leaf(t, c2.y) ? -1.0 : code_area(t, c2.y);
                         ++n;
+                        if (n == 8) opening = false;
                 }
         }
-        // child boxes and octant slots: slot s takes the child farthest along
-        // (+-1, +-1, +-1) (bit a of s set = +), greedily by decreasing reach
-        double clo[8][3], chi[8][3], pc[3] = {0, 0, 0};
-        float cc[8][3];
-        for (int k = 0; k < n; ++k) {
-                code_bounds(t, kids[k], clo[k], chi[k]);
-                for (int a = 0; a < 3; ++a) pc[a] += 0.5 * (clo[k][a] + chi[k][a]) / n;
+        const bool mine = j < n;  // this lane holds a child
+
+        // ---- boxes, centroid of the child centres (summed in child order)
+        double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, term[3] = {0, 0, 0};
+        if (mine) {
+                code_bounds(t, kid, lo, hi);
+                for (int a = 0; a < 3; ++a) term[a] = 0.5 * (lo[a] + hi[a]) / n;
         }
-        for (int k = 0; k < n; ++k)
-                for (int a = 0; a < 3; ++a) cc[k][a] = (float)(0.5 * (clo[k][a] + chi[k][a]) - pc[a]);
-        float cost[8][8];
-        for (int k = 0; k < n; ++k)
+        double pc[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                        const double v = __shfl_sync(FULL, term[a], base + k);
+                        if (k < n) pc[a] += v;
+                }
+
+        // ---- slots: slot s takes the child farthest along (+-1, +-1, +-1)
+        float cost[8];
+        {
+                float cc[3];
+                for (int a = 0; a < 3; ++a) cc[a] = mine ? (float)(0.5 * (lo[a] + hi[a]) - pc[a]) : 0.0f;
+#pragma unroll
                 for (int s2 = 0; s2 < 8; ++s2)
-                        cost[k][s2] = -((s2 & 1 ? cc[k][0] : -cc[k][0]) + (s2 & 2 ? cc[k][1] : -cc[k][1]) +
-                                        (s2 & 4 ? cc[k][2] : -cc[k][2]));
-        int kid_in_slot[8];
-        unsigned kfree = (1u << n) - 1u, sfree = 0xFFu;
-        for (int i = 0; i < 8; ++i) kid_in_slot[i] = -1;
-        for (int round = 0; round < n; ++round) {
-                float best = CUDART_INF_F;
-                int bk = -1, bs = -1;
-                for (int k = 0; k < n; ++k) {
-                        if (!((kfree >> k) & 1u)) continue;
+                        cost[s2] = -((s2 & 1 ? cc[0] : -cc[0]) + (s2 & 2 ? cc[1] : -cc[1]) + (s2 & 4 ? cc[2] : -cc[2]));
+        }
+        int my_slot = -1;
+        unsigned sfree = 0xFFu;
+        bool assigning = true;
+#pragma unroll 1
+        for (int round = 0; round < 8; ++round) {
+                float lb = CUDART_INF_F;
+                int ls = -1;
+                if (mine && my_slot < 0) {
+#pragma unroll
                         for (int s2 = 0; s2 < 8; ++s2)
-                                if (((sfree >> s2) & 1u) && cost[k][s2] < best) {
-                                        best = cost[k][s2];
-                                        bk = k;
-                                        bs = s2;
+                                if (((sfree >> s2) & 1u) && cost[s2] < lb) {
+                                        lb = cost[s2];
+                                        ls = s2;
                                 }
                 }
-                if (bk < 0) break;
-                kfree &= ~(1u << bk);
-                sfree &= ~(1u << bs);
-                kid_in_slot[bs] = bk;
+                float best_c;
+                const int bk = g8_argmin(lb, j, &best_c);
+                const int bs = __shfl_sync(FULL, ls, base + bk);
+                if (round >= n || !(best_c < CUDART_INF_F)) assigning = false;
+                if (assigning) {
+                        if (j == bk) my_slot = bs;
+                        sfree &= ~(1u << bs);
+                }
         }
-        WideNode w;
-        memset(&w, 0, sizeof(w));
-        int nq = 0, order[8];
-        double ql[3][8], qh[3][8];
-        for (int s = 0; s < 8; ++s)
-                if (kid_in_slot[s] >= 0) {
-                        const int k = kid_in_slot[s];
-                        for (int a = 0; a < 3; ++a) {
-                                ql[a][nq] = clo[k][a];
-                                qh[a][nq] = chi[k][a];
+        // slot -> child + 1, four bits per slot
+        const uint32_t slot_map = g8_or((mine && my_slot >= 0) ? (uint32_t)(j + 1) << (4 * my_slot) : 0u);
+
+        // ---- zero the record, then quantise: lane s, three axes of slot s
+        if (j < 5) reinterpret_cast<uint4 *>(wn)[j] = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+        {
+                const int k_in = (int)((slot_map >> (4 * j)) & 0xFu) - 1;  // child in slot j, or -1
+                const int src = base + (k_in >= 0 ? k_in : 0);
+#pragma unroll 1
+                for (int a = 0; a < 3; ++a) {
+                        // the axis's extent over every placed child
+                        double alo = CUDART_INF, ahi = -CUDART_INF;
+                        int nq = 0;
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                                const double l = __shfl_sync(FULL, a == 0 ? lo[0] : (a == 1 ? lo[1] : lo[2]), base + k);
+                                const double h = __shfl_sync(FULL, a == 0 ? hi[0] : (a == 1 ? hi[1] : hi[2]), base + k);
+                                const int ks = __shfl_sync(FULL, my_slot, base + k);
+                                if (k < n && ks >= 0) {  // child k has a slot
+                                        ++nq;
+                                        alo = fmin(alo, l);
+                                        ahi = fmax(ahi, h);
+                                }
                         }
-                        order[nq++] = s;
-                }
-        float pxyz[3] = {0, 0, 0};
-        uint8_t ee[3] = {127, 127, 127};
-        for (int a = 0; a < 3; ++a) {
-                uint8_t qlo8[8], qhi8[8];
-                if (nq > 0) quantise_axis_dev(ql[a], qh[a], nq, &pxyz[a], &ee[a], qlo8, qhi8);
-                for (int s = 0; s < 8; ++s) {
-                        w.qlo[a][s] = 255;
-                        w.qhi[a][s] = 0;
-                }
-                for (int i = 0; i < nq; ++i) {
-                        w.qlo[a][order[i]] = qlo8[i];
-                        w.qhi[a][order[i]] = qhi8[i];
-                }
-        }
-        w.px = pxyz[0];
-        w.py = pxyz[1];
-        w.pz = pxyz[2];
-        w.ex = ee[0];
-        w.ey = ee[1];
-        w.ez = ee[2];
-        int n_int = 0, n_tri = 0;
-        for (int k = 0; k < n; ++k) {
-                if (code_leaf(t, kids[k]))
-                        n_tri += code_count(t, kids[k]);
-                else
-                        ++n_int;
-        }
-        const uint32_t cbase = n_int ? atomicAdd(counters + 0, (uint32_t)n_int) : 0u;
-        const uint32_t tbase = n_tri ? atomicAdd(counters + 1, (uint32_t)n_tri) : 0u;
-        if (cbase + (uint32_t)n_int > node_cap || tbase + (uint32_t)n_tri > tri_cap) {
-                atomicOr(err, kErrBadIndex);
-                return;
-        }
-        w.child_base = cbase;
-        w.tri_base = tbase;
-        uint32_t tri_off = 0, int_rank = 0;
-        for (int s = 0; s < 8; ++s) {
-                const int k = kid_in_slot[s];
-                if (k < 0) continue;
-                const int code = kids[k];
-                if (!code_leaf(t, code)) {
-                        w.imask |= (uint8_t)(1u << s);
-                        const uint32_t q = atomicAdd(n_next, 1u);
-                        next[q] = make_int2(code, (int)(cbase + int_rank));
-                        ++int_rank;
-                } else {
-                        int leaves[4];
-                        const int cnt = code_leaves(t, code, leaves);
-                        w.meta[s] = (uint8_t)(0x80u | ((uint32_t)(cnt - 1) << 5) | tri_off);
-                        for (int j = 0; j < cnt; ++j) {
-                                const uint32_t p = (uint32_t)(t.keys[leaves[j]] & 0xFFFFFFFFu);
-                                float4 a = t.pv0[p];
-                                a.w = __int_as_float((int)p);
-                                float4 b = t.pv1[p], c = t.pv2[p];
-                                b.w = 0.0f;
-                                c.w = 0.0f;
-                                tv0[tbase + tri_off + j] = a;
-                                tv1[tbase + tri_off + j] = b;
-                                tv2[tbase + tri_off + j] = c;
+                        float p = 0.0f;
+                        int e = 127;
+                        double margin = 0.0, step = 1.0;
+                        if (nq > 0) axis_grid(alo, ahi, &p, &e, &margin, &step);
+                        const double cl = __shfl_sync(FULL, a == 0 ? lo[0] : (a == 1 ? lo[1] : lo[2]), src);
+                        const double ch = __shfl_sync(FULL, a == 0 ? hi[0] : (a == 1 ? hi[1] : hi[2]), src);
+                        uint8_t ql = 255, qh = 0;
+                        if (k_in >= 0) {
+                                ql = quantise_lo(cl, margin, p, step);
+                                qh = quantise_hi(ch, margin, p, step);
                         }
-                        tri_off += (uint32_t)cnt;
+                        wn[32 + 8 * a + j] = ql;
+                        wn[56 + 8 * a + j] = qh;
+                        if (j == 0) {
+                                reinterpret_cast<float *>(wn)[a] = p;
+                                wn[12 + a] = (uint8_t)e;
+                        }
                 }
         }
-        nodes[item.y] = w;
+
+        // ---- interior children, leaf triangles
+        const bool is_leaf = mine && code_leaf(t, kid);
+        const bool is_int = mine && my_slot >= 0 && !is_leaf;
+        int leaves[4];
+        int cnt = 0;
+        if (is_leaf && my_slot >= 0) cnt = code_leaves(t, kid, leaves);
+        const uint32_t imask = g8_or(is_int ? 1u << my_slot : 0u);
+        const uint32_t n_int = (uint32_t)__popc(imask);
+        const uint32_t n_tri = g8_sum(is_leaf ? (uint32_t)code_count(t, kid) : 0u);
+        uint32_t cbase = 0u, tbase = 0u, qbase = 0u;
+        int overflow = valid ? 0 : 1;
+        if (j == 0 && valid) {
+                cbase = n_int ? atomicAdd(counters + 0, n_int) : 0u;
+                tbase = n_tri ? atomicAdd(counters + 1, n_tri) : 0u;
+                if (cbase + n_int > node_cap || tbase + n_tri > tri_cap) {
+                        atomicOr(err, kErrBadIndex);
+                        overflow = 1;
+                } else if (n_int) {
+                        qbase = atomicAdd(n_next, n_int);
+                }
+        }
+        overflow = __shfl_sync(FULL, overflow, base);
+        cbase = __shfl_sync(FULL, cbase, base);
+        tbase = __shfl_sync(FULL, tbase, base);
+        qbase = __shfl_sync(FULL, qbase, base);
+        // a leaf child's triangles follow those of the leaf children in lower slots
+        uint32_t tri_off = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+                const int ks = __shfl_sync(FULL, my_slot, base + k);
+                const int kc = __shfl_sync(FULL, cnt, base + k);
+                if (k < n && ks >= 0 && ks < my_slot) tri_off += (uint32_t)kc;
+        }
+        if (!overflow) {
+                if (j == 0) {
+                        wn[15] = (uint8_t)imask;
+                        reinterpret_cast<uint32_t *>(wn)[4] = cbase;
+                        reinterpret_cast<uint32_t *>(wn)[5] = tbase;
+                }
+                if (is_int) {
+                        const uint32_t rank = (uint32_t)__popc(imask & ((1u << my_slot) - 1u));
+                        next[qbase + rank] = make_int2(kid, (int)(cbase + rank));
+                }
+                if (cnt > 0) {
+                        wn[24 + my_slot] = (uint8_t)(0x80u | ((uint32_t)(cnt - 1) << 5) | tri_off);
+                        for (int q = 0; q < cnt; ++q) {
+                                const uint32_t pidx = (uint32_t)(t.keys[leaves[q]] & 0xFFFFFFFFu);
+                                float4 va = t.pv0[pidx];
+                                va.w = __int_as_float((int)pidx);
+                                float4 vb = t.pv1[pidx], vc = t.pv2[pidx];
+                                vb.w = 0.0f;
+                                vc.w = 0.0f;
+                                tv0[tbase + tri_off + q] = va;
+                                tv1[tbase + tri_off + q] = vb;
+                                tv2[tbase + tri_off + q] = vc;
+                        }
+                }
+        }
+        __syncwarp();
+        if (!overflow && j < 5) reinterpret_cast<uint4 *>(nodes + item.y)[j] = reinterpret_cast<const uint4 *>(wn)[j];
 }
 
 template <class T>
@@ -696,7 +808,7 @@ gzg_status gpu_build_wide(const float4_ *pv0, const float4_ *pv1, const float4_ 
         while (level_items > 0) {
                 if (++depth > 64) return set_error(GZG_ERR_KERNEL_FAULT, "gzg_gpu_build_scene: tree deeper than 64 levels");
                 GZG_CK(cudaMemsetAsync(counts + 3, 0, 4, st), "build: counters");
-                k_collapse<<<(level_items + 127) / 128, 128, 0, st>>>(t, qa, counts + 2, qb, counts + 3, counts, nodes,
+                k_collapse<<<(level_items + 15) / 16, 128, 0, st>>>(t, qa, counts + 2, qb, counts + 3, counts, nodes,
                                                                      tv0, tv1, tv2, cap, cap, err);
                 GZG_CK(cudaMemcpyAsync(counts + 2, counts + 3, 4, cudaMemcpyDeviceToDevice, st), "build: counters");
                 GZG_CK(cudaMemcpyAsync(pinned, counts + 3, 4, cudaMemcpyDeviceToHost, st), "build: counters");
