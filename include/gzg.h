@@ -278,7 +278,14 @@ GZG_API gzg_status gzg_gpu_occluded_batch(gzg_scene *scene, const gzg_ray *rays,
                                           const float *t_max_values, int64_t count,
                                           uint8_t *occluded, const gzg_trace_options *options);
 
-/* Device-resident closest hit: rays and hits are device pointers. */
+/* Device-resident closest hit: rays and hits are device pointers.  The
+ * launch is queued on `stream` (null: the legacy default stream) and the call
+ * returns without waiting.  Device calls on one scene may be queued from
+ * several threads and on several streams at once.  Each launch takes one of
+ * the scene's 32 pull counters and waits, on its own stream, for the last
+ * launch that used the same counter.  The first device call on a scene
+ * allocates those counters (128 bytes and 32 events).  A stream being
+ * captured into a graph gets a launch without a counter. */
 GZG_API gzg_status gzg_trace_closest_device(gzg_scene *scene, const gzg_ray_d *rays, int64_t count,
                                             gzg_hit_d *hits, const gzg_trace_options *options,
                                             void *stream);
