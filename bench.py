@@ -17,7 +17,11 @@ outputs (256 MiB of hits) are larger than the 126 MB L2, so no flush is done.
             wide node + 48 B per triangle, counts from an instrumented replay)
             over the average launch time, against the measured HBM copy
             bandwidth; `coherent` and `incoherent` give the same for each half
-            of the rays launched alone
+            of the rays launched alone; `io_lower_bound` the ray I/O alone
+            (48 B per ray) and `reference_layout` the bytes the same launch
+            time would move in the reference's layout (BVH2 records and
+            triangle tests counted by an instrumented replay of the
+            reference-order kernel, 104 B per triangle test, 76 B of ray I/O)
   cpu_baseline  the oracle (CPU restatement of the reference traversal, over
             a tree built by the oracle's own SAH builder) on the host cores
   render, batch, adjoint, instanced, device_build
@@ -652,6 +656,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     nodes_per_launch, tris_per_launch, rays_counted = [int(x) for x in cnt.cpu()]
     assert rays_counted == n, (rays_counted, n)
+    # the same rays through the reference's own node order and layout (k_bvh2,
+    # untimed): 32-byte BVH2 records fetched (one per iteration, two per
+    # interior step) and triangle tests, for the reference-layout bytes
+    from gonzales_b200._ffi import TRAVERSAL_BVH2
+    cnt.zero_()
+    acc.trace_closest(rays_d, hits_d, options(traversal=TRAVERSAL_BVH2, fetch_counters=cnt.data_ptr()))
+    torch.cuda.synchronize()
+    bvh2_records, bvh2_tris, _ = [int(x) for x in cnt.cpu()]
 
     for _ in range(args.warmup):
         acc.trace_closest(rays_d, hits_d)
@@ -767,6 +779,17 @@ def run_ours(args):
                     "kernel": "k_wide_persistent (closest hit)",
                     "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_per_launch / n,
                     "tris_per_ray": tris_per_launch / n}
+        # ray I/O alone (32 B device ray in, 16 B hit out): the lower bound of any layout
+        roofline["io_lower_bound"] = {"bytes_per_ray": 48, "achieved": 48.0 * n / avg_launch_s / 1e9,
+                                      "frac": 48.0 * n / avg_launch_s / 1e9 / peak}
+        # the reference's layout for the same rays: 32 B BVH2 records, 104 B per
+        # triangle test (32 B PrimId_C + 24 B int64 indices + 3 x 16 B points),
+        # 76 B of ray I/O (Ray_C + tMax in, Intersection_C out); bytes that the
+        # kernel's time would have to move in that layout
+        ref_bytes = 76.0 * n + 32.0 * bvh2_records + 104.0 * bvh2_tris
+        roofline["reference_layout"] = {
+            "bytes_per_ray": ref_bytes / n, "node_records_per_ray": bvh2_records / n,
+            "tris_per_ray": bvh2_tris / n, "equivalent_gbs": ref_bytes / avg_launch_s / 1e9}
         for label, hv in halves.items():
             hb = hv["rays"] * 48 + hv["nodes"] * 80 + hv["tris"] * 48
             ach = hb / hv["launch_s"] / 1e9

@@ -6,7 +6,9 @@ stream-ordered pool, so launches that run at the same time on different
 streams must never share one: a shared counter would skip chunks (rays left
 unwritten) or trace some twice.  Launches of more than 2^30 rays are split
 into consecutive launches over slices of the arrays; every slice must land
-at its own offset.
+at its own offset.  A device call on a stream being captured into a CUDA
+graph runs the static schedule; the graph's replays must equal the eager
+call.
 """
 import numpy as np
 import pytest
@@ -93,4 +95,35 @@ def test_launch_above_2_pow_30_rays_is_split_into_slices():
         assert torch.equal(got, exp)
         # no slot of the whole output was left unwritten
         assert not torch.isnan(hits[:, 0]).any().item()
+        assert acc.error_word() == 0
+
+
+def test_device_trace_captured_in_a_cuda_graph_matches_eager_launch():
+    # a stream under capture gets the static schedule (no pull counter, no
+    # event waits across the capture's boundary); replays equal the eager call
+    hs = scenes.raycast_scene(subdiv=5).build()
+    with GpuAccelerator(hs) as acc:
+        o, d, t = scenes.raycast_rays(hs, 256, 256, 300000, seed=0x5E)
+        rays = torch.from_numpy(scenes.pack_device_rays(o, d, t)).cuda()
+        n = rays.shape[0]
+        want = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        acc.trace_closest(rays, want)
+        torch.cuda.synchronize()
+        got = torch.full((n, 4), float("nan"), dtype=torch.float32, device="cuda")
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            acc.trace_closest(rays, got, stream=side)  # warm-up outside the capture
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        got.fill_(float("nan"))
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            acc.trace_closest(rays, got, stream=torch.cuda.current_stream())
+        for _ in range(2):
+            got.fill_(float("nan"))
+            graph.replay()
+            torch.cuda.synchronize()
+            assert torch.equal(got.view(torch.int32), want.view(torch.int32))
+        del graph
         assert acc.error_word() == 0
