@@ -17,11 +17,14 @@
 //      their mutual nearest neighbour in Morton order, then compact), whose
 //      lower surface-area cost did not traverse faster on the ray-cast mesh;
 //   5. (bounds come with the tree)
-//   6. collapse into wide nodes level by level, as the host converter does
-//      (wide_bvh.cpp): a wide node opens the interior child of largest
-//      surface area until it has 8 children; a binary node covering at most
-//      leaf_size prims is a leaf; children go to octant slots and their
-//      boxes are quantised outward to 8 bits per plane.
+//   6. collapse into wide nodes level by level: a wide node opens the
+//      interior child of largest surface area until it has 8 children (a
+//      greedy choice: the host converter, wide_bvh.cpp, minimises the summed
+//      node area over the whole subtree instead, which needs the finished
+//      binary tree's tables before the first wide node); a binary node
+//      covering at most leaf_size prims is a leaf; children go to octant
+//      slots and their boxes are quantised outward to 8 bits per plane as
+//      the host converter does.
 // The result uses the host converter's layout exactly (WideNode, leaf-order
 // triangle records with the prim index in v0.w), so every traversal kernel
 // runs on it unchanged.
@@ -423,9 +426,8 @@ __device__ __forceinline__ uint32_t g8_sum(uint32_t v) {
 }
 
 // One level of the collapse, one group of 8 lanes per item (binary code, wide
-// node index), four items per warp.  The steps are the host converter's, with
-// the serial loops spread over the group's lanes (lane j of a group = child j
-// or slot j):
+// node index), four items per warp, with the serial loops of one node spread
+// over the group's lanes (lane j of a group = child j or slot j):
 //   - lane j < n holds child j while the node opens the interior child of
 //     largest surface area (lowest index on ties) until it has 8 children;
 //   - lane j loads child j's box and its 8 slot costs; each of n rounds gives

@@ -843,9 +843,11 @@ template <int RAYFMT, int OUTFMT, bool ANY, int LEAF>
 cudaError_t launch_wide_depth(const DevScene &s, const LaunchParams &p, const void *rays, const float *tmax, int64_t n,
                               void *out, cudaStream_t st) {
         const bool persistent = p.traversal == GZG_TRAVERSAL_WIDE;
-        // The stack holds at most depth - 1 groups; a requested depth below
-        // that is raised so no ray can overflow it.
-        const int need = p.wide_depth > 1 ? p.wide_depth : 1;
+        // A ray pushes at most one group (the rest of a node's interior hits)
+        // per level whose nodes have interior children, so the stack holds at
+        // most depth - 1 groups; a requested depth below that is raised so no
+        // ray can overflow it (an overflow would set kErrStackOverflow).
+        const int need = p.wide_depth > 2 ? p.wide_depth - 1 : 1;
         const int want = p.stack_depth > need ? p.stack_depth : need;
         if (want <= 8) {
                 TraceKernel k = persistent ? k_wide_persistent<RAYFMT, OUTFMT, ANY, 8, LEAF> : k_wide<RAYFMT, OUTFMT, ANY, 8, LEAF>;

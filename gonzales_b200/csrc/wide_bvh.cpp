@@ -9,8 +9,11 @@
 //      prims the reference never intersects (id2 == -1, kernel.mojo:273-275)
 //      are dropped, larger leaves are split in order into groups of 4.  Node
 //      boxes are the BVH2 boxes the host built.
-//   3. Collapse: a wide node takes its binary children and repeatedly opens
-//      the interior child with the largest surface area until it has 8.
+//   3. Collapse: each wide node's children (at most 8 leaves or interior
+//      binary nodes below it) are the ones that minimise the summed surface
+//      area of the wide nodes beneath it, the SAH cost of node opens, by
+//      dynamic programming over the binary tree (Ylitie, Karras and Laine
+//      2017, without their leaf merging: leaves stay the lifted BVH2 leaves).
 //   4. Assign children to slots by octant (front-to-back order for a ray is
 //      slot ^ sign-bits) and quantise child boxes to 8 bits per plane,
 //      rounding outward with a small extra margin.
@@ -321,7 +324,64 @@ class Converter {
                 }
         }
 
+        // area_[8b + i - 1] = least summed surface area of the wide nodes
+        // needed to represent the subtree of binary node b by at most i
+        // children of a wide node: a leaf costs nothing, an interior node
+        // kept as one child becomes a wide node (its area plus its subtree
+        // spread over 8 children), an interior node spread over j >= 2
+        // children costs the best split of j between its two subtrees.
+        // pick_ records the choice (0 = one child, j = spread over j), split_
+        // the share of the left subtree when spread over j.  Children come
+        // before parents in bin_, so one pass in index order fills the tables.
+        std::vector<double> area_;
+        std::vector<uint8_t> pick_, split_;
+        void collapse_tables() {
+                const size_t nb = bin_.size();
+                area_.assign(nb * 8, 0.0);
+                pick_.assign(nb * 8, 0);
+                split_.assign(nb * 8, 0);
+                for (size_t b = 0; b < nb; ++b) {
+                        const BinNode &c = bin_[b];
+                        if (c.leaf()) continue;
+                        const double *al = &area_[(size_t)c.l * 8], *ar = &area_[(size_t)c.r * 8];
+                        double spread[9];
+                        for (int j = 2; j <= 8; ++j) {
+                                spread[j] = std::numeric_limits<double>::infinity();
+                                for (int k = 1; k < j; ++k) {
+                                        const double v = al[k - 1] + ar[j - k - 1];
+                                        if (v < spread[j]) {
+                                                spread[j] = v;
+                                                split_[b * 8 + (j - 1)] = (uint8_t)k;
+                                        }
+                                }
+                        }
+                        double best = c.area() + spread[8];
+                        int best_pick = 0;
+                        area_[b * 8] = best;
+                        for (int i = 2; i <= 8; ++i) {
+                                if (spread[i] < best) {
+                                        best = spread[i];
+                                        best_pick = i;
+                                }
+                                area_[b * 8 + (i - 1)] = best;
+                                pick_[b * 8 + (i - 1)] = (uint8_t)best_pick;
+                        }
+                }
+        }
+        // Appends the children that represent binary node b with at most i.
+        void collapse_children(int32_t b, int i, std::vector<int32_t> &kids) const {
+                const int p = pick_[(size_t)b * 8 + (i - 1)];
+                if (bin_[b].leaf() || p == 0) {
+                        kids.push_back(b);
+                        return;
+                }
+                const int k = split_[(size_t)b * 8 + (p - 1)];
+                collapse_children(bin_[b].l, k, kids);
+                collapse_children(bin_[b].r, p - k, kids);
+        }
+
         void collapse(WideBvh *out) {
+                collapse_tables();
                 out->nodes.clear();
                 out->v0.clear();
                 out->v1.clear();
@@ -331,6 +391,8 @@ class Converter {
                         uint32_t node;
                         int depth;
                 };
+                // the children of the wide node rooted at binary node b: its
+                // two subtrees spread over 8 children by the tables' best split
                 auto open_kids = [&](int32_t b) {
                         std::vector<int32_t> kids;
                         if (b < 0) return kids;
@@ -338,23 +400,9 @@ class Converter {
                                 kids.push_back(b);
                                 return kids;
                         }
-                        kids.push_back(bin_[b].l);
-                        kids.push_back(bin_[b].r);
-                        while (kids.size() < 8) {
-                                int best = -1;
-                                double best_a = -1;
-                                for (int i = 0; i < (int)kids.size(); ++i) {
-                                        const BinNode &c = bin_[kids[i]];
-                                        if (!c.leaf() && c.area() > best_a) {
-                                                best_a = c.area();
-                                                best = i;
-                                        }
-                                }
-                                if (best < 0) break;
-                                int32_t open = kids[best];
-                                kids[best] = bin_[open].l;
-                                kids.insert(kids.begin() + best + 1, bin_[open].r);
-                        }
+                        const int k = split_[(size_t)b * 8 + 7];
+                        collapse_children(bin_[b].l, k, kids);
+                        collapse_children(bin_[b].r, 8 - k, kids);
                         return kids;
                 };
                 std::vector<Job> queue;
