@@ -311,12 +311,14 @@ __global__ void __launch_bounds__(256) k_wide(DevScene s, const void *__restrict
 // the slowest ray of a fixed 32-ray batch finishes.  Each iteration opens one
 // node and tests its triangles.  A miss reads its tMax again at the end
 // instead of keeping it in a register.
-// Capped at 72 registers (7 blocks of 128 per SM): closest hit, 80 registers
-// uncapped, goes 4,011 -> 4,123 Mrays/s on the ray-cast workload; any hit
-// (71-72 uncapped) 5,238 -> 5,205.  Looser minimums are not the uncapped
-// build: at 6 blocks any hit takes 80 registers and drops to 4,779.
+// Capped at 64 registers (8 blocks of 128 per SM).  With the pull counter the
+// extra warps pay for closest hit's 28 bytes of spills: ray-cast halves
+// against 7 blocks (72 registers, no spills), incoherent 3,170 -> 3,261
+// Mrays/s closest and 3,827 -> 4,148 any hit, coherent 8,362 -> 8,456 closest
+// and 9,692 -> 10,197 any hit.  9 blocks (56 registers, 84 bytes of spills)
+// was slower than 7.  On the static schedule 8 blocks was slower than 7.
 template <int RAYFMT, int OUTFMT, bool ANY, int STACK, int LEAF>
-__global__ void __launch_bounds__(128, 7) k_wide_persistent(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(128, 8) k_wide_persistent(DevScene s, const void *__restrict__ rays,
                                                          const float *__restrict__ tmaxs, int64_t n,
                                                          void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
@@ -457,6 +459,20 @@ __device__ __forceinline__ void set_ray_dirs(WideRay &r) {
                 ((__float_as_uint(r.rdz) >> 31) << 2);
 }
 
+// The world-space ray of device-ray slot i, read again from the ray array (the
+// two-level kernel keeps it out of registers: it is needed only when a ray
+// enters or leaves an instance).
+__device__ __forceinline__ void world_ray(const void *rays, int i, WideRay &r) {
+        const float4 *p = reinterpret_cast<const float4 *>(rays) + 2 * (size_t)i;
+        const float4 a = __ldg(p), b = __ldg(p + 1);
+        r.ox = a.x;
+        r.oy = a.y;
+        r.oz = a.z;
+        r.dx = b.x;
+        r.dy = b.y;
+        r.dz = b.z;
+}
+
 // Transform*Point / Transform*Vector of Geometry/Transform.swift:31-65 with a
 // 3x4 affine matrix (w = 1, so the division is exact and omitted), each product
 // and sum rounded separately in the reference's order.
@@ -475,12 +491,15 @@ __device__ __forceinline__ float xf_vector(const float4 &row, float x, float y, 
 // ray to object space and descends into the bottom-level root.  Popping the
 // marker restores the world ray.  Bottom-level trees are ordinary wide trees
 // stored after the top-level nodes in the same arrays.
-// Bounded to 128-thread blocks, 7 resident per SM (at most 72 registers, a
-// few dozen bytes of spills): the unbounded build's 99 registers left 4 blocks
-// per SM; 6 blocks (80 registers) gave 1.6x its camera-ray rate and 7 another
-// 2 % on the two-level frame (1,187 -> 1,162 ms); 5 and 8 were slower.
+// The world ray is not kept in registers: it is read again from the ray
+// array when a ray enters or leaves an instance.  Bounded to 128-thread
+// blocks, 8 resident per SM (64 registers, 12-36 bytes of spills): the
+// unbounded build's 99 registers left 4 blocks per SM; 6 blocks (80 registers)
+// gave 1.6x its camera-ray rate and 7 another 2 % on the two-level frame
+// (1,187 -> 1,162 ms); with the pull counter and the world ray out of
+// registers, 8 blocks another 1.3 % (16-spp frame 265.5 -> 262.0 ms).
 template <int OUTFMT, bool ANY, int STACK>
-__global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const void *__restrict__ rays,
+__global__ void __launch_bounds__(128, 8) k_wide_instanced(DevScene s, const void *__restrict__ rays,
                                                         const float *__restrict__ tmaxs, int64_t n,
                                                         void *__restrict__ out) {
         extern __shared__ uint2 smem_stack[];
@@ -495,8 +514,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
         const int stride = blockDim.x;
         int ray_i = -1;
         WideRay r;
-        float wox = 0, woy = 0, woz = 0, wdx = 0, wdy = 0, wdz = 0;  // world ray
-        float tmax = 0.0f, thit = 0.0f, bu = 0.0f, bv = 0.0f;
+        float thit = 0.0f, bu = 0.0f, bv = 0.0f;
         int prim = -1, hit_inst = -1, cur_inst = -1, sp = 0;
         uint2 group = make_uint2(0u, 0u);
         uint32_t pend_base = 0, pend_mask = 0;
@@ -512,14 +530,14 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                         if (ray_i < 0 && rank < avail) {
                                 ray_i = (int)(cc.cursor + (uint32_t)rank);
                                 const RayIn in = load_ray<kRayDevice>(rays, tmaxs, ray_i);
-                                wox = r.ox = in.ox;
-                                woy = r.oy = in.oy;
-                                woz = r.oz = in.oz;
-                                wdx = r.dx = in.dx;
-                                wdy = r.dy = in.dy;
-                                wdz = r.dz = in.dz;
+                                r.ox = in.ox;
+                                r.oy = in.oy;
+                                r.oz = in.oz;
+                                r.dx = in.dx;
+                                r.dy = in.dy;
+                                r.dz = in.dz;
                                 set_ray_dirs(r);
-                                tmax = thit = in.tmax;
+                                thit = in.tmax;
                                 bu = bv = 0.0f;
                                 prim = hit_inst = cur_inst = -1;
                                 sp = 0;
@@ -542,12 +560,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                 --sp;
                                 const uint2 e = stack[sp * stride];
                                 if (e.x == 0xFFFFFFFFu) {
-                                        r.ox = wox;
-                                        r.oy = woy;
-                                        r.oz = woz;
-                                        r.dx = wdx;
-                                        r.dy = wdy;
-                                        r.dz = wdz;
+                                        world_ray(rays, ray_i, r);
                                         set_ray_dirs(r);
                                         cur_inst = -1;
                                 } else if (e.x & 0x80000000u) {
@@ -615,12 +628,14 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                                 ++sp;
                                 const float4 m0 = __ldg(s.instances + 4 * inst), m1 = __ldg(s.instances + 4 * inst + 1),
                                              m2 = __ldg(s.instances + 4 * inst + 2), m3 = __ldg(s.instances + 4 * inst + 3);
-                                r.ox = xf_point(m0, wox, woy, woz);
-                                r.oy = xf_point(m1, wox, woy, woz);
-                                r.oz = xf_point(m2, wox, woy, woz);
-                                r.dx = xf_vector(m0, wdx, wdy, wdz);
-                                r.dy = xf_vector(m1, wdx, wdy, wdz);
-                                r.dz = xf_vector(m2, wdx, wdy, wdz);
+                                WideRay w;
+                                world_ray(rays, ray_i, w);
+                                r.ox = xf_point(m0, w.ox, w.oy, w.oz);
+                                r.oy = xf_point(m1, w.ox, w.oy, w.oz);
+                                r.oz = xf_point(m2, w.ox, w.oy, w.oz);
+                                r.dx = xf_vector(m0, w.dx, w.dy, w.dz);
+                                r.dy = xf_vector(m1, w.dx, w.dy, w.dz);
+                                r.dz = xf_vector(m2, w.dx, w.dy, w.dz);
                                 set_ray_dirs(r);
                                 cur_inst = inst;
                                 group = make_uint2((uint32_t)__float_as_int(m3.x), (1u << 24) | (1u << r.oct));
@@ -645,7 +660,7 @@ __global__ void __launch_bounds__(128, 7) k_wide_instanced(DevScene s, const voi
                 if (fault || (!finished && pend_mask == 0 && (group.y >> 24) == 0 && sp == 0)) finished = true;
                 if (finished) {
                         if (prim < 0) {
-                                thit = tmax;
+                                thit = load_ray<kRayDevice>(rays, tmaxs, ray_i).tmax;
                                 bu = 0.0f;
                                 bv = 0.0f;
                                 hit_inst = -1;
