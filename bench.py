@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--small", action="store_true", help="small case for profiler captures")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-batch", action="store_true", help="omit the scene-batch and adjoint legs")
-    ap.add_argument("--case", default=None, choices=["instanced-small", "build", "incoherent", "coherent", "mixed"],
+    ap.add_argument("--case", default=None,
+                    choices=["instanced-small", "build", "incoherent", "coherent", "mixed", "render"],
                     help="run one small case alone (profiler captures) and print its own JSON line")
     return ap.parse_args()
 
@@ -847,6 +848,8 @@ def run_case(args):
                        the general materials and the medium, in 2^20-path
                        waves (after one warm-up frame)
       build            the device tree build of the ray-cast mesh (three builds)
+      render           one frame of the box scene (256 x 256, 16 spp, depth 5)
+                       after three warm-up frames
       incoherent       the ray-cast mesh's 8,388,608 incoherent rays alone:
       coherent         or its 8,388,608 coherent rays alone,
       mixed            or all 16,777,216 rays (the bench's launch); tuned
@@ -887,6 +890,25 @@ def run_case(args):
         acc.close()
         for b in blas:
             b.close()
+    elif args.case == "render":
+        hs = scenes.box_scene().build()
+        with GpuAccelerator(hs) as acc_box:
+            p = F.render_params(**RENDER, use_graph=1)
+            rgb = torch.zeros((RENDER["height"], RENDER["width"], 3), device="cuda")
+            w = torch.zeros((RENDER["height"], RENDER["width"]), device="cuda")
+            with Renderer(acc_box, p) as r:
+                for _ in range(3):
+                    r.render(rgb, w)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.profiler.start()  # the timed frame only, for --profile-from-start off
+                e0.record()
+                r.render(rgb, w)
+                e1.record()
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
+            out = {"case": args.case, "ms_per_frame": e0.elapsed_time(e1), "error_word": acc_box.error_word()}
     elif args.case in ("incoherent", "coherent", "mixed"):
         cfg, hs, o, d, t, name = workload(False, 0)
         nc = cfg["width"] * cfg["height"]

@@ -25,16 +25,18 @@ struct ZSobolConfig {
 
 __device__ __forceinline__ uint32_t zs_reverse_bits(uint32_t v) { return __brev(v); }
 
-// mixBits (ZSobolSampler.swift:90-101).
-__device__ __forceinline__ uint32_t zs_mix_bits(uint64_t v) {
-        uint32_t x = (uint32_t)(v & 0xFFFFFFFFull);
-        x ^= (uint32_t)(v >> 32);
+// mixBits (ZSobolSampler.swift:90-101): the 64-bit argument folded to 32
+// bits by xor, then the 32-bit finaliser.
+__device__ __forceinline__ uint32_t zs_mix_bits32(uint32_t x) {
         x ^= x >> 16;
         x *= 0x85ebca77u;
         x ^= x >> 13;
         x *= 0xc2b2ae35u;
         x ^= x >> 16;
         return x;
+}
+__device__ __forceinline__ uint32_t zs_mix_bits(uint64_t v) {
+        return zs_mix_bits32((uint32_t)(v & 0xFFFFFFFFull) ^ (uint32_t)(v >> 32));
 }
 
 // FastOwenScrambler (ZSobolSampler.swift:43-67).
@@ -66,12 +68,46 @@ __device__ __forceinline__ uint64_t zs_morton2(uint32_t x, uint32_t y) {
 
 __device__ __forceinline__ uint64_t zs_shr(uint64_t v, int s) { return s >= 64 ? 0ull : (v >> s); }
 
-// getSampleIndex (ZSobolSampler.swift:138-166); the 24 permutations of
-// ZSobolSampler.swift:105-112 packed two bits per entry.
+// The 24 permutations of ZSobolSampler.swift:105-112 packed two bits per
+// entry: perm[p][d] = (kZsPermPacked[p] >> (2 * d)) & 3.
+__device__ __forceinline__ int zs_perm(int p, int digit) {
+        const uint8_t kZsPermPacked[24] = {0xE4, 0xB4, 0xD8, 0x78, 0x6C, 0x9C, 0xE1, 0xB1, 0xC9, 0x39, 0x2D, 0x8D,
+                                           0xC6, 0x36, 0xD2, 0x72, 0x4E, 0x1E, 0x27, 0x87, 0x1B, 0x4B, 0x63, 0x93};
+        return (kZsPermPacked[p] >> (2 * digit)) & 3;
+}
+
+__device__ __forceinline__ uint32_t zs_shr32(uint32_t v, int s) { return s >= 32 ? 0u : (v >> s); }
+
+// getSampleIndex when the Morton index (pixel Morton code << log2 spp |
+// sample) is below 2^32 and has at most 16 base-4 digits, as for 2048 x 2048
+// pixels at up to 1024 spp: the same bits as the 64-bit form in 32-bit
+// arithmetic.  mixBits folds its argument to 32 bits by xor, so for
+// higher < 2^32, mixBits(higher ^ dim x 0x55555555) is
+// mixBits32(higher ^ fold(dim x 0x55555555)).
+__device__ __forceinline__ uint32_t zs_sample_index32(const ZSobolConfig &c, uint32_t morton, int dim) {
+        const uint64_t dmul = 0x55555555ull * (uint64_t)(int64_t)dim;
+        const uint32_t dfold = (uint32_t)(dmul & 0xFFFFFFFFull) ^ (uint32_t)(dmul >> 32);
+        uint32_t idx = 0;
+        const bool pow2 = (c.log2spp & 1) == 1;
+        const int last = pow2 ? 1 : 0;
+        for (int di = c.n_base4_digits - 1; di >= last; --di) {
+                const int shift = 2 * di - (pow2 ? 1 : 0);
+                const int digit = (int)(zs_shr32(morton, shift) & 3u);
+                const uint32_t h = zs_mix_bits32(zs_shr32(morton, shift + 2) ^ dfold);
+                idx |= (uint32_t)zs_perm((int)((h >> 24) % 24u), digit) << shift;
+        }
+        if (pow2) {
+                int digit = (int)(morton & 1u);
+                const uint32_t h = zs_mix_bits32((morton >> 1) ^ dfold);
+                digit ^= (int)(h & 1u);
+                idx |= (uint32_t)digit;
+        }
+        return idx;
+}
+
+// getSampleIndex (ZSobolSampler.swift:138-166).
 __device__ __forceinline__ uint64_t zs_sample_index(const ZSobolConfig &c, const ZSobol &s) {
-        // perm[p][d] = (kPermPacked[p] >> (2 * d)) & 3
-        const uint8_t kPermPacked[24] = {0xE4, 0xB4, 0xD8, 0x78, 0x6C, 0x9C, 0xE1, 0xB1, 0xC9, 0x39, 0x2D, 0x8D,
-                                         0xC6, 0x36, 0xD2, 0x72, 0x4E, 0x1E, 0x27, 0x87, 0x1B, 0x4B, 0x63, 0x93};
+        if ((s.morton >> 32) == 0 && c.n_base4_digits <= 16) return zs_sample_index32(c, (uint32_t)s.morton, s.dim);
         uint64_t idx = 0;
         const bool pow2 = (c.log2spp & 1) == 1;
         const int last = pow2 ? 1 : 0;
@@ -81,9 +117,7 @@ __device__ __forceinline__ uint64_t zs_sample_index(const ZSobolConfig &c, const
                 const int digit = (int)(zs_shr(s.morton, shift) & 3u);
                 const uint64_t higher = zs_shr(s.morton, shift + 2);
                 const uint32_t h = zs_mix_bits(higher ^ dmul);
-                const int p = (int)((h >> 24) % 24u);
-                const int pd = (kPermPacked[p] >> (2 * digit)) & 3;
-                idx |= (uint64_t)pd << shift;
+                idx |= (uint64_t)zs_perm((int)((h >> 24) % 24u), digit) << shift;
         }
         if (pow2) {
                 int digit = (int)(s.morton & 1u);
@@ -99,12 +133,21 @@ __device__ __forceinline__ uint64_t zs_sample_index(const ZSobolConfig &c, const
 __device__ __forceinline__ float zs_sobol_sample(const ZSobolConfig &c, uint64_t index, int dim, uint32_t scramble) {
         const uint32_t *m = c.matrices + (size_t)dim * kSobolColumns;
         uint32_t acc = 0;
-        uint64_t cur = index;
-        while (cur != 0) {
-                const int bit = __ffsll((long long)cur) - 1;
-                if (bit >= kSobolColumns) break;
-                acc ^= __ldg(m + bit);
-                cur &= cur - 1;
+        if ((index >> 32) == 0) {
+                // 32-bit scan of the set bits (every bit is below kSobolColumns)
+                uint32_t cur = (uint32_t)index;
+                while (cur != 0u) {
+                        acc ^= __ldg(m + (__ffs(cur) - 1));
+                        cur &= cur - 1u;
+                }
+        } else {
+                uint64_t cur = index;
+                while (cur != 0) {
+                        const int bit = __ffsll((long long)cur) - 1;
+                        if (bit >= kSobolColumns) break;
+                        acc ^= __ldg(m + bit);
+                        cur &= cur - 1;
+                }
         }
         const uint32_t r = zs_owen(acc, scramble);
         const float f = __fmul_rn(__uint2float_rn(r), 2.32830643653869628906e-10f);
