@@ -128,16 +128,20 @@ __device__ __forceinline__ uint64_t zs_sample_index(const ZSobolConfig &c, const
         return idx;
 }
 
-// sobolSample (ZSobolSampler.swift:6-31): XOR of the matrix columns of the set
-// index bits, scrambled, times 2^-32, clamped below 1.
-__device__ __forceinline__ float zs_sobol_sample(const ZSobolConfig &c, uint64_t index, int dim, uint32_t scramble) {
-        const uint32_t *m = c.matrices + (size_t)dim * kSobolColumns;
-        uint32_t acc = 0;
+// sobolSample (ZSobolSampler.swift:6-31) of N consecutive dimensions d0.. for
+// one index: the XOR of the matrix columns of the index's set bits, in one
+// scan of those bits (the N columns of a bit are independent loads).
+template <int N>
+__device__ __forceinline__ void zs_sobol_bits(const ZSobolConfig &c, uint64_t index, int d0, uint32_t acc[N]) {
+        const uint32_t *m = c.matrices + (size_t)d0 * kSobolColumns;
+#pragma unroll
+        for (int k = 0; k < N; ++k) acc[k] = 0u;
         if ((index >> 32) == 0) {
-                // 32-bit scan of the set bits (every bit is below kSobolColumns)
                 uint32_t cur = (uint32_t)index;
                 while (cur != 0u) {
-                        acc ^= __ldg(m + (__ffs(cur) - 1));
+                        const int bit = __ffs(cur) - 1;
+#pragma unroll
+                        for (int k = 0; k < N; ++k) acc[k] ^= __ldg(m + k * kSobolColumns + bit);
                         cur &= cur - 1u;
                 }
         } else {
@@ -145,10 +149,15 @@ __device__ __forceinline__ float zs_sobol_sample(const ZSobolConfig &c, uint64_t
                 while (cur != 0) {
                         const int bit = __ffsll((long long)cur) - 1;
                         if (bit >= kSobolColumns) break;
-                        acc ^= __ldg(m + bit);
+#pragma unroll
+                        for (int k = 0; k < N; ++k) acc[k] ^= __ldg(m + k * kSobolColumns + bit);
                         cur &= cur - 1;
                 }
         }
+}
+
+// Owen scramble, times 2^-32, clamped below 1 (the tail of sobolSample).
+__device__ __forceinline__ float zs_finish(uint32_t acc, uint32_t scramble) {
         const uint32_t r = zs_owen(acc, scramble);
         const float f = __fmul_rn(__uint2float_rn(r), 2.32830643653869628906e-10f);
         const float one_minus_eps = 1.0f - 1e-6f;
@@ -173,7 +182,9 @@ __device__ __forceinline__ float zs_get1d(const ZSobolConfig &c, ZSobol &s) {
         const uint32_t h = zs_hash(c, s.dim);
         if (s.dim >= kSobolDims) s.dim = 2;
         s.dim += 1;
-        return zs_sobol_sample(c, idx, s.dim - 1, h);
+        uint32_t acc[1];
+        zs_sobol_bits<1>(c, idx, s.dim - 1, acc);
+        return zs_finish(acc[0], h);
 }
 
 // get2D (ZSobolSampler.swift:221-244).
@@ -182,8 +193,10 @@ __device__ __forceinline__ void zs_get2d(const ZSobolConfig &c, ZSobol &s, float
         const uint32_t h0 = zs_hash(c, s.dim);
         if (s.dim + 1 >= kSobolDims) s.dim = 2;
         s.dim += 2;
-        a = zs_sobol_sample(c, idx, s.dim - 2, h0);
-        b = zs_sobol_sample(c, idx, s.dim - 1, 0u);
+        uint32_t acc[2];
+        zs_sobol_bits<2>(c, idx, s.dim - 2, acc);
+        a = zs_finish(acc[0], h0);
+        b = zs_finish(acc[1], 0u);
 }
 
 // get3D (ZSobolSampler.swift:249-280).
@@ -193,9 +206,11 @@ __device__ __forceinline__ void zs_get3d(const ZSobolConfig &c, ZSobol &s, float
         const uint32_t h2 = zs_hash(c, s.dim + 2);
         if (s.dim + 2 >= kSobolDims) s.dim = 2;
         s.dim += 3;
-        a = zs_sobol_sample(c, idx, s.dim - 3, h0);
-        b = zs_sobol_sample(c, idx, s.dim - 2, 0u);
-        d = zs_sobol_sample(c, idx, s.dim - 1, h2);
+        uint32_t acc[3];
+        zs_sobol_bits<3>(c, idx, s.dim - 3, acc);
+        a = zs_finish(acc[0], h0);
+        b = zs_finish(acc[1], 0u);
+        d = zs_finish(acc[2], h2);
 }
 
 }  // namespace gzg
