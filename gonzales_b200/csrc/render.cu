@@ -1200,14 +1200,17 @@ __device__ void shade_medium(const Wave &w, const DevScene &s, const SceneConst 
 // hits and misses and queues hits on the general materials on their kind's
 // shade queue, which the kShadeDielectric .. kShadeCoatedConductor launches
 // then shade (one material kind per kernel: coherent warps, one BSDF's code).
-// Register bounds per kind: the split kernel at 6 blocks of 128 per SM (80
-// registers instead of 98), diffuse, dielectric and conductor at 5, the
-// layered kinds at 3 (their natural occupancy): 1,099 -> 1,091 ms on the
-// two-level frame.  Capping the layered kinds at 4 blocks spilled and lost.
+// Register bounds per kind, blocks of 128 per SM: the layered kinds at 3
+// (their natural occupancy; 4 spilled and lost); the split kernel at 7 and
+// the dielectric and conductor kinds at 6 (16-spp two-level frame 245.8 ->
+// 244.0 ms against 6 and 5); the diffuse kind at 7 (72 registers, about 100
+// bytes of spills: box-scene frame 1.508 -> 1.422 ms against 5 blocks; 6:
+// 1.447, 8: 1.454).
 template <int kKind>
-__global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 6
+__global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 7
                                       : (kKind == kShadeCoated || kKind == kShadeCoatedConductor) ? 3
-                                                                                                  : 5)
+                                      : kKind == kShadeDiffuse                                    ? 7
+                                                                                                  : 6)
     k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
         const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
         uint32_t i;
