@@ -1200,15 +1200,16 @@ __device__ void shade_medium(const Wave &w, const DevScene &s, const SceneConst 
 // hits and misses and queues hits on the general materials on their kind's
 // shade queue, which the kShadeDielectric .. kShadeCoatedConductor launches
 // then shade (one material kind per kernel: coherent warps, one BSDF's code).
-// Register bounds per kind, blocks of 128 per SM: the layered kinds at 3
-// (their natural occupancy; 4 spilled and lost); the split kernel at 7 and
-// the dielectric and conductor kinds at 6 (16-spp two-level frame 245.8 ->
+// Register bounds per kind, blocks of 128 per SM: the layered kinds at 4
+// (128 registers, 140-176 bytes of spills; 16-spp two-level frame 245.3 ->
+// 242.1 ms against their natural 3, which won before the 32-bit sampler); the
+// split kernel at 7 and the dielectric and conductor kinds at 6 (245.8 ->
 // 244.0 ms against 6 and 5); the diffuse kind at 7 (72 registers, about 100
 // bytes of spills: box-scene frame 1.508 -> 1.422 ms against 5 blocks; 6:
 // 1.447, 8: 1.454).
 template <int kKind>
 __global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 7
-                                      : (kKind == kShadeCoated || kKind == kShadeCoatedConductor) ? 3
+                                      : (kKind == kShadeCoated || kKind == kShadeCoatedConductor) ? 4
                                       : kKind == kShadeDiffuse                                    ? 7
                                                                                                   : 6)
     k_shade(Wave w, DevScene s, int bounce, int cur, int sorted) {
