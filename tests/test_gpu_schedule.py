@@ -1,10 +1,11 @@
 """The persistent kernels' chunk schedule on the device calls.
 
 A persistent traversal launch hands its rays out in 32-ray chunks through a
-pull counter.  Launches on callers' streams take that counter from a
-stream-ordered pool, so launches that run at the same time on different
-streams must never share one: a shared counter would skip chunks (rays left
-unwritten) or trace some twice.  Launches of more than 2^30 rays are split
+pull counter.  Launches on callers' streams take that counter from the
+scene's ring of counters, each of which waits for the last launch that used
+it, so launches that run at the same time on different streams must never
+share one: a shared counter would skip chunks (rays left unwritten) or trace
+some twice.  Launches of more than 2^30 rays are split
 into consecutive launches over slices of the arrays; every slice must land
 at its own offset.  A device call on a stream being captured into a CUDA
 graph runs the static schedule; the graph's replays must equal the eager

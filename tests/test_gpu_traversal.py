@@ -329,3 +329,61 @@ def test_full_size_watertight_parity(full):
     assert counts["fail"] == 0, (counts, fails[:10])
     assert counts["exact"] >= 0.9999 * counts["rays"], counts
     assert acc.error_word() == 0
+
+
+def _edge_scene(kind, rng):
+    """Meshes for the wide conversion's edge cases: a few triangles, a cluster
+    whose triangle boxes all share one centre (the SAH builder keeps them in
+    one leaf of 40 prims, which the conversion splits into groups of 4 before
+    choosing the wide nodes), and a grid of small triangles (a deep binary
+    tree)."""
+    sb = scenes.SceneBuilder()
+    m = sb.add_material()
+    if kind in ("1", "2", "3", "9"):
+        for _ in range(int(kind)):
+            c = rng.uniform(-1, 1, 3)
+            pts = (c + rng.normal(scale=0.4, size=(3, 3))).astype(np.float32)
+            sb.add_mesh(pts, [[0, 1, 2]], m)
+    elif kind == "same-centroid":
+        # triangles (p, -p, r) with |r| <= |p| per axis: every box is
+        # [-|p|, |p|], centred exactly on the origin (exact float values)
+        for _ in range(40):
+            p = rng.integers(16, 64, 3) * rng.choice([-1, 1], 3) / 64.0
+            r = p * rng.integers(-64, 65, 3) / 64.0
+            sb.add_mesh(np.array([p, -p, r], np.float32), [[0, 1, 2]], m)
+    else:  # grid
+        g = np.stack(np.meshgrid(np.linspace(-1, 1, 11), np.linspace(-1, 1, 16)), -1).reshape(-1, 2)
+        pts = np.concatenate([g, rng.uniform(-0.05, 0.05, (len(g), 1))], 1).astype(np.float32)
+        tris = []
+        for j in range(15):
+            for i in range(10):
+                a = j * 11 + i
+                tris += [[a, a + 1, a + 12], [a, a + 12, a + 11]]
+        sb.add_mesh(pts, tris, m)
+    return sb.build()
+
+
+@pytest.mark.parametrize("kind", ["1", "2", "3", "9", "same-centroid", "grid"])
+def test_wide_conversion_edge_cases(kind):
+    """The host conversion's chosen wide nodes on tiny, degenerate and deep
+    binary trees: closest hits equal the oracle's (exact or a counted tie,
+    never missed or farther), any hit agrees on hit / miss, and no kernel sets
+    an error bit."""
+    rng = np.random.default_rng(0x5EED + len(kind))
+    hs = _edge_scene(kind, rng)
+    n = 4096
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    o = (dirs * 4.0).astype(np.float32)
+    d = rng.normal(scale=0.5, size=(n, 3)) - o
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    t = np.full(n, np.inf, np.float32)
+    with GpuAccelerator(hs) as acc:
+        isect, idx, _ = H.oracle_closest(hs, o, d, t)
+        assert (idx >= 0).any()
+        gpu = device_closest(acc, o, d, t)
+        counts, _ = _check(hs, o, d, t, gpu, isect, idx)
+        assert counts["fail"] == 0, counts
+        anyp = device_any(acc, o, d, t)
+        assert np.array_equal(anyp >= 0, idx >= 0)
+        assert acc.error_word() == 0
