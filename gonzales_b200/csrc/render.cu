@@ -1203,12 +1203,13 @@ __device__ void shade_medium(const Wave &w, const DevScene &s, const SceneConst 
 // Register bounds per kind, blocks of 128 per SM: the layered kinds at 4
 // (128 registers, 140-176 bytes of spills; 16-spp two-level frame 245.3 ->
 // 242.1 ms against their natural 3, which won before the 32-bit sampler); the
-// split kernel at 7 and the dielectric and conductor kinds at 6 (245.8 ->
-// 244.0 ms against 6 and 5); the diffuse kind at 7 (72 registers, about 100
+// split kernel at 8 and the dielectric and conductor kinds at 6 (245.8 ->
+// 244.0 ms with the split kernel at 7 against 6 and 5, 242.3 -> 241.2 ms at 8;
+// the other two kinds at 7: 241.9 ms); the diffuse kind at 7 (72 registers, about 100
 // bytes of spills: box-scene frame 1.508 -> 1.422 ms against 5 blocks; 6:
 // 1.447, 8: 1.454).
 template <int kKind>
-__global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 7
+__global__ void __launch_bounds__(128, kKind == kShadeSplit                                  ? 8
                                       : (kKind == kShadeCoated || kKind == kShadeCoatedConductor) ? 4
                                       : kKind == kShadeDiffuse                                    ? 7
                                                                                                   : 6)
